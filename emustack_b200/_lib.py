@@ -1,0 +1,119 @@
+"""ctypes binding of libemustack_gsm.so (declarations: include/emustack_gsm.h).
+
+The CUDA library is the only compute path of this package: if it is missing
+or cannot be loaded, every solve raises.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libemustack_gsm.so')
+
+EMU_OK = 0
+STATUS_NAMES = {
+    0: 'EMU_OK', 1: 'EMU_E_ARG', 2: 'EMU_E_SHAPE', 3: 'EMU_E_SINGULAR',
+    4: 'EMU_E_NONFINITE', 5: 'EMU_E_WORKSPACE', 6: 'EMU_E_TIMEOUT',
+    7: 'EMU_E_CUDA', 8: 'EMU_E_UNSUPPORTED',
+}
+
+POL = {'TE': 0, 'TM': 1, 'un': 2, 'R Circ': 3, 'L Circ': 4}
+POL_INCOMING = -1
+
+PT_WOOD_AIR = 1
+PT_WOOD_LAYER = 2
+PT_NO_PROP_SUB = 4
+PT_NO_PROP_SUP = 8
+PT_NONFINITE = 16
+
+vp = C.c_void_p
+
+
+class EmuFilmStackBatch(C.Structure):
+    _fields_ = [
+        ('n_points', C.c_int), ('n_layers', C.c_int), ('n_pw', C.c_int), ('world_1d', C.c_int),
+        ('period', C.c_double), ('period_y', C.c_double),
+        ('d_px', vp), ('d_py', vp), ('d_wl_nm', vp), ('d_k_pll', vp), ('d_n', vp),
+        ('d_heights_nm', vp), ('heights_per_point', C.c_int), ('pol', C.c_int),
+        ('d_incoming', vp), ('d_shears', vp), ('shear_ncoord', C.c_int),
+        ('d_R_net', vp), ('d_T_net', vp), ('d_a_list', vp), ('d_t_list', vp), ('d_r_list', vp),
+        ('d_flags', vp),
+        ('d_kz', vp), ('d_layer_rt', vp), ('d_vec_coef_down', vp), ('d_vec_coef_up', vp),
+        ('d_fluxes', vp), ('d_sort_order', vp), ('d_specular', vp), ('d_num_prop', vp),
+    ]
+
+
+class EmuError(RuntimeError):
+    def __init__(self, status, what=''):
+        self.status = status
+        super().__init__('%s failed: %s' % (what, STATUS_NAMES.get(status, status)))
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError('libemustack_gsm.so is not built (run emustack_b200.build.build_library()); '
+                           'emustack_b200 has no CPU fallback')
+    L = C.CDLL(LIB_PATH)
+    L.emu_version.restype = C.c_int
+    L.emu_status_string.restype = C.c_char_p
+    L.emu_status_string.argtypes = [C.c_int]
+    L.emu_launch_count.restype = C.c_longlong
+    L.emu_grating_orders.restype = C.c_int
+    L.emu_grating_orders.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, vp, vp, C.c_int,
+                                     C.POINTER(C.c_int)]
+    L.emu_film_stack_workspace_size.restype = C.c_size_t
+    L.emu_film_stack_workspace_size.argtypes = [C.POINTER(EmuFilmStackBatch)]
+    L.emu_film_stack_batch.restype = C.c_int
+    L.emu_film_stack_batch.argtypes = [C.POINTER(EmuFilmStackBatch), vp, C.c_size_t, vp]
+    _extra_signatures(L)
+    _lib = L
+    return L
+
+
+def _extra_signatures(L):
+    """Signatures of the entry points added beyond the film path."""
+    for name, res, args in EXTRA_SIGNATURES:
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+
+
+EXTRA_SIGNATURES = []
+
+
+def check(status, what):
+    if status != EMU_OK:
+        raise EmuError(status, what)
+
+
+def ptr(t):
+    """Device (or host) address of a torch tensor, None for None."""
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class EmuAnalloModes(C.Structure):
+    _fields_ = [
+        ('n_points', C.c_int), ('n_pw', C.c_int), ('world_1d', C.c_int),
+        ('period', C.c_double), ('period_y', C.c_double),
+        ('d_px', vp), ('d_py', vp), ('d_wl_nm', vp), ('d_k_pll', vp), ('d_n', vp),
+        ('d_sort_in', vp), ('d_kz', vp), ('d_alphas', vp), ('d_betas', vp),
+        ('d_sort_out', vp), ('d_specular', vp), ('d_num_prop', vp), ('d_wood', vp),
+    ]
+
+
+EXTRA_SIGNATURES.append(('emu_anallo_modes', C.c_int, [C.POINTER(EmuAnalloModes), vp]))

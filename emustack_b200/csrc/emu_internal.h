@@ -1,0 +1,26 @@
+// Internal helpers shared by the translation units of libemustack_gsm.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/emustack_gsm.h"
+
+namespace emu {
+
+// Counts kernel launches made by this library (reported by emu_launch_count).
+void note_launch(int n = 1);
+
+// Map the last CUDA error to a status (and clear it).
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? EMU_OK : EMU_E_CUDA; }
+
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? EMU_OK : EMU_E_CUDA;
+}
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace emu

@@ -1,0 +1,191 @@
+/*
+ * emustack_gsm.h -- C ABI of the B200-native EMUstack GSM stage.
+ *
+ * The generalised scattering-matrix (GSM) stage of EMUstack computes, for a
+ * stack of homogeneous films and periodic nanostructured layers, the
+ * interface scattering matrices, the net reflection/transmission matrices
+ * R_net / T_net and the energy fluxes (per-layer absorptance a_list,
+ * t_list, r_list).  In the reference this is Python + numpy/LAPACK
+ * (backend/stack.py, backend/mode_calcs.py) fed by the Fortran overlap
+ * integrals backend/fortran/J_overlap.f and J_dagger_overlap.f (bound to
+ * Python through f2py).  Every entry point below replaces one of those
+ * pieces; the citation beside each names the reference interface it stands
+ * in for (paths relative to the EMUstack source tree).
+ *
+ * Conventions
+ *   - Every function returns an int status (EMU_OK = 0); none aborts.
+ *   - Pointers named d_* are CUDA device pointers; h_* are host pointers.
+ *   - Complex numbers are interleaved (re, im) doubles (emu_c128), the layout
+ *     of numpy complex128 and std::complex<double>.  Matrices are row-major
+ *     (C order), batch index outermost.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls are asynchronous on that stream unless stated.
+ *   - The caller owns every buffer.  Functions that need scratch memory take
+ *     (d_workspace, workspace_bytes) and have a *_workspace_size query.
+ */
+#ifndef EMUSTACK_GSM_H
+#define EMUSTACK_GSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define EMU_OK 0
+#define EMU_E_ARG 1          /* null pointer, bad enum, inconsistent sizes  */
+#define EMU_E_SHAPE 2        /* unsupported or inconsistent dimensions      */
+#define EMU_E_SINGULAR 3     /* exactly singular matrix in a solve          */
+#define EMU_E_NONFINITE 4    /* NaN / Inf produced                          */
+#define EMU_E_WORKSPACE 5    /* workspace too small                         */
+#define EMU_E_TIMEOUT 6      /* a bounded device-side wait gave up          */
+#define EMU_E_CUDA 7         /* CUDA launch / runtime error                 */
+#define EMU_E_UNSUPPORTED 8
+
+/* Polarisations of the specular incidence vector
+ * (backend/mode_calcs.py:220-250 Anallo.specular_incidence). */
+#define EMU_POL_TE 0
+#define EMU_POL_TM 1
+#define EMU_POL_UN 2
+#define EMU_POL_RCIRC 3
+#define EMU_POL_LCIRC 4
+#define EMU_POL_INCOMING (-1) /* use the caller's incoming amplitudes        */
+
+/* Per-point status bits written by emu_film_stack_batch. */
+#define EMU_PT_WOOD_AIR 1u        /* air reference hit a Wood anomaly        */
+#define EMU_PT_WOOD_LAYER 2u      /* some layer hit a Wood anomaly           */
+#define EMU_PT_NO_PROP_SUB 4u     /* no propagating orders in the substrate  */
+#define EMU_PT_NO_PROP_SUP 8u     /* no propagating orders in the superstrate*/
+#define EMU_PT_NONFINITE 16u      /* NaN / Inf in an output of this point    */
+
+typedef struct {
+  double re, im;
+} emu_c128;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int emu_version(void);
+
+/* Human-readable name of a status code. */
+const char *emu_status_string(int status);
+
+/* Number of CUDA kernels this library launched since load (all entry points,
+ * all devices).  Host-side counter, incremented at each launch. */
+long long emu_launch_count(void);
+
+/* ------------------------------------------------------------ a1: orders
+ * Plane-wave diffraction orders inside the disc
+ *   (px/d)^2 + (py/dy)^2 <= (max_order / max(d, dy))^2,
+ * px outer, py inner, evaluated in IEEE double without contraction so that
+ * the set matches the reference exactly (including orders dropped by
+ * rounding on the circle).
+ * Replaces Modes.calc_2d_grating_orders / calc_1d_grating_orders
+ * (backend/mode_calcs.py:55-74) and the order loop of pw_ordering
+ * (backend/fortran/pw_ordering.f:54-78).
+ * h_px / h_py may be NULL to query the count; capacity is their length.
+ * world_1d != 0 gives px = -max_order..max_order and py = 0. */
+int emu_grating_orders(int max_order, double period, double period_y, int world_1d,
+                       int32_t *h_px, int32_t *h_py, int capacity, int *h_count);
+
+/* ------------------------------------------- a2: analytic film modes
+ * k_z of one homogeneous film per point, sorted: the air reference sorts by
+ * -Re k_z + Im k_z (d_sort_in == NULL, backend/mode_calcs.py:164-171), any
+ * other film applies the air's sort order (d_sort_in = the air's d_sort_out,
+ * backend/mode_calcs.py:172-175).  Includes the Wood-anomaly retry with
+ * k_parallel * (1 - 1e-9) (backend/mode_calcs.py:147-162), the specular
+ * order and the number of propagating orders (k_z.imag == 0).
+ * Replaces Anallo.calc_kz (backend/mode_calcs.py:116-186).  Ties in the air
+ * sort keys are ranked by order index (numpy's argsort leaves their order
+ * unspecified; tied orders have identical k_z). */
+typedef struct {
+  int n_points;            /* B films (each with its own wavelength)        */
+  int n_pw;                /* Npw                                           */
+  int world_1d;
+  double period, period_y; /* nm                                            */
+  const int32_t *d_px;     /* [Npw]                                         */
+  const int32_t *d_py;     /* [Npw]                                         */
+  const double *d_wl_nm;   /* [B]                                           */
+  const double *d_k_pll;   /* [B][2] nm^-1                                  */
+  const emu_c128 *d_n;     /* [B] refractive index (loss applied)           */
+  const int32_t *d_sort_in;/* [B][Npw] or NULL (air reference)              */
+  emu_c128 *d_kz;          /* [B][Npw] sorted k_z (required)                */
+  double *d_alphas;        /* [B][Npw] unsorted alphas (optional)           */
+  double *d_betas;         /* [B][Npw] unsorted betas (optional)            */
+  int32_t *d_sort_out;     /* [B][Npw] sort order used (optional)           */
+  int32_t *d_specular;     /* [B] (optional)                                */
+  int32_t *d_num_prop;     /* [B] (optional)                                */
+  int32_t *d_wood;         /* [B] 1 if the Wood retry was taken (optional)  */
+} EmuAnalloModes;
+
+int emu_anallo_modes(const EmuAnalloModes *p, void *stream);
+
+/* ------------------------------------- a2-a4, a7, a9, a10: film stacks
+ * Batched solve of all-film stacks: every layer is a homogeneous film, so
+ * every interface, propagation and cascade matrix is diagonal and the stage
+ * reduces to independent scalar recursions per plane-wave order.  One
+ * launch computes, for each spectral point b:
+ *   - the air reference's k_z, its sort order (argsort(-Re kz + Im kz)),
+ *     the specular order and the propagating counts
+ *     (backend/mode_calcs.py:116-186, backend/objects.py:1745-1777);
+ *   - every film's k_z = sqrt(k^2 - alpha^2 - beta^2) with the Wood-anomaly
+ *     retry and impedances Z (backend/mode_calcs.py:116-218);
+ *   - the air/film Fresnel interfaces (backend/mode_calcs.py:451-477);
+ *   - the cascade R_net, T_net with optional shears
+ *     (backend/stack.py:196-287, backend/mode_calcs.py:76-87);
+ *   - the energy fluxes and a_list / t_list / r_list (backend/stack.py:289-426).
+ * Layers are ordered bottom (substrate, index 0) to top (superstrate,
+ * index L-1) as in Stack(layers).  n is the refractive index with the
+ * layer's `loss` flag already applied (imaginary part zeroed when False).
+ */
+typedef struct {
+  int n_points;          /* B                                               */
+  int n_layers;          /* L >= 2, substrate and superstrate included      */
+  int n_pw;              /* Npw, orders per polarisation (P = 2 Npw)        */
+  int world_1d;          /* 1: 1D order set, beta = beta0                   */
+  double period;         /* nm                                              */
+  double period_y;       /* nm                                              */
+  const int32_t *d_px;   /* [Npw] orders from emu_grating_orders            */
+  const int32_t *d_py;   /* [Npw]                                           */
+  const double *d_wl_nm; /* [B] wavelengths (nm)                            */
+  const double *d_k_pll; /* [B][2] k_parallel (nm^-1), Light.k_pll          */
+  const emu_c128 *d_n;   /* [B][L] refractive indices                       */
+  const double *d_heights_nm; /* [L-2] or [B][L-2] finite-layer heights     */
+  int heights_per_point; /* 0: one height list for all points               */
+  int pol;               /* EMU_POL_*                                       */
+  const emu_c128 *d_incoming; /* [B][P] when pol == EMU_POL_INCOMING        */
+  const double *d_shears;/* [L][2] layer shifts (unit-cell units) or NULL   */
+  int shear_ncoord;      /* 1 (1D) or 2                                     */
+  /* outputs (required) */
+  emu_c128 *d_R_net;     /* [B][P] diagonal of R_net (sorted order)         */
+  emu_c128 *d_T_net;     /* [B][P] diagonal of T_net                        */
+  double *d_a_list;      /* [B][L-1] per-layer absorptance, total last      */
+  double *d_t_list;      /* [B][L-1]                                        */
+  double *d_r_list;      /* [B]                                             */
+  uint32_t *d_flags;     /* [B] EMU_PT_* bits                               */
+  /* optional outputs (NULL to skip) */
+  emu_c128 *d_kz;        /* [B][L][Npw] sorted k_z of every layer           */
+  emu_c128 *d_layer_rt;  /* [B][L][2][P] R12, T12 diagonals (R21=-R12, T21=T12) */
+  emu_c128 *d_vec_coef_down; /* [B][L][P]                                   */
+  emu_c128 *d_vec_coef_up;   /* [B][L-1][P]                                 */
+  double *d_fluxes;      /* [B][L+1][2]: down fluxes 0..L-1 (complex), up0  */
+  int32_t *d_sort_order; /* [B][Npw] air sort order (argsort result)        */
+  int32_t *d_specular;   /* [B] specular order index                        */
+  int32_t *d_num_prop;   /* [B][L+1] propagating orders per layer, air last */
+} EmuFilmStackBatch;
+
+size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p);
+int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspace,
+                         size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------- measurement
+ * FP64 FMA throughput probe: blocks x threads threads each run 64 dependent
+ * FMA chains of `iters` steps (2*64*iters*threads*blocks flops).  Used as the
+ * FP64 roofline denominator of the film kernels; the reference has no
+ * counterpart (it has no GPU path). */
+int emu_probe_fp64(int blocks, int threads, int iters, double *d_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMUSTACK_GSM_H */

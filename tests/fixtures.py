@@ -78,3 +78,19 @@ def oracle_point(pt, use_J=True):
     res.layers = layers
     res.air = air
     return res
+
+
+def film_inputs(pt):
+    """Inputs of an all-film golden point for emustack_b200.films."""
+    n = []
+    for L in pt['layers']:
+        if L['kind'] != 'film':
+            return None
+        v = complex(L['n'])
+        n.append(v if bool(L['loss']) else complex(v.real, 0.0))
+    shears = pt.get('shears')
+    return dict(wl=float(pt['wl_nm']), k_pll=np.asarray(pt['k_pll'], float), n=np.array(n),
+                heights=np.asarray(pt['heights_nm'], float), pol=pt['pol'],
+                incoming=pt.get('incoming'), shears=None if shears is None else np.asarray(shears, float),
+                period=float(pt['period']), period_y=float(pt['period_y']),
+                max_order=int(pt['max_order']), world_1d=bool(pt['world_1d']))
