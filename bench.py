@@ -333,13 +333,13 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--cpu-sample', type=int, default=0,
-                    help='points in the CPU sample (default: 2 per host core, >= 32)')
+                    help='points in the CPU sample (default: 8 per host core, >= 64)')
     args = ap.parse_args()
     rank = int(os.environ.get('RANK', '0'))
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
     cores = len(os.sched_getaffinity(0))
-    sample = args.cpu_sample or max(32, 2 * cores)
+    sample = args.cpu_sample or max(64, 8 * cores)
 
     if args.impl == 'reference':
         if rank != 0:

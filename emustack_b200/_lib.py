@@ -117,3 +117,47 @@ class EmuAnalloModes(C.Structure):
 
 
 EXTRA_SIGNATURES.append(('emu_anallo_modes', C.c_int, [C.POINTER(EmuAnalloModes), vp]))
+
+
+class EmuLayer(C.Structure):
+    _fields_ = [
+        ('M', C.c_int), ('dense', C.c_int),
+        ('d_R12', vp), ('d_T12', vp), ('d_R21', vp), ('d_T21', vp),
+        ('stride_R12', C.c_longlong), ('stride_T12', C.c_longlong),
+        ('stride_R21', C.c_longlong), ('stride_T21', C.c_longlong),
+        ('d_kz', vp), ('stride_kz', C.c_longlong), ('height_norm', C.c_double),
+    ]
+
+
+class EmuStackDense(C.Structure):
+    _fields_ = [
+        ('batch', C.c_int), ('n_layers', C.c_int), ('P', C.c_int),
+        ('h_layers', C.POINTER(EmuLayer)), ('h_shears', C.POINTER(C.c_double)),
+        ('shear_ncoord', C.c_int), ('d_air_alphas', vp), ('d_air_betas', vp),
+        ('calc_fluxes', C.c_int), ('pol', C.c_int), ('d_incoming', vp), ('d_specular', vp),
+        ('d_num_prop', vp), ('d_R_net', vp), ('d_T_net', vp), ('d_fluxes', vp),
+        ('d_a_list', vp), ('d_t_list', vp), ('d_r_list', vp), ('d_flags', vp), ('d_info', vp),
+        ('d_vec_coef_down', vp), ('d_vec_coef_up', vp),
+        ('vec_coef_down_stride', C.c_longlong), ('vec_coef_up_stride', C.c_longlong),
+        ('save_lists', C.c_int), ('d_tnet_list', vp), ('d_rnet_list', vp),
+    ]
+
+
+class EmuC128(C.Structure):
+    _fields_ = [('re', C.c_double), ('im', C.c_double)]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_zgemm_batched', C.c_int, [C.c_int, C.c_int, C.c_int, EmuC128, vp, C.c_int, C.c_longlong,
+                                    vp, C.c_int, C.c_longlong, EmuC128, vp, C.c_int, C.c_longlong,
+                                    C.c_int, vp]),
+    ('emu_zgesv_batched', C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.c_longlong, vp, vp, C.c_int,
+                                    C.c_longlong, vp, C.c_int, vp]),
+    ('emu_film_interface_batch', C.c_int, [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]),
+    ('emu_interface_dense_workspace_size', C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    ('emu_interface_dense_batch', C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp,
+                                            vp, vp, vp, vp, C.c_size_t, vp]),
+    ('emu_stack_dense_workspace_size', C.c_size_t, [C.POINTER(EmuStackDense)]),
+    ('emu_stack_dense_list_stride', C.c_longlong, [C.POINTER(EmuStackDense)]),
+    ('emu_stack_dense_batch', C.c_int, [C.POINTER(EmuStackDense), vp, C.c_size_t, vp]),
+])

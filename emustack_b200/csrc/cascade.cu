@@ -1,0 +1,552 @@
+// Dense GSM cascade and energy fluxes for stacks with nanostructured layers
+// (backend/stack.py:162-426), batched: one CTA per spectral point walks the
+// stack bottom to top with LU solves and GEMMs in FP64, keeps the matrices
+// the flux pass needs in its workspace, then walks top to bottom with
+// matrix-vector products and the U-weighted air-gap fluxes.
+//
+// Film layers (diagonal interfaces) take diagonal-aware steps: their
+// products are row scalings and their right-hand sides diagonal matrices.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "dense_la.cuh"
+#include "emu_internal.h"
+
+namespace {
+
+using namespace emu;
+
+constexpr int kMaxLayers = 64;
+
+struct DLayer {
+  const cd *R12, *T12, *R21, *T21, *kz;
+  long long sR12, sT12, sR21, sT21, skz;
+  int M, dense;
+  double hn, sh0, sh1;
+};
+
+struct StackArgs {
+  DLayer lay[kMaxLayers];
+  int B, L, P, npw, D, ncoord, has_shear, calc_fluxes, pol, save_lists;
+  const double *alphas, *betas;
+  const cd *incoming;
+  const int *spec, *nprop;
+  cd *R_net, *T_net;
+  double *fluxes, *a_list, *t_list, *r_list;
+  unsigned *flags;
+  int *info;
+  cd *vcd, *vcu;
+  long long vcd_stride, vcu_stride;
+  cd *tnl, *rnl;
+  cd *ws;
+  long long ws_stride;
+  int *ipiv;
+  double inv_sqrt2;
+};
+
+struct Smem {
+  GemmSmem gs;
+  LuSmem ls;
+  double red[2 * kDLThreads / 32];
+};
+
+// ---- small CTA helpers ------------------------------------------------------
+__device__ void copy_mat(cd *dst, int ldd, const cd *src, int lds, int rows, int cols) {
+  for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
+    const int r = e / cols, c = e % cols;
+    dst[(size_t)r * ldd + c] = src[(size_t)r * lds + c];
+  }
+}
+
+__device__ void diag_to_dense(cd *dst, int n, const cd *d) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e % n;
+    dst[e] = (r == c) ? d[r] : cd{0.0, 0.0};
+  }
+}
+
+// y = A x, A rows x cols (lda); one warp per row.
+__device__ void matvec(cd *y, const cd *A, int lda, const cd *x, int rows, int cols) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = w; r < rows; r += nw) {
+    cd s = cd{0.0, 0.0};
+    for (int c = lane; c < cols; c += 32) s = cadd(s, cmul(A[(size_t)r * lda + c], x[c]));
+    for (int o = 16; o > 0; o >>= 1) {
+      s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+    }
+    if (lane == 0) y[r] = s;
+  }
+}
+
+__device__ double block_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+  __syncthreads();
+  if (threadIdx.x == 0) red[0] = s;
+  __syncthreads();
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
+__device__ __forceinline__ cd shear_q(const StackArgs &a, int b, int pos, double c0, double c1) {
+  const int u = pos % a.npw;  // unsorted air order of the same index (reference behaviour)
+  const double al = a.alphas[(size_t)b * a.npw + u];
+  const double be = a.betas ? a.betas[(size_t)b * a.npw + u] : 0.0;
+  const double th = (a.ncoord == 1) ? al * c0 : al * c0 + be * c1;
+  double s, c;
+  sincos(th, &s, &c);
+  return cd{c, s};
+}
+
+__device__ __forceinline__ cd incidence(const StackArgs &a, int b, int pos, int spec) {
+  if (a.pol == EMU_POL_INCOMING) return a.incoming[(size_t)b * a.P + pos];
+  const bool te = pos == spec, tm = pos == spec + a.npw;
+  switch (a.pol) {
+    case EMU_POL_TE: return te ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    case EMU_POL_TM: return tm ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    case EMU_POL_UN: return (te || tm) ? cd{a.inv_sqrt2, 0.0} : cd{0.0, 0.0};
+    case EMU_POL_RCIRC: return te ? cd{a.inv_sqrt2, 0.0} : (tm ? cd{0.0, a.inv_sqrt2} : cd{0.0, 0.0});
+    case EMU_POL_LCIRC: return te ? cd{a.inv_sqrt2, 0.0} : (tm ? cd{0.0, -a.inv_sqrt2} : cd{0.0, 0.0});
+  }
+  return cd{0.0, 0.0};
+}
+
+__global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
+  __shared__ Smem sm;
+  const int b = blockIdx.x;
+  const int L = a.L, P = a.P, D = a.D, npw = a.npw;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const size_t DD = (size_t)D * D;
+  cd *base = a.ws + (size_t)b * a.ws_stride;
+  cd *Rl = base;                              // rnet_list: 2L-2 slots
+  cd *X1l = Rl + (size_t)(2 * L - 2) * DD;    // inv_t21_list: L-1 slots (P x M_i)
+  cd *X2l = X1l + (size_t)(L - 1) * DD;       // inv_t12_list: L-2 slots (M_i x P)
+  cd *Pl = X2l + (size_t)(L > 2 ? L - 2 : 0) * DD;  // P_list: L-2 vectors
+  cd *tnet = Pl + (size_t)(L > 2 ? L - 2 : 0) * D;
+  cd *T = tnet + DD;
+  cd *Y = T + DD;
+  cd *Z = Y + DD;
+  cd *V = Z + DD;  // 6 vectors of D
+  int *ipiv = a.ipiv + (size_t)b * D;
+  int info = 0;
+  const int M0 = a.lay[0].M;
+
+  auto lay_ptr = [&](const cd *p, long long s) { return p + (size_t)b * s; };
+
+  // ---- substrate: tnet = T12_0, rnet = R12_0
+  {
+    const DLayer &l0 = a.lay[0];
+    if (l0.dense) {
+      copy_mat(tnet, P, lay_ptr(l0.T12, l0.sT12), P, M0, P);
+      copy_mat(Rl, P, lay_ptr(l0.R12, l0.sR12), P, P, P);
+    } else {
+      diag_to_dense(tnet, P, lay_ptr(l0.T12, l0.sT12));
+      diag_to_dense(Rl, P, lay_ptr(l0.R12, l0.sR12));
+    }
+    __syncthreads();
+    if (a.save_lists) {
+      copy_mat(a.tnl + (size_t)b * (2 * L - 2) * DD, P, tnet, P, M0, P);
+      copy_mat(a.rnl + (size_t)b * (2 * L - 2) * DD, P, Rl, P, P, P);
+    }
+  }
+  int slot = 0;       // index of the current rnet in Rl
+  int tcols = P;      // columns of tnet
+  for (int i = 1; i < L; ++i) {
+    const DLayer &ly = a.lay[i];
+    const int M = ly.M;
+    cd *rnet = Rl + (size_t)slot * DD;      // P x P here
+    cd *X1 = X1l + (size_t)(i - 1) * DD;     // P x M
+    cd *rn1 = Rl + (size_t)(slot + 1) * DD;  // M x M after the gap
+    // ---------------- air gap below layer i (stack.py:229-247, 263-278)
+    // shear: rnet' = Qinv rnet Q, tnet' = tnet Q
+    const cd *rg = rnet;
+    if (a.has_shear) {
+      double c0, c1;
+      if (i < L - 1) {
+        c0 = a.lay[i - 1].sh0 - ly.sh0;
+        c1 = a.lay[i - 1].sh1 - ly.sh1;
+      } else {
+        c0 = ly.sh0;
+        c1 = ly.sh1;
+      }
+      for (int e = tid; e < P * P; e += nt) {
+        const int r = e / P, c = e % P;
+        Z[e] = cmul(cmul(shear_q(a, b, r, -1 * c0, -1 * c1), rnet[e]), shear_q(a, b, c, c0, c1));
+      }
+      for (int e = tid; e < M0 * tcols; e += nt) {
+        const int c = e % tcols;
+        tnet[e] = cmul(tnet[e], shear_q(a, b, c, c0, c1));
+      }
+      __syncthreads();
+      rg = Z;
+    }
+    // T = I - R12 rnet'
+    if (ly.dense) {
+      for (int e = tid; e < P * P; e += nt) T[e] = cd{(e / P == e % P) ? 1.0 : 0.0, 0.0};
+      __syncthreads();
+      cta_gemm(P, P, P, cd{-1.0, 0.0}, lay_ptr(ly.R12, ly.sR12), P, rg, P, cd{1.0, 0.0}, T, P, sm.gs);
+      copy_mat(X1, M, lay_ptr(ly.T21, ly.sT21), M, P, M);
+    } else {
+      const cd *r12 = lay_ptr(ly.R12, ly.sR12);
+      for (int e = tid; e < P * P; e += nt) {
+        const int r = e / P, c = e % P;
+        T[e] = csub(cd{(r == c) ? 1.0 : 0.0, 0.0}, cmul(r12[r], rg[e]));
+      }
+      diag_to_dense(X1, P, lay_ptr(ly.T21, ly.sT21));
+    }
+    __syncthreads();
+    int inf = cta_getrf(P, T, P, ipiv, sm.ls, sm.gs);
+    if (inf && !info) info = (2 * i - 1) * 100000 + inf;
+    __syncthreads();
+    cta_getrs(P, M, T, P, ipiv, X1, M, sm.gs);
+    // tnet = tnet X1 ; rnet_new = R21 + T12 rnet' X1
+    cta_gemm(M0, M, P, cd{1.0, 0.0}, tnet, tcols, X1, M, cd{0.0, 0.0}, Y, M, sm.gs);
+    __syncthreads();
+    copy_mat(tnet, M, Y, M, M0, M);
+    tcols = M;
+    if (ly.dense) {
+      cta_gemm(M, P, P, cd{1.0, 0.0}, lay_ptr(ly.T12, ly.sT12), P, rg, P, cd{0.0, 0.0}, Y, P, sm.gs);
+      copy_mat(rn1, M, lay_ptr(ly.R21, ly.sR21), M, M, M);
+      __syncthreads();
+      cta_gemm(M, M, P, cd{1.0, 0.0}, Y, P, X1, M, cd{1.0, 0.0}, rn1, M, sm.gs);
+    } else {
+      cta_gemm(P, P, P, cd{1.0, 0.0}, rg, P, X1, P, cd{0.0, 0.0}, Y, P, sm.gs);
+      __syncthreads();
+      const cd *t12 = lay_ptr(ly.T12, ly.sT12);
+      const cd *r21 = lay_ptr(ly.R21, ly.sR21);
+      for (int e = tid; e < P * P; e += nt) {
+        const int r = e / P, c = e % P;
+        const cd v = cmul(t12[r], Y[e]);
+        rn1[e] = (r == c) ? cadd(r21[r], v) : v;
+      }
+    }
+    __syncthreads();
+    slot += 1;
+    if (a.save_lists) {
+      copy_mat(a.tnl + ((size_t)b * (2 * L - 2) + slot) * DD, tcols, tnet, tcols, M0, tcols);
+      copy_mat(a.rnl + ((size_t)b * (2 * L - 2) + slot) * DD, M, rn1, M, M, M);
+    }
+    if (i == L - 1) break;
+    // ---------------- through layer i (stack.py:249-262)
+    cd *pd = Pl + (size_t)(i - 1) * D;
+    const cd *kz = lay_ptr(ly.kz, ly.skz);
+    for (int r = tid; r < M; r += nt) pd[r] = cexp_ikh(kz[r], ly.hn);
+    __syncthreads();
+    cd *X2 = X2l + (size_t)(i - 1) * DD;      // M x P
+    cd *rn2 = Rl + (size_t)(slot + 1) * DD;   // P x P
+    // T = I - R21 (Pd rnet Pd)
+    if (ly.dense) {
+      for (int e = tid; e < M * M; e += nt) {
+        const int r = e / M, c = e % M;
+        Z[e] = cmul(cmul(pd[r], rn1[e]), pd[c]);
+        T[e] = cd{(r == c) ? 1.0 : 0.0, 0.0};
+      }
+      __syncthreads();
+      cta_gemm(M, M, M, cd{-1.0, 0.0}, lay_ptr(ly.R21, ly.sR21), M, Z, M, cd{1.0, 0.0}, T, M, sm.gs);
+      copy_mat(X2, P, lay_ptr(ly.T12, ly.sT12), P, M, P);
+    } else {
+      const cd *r21 = lay_ptr(ly.R21, ly.sR21);
+      for (int e = tid; e < M * M; e += nt) {
+        const int r = e / M, c = e % M;
+        T[e] = csub(cd{(r == c) ? 1.0 : 0.0, 0.0}, cmul(cmul(cmul(r21[r], pd[r]), rn1[e]), pd[c]));
+      }
+      diag_to_dense(X2, P, lay_ptr(ly.T12, ly.sT12));
+    }
+    __syncthreads();
+    inf = cta_getrf(M, T, M, ipiv, sm.ls, sm.gs);
+    if (inf && !info) info = (2 * i) * 100000 + inf;
+    __syncthreads();
+    cta_getrs(M, P, T, M, ipiv, X2, P, sm.gs);
+    // PX2 = Pd X2 (into Z) ; tnet = tnet PX2
+    for (int e = tid; e < M * P; e += nt) Z[e] = cmul(pd[e / P], X2[e]);
+    __syncthreads();
+    cta_gemm(M0, P, M, cd{1.0, 0.0}, tnet, tcols, Z, P, cd{0.0, 0.0}, Y, P, sm.gs);
+    __syncthreads();
+    copy_mat(tnet, P, Y, P, M0, P);
+    tcols = P;
+    __syncthreads();
+    // rnet = R12 + (T21 Pd) rnet PX2
+    if (ly.dense) {
+      cta_gemm(P, M, M, cd{1.0, 0.0}, lay_ptr(ly.T21, ly.sT21), M, rn1, M, cd{0.0, 0.0}, Y, M, sm.gs,
+               pd, nullptr);
+      copy_mat(rn2, P, lay_ptr(ly.R12, ly.sR12), P, P, P);
+      __syncthreads();
+      cta_gemm(P, P, M, cd{1.0, 0.0}, Y, M, Z, P, cd{1.0, 0.0}, rn2, P, sm.gs);
+    } else {
+      cta_gemm(P, P, P, cd{1.0, 0.0}, rn1, P, Z, P, cd{0.0, 0.0}, Y, P, sm.gs, nullptr, nullptr);
+      __syncthreads();
+      const cd *t21 = lay_ptr(ly.T21, ly.sT21);
+      const cd *r12 = lay_ptr(ly.R12, ly.sR12);
+      for (int e = tid; e < P * P; e += nt) {
+        const int r = e / P, c = e % P;
+        const cd v = cmul(cmul(t21[r], pd[r]), Y[e]);
+        rn2[e] = (r == c) ? cadd(r12[r], v) : v;
+      }
+    }
+    __syncthreads();
+    slot += 1;
+    if (a.save_lists) {
+      copy_mat(a.tnl + ((size_t)b * (2 * L - 2) + slot) * DD, P, tnet, P, M0, P);
+      copy_mat(a.rnl + ((size_t)b * (2 * L - 2) + slot) * DD, P, rn2, P, P, P);
+    }
+  }
+  // outputs R_net (P x P), T_net (M0 x P)
+  const cd *Rtop = Rl + (size_t)slot * DD;
+  copy_mat(a.R_net + (size_t)b * P * P, P, Rtop, P, P, P);
+  copy_mat(a.T_net + (size_t)b * M0 * P, P, tnet, P, M0, P);
+  __syncthreads();
+  if (tid == 0 && a.info) a.info[b] = info;
+  if (!a.calc_fluxes) return;
+
+  // ---------------- fluxes, top to bottom (stack.py:289-426)
+  cd *d = V, *f1m = V + D, *f1p = V + 2 * D, *f2m = V + 3 * D, *f2p = V + 4 * D, *tmp = V + 5 * D;
+  const int spec = a.spec[b];
+  const int np_air = a.nprop[3 * b + 0], np_in = a.nprop[3 * b + 1], np_out = a.nprop[3 * b + 2];
+  for (int j = tid; j < P; j += nt) d[j] = incidence(a, b, j, spec);
+  __syncthreads();
+  matvec(f1p, Rtop, P, d, P, P);  // d_plus
+  matvec(f1m, X1l + (size_t)(L - 2) * DD, P, d, P, P);
+  __syncthreads();
+  cd *vcd = a.vcd ? a.vcd + (size_t)b * a.vcd_stride : nullptr;
+  cd *vcu = a.vcu ? a.vcu + (size_t)b * a.vcu_stride : nullptr;
+  size_t od = 0, ou = 0;
+  double s_in = 0.0, s_up = 0.0;
+  for (int j = tid; j < P; j += nt) {
+    if ((j % npw) < np_in) {
+      s_in += cabs2(d[j]);
+      s_up += cabs2(f1p[j]);
+    }
+    if (vcd) vcd[j] = d[j];
+    if (vcu) vcu[j] = f1p[j];
+  }
+  od = P;
+  ou = P;
+  const double df0 = block_sum(s_in, sm.red);
+  const double up0 = block_sum(s_up, sm.red);
+  double *fo = a.fluxes ? a.fluxes + (size_t)b * (L + 1) * 2 : nullptr;
+  double gre[kMaxLayers], gim[kMaxLayers];
+  for (int q = 0; q < L - 2; ++q) {
+    const int k = L - 2 - q;
+    const int M = a.lay[k].M;
+    const cd *pd = Pl + (size_t)(k - 1) * D;
+    matvec(f1p, Rl + (size_t)(2 * k) * DD, P, f1m, P, P);
+    __syncthreads();
+    double sr = 0.0, si = 0.0;
+    for (int j = tid; j < P; j += nt) {
+      const cd fm = f1m[j], fp = f1p[j];
+      const bool prop = (j % npw) < np_air;
+      const bool tm = j >= npw;
+      if (prop) {
+        sr += cabs2(fm) - cabs2(fp);
+      } else {
+        const cd u = cmul(cconj(fm), fp), v = cmul(cconj(fp), fm);
+        cd dd = csub(v, u);
+        cd t = cd{-dd.y, dd.x};
+        if (tm) t = cneg(t);
+        sr += t.x;
+        si += t.y;
+      }
+    }
+    gre[q] = block_sum(sr, sm.red);
+    gim[q] = block_sum(si, sm.red);
+    matvec(f2m, X2l + (size_t)(k - 1) * DD, P, f1m, M, P);
+    __syncthreads();
+    for (int j = tid; j < M; j += nt) tmp[j] = cmul(pd[j], f2m[j]);
+    __syncthreads();
+    matvec(f2p, Rl + (size_t)(2 * k - 1) * DD, M, tmp, M, M);
+    matvec(f1m, X1l + (size_t)(k - 1) * DD, M, tmp, P, M);
+    __syncthreads();
+    for (int j = tid; j < M; j += nt) {
+      if (vcd) vcd[od + j] = f2m[j];
+      if (vcu) vcu[ou + j] = f2p[j];
+    }
+    od += M;
+    ou += M;
+    __syncthreads();
+  }
+  // bottom: f2m = tnet_list[0] f1m = T12_0 f1m
+  {
+    const DLayer &l0 = a.lay[0];
+    if (l0.dense) {
+      matvec(f2m, lay_ptr(l0.T12, l0.sT12), P, f1m, M0, P);
+    } else {
+      const cd *t12 = lay_ptr(l0.T12, l0.sT12);
+      for (int j = tid; j < P; j += nt) f2m[j] = cmul(t12[j], f1m[j]);
+    }
+    __syncthreads();
+    double so = 0.0;
+    for (int j = tid; j < M0; j += nt) {
+      if (vcd) vcd[od + j] = f2m[j];
+      if (!l0.dense && (j % npw) < np_out) so += cabs2(f2m[j]);
+    }
+    const double dsub = block_sum(so, sm.red);
+    if (tid == 0) {
+      if (fo) {
+        fo[0] = df0;
+        fo[1] = 0.0;
+        for (int q = 0; q < L - 2; ++q) {
+          fo[2 * (q + 1)] = gre[q];
+          fo[2 * (q + 1) + 1] = gim[q];
+        }
+        fo[2 * (L - 1)] = dsub;
+        fo[2 * (L - 1) + 1] = 0.0;
+        fo[2 * L] = up0;
+        fo[2 * L + 1] = 0.0;
+      }
+      uint32_t flags = 0;
+      if (np_in == 0) flags |= EMU_PT_NO_PROP_SUP;
+      if (!l0.dense && np_out == 0) flags |= EMU_PT_NO_PROP_SUB;
+      if (a.a_list && !l0.dense) {
+        double *al = a.a_list + (size_t)b * (L - 1);
+        double *tl = a.t_list + (size_t)b * (L - 1);
+        auto dfa = [&](int i) -> double {
+          if (i == 0) return fabs(df0);
+          if (i == L - 1) return fabs(dsub);
+          return hypot(gre[i - 1], gim[i - 1]);
+        };
+        if (np_out != 0) {
+          for (int i = 1; i <= L - 2; ++i) al[i - 1] = fabs(dfa(i) - dfa(i + 1));
+          al[L - 2] = fabs(df0 - dsub - up0);
+          for (int i = 0; i <= L - 3; ++i) tl[i] = fabs(dfa(i + 2) / dfa(i));
+          tl[L - 2] = fabs(dsub / df0);
+          a.r_list[b] = fabs(up0 / df0);
+        } else {
+          for (int i = 0; i < L - 1; ++i) al[i] = tl[i] = 0.0;
+          a.r_list[b] = 0.0;
+        }
+        bool fin = isfinite(a.r_list[b]);
+        for (int i = 0; i < L - 1; ++i) fin = fin && isfinite(al[i]) && isfinite(tl[i]);
+        if (!fin) flags |= EMU_PT_NONFINITE;
+      }
+      if (a.flags) a.flags[b] = flags;
+    }
+  }
+}
+
+}  // namespace
+
+namespace {
+
+int max_dim(const EmuStackDense *p) {
+  int D = p->P;
+  for (int i = 0; i < p->n_layers; ++i) D = p->h_layers[i].M > D ? p->h_layers[i].M : D;
+  return D;
+}
+
+long long per_solve_elems(const EmuStackDense *p) {
+  const long long L = p->n_layers, D = max_dim(p);
+  const long long Lf = L > 2 ? L - 2 : 0;
+  return (2 * L - 2 + L - 1 + Lf + 4) * D * D + Lf * D + 6 * D;
+}
+
+int validate(const EmuStackDense *p) {
+  if (!p || !p->h_layers) return EMU_E_ARG;
+  if (p->batch < 0 || p->n_layers < 2 || p->n_layers > kMaxLayers || p->P < 2 || (p->P % 2))
+    return EMU_E_SHAPE;
+  for (int i = 0; i < p->n_layers; ++i) {
+    const EmuLayer &l = p->h_layers[i];
+    if (l.M < 1) return EMU_E_SHAPE;
+    if (!l.dense && l.M != p->P) return EMU_E_SHAPE;
+    if (!l.d_R12 || !l.d_T12 || !l.d_R21 || !l.d_T21) return EMU_E_ARG;
+    if (i > 0 && i < p->n_layers - 1 && !l.d_kz) return EMU_E_ARG;
+  }
+  if (p->h_layers[p->n_layers - 1].M != p->P) return EMU_E_SHAPE;
+  if (!p->d_R_net || !p->d_T_net) return EMU_E_ARG;
+  if (p->calc_fluxes) {
+    if (p->h_layers[p->n_layers - 1].dense) return EMU_E_UNSUPPORTED;  // needs a film on top
+    if (!p->d_specular || !p->d_num_prop) return EMU_E_ARG;
+    if (p->pol == EMU_POL_INCOMING && !p->d_incoming) return EMU_E_ARG;
+    if (p->pol < EMU_POL_INCOMING || p->pol > EMU_POL_LCIRC) return EMU_E_ARG;
+  }
+  if (p->h_shears && (!p->d_air_alphas || (p->shear_ncoord == 2 && !p->d_air_betas))) return EMU_E_ARG;
+  if (p->save_lists && (!p->d_tnet_list || !p->d_rnet_list)) return EMU_E_ARG;
+  return EMU_OK;
+}
+
+}  // namespace
+
+extern "C" size_t emu_stack_dense_workspace_size(const EmuStackDense *p) {
+  if (validate(p) != EMU_OK) return 0;
+  const long long D = max_dim(p);
+  return (size_t)p->batch * ((size_t)per_solve_elems(p) * sizeof(cd) + align_up((size_t)D * 4, 16)) + 256;
+}
+
+extern "C" long long emu_stack_dense_list_stride(const EmuStackDense *p) {
+  if (validate(p) != EMU_OK) return 0;
+  const long long D = max_dim(p);
+  return D * D;
+}
+
+extern "C" int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace,
+                                     size_t workspace_bytes, void *stream) {
+  int st = validate(p);
+  if (st != EMU_OK) return st;
+  if (p->batch == 0) return EMU_OK;
+  if (!d_workspace || workspace_bytes < emu_stack_dense_workspace_size(p)) return EMU_E_WORKSPACE;
+  StackArgs a;
+  memset(&a, 0, sizeof(a));
+  a.B = p->batch;
+  a.L = p->n_layers;
+  a.P = p->P;
+  a.npw = p->P / 2;
+  a.D = max_dim(p);
+  for (int i = 0; i < p->n_layers; ++i) {
+    const EmuLayer &l = p->h_layers[i];
+    DLayer &d = a.lay[i];
+    d.R12 = (const cd *)l.d_R12;
+    d.T12 = (const cd *)l.d_T12;
+    d.R21 = (const cd *)l.d_R21;
+    d.T21 = (const cd *)l.d_T21;
+    d.kz = (const cd *)l.d_kz;
+    d.sR12 = l.stride_R12;
+    d.sT12 = l.stride_T12;
+    d.sR21 = l.stride_R21;
+    d.sT21 = l.stride_T21;
+    d.skz = l.stride_kz;
+    d.M = l.M;
+    d.dense = l.dense;
+    d.hn = l.height_norm;
+    d.sh0 = p->h_shears ? p->h_shears[2 * i] : 0.0;
+    d.sh1 = p->h_shears ? p->h_shears[2 * i + 1] : 0.0;
+  }
+  a.ncoord = p->shear_ncoord;
+  a.has_shear = p->h_shears != nullptr;
+  a.alphas = p->d_air_alphas;
+  a.betas = p->d_air_betas;
+  a.calc_fluxes = p->calc_fluxes;
+  a.pol = p->pol;
+  a.incoming = (const cd *)p->d_incoming;
+  a.spec = p->d_specular;
+  a.nprop = p->d_num_prop;
+  a.R_net = (cd *)p->d_R_net;
+  a.T_net = (cd *)p->d_T_net;
+  a.fluxes = p->d_fluxes;
+  a.a_list = p->d_a_list;
+  a.t_list = p->d_t_list;
+  a.r_list = p->d_r_list;
+  a.flags = p->d_flags;
+  a.info = p->d_info;
+  a.vcd = (cd *)p->d_vec_coef_down;
+  a.vcu = (cd *)p->d_vec_coef_up;
+  a.vcd_stride = p->vec_coef_down_stride;
+  a.vcu_stride = p->vec_coef_up_stride;
+  a.save_lists = p->save_lists;
+  a.tnl = (cd *)p->d_tnet_list;
+  a.rnl = (cd *)p->d_rnet_list;
+  a.ws = (cd *)d_workspace;
+  a.ws_stride = per_solve_elems(p);
+  a.ipiv = (int *)((char *)d_workspace + align_up((size_t)p->batch * a.ws_stride * sizeof(cd), 16));
+  a.inv_sqrt2 = 1.0 / sqrt(2.0);
+  stack_dense_kernel<<<p->batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);
+  emu::note_launch();
+  return emu::check_launch();
+}

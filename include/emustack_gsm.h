@@ -178,6 +178,97 @@ size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p);
 int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspace,
                          size_t workspace_bytes, void *stream);
 
+/* ------------------------------------------ dense linear algebra
+ * Batched complex128 GEMM, C_b = alpha A_b B_b + beta C_b (row-major; A_b is
+ * m x k, B_b k x n), and batched LU solve A_b X_b = B_b with partial pivoting
+ * (A_b overwritten by its LU factors, B_b by X_b; ipiv 0-based; info[b] = 0
+ * or j+1 for the first exactly-zero pivot).  These stand in for the
+ * np.matrix products and np.linalg.solve (LAPACK zgesv) calls of
+ * backend/stack.py:229-278 and backend/mode_calcs.py:498-513. */
+int emu_zgemm_batched(int m, int n, int k, emu_c128 alpha, const emu_c128 *d_A, int lda,
+                      long long stride_A, const emu_c128 *d_B, int ldb, long long stride_B,
+                      emu_c128 beta, emu_c128 *d_C, int ldc, long long stride_C, int batch,
+                      void *stream);
+int emu_zgesv_batched(int n, int nrhs, emu_c128 *d_A, int lda, long long stride_A,
+                      int32_t *d_ipiv, emu_c128 *d_B, int ldb, long long stride_B,
+                      int32_t *d_info, int batch, void *stream);
+
+/* ---------------------------------------------- a7: film interfaces
+ * R12 = (Z2 - Z1)/(Z2 + Z1), T12 = 2 sqrt(Z2) sqrt(Z1)/(Z2 + Z1) for every
+ * order and polarisation, Z from each film's sorted k_z, index n and the
+ * normalised wavelength (R21 = -R12, T21 = T12).  Replaces r_t_mat_anallo
+ * (backend/mode_calcs.py:451-477).  Outputs are the diagonals, [B][2 Npw]. */
+int emu_film_interface_batch(int batch, int n_pw, const emu_c128 *d_kz1, const emu_c128 *d_n1,
+                             const emu_c128 *d_kz2, const emu_c128 *d_n2,
+                             const double *d_wl_norm, emu_c128 *d_R12, emu_c128 *d_T12,
+                             void *stream);
+
+/* ---------------------------------- a8: film / nanostructure interface
+ * Batched r_t_mat_tf_ns (backend/mode_calcs.py:480-515): for each b,
+ *   z = sqrt(1/Z_film), A = z o J, B = J_dag o z, S = I + B A,
+ *   R12 = -I + 2 A S^-1 B (P x P), T12 = 2 S^-1 B (M x P),
+ *   R21 = S^-1 (I - B A) (M x M), T21 = 2 A S^-1 (P x M),
+ * with Z_film from the film's sorted k_z [b][P/2], index n [b] and
+ * normalised wavelength [b] (backend/mode_calcs.py:199-218).
+ * J [b][P][M] (already divided by the area ratio, mode_calcs.py:384-386),
+ * J_dag [b][M][P].  info[b] != 0 marks an exactly singular I + B A. */
+size_t emu_interface_dense_workspace_size(int batch, int P, int M);
+int emu_interface_dense_batch(int batch, int P, int M, const emu_c128 *d_film_kz,
+                              const emu_c128 *d_film_n, const double *d_wl_norm,
+                              const emu_c128 *d_J, const emu_c128 *d_J_dag, emu_c128 *d_R12,
+                              emu_c128 *d_T12, emu_c128 *d_R21, emu_c128 *d_T21,
+                              int32_t *d_info, void *d_workspace, size_t workspace_bytes,
+                              void *stream);
+
+/* ------------------------------- a9, a10: dense cascade and fluxes
+ * Net scattering matrices and energy fluxes of stacks with nanostructured
+ * layers (backend/stack.py:162-426), one spectral point per batch item,
+ * every item with the same layer shapes.  Layer i (bottom = 0) gives its
+ * air-interface matrices: dense ones as R12 [P][P], T12 [M][P],
+ * R21 [M][M], T21 [P][M]; film ones (dense = 0, M = P) as diagonals [P].
+ * A zero stride shares a matrix across the batch. */
+typedef struct {
+  int M;                 /* modes of the layer (P for a film)               */
+  int dense;             /* 1: dense interface matrices; 0: film diagonals  */
+  const emu_c128 *d_R12, *d_T12, *d_R21, *d_T21;
+  long long stride_R12, stride_T12, stride_R21, stride_T21; /* elements    */
+  const emu_c128 *d_kz;  /* [b][M] k_z (finite layers)                      */
+  long long stride_kz;
+  double height_norm;    /* height / period (finite layers)                 */
+} EmuLayer;
+
+typedef struct {
+  int batch, n_layers, P;
+  const EmuLayer *h_layers;    /* host array [n_layers], bottom to top      */
+  const double *h_shears;      /* host [n_layers][2] or NULL                */
+  int shear_ncoord;            /* 1 or 2                                    */
+  const double *d_air_alphas;  /* [batch][P/2] air alphas, unsorted         */
+  const double *d_air_betas;   /* [batch][P/2] or NULL (1D)                 */
+  int calc_fluxes;             /* needs a film superstrate                  */
+  int pol;                     /* EMU_POL_*                                 */
+  const emu_c128 *d_incoming;  /* [batch][P] for EMU_POL_INCOMING           */
+  const int32_t *d_specular;   /* [batch] superstrate specular order        */
+  const int32_t *d_num_prop;   /* [batch][3] propagating orders: air, superstrate, substrate */
+  emu_c128 *d_R_net;           /* [batch][P][P]                             */
+  emu_c128 *d_T_net;           /* [batch][M0][P]                            */
+  double *d_fluxes;            /* [batch][L+1][2] or NULL: down fluxes (incoming, air gaps top
+                                  to bottom, substrate) then the reflected flux */
+  double *d_a_list, *d_t_list, *d_r_list; /* film substrate only, or NULL  */
+  uint32_t *d_flags;           /* [batch] EMU_PT_* or NULL                  */
+  int32_t *d_info;             /* [batch] 0 or the first singular solve     */
+  emu_c128 *d_vec_coef_down;   /* [batch][stride] or NULL                   */
+  emu_c128 *d_vec_coef_up;
+  long long vec_coef_down_stride, vec_coef_up_stride;
+  int save_lists;              /* 1: fill d_tnet_list / d_rnet_list         */
+  emu_c128 *d_tnet_list;       /* [batch][2L-2][list_stride]                */
+  emu_c128 *d_rnet_list;
+} EmuStackDense;
+
+size_t emu_stack_dense_workspace_size(const EmuStackDense *p);
+long long emu_stack_dense_list_stride(const EmuStackDense *p);
+int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace, size_t workspace_bytes,
+                          void *stream);
+
 /* ------------------------------------------------------- measurement
  * FP64 FMA throughput probe: blocks x threads threads each run 64 dependent
  * FMA chains of `iters` steps (2*64*iters*threads*blocks flops).  Used as the

@@ -343,6 +343,8 @@ def main():
         sim = synth_struct(light, per, M_, len(air.k_z), 50.0)
         R12, T12, R21, T21 = mode_calcs.r_t_mat_tf_ns(air, sim)
         d['q%d_Z_air' % q] = _arr(air.Z())
+        d['q%d_air_kz' % q] = _arr(air.k_z[:len(air.k_z) // 2])
+        d['q%d_wl_norm' % q] = _arr(air.wl_norm())
         d['q%d_J' % q] = _arr(sim.J)
         d['q%d_J_dag' % q] = _arr(sim.J_dag)
         for nm, m in (('R12', R12), ('T12', T12), ('R21', R21), ('T21', T21)):

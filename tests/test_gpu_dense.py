@@ -1,0 +1,156 @@
+"""GPU parity of the dense GSM path: batched complex LU / GEMM, the
+film/nanostructure interface (backend/mode_calcs.py:480-515), the cascade
+and fluxes (backend/stack.py:162-426) for stacks with nanostructured
+layers, through the drop-in objects.  FP64 throughout; held to
+rtol 1e-9 / atol 1e-10 against the reference's outputs (product bar: 1e-6
+absolute on R, T, A)."""
+import numpy as np
+import pytest
+import torch
+
+from fixtures import load_points, load_raw
+
+pytestmark = pytest.mark.gpu
+
+TOL = dict(rtol=1e-9, atol=1e-10)
+
+
+def _rand(shape, rng):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+@pytest.mark.parametrize('m,n,k,b', [(1, 1, 1, 1), (5, 7, 3, 2), (64, 64, 64, 1), (70, 130, 65, 3),
+                                     (200, 17, 300, 2)])
+def test_zgemm_batched(m, n, k, b):
+    from emustack_b200.dense import zgemm_batched
+    rng = np.random.default_rng(m * 1000 + n)
+    A, B, Cc = _rand((b, m, k), rng), _rand((b, k, n), rng), _rand((b, m, n), rng)
+    dA, dB, dC = (torch.tensor(x, device='cuda') for x in (A, B, Cc))
+    out = zgemm_batched(dA, dB, dC, alpha=0.5 - 2j, beta=1.5 + 0.25j).cpu().numpy()
+    np.testing.assert_allclose(out, (0.5 - 2j) * A @ B + (1.5 + 0.25j) * Cc, rtol=1e-12, atol=1e-11)
+
+
+@pytest.mark.parametrize('n,nrhs,b', [(1, 1, 1), (7, 3, 2), (33, 40, 2), (100, 58, 3), (261, 5, 1)])
+def test_zgesv_batched(n, nrhs, b):
+    from emustack_b200.dense import zgesv_batched
+    rng = np.random.default_rng(n)
+    A = _rand((b, n, n), rng) + 3 * np.eye(n)
+    Bm = _rand((b, n, nrhs), rng)
+    X, ipiv, info = zgesv_batched(torch.tensor(A, device='cuda'), torch.tensor(Bm, device='cuda'))
+    assert (info.cpu().numpy() == 0).all()
+    np.testing.assert_allclose(X.cpu().numpy(), np.linalg.solve(A, Bm), rtol=1e-10, atol=1e-10)
+
+
+def test_zgesv_singular_reports_info():
+    from emustack_b200.dense import zgesv_batched
+    A = np.zeros((1, 4, 4), complex)
+    A[0, :3, :3] = np.eye(3)
+    _, _, info = zgesv_batched(torch.tensor(A, device='cuda'), torch.ones((1, 4, 1), dtype=torch.complex128,
+                                                                          device='cuda'))
+    assert int(info[0]) == 4
+
+
+def test_interface_dense_matches_reference():
+    """r_t_mat_tf_ns outputs of the reference at (P, M) = (58, 60), (58, 40), (26, 46)."""
+    from emustack_b200.dense import interface_dense
+    raw = load_raw('interfaces')
+    for q in range(int(raw['n_shapes'])):
+        J, Jd = raw['q%d_J' % q], raw['q%d_J_dag' % q]
+        kz = raw['q%d_air_kz' % q]
+        npw = kz.shape[0]
+        dev = 'cuda'
+        R12, T12, R21, T21, info = interface_dense(
+            torch.tensor(kz.reshape(1, npw), device=dev), torch.tensor([1.0 + 0j], device=dev),
+            torch.tensor([float(raw['q%d_wl_norm' % q])], device=dev),
+            torch.tensor(J[None], device=dev), torch.tensor(Jd[None], device=dev))
+        assert int(info[0]) == 0
+        for nm, t in (('R12', R12), ('T12', T12), ('R21', R21), ('T21', T21)):
+            np.testing.assert_allclose(t[0].cpu().numpy(), raw['q%d_%s' % (q, nm)], rtol=1e-8, atol=1e-9,
+                                       err_msg='shape %d %s' % (q, nm))
+
+
+def _dropin_stack(pt, use_J):
+    """Build a drop-in Stack for a golden point: films from n, structured
+    layers from J/J_dag (computed interface) or from the stored interface
+    matrices injected into the interface memo (as the golden replay does)."""
+    from emustack_b200 import objects, materials
+    from emustack_b200.mode_calcs import Simmo, _interfaces_i_have_known
+    from emustack_b200.stack import Stack
+    light = objects.Light(float(pt['wl_nm']), max_order_PWs=int(pt['max_order']),
+                          k_parallel=np.asarray(pt['k_pll'], float))
+    per, per_y, w1d = float(pt['period']), float(pt['period_y']), bool(pt['world_1d'])
+    hs = list(np.asarray(pt['heights_nm'], float))
+    nl = len(pt['layers'])
+    lays = []
+    for i, L in enumerate(pt['layers']):
+        h = 'semi_inf' if i in (0, nl - 1) else hs[i - 1]
+        if L['kind'] == 'film':
+            tf = objects.ThinFilm(per, per_y, height_nm=h, world_1d=w1d,
+                                  material=materials.Material(complex(L['n'])), loss=bool(L['loss']))
+            lays.append(tf.calc_modes(light))
+        else:
+            ns = objects.NanoStruct('1D_array' if w1d else '2D_array', per, 100, period_y=per_y,
+                                    height_nm=h, world_1d=w1d)
+            if use_J and 'J' in L:
+                lays.append(ns.calc_modes(light, k_z=L['k_z'], J=L['J'], J_dag=L['J_dag']))
+            else:
+                sim = Simmo(ns, light)
+                sim.k_z = np.asarray(L['k_z'])
+                air = sim.air_ref()
+                dev = 'cuda'
+                _interfaces_i_have_known[(id(air), id(sim))] = {'dev': tuple(
+                    torch.tensor(np.asarray(L[m]), device=dev).unsqueeze(0)
+                    for m in ('R12', 'T12', 'R21', 'T21')) + (True,)}
+                lays.append(sim)
+    shears = pt.get('shears')
+    st = Stack(lays, shears=None if shears is None else [np.asarray(s) for s in shears])
+    return st
+
+
+@pytest.mark.parametrize('name', ['case_1', 'case_2', 'case_3', 'case_4', 'case_5', 'synth_config1',
+                                  'synth_shear'])
+def test_dense_stack_matches_golden(name):
+    pts, raw = load_points(name)
+    for p, pt in enumerate(pts):
+        st = _dropin_stack(pt, use_J=True)
+        st.calc_scat(pol=pt['pol'])
+        msg = '%s p%d' % (name, p)
+        np.testing.assert_allclose(st.R_net, pt['R_net'], **TOL, err_msg=msg + ' R_net')
+        np.testing.assert_allclose(st.T_net, pt['T_net'], **TOL, err_msg=msg + ' T_net')
+        np.testing.assert_allclose(np.asarray(st.a_list, float), pt['a_list'], **TOL, err_msg=msg + ' a')
+        np.testing.assert_allclose(np.asarray(st.t_list, float), pt['t_list'], **TOL, err_msg=msg + ' t')
+        np.testing.assert_allclose(np.asarray(st.r_list, float), pt['r_list'], **TOL, err_msg=msg + ' r')
+        for i, L in enumerate(pt['layers']):
+            for m in ('R12', 'T12', 'R21', 'T21'):
+                np.testing.assert_allclose(getattr(st.layers[i], m), L[m], **TOL, err_msg='%s lay%d %s' % (msg, i, m))
+        for a, b in zip(st.vec_coef_down, pt['vec_coef_down']):
+            np.testing.assert_allclose(np.ravel(a), b, **TOL)
+        for a, b in zip(st.vec_coef_up, pt['vec_coef_up']):
+            np.testing.assert_allclose(np.ravel(a), b, **TOL)
+        key = 'p%d_stored_R_net' % p
+        if key in raw:
+            np.testing.assert_allclose(st.R_net, raw[key], rtol=1e-6, atol=1e-6)
+
+
+def test_save_scat_list_matches_oracle():
+    from fixtures import oracle_point
+    pts, raw = load_points('synth_config1')
+    pt = pts[1]
+    st = _dropin_stack(pt, use_J=True)
+    st.calc_scat(pol='TE', save_scat_list=True)
+    ref = oracle_point(pt)
+    assert len(st.rnet_list) == len(ref.rnet_list)
+    for a, b in zip(st.rnet_list, ref.rnet_list):
+        np.testing.assert_allclose(a, b, **TOL)
+    for a, b in zip(st.tnet_list, ref.tnet_list):
+        np.testing.assert_allclose(a, b, **TOL)
+
+
+def test_film_stack_through_dense_path_matches_film_kernel():
+    """save_scat_list forces the dense path for an all-film stack; both paths agree."""
+    pts, raw = load_points('films10')
+    pt = pts[0]
+    st = _dropin_stack(pt, use_J=False)
+    st.calc_scat(pol=pt['pol'], save_scat_list=True)
+    np.testing.assert_allclose(st.R_net, pt['R_net'], **TOL)
+    np.testing.assert_allclose(np.asarray(st.a_list, float), pt['a_list'], **TOL)
