@@ -161,3 +161,32 @@ EXTRA_SIGNATURES.extend([
     ('emu_stack_dense_list_stride', C.c_longlong, [C.POINTER(EmuStackDense)]),
     ('emu_stack_dense_batch', C.c_int, [C.POINTER(EmuStackDense), vp, C.c_size_t, vp]),
 ])
+
+
+class EmuOverlap(C.Structure):
+    _fields_ = [
+        ('batch', C.c_int), ('nval', C.c_int), ('nel', C.c_int), ('npt', C.c_int),
+        ('n_pw', C.c_int), ('max_order', C.c_int),
+        ('d_px', vp), ('d_py', vp), ('d_x', vp), ('d_table_nod', vp),
+        ('d', C.c_double), ('dy', C.c_double), ('d_bloch', vp), ('d_k0', vp),
+        ('d_sol1', vp), ('d_sol2', vp), ('d_scale2', vp), ('d_perm2', vp),
+        ('area_norm', C.c_double), ('d_J', vp), ('d_J_dag', vp), ('d_index_pw_inv', vp),
+        ('elements_per_chunk', C.c_int),
+    ]
+
+
+class EmuNormalise(C.Structure):
+    _fields_ = [
+        ('batch', C.c_int), ('nval', C.c_int), ('nel', C.c_int), ('npt', C.c_int),
+        ('d_x', vp), ('d_table_nod', vp), ('d_type_el', vp), ('d_pp', vp), ('d_k0', vp),
+        ('d_beta1', vp), ('d_sol1', vp), ('d_sol2', vp), ('d_diag', vp), ('d_scale', vp),
+        ('d_n_small', vp),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_overlap_workspace_size', C.c_size_t, [C.POINTER(EmuOverlap)]),
+    ('emu_overlap_batch', C.c_int, [C.POINTER(EmuOverlap), vp, C.c_size_t, vp]),
+    ('emu_mode_overlap_workspace_size', C.c_size_t, [C.POINTER(EmuNormalise)]),
+    ('emu_mode_overlap_diag', C.c_int, [C.POINTER(EmuNormalise), vp, C.c_size_t, vp]),
+])

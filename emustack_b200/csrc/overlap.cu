@@ -1,0 +1,665 @@
+// Bloch-mode / plane-wave overlap integrals J and J_dag
+// (backend/fortran/J_overlap.f:92-198, J_dagger_overlap.f:93-199) and the
+// Bloch-mode orthogonality / normalisation factors
+// (backend/fortran/orthogonal.f:84-248, normalisation.f:15-31).
+//
+// The reference loops element x quadrature point x plane wave x mode and
+// re-interpolates the P2 field for every plane wave.  Here the quadrature
+// is folded into a plane-wave table first:
+//   E~_s(el, node) = sum_q w_q |det_el| exp(-i k_s . x_q) phi_node(xi_q)
+// (16 quadrature points, affine element map), so that
+//   G_c[s, n] = sum_{el,node} E~_s(el, node) sol(c, node, n, el),  c = x, y
+// is one complex GEMM with K = 6 nel, and
+//   J_E = (beta o G_x - alpha o G_y) / |k_s|,  J_K = (alpha o G_x + beta o G_y) / |k_s|
+// in the epilogue (rows in the sorted plane-wave order of pw_ordering.f).
+// J_dag uses conj(E~) (exp(+i k.x)) and the adjoint fields.
+// The exponentials factor as exp(-i(a0 x + b0 y)) (exp(-i 2 pi x / d))^px
+// (exp(-i 2 pi y / dy))^py: per quadrature point one base phase and two
+// short power tables replace a sine/cosine per plane wave.
+#include <cuda_runtime.h>
+
+#include "dense_la.cuh"
+#include "emu_internal.h"
+
+namespace {
+
+using namespace emu;
+
+__constant__ double c_wq[16], c_xq[16], c_yq[16];
+__constant__ double c_phi2[16][6];       // P2 basis at the quadrature points
+__constant__ double c_g3[16][2][10];     // P3 gradients (reference triangle)
+
+// 16-point symmetric rule of Lyness & Jespersen (J. Inst. Math. Appl. 15,
+// 1975), as tabulated in backend/fortran/quad_triangle.f:56-145.
+void quad_table(double *w, double *x, double *y) {
+  const double wbar = 1.443156076777862e-1 / 2.0, w1 = 2.852749028018549e-1 / 6.0;
+  const double w2 = 9.737549286959440e-2 / 6.0, w3 = 3.096521116041552e-1 / 6.0;
+  const double w4 = 1.633818850466092e-1 / 12.0;
+  const double cb = 1.0 / 3.0, a1 = 4.592925882927229e-1, b1 = 8.141482341455413e-2;
+  const double a2 = 5.054722831703103e-2, b2 = 8.989055433659379e-1;
+  const double a3 = 1.705693077517601e-1, b3 = 6.588613844964797e-1;
+  const double a4 = 7.284923929554041e-1, b4 = 2.63112829634638689e-1, c4 = 8.394777409957211e-3;
+  const double X[16] = {cb, a1, a1, b1, a2, a2, b2, a3, a3, b3, a4, b4, b4, c4, c4, a4};
+  const double Y[16] = {cb, a1, b1, a1, a2, b2, a2, a3, b3, a3, b4, a4, c4, b4, a4, c4};
+  const double W[16] = {wbar, w1, w1, w1, w2, w2, w2, w3, w3, w3, w4, w4, w4, w4, w4, w4};
+  for (int i = 0; i < 16; ++i) {
+    w[i] = W[i];
+    x[i] = X[i];
+    y[i] = Y[i];
+  }
+}
+
+int upload_tables() {
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && done[dev]) return EMU_OK;
+  double w[16], x[16], y[16], phi[16][6], g[16][2][10];
+  quad_table(w, x, y);
+  for (int q = 0; q < 16; ++q) {
+    const double x0 = x[q], y0 = y[q];
+    // P2 basis (backend/fortran/phi2_2d_mat_J.f:17-30)
+    phi[q][0] = (-1 + x0 + y0) * (-1 + 2 * x0 + 2 * y0);
+    phi[q][1] = x0 * (-1 + 2 * x0);
+    phi[q][2] = y0 * (-1 + 2 * y0);
+    phi[q][3] = -4 * x0 * (-1 + x0 + y0);
+    phi[q][4] = 4 * x0 * y0;
+    phi[q][5] = -4 * y0 * (-1 + x0 + y0);
+    // P3 gradients (backend/fortran/phi3_2d_mat.f:17-64)
+    const double t = (-11 - 27 * x0 * x0 + x0 * (36 - 54 * y0) + 36 * y0 - 27 * y0 * y0) / 2.;
+    g[q][0][0] = t; g[q][1][0] = t;
+    g[q][0][1] = 1 - 9 * x0 + (27 * x0 * x0) / 2.; g[q][1][1] = 0;
+    g[q][0][2] = 0; g[q][1][2] = 1 - 9 * y0 + (27 * y0 * y0) / 2.;
+    g[q][0][3] = (9 * (2 + 9 * x0 * x0 - 5 * y0 + 3 * y0 * y0 + 2 * x0 * (-5 + 6 * y0))) / 2.;
+    g[q][1][3] = (9 * x0 * (-5 + 6 * x0 + 6 * y0)) / 2.;
+    g[q][0][4] = (-9 * (1 + 9 * x0 * x0 - y0 + x0 * (-8 + 6 * y0))) / 2.;
+    g[q][1][4] = (-9 * x0 * (-1 + 3 * x0)) / 2.;
+    g[q][0][5] = (9 * (-1 + 6 * x0) * y0) / 2.;
+    g[q][1][5] = (9 * x0 * (-1 + 3 * x0)) / 2.;
+    g[q][0][6] = (9 * y0 * (-1 + 3 * y0)) / 2.;
+    g[q][1][6] = (9 * x0 * (-1 + 6 * y0)) / 2.;
+    g[q][0][7] = (-9 * y0 * (-1 + 3 * y0)) / 2.;
+    g[q][1][7] = (-9 * (1 - 8 * y0 + 9 * y0 * y0 + x0 * (-1 + 6 * y0))) / 2.;
+    g[q][0][8] = (9 * y0 * (-5 + 6 * x0 + 6 * y0)) / 2.;
+    g[q][1][8] = (9 * (2 + 3 * x0 * x0 - 10 * y0 + 9 * y0 * y0 + x0 * (-5 + 12 * y0))) / 2.;
+    g[q][0][9] = -27 * y0 * (-1 + 2 * x0 + y0);
+    g[q][1][9] = -27 * x0 * (-1 + x0 + 2 * y0);
+  }
+  if (cudaMemcpyToSymbol(c_wq, w, sizeof(w)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_xq, x, sizeof(x)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_yq, y, sizeof(y)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_phi2, phi, sizeof(phi)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_g3, g, sizeof(g)) != cudaSuccess)
+    return EMU_E_CUDA;
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return EMU_OK;
+}
+
+// Element geometry: vertices, affine map x = B xi + x1, |det B| and T = B^-1
+// (backend/fortran/jacobian_p1_2d.f:68-133).
+struct Geo {
+  double x1, y1, B00, B01, B10, B11, adet, T00, T01, T10, T11;
+};
+
+__device__ __forceinline__ Geo element_geo(const double *x, const int64_t *tn, long el) {
+  const int64_t n1 = tn[el * 6 + 0] - 1, n2 = tn[el * 6 + 1] - 1, n3 = tn[el * 6 + 2] - 1;
+  Geo g;
+  g.x1 = x[2 * n1];
+  g.y1 = x[2 * n1 + 1];
+  g.B00 = x[2 * n2] - g.x1;
+  g.B01 = x[2 * n3] - g.x1;
+  g.B10 = x[2 * n2 + 1] - g.y1;
+  g.B11 = x[2 * n3 + 1] - g.y1;
+  const double det = g.B00 * g.B11 - g.B01 * g.B10;
+  g.adet = fabs(det);
+  g.T00 = g.B11 / det;
+  g.T01 = -g.B01 / det;
+  g.T10 = -g.B10 / det;
+  g.T11 = g.B00 / det;
+  return g;
+}
+
+// ---------------------------------------------------------------- setup
+// Plane-wave data per problem: sorted position (pw_ordering.f:54-78 with the
+// z_indexx.f key -Re(kz^2)), alpha, beta and 1/|k| by sorted row.
+struct PwArgs {
+  int batch, npw;
+  const int32_t *px, *py;
+  double d, dy;
+  const double *bloch, *k0;
+  int32_t *pos;       // [batch][npw] sorted position of generation-order s
+  double *tab;        // [batch][npw][3]: alpha, beta, 1/|k| by sorted row
+  int32_t *out_inv;   // optional copy of pos
+};
+
+__global__ void pw_setup_kernel(PwArgs a) {
+  extern __shared__ double keys[];
+  const int b = blockIdx.x;
+  const double bx = a.bloch[2 * b], by = a.bloch[2 * b + 1], k0 = a.k0[b];
+  const double vkx = 2.0 * 3.141592653589793 / a.d, vky = 2.0 * 3.141592653589793 / a.dy;
+  for (int s = threadIdx.x; s < a.npw; s += blockDim.x) {
+    const double al = bx + vkx * a.px[s], be = by + vky * a.py[s];
+    const cd bz = csqrt_p(cd{k0 * k0 - al * al - be * be, 0.0});
+    keys[s] = -(bz.x * bz.x - bz.y * bz.y);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < a.npw; s += blockDim.x) {
+    const double ks = keys[s];
+    int r = 0;
+    for (int v = 0; v < a.npw; ++v) r += (keys[v] < ks) || (keys[v] == ks && v < s);
+    a.pos[(size_t)b * a.npw + s] = r;
+    if (a.out_inv) a.out_inv[(size_t)b * a.npw + s] = r;
+    const double al = bx + vkx * a.px[s], be = by + vky * a.py[s];
+    double *t = a.tab + ((size_t)b * a.npw + r) * 3;
+    t[0] = al;
+    t[1] = be;
+    t[2] = 1.0 / sqrt(al * al + be * be);
+  }
+}
+
+// ---------------------------------------------------------------- E~ table
+// One warp per element: lanes build the per-quadrature-point phase tables in
+// shared memory, then each lane owns plane waves s and accumulates the six
+// node sums E~_s(el, node).  Output row = sorted position of s, column
+// (el - e0) * 6 + node; rows padded to ldE.
+struct EtArgs {
+  int npw, mo, e0, ne;
+  const int32_t *px, *py, *pos;
+  const double *x;
+  const int64_t *tn;
+  double d, dy;
+  const double *bloch;  // this problem's k_parallel * period (2 values)
+  cd *E;
+  long long ldE;
+};
+
+constexpr int kEtWarps = 4;
+constexpr int kMaxOrd = 24;  // |px|, |py| <= kMaxOrd
+
+// dynamic shared memory per warp: base[16], tx[16][no], ty[16][no] (cd), cq[16]
+__host__ __device__ inline size_t et_warp_bytes(int mo) {
+  return sizeof(cd) * (16 + 2 * 16 * (size_t)(2 * mo + 1)) + sizeof(double) * 16;
+}
+
+__global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
+  extern __shared__ __align__(16) unsigned char et_smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int no = 2 * a.mo + 1;
+  cd *wb = (cd *)(et_smem + (size_t)w * et_warp_bytes(a.mo));
+  cd *base = wb;                 // [16]
+  cd *tx = base + 16;            // [16][no]
+  cd *ty = tx + 16 * no;         // [16][no]
+  double *cq = (double *)(ty + 16 * no);
+  const double bx = a.bloch[0], by = a.bloch[1];
+  for (long el0 = (long)blockIdx.x * kEtWarps; el0 < a.ne; el0 += (long)gridDim.x * kEtWarps) {
+    const long el = el0 + w;
+    const bool ok = el < a.ne;
+    if (ok && lane < 16) {
+      const Geo g = element_geo(a.x, a.tn, a.e0 + el);
+      const int q = lane;
+      const double xg = g.x1 + g.B00 * c_xq[q] + g.B01 * c_yq[q];
+      const double yg = g.y1 + g.B10 * c_xq[q] + g.B11 * c_yq[q];
+      cq[q] = c_wq[q] * g.adet;
+      double s, c;
+      sincos(-(bx * xg + by * yg), &s, &c);
+      base[q] = cd{c, s};
+      // powers of exp(-i 2 pi x / d) and exp(-i 2 pi y / dy), exponents -mo..mo
+      double sx, cx, sy, cy;
+      sincos(-2.0 * 3.141592653589793 / a.d * xg, &sx, &cx);
+      sincos(-2.0 * 3.141592653589793 / a.dy * yg, &sy, &cy);
+      const cd ux = cd{cx, sx}, uy = cd{cy, sy};
+      cd px = cd{1.0, 0.0}, py = cd{1.0, 0.0};
+      tx[q * no + a.mo] = px;
+      ty[q * no + a.mo] = py;
+      for (int p = 1; p <= a.mo; ++p) {
+        px = cmul(px, ux);
+        py = cmul(py, uy);
+        tx[q * no + a.mo + p] = px;
+        tx[q * no + a.mo - p] = cconj(px);
+        ty[q * no + a.mo + p] = py;
+        ty[q * no + a.mo - p] = cconj(py);
+      }
+    }
+    __syncwarp();
+    if (ok) {
+      for (int s = lane; s < a.npw; s += 32) {
+        const int ix = a.px[s] + a.mo, iy = a.py[s] + a.mo;
+        cd acc[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] = cd{0.0, 0.0};
+#pragma unroll 4
+        for (int q = 0; q < 16; ++q) {
+          const cd e = cscale(cmul(cmul(base[q], tx[q * no + ix]), ty[q * no + iy]), cq[q]);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            acc[k].x = fma(e.x, c_phi2[q][k], acc[k].x);
+            acc[k].y = fma(e.y, c_phi2[q][k], acc[k].y);
+          }
+        }
+        cd *row = a.E + (size_t)a.pos[s] * a.ldE + (size_t)el * 6;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) row[k] = acc[k];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- repack
+// S[(el - e0) * 6 + node][c * nval + n] = sol[el][n][node][c], c = 0, 1
+// (the transverse field of the reference layout sol(3, 13, nval, nel)).
+__global__ void repack_kernel(const cd *sol, int nval, long e0, long ne, cd *S) {
+  const long total = ne * 6 * 2 * (long)nval;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int n = (int)(i % nval);
+    long r = i / nval;
+    const int c = (int)(r % 2);
+    r /= 2;
+    const int node = (int)(r % 6);
+    const long el = r / 6;
+    S[(size_t)(el * 6 + node) * 2 * nval + (size_t)c * nval + n] =
+        sol[((size_t)(e0 + el) * nval + n) * 39 + node * 3 + c];
+  }
+}
+
+// ---------------------------------------------------------------- GEMM
+// G[b] (+)= op(E) S with op = identity or conjugation, row-major; grid
+// (n-tiles, m-tiles, chunks), chunk c writes G_part[c].
+struct OvGemm {
+  int m, n, k;
+  const cd *E;
+  long long ldE;
+  const cd *S;
+  cd *G;
+  long long sG;
+  int conjA;
+  int kchunk;
+};
+
+__global__ void __launch_bounds__(kDLThreads) ov_gemm_kernel(OvGemm g) {
+  __shared__ GemmSmem sm;
+  const int c = blockIdx.z;
+  const int k0 = c * g.kchunk;
+  const int kk = min(g.kchunk, g.k - k0);
+  if (kk <= 0) return;
+  const int r0 = blockIdx.y * kTM, c0 = blockIdx.x * kTN;
+  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+  cd acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = cd{0.0, 0.0};
+  const cd *A = g.E + k0;
+  const cd *B = g.S + (size_t)k0 * g.n;
+  for (int kb = 0; kb < kk; kb += kTK) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = tid / 8 + 32 * h, cc = tid % 8;
+      const int gr = r0 + r, gc = kb + cc;
+      cd v = cd{0.0, 0.0};
+      if (gr < g.m && gc < kk) {
+        v = A[(size_t)gr * g.ldE + gc];
+        if (g.conjA) v.y = -v.y;
+      }
+      sm.As[cc][r] = v;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = tid / 64 + 4 * h, cc = tid % 64;
+      const int gr = kb + r, gc = c0 + cc;
+      sm.Bs[r][cc] = (gr < kk && gc < g.n) ? B[(size_t)gr * g.n + gc] : cd{0.0, 0.0};
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kTK; ++q) {
+      cd a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sm.As[q][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = sm.Bs[q][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+        }
+    }
+    __syncthreads();
+  }
+  cd *G = g.G + (size_t)c * g.sG;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gr = r0 + ty + 16 * i;
+    if (gr >= g.m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gc = c0 + tx + 16 * j;
+      if (gc < g.n) G[(size_t)gr * g.n + gc] = acc[i][j];
+    }
+  }
+}
+
+// Sum the chunk partials into the accumulator (fixed order: deterministic).
+__global__ void reduce_parts_kernel(const cd *parts, int nparts, long long stride, cd *acc, long long n,
+                                    int first) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    cd s = first ? cd{0.0, 0.0} : acc[i];
+    for (int p = 0; p < nparts; ++p) s = cadd(s, parts[(size_t)p * stride + i]);
+    acc[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------- epilogue
+// J[row][n]: rows 0..npw-1 = J_E, npw..2npw-1 = J_K (sorted order), divided
+// by area_norm; J_dag[i][row] uses adjoint column perm[i] scaled by scale[i].
+__global__ void epilogue_kernel(const cd *G, const double *tab, int npw, int nval, double inv_area,
+                                int dagger, const cd *scale, const int32_t *perm, cd *out) {
+  const long total = (long)npw * nval;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nval), n = (int)(i % nval);
+    const double al = tab[3 * r], be = tab[3 * r + 1], nm = tab[3 * r + 2];
+    const int src = (dagger && perm) ? perm[n] : n;
+    const cd gx = G[(size_t)r * 2 * nval + src], gy = G[(size_t)r * 2 * nval + nval + src];
+    cd je = cscale(cd{be * gx.x - al * gy.x, be * gx.y - al * gy.y}, nm);
+    cd jk = cscale(cd{al * gx.x + be * gy.x, al * gx.y + be * gy.y}, nm);
+    if (!dagger) {
+      out[(size_t)r * nval + n] = cscale(je, inv_area);
+      out[(size_t)(npw + r) * nval + n] = cscale(jk, inv_area);
+    } else {
+      if (scale) {
+        je = cmul(je, scale[n]);
+        jk = cmul(jk, scale[n]);
+      }
+      out[(size_t)n * 2 * npw + r] = je;
+      out[(size_t)n * 2 * npw + npw + r] = jk;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- orthogonality
+// Per element, the 12 x 22 real matrix of orthogonal.f:110-193 without the
+// pp(type_el) / k0 factor: rows (component, P2 node), columns P2 mass part
+// (12) then -grad P3 part (10).
+__device__ void element_scal(const Geo &g, double ms[12][22]) {
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 22; ++j) ms[i][j] = 0.0;
+  for (int q = 0; q < 16; ++q) {
+    const double c = c_wq[q] * g.adet;
+    double g3[2][10];
+    for (int j = 0; j < 10; ++j) {
+      g3[0][j] = g.T00 * c_g3[q][0][j] + g.T10 * c_g3[q][1][j];
+      g3[1][j] = g.T01 * c_g3[q][0][j] + g.T11 * c_g3[q][1][j];
+    }
+    for (int it = 0; it < 6; ++it) {
+      const double pi = c_phi2[q][it] * c;
+      for (int jt = 0; jt < 6; ++jt) {
+        const double v = pi * c_phi2[q][jt];
+        ms[2 * it][2 * jt] += v;
+        ms[2 * it + 1][2 * jt + 1] += v;
+      }
+      for (int jt = 0; jt < 10; ++jt) {
+        ms[2 * it][12 + jt] -= pi * g3[0][jt];
+        ms[2 * it + 1][12 + jt] -= pi * g3[1][jt];
+      }
+    }
+  }
+}
+
+// sol_el_1 entry j of mode n (orthogonal.f:205-227), without the beta factor
+__device__ __forceinline__ cd sol1_entry(const cd *s1, int j) {
+  if (j < 12) return s1[(j >> 1) * 3 + (j & 1)];
+  const int t = j - 12;  // P3 nodes: vertices 0..2, then nodes 6..12
+  return s1[(t < 3 ? t : t + 3) * 3 + 2];
+}
+
+struct DiagArgs {
+  int nval;
+  long nel, chunk;
+  const double *x;
+  const int64_t *tn, *type_el;
+  const cd *pp, *beta1, *sol1, *sol2;
+  const double *k0;
+  cd *part;  // [nchunks][nval]
+};
+
+__global__ void __launch_bounds__(128) diag_kernel(DiagArgs a) {
+  __shared__ double ms[12][22];
+  __shared__ cd ppk;
+  const long c = blockIdx.x;
+  const long e0 = c * a.chunk, e1 = min(a.nel, e0 + a.chunk);
+  for (int n0 = 0; n0 < a.nval; n0 += blockDim.x) {
+    const int n = n0 + threadIdx.x;
+    cd acc = cd{0.0, 0.0};
+    for (long el = e0; el < e1; ++el) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const Geo g = element_geo(a.x, a.tn, el);
+        element_scal(g, ms);
+        const cd p = a.pp[a.type_el[el] - 1];
+        ppk = cd{p.x / a.k0[0], p.y / a.k0[0]};
+      }
+      __syncthreads();
+      if (n < a.nval) {
+        const cd *s1 = a.sol1 + ((size_t)el * a.nval + n) * 39;
+        const cd *s2 = a.sol2 + ((size_t)el * a.nval + n) * 39;
+        cd s1v[22];
+#pragma unroll
+        for (int j = 0; j < 22; ++j) s1v[j] = sol1_entry(s1, j);
+        cd e = cd{0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          cd v = cd{0.0, 0.0};
+#pragma unroll
+          for (int j = 0; j < 22; ++j) {
+            v.x = fma(ms[i][j], s1v[j].x, v.x);
+            v.y = fma(ms[i][j], s1v[j].y, v.y);
+          }
+          e = cadd(e, cmul(v, s2[(i >> 1) * 3 + (i & 1)]));
+        }
+        acc = cadd(acc, cmul(e, ppk));
+      }
+    }
+    if (n < a.nval) a.part[(size_t)c * a.nval + n] = acc;
+  }
+}
+
+// diag(n) = beta1(n) sum_chunks part ; scale = 1/sqrt(diag)^2 (or 1)
+__global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, const cd *beta1, cd *diag,
+                                   cd *scale, int *n_small) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nval; n += gridDim.x * blockDim.x) {
+    cd s = cd{0.0, 0.0};
+    for (int c = 0; c < nchunks; ++c) s = cadd(s, part[(size_t)c * nval + n]);
+    s = cmul(s, beta1[n]);
+    diag[n] = s;
+    if (hypot(s.x, s.y) <= 1e-7) atomicAdd(n_small, 1);
+    const cd z = csqrt_p(s);
+    scale[n] = (hypot(z.x, z.y) > 1e-8) ? crecip(cmul(z, z)) : cd{1.0, 0.0};
+  }
+}
+
+}  // namespace
+
+// =============================================================== C ABI
+extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
+  if (!p || p->n_pw < 1 || p->nval < 1 || p->nel < 1) return 0;
+  const long long npw = p->n_pw, M = p->nval;
+  const long long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
+  const long long ne = chunk < p->nel ? chunk : p->nel;
+  const long long nparts = 4;
+  size_t b = 0;
+  b += align_up(sizeof(int32_t) * npw, 256);                 // pos
+  b += align_up(sizeof(double) * 3 * npw, 256);              // tab
+  b += align_up(sizeof(cd) * npw * 6 * ne, 256);             // E~ chunk
+  b += align_up(sizeof(cd) * 6 * ne * 2 * M, 256);           // S chunk
+  b += 2 * align_up(sizeof(cd) * npw * 2 * M, 256);          // G, Gd
+  b += align_up(sizeof(cd) * nparts * npw * 2 * M, 256);     // partials
+  return b + 256;
+}
+
+extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t workspace_bytes,
+                                 void *stream) {
+  if (!p) return EMU_E_ARG;
+  if (p->batch < 0 || p->nval < 1 || p->nel < 1 || p->npt < 3 || p->n_pw < 1) return EMU_E_SHAPE;
+  if (!p->d_px || !p->d_py || !p->d_x || !p->d_table_nod || !p->d_bloch || !p->d_k0) return EMU_E_ARG;
+  if (!(p->d > 0) || !(p->dy > 0) || !(p->area_norm > 0)) return EMU_E_ARG;
+  if ((p->d_sol1 == nullptr) != (p->d_J == nullptr) || (p->d_sol2 == nullptr) != (p->d_J_dag == nullptr))
+    return EMU_E_ARG;
+  if (p->max_order < 0 || p->max_order > kMaxOrd) return EMU_E_UNSUPPORTED;
+  if (p->batch == 0) return EMU_OK;
+  if (!d_workspace || workspace_bytes < emu_overlap_workspace_size(p)) return EMU_E_WORKSPACE;
+  int st = upload_tables();
+  if (st != EMU_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int npw = p->n_pw, M = p->nval;
+  const long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
+  const long nec = chunk < p->nel ? chunk : p->nel;
+  const int nparts = 4;
+  char *w = (char *)d_workspace;
+  auto take = [&](size_t bytes) {
+    char *r = w;
+    w += align_up(bytes, 256);
+    return (void *)r;
+  };
+  int32_t *pos = (int32_t *)take(sizeof(int32_t) * npw);
+  double *tab = (double *)take(sizeof(double) * 3 * npw);
+  cd *E = (cd *)take(sizeof(cd) * (size_t)npw * 6 * nec);
+  cd *S = (cd *)take(sizeof(cd) * 6 * (size_t)nec * 2 * M);
+  cd *G = (cd *)take(sizeof(cd) * (size_t)npw * 2 * M);
+  cd *Gd = (cd *)take(sizeof(cd) * (size_t)npw * 2 * M);
+  cd *parts = (cd *)take(sizeof(cd) * (size_t)nparts * npw * 2 * M);
+  const long long gsz = (long long)npw * 2 * M;
+  const int sms = emu::sm_count();
+  const size_t et_smem = kEtWarps * et_warp_bytes(p->max_order);
+  if (et_smem > 48 * 1024 &&
+      cudaFuncSetAttribute(etable_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)et_smem) !=
+          cudaSuccess)
+    return EMU_E_CUDA;
+  for (int b = 0; b < p->batch; ++b) {
+    PwArgs pa;
+    pa.batch = 1;
+    pa.npw = npw;
+    pa.px = p->d_px;
+    pa.py = p->d_py;
+    pa.d = p->d;
+    pa.dy = p->dy;
+    pa.bloch = p->d_bloch + 2 * b;
+    pa.k0 = p->d_k0 + b;
+    pa.pos = pos;
+    pa.tab = tab;
+    pa.out_inv = p->d_index_pw_inv ? p->d_index_pw_inv + (size_t)b * npw : nullptr;
+    pw_setup_kernel<<<1, 256, sizeof(double) * npw, s>>>(pa);
+    emu::note_launch();
+    for (int pass = 0; pass < 2; ++pass) {
+      const cd *sol = (const cd *)(pass == 0 ? p->d_sol1 : p->d_sol2);
+      if (!sol) continue;
+      sol += (size_t)b * p->nel * M * 39;
+      cd *acc = pass == 0 ? G : Gd;
+      int first = 1;
+      for (long e0 = 0; e0 < p->nel; e0 += nec) {
+        const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
+        EtArgs ea;
+        ea.npw = npw;
+        ea.mo = p->max_order;
+        ea.e0 = (int)e0;
+        ea.ne = (int)ne;
+        ea.px = p->d_px;
+        ea.py = p->d_py;
+        ea.pos = pos;
+        ea.x = p->d_x;
+        ea.tn = p->d_table_nod;
+        ea.d = p->d;
+        ea.dy = p->dy;
+        ea.bloch = p->d_bloch + 2 * b;
+        ea.E = E;
+        ea.ldE = 6 * ne;
+        const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
+        etable_kernel<<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
+        const long long rn = ne * 6 * 2 * (long long)M;
+        const long long rg = (rn + 255) / 256;
+        repack_kernel<<<(int)(rg < 16 * sms ? rg : 16 * sms), 256, 0, s>>>(sol, M, e0, ne, S);
+        OvGemm g;
+        g.m = npw;
+        g.n = 2 * M;
+        g.k = (int)(6 * ne);
+        g.E = E;
+        g.ldE = 6 * ne;
+        g.S = S;
+        g.G = parts;
+        g.sG = gsz;
+        g.conjA = pass;
+        g.kchunk = (int)(((6 * ne + nparts - 1) / nparts + kTK - 1) / kTK * kTK);
+        const int used = (g.k + g.kchunk - 1) / g.kchunk;
+        dim3 grid((2 * M + kTN - 1) / kTN, (npw + kTM - 1) / kTM, used);
+        ov_gemm_kernel<<<grid, kDLThreads, 0, s>>>(g);
+        const long long rgs = (gsz + 255) / 256;
+        reduce_parts_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(parts, used, gsz, acc, gsz,
+                                                                                  first);
+        emu::note_launch(4);
+        first = 0;
+      }
+      const long long et = (long long)npw * M;
+      const int eb = (int)((et + 255) / 256 < 8 * sms ? (et + 255) / 256 : 8 * sms);
+      if (pass == 0) {
+        epilogue_kernel<<<eb, 256, 0, s>>>(G, tab, npw, M, 1.0 / p->area_norm, 0, nullptr, nullptr,
+                                           (cd *)p->d_J + (size_t)b * 2 * npw * M);
+      } else {
+        epilogue_kernel<<<eb, 256, 0, s>>>(
+            Gd, tab, npw, M, 1.0, 1, p->d_scale2 ? (const cd *)p->d_scale2 + (size_t)b * M : nullptr,
+            p->d_perm2 ? p->d_perm2 + (size_t)b * M : nullptr, (cd *)p->d_J_dag + (size_t)b * 2 * npw * M);
+      }
+      emu::note_launch();
+    }
+  }
+  return emu::check_launch();
+}
+
+// ---------------------------------------------------------------- normalisation
+extern "C" size_t emu_mode_overlap_workspace_size(const EmuNormalise *p) {
+  if (!p || p->nval < 1 || p->nel < 1) return 0;
+  const long long chunk = 64;
+  const long long nch = (p->nel + chunk - 1) / chunk;
+  return align_up(sizeof(cd) * nch * p->nval, 256) + 256;
+}
+
+extern "C" int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t workspace_bytes,
+                                     void *stream) {
+  if (!p) return EMU_E_ARG;
+  if (p->batch < 0 || p->nval < 1 || p->nel < 1) return EMU_E_SHAPE;
+  if (!p->d_x || !p->d_table_nod || !p->d_type_el || !p->d_pp || !p->d_k0 || !p->d_beta1 ||
+      !p->d_sol1 || !p->d_sol2 || !p->d_diag || !p->d_scale || !p->d_n_small)
+    return EMU_E_ARG;
+  if (p->batch == 0) return EMU_OK;
+  if (!d_workspace || workspace_bytes < emu_mode_overlap_workspace_size(p)) return EMU_E_WORKSPACE;
+  int st = upload_tables();
+  if (st != EMU_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long chunk = 64;
+  const long nch = (p->nel + chunk - 1) / chunk;
+  cd *part = (cd *)d_workspace;
+  if (cudaMemsetAsync(p->d_n_small, 0, sizeof(int32_t) * p->batch, s) != cudaSuccess) return EMU_E_CUDA;
+  for (int b = 0; b < p->batch; ++b) {
+    DiagArgs a;
+    a.nval = p->nval;
+    a.nel = p->nel;
+    a.chunk = chunk;
+    a.x = p->d_x;
+    a.tn = p->d_table_nod;
+    a.type_el = p->d_type_el;
+    a.pp = (const cd *)p->d_pp;
+    a.beta1 = (const cd *)p->d_beta1 + (size_t)b * p->nval;
+    a.sol1 = (const cd *)p->d_sol1 + (size_t)b * p->nel * p->nval * 39;
+    a.sol2 = (const cd *)p->d_sol2 + (size_t)b * p->nel * p->nval * 39;
+    a.k0 = p->d_k0 + b;
+    a.part = part;
+    diag_kernel<<<(int)nch, 128, 0, s>>>(a);
+    diag_finish_kernel<<<(p->nval + 127) / 128, 128, 0, s>>>(
+        part, (int)nch, p->nval, a.beta1, (cd *)p->d_diag + (size_t)b * p->nval,
+        (cd *)p->d_scale + (size_t)b * p->nval, p->d_n_small + b);
+    emu::note_launch(2);
+  }
+  return emu::check_launch();
+}

@@ -28,10 +28,22 @@ def _c(x):
     return EmuC128(float(np.real(x)), float(np.imag(x)))
 
 
+def _need(t, dtype, name, ndim=None):
+    """Fail loudly on tensors the C ABI would misread."""
+    if t is None or not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
+        raise TypeError('%s must be a contiguous CUDA %s tensor' % (name, dtype))
+    if ndim is not None and t.dim() != ndim:
+        raise ValueError('%s must have %d dimensions' % (name, ndim))
+
+
 def zgemm_batched(A, B, C_=None, alpha=1.0, beta=0.0):
     """C = alpha A B + beta C for batched row-major complex128 tensors [b, m, k] x [b, k, n]."""
+    _need(A, c128, 'A', 3)
+    _need(B, c128, 'B', 3)
     bsz, m, k = A.shape
     n = B.shape[2]
+    if B.shape[:2] != (bsz, k):
+        raise ValueError('inner dimensions differ')
     if C_ is None:
         C_ = torch.zeros((bsz, m, n), dtype=c128, device=A.device)
     check(lib().emu_zgemm_batched(m, n, k, _c(alpha), ptr(A), k, m * k, ptr(B), n, k * n, _c(beta),
@@ -41,6 +53,8 @@ def zgemm_batched(A, B, C_=None, alpha=1.0, beta=0.0):
 
 def zgesv_batched(A, B):
     """Solve A X = B in place (A overwritten with its LU); returns (X, ipiv, info)."""
+    _need(A, c128, 'A', 3)
+    _need(B, c128, 'B', 3)
     bsz, n, _ = A.shape
     nrhs = B.shape[2]
     ipiv = torch.empty((bsz, n), dtype=torch.int32, device=A.device)
@@ -57,6 +71,9 @@ def film_interface(kz1, n1, kz2, n2, wl_norm):
     side, the air reference in a Stack); n1, n2: complex128 [B]; wl_norm
     float64 [B].  Returns R12, T12 diagonals [B, 2 Npw] (R21 = -R12, T21 = T12).
     """
+    for t, nm in ((kz1, 'kz1'), (n1, 'n1'), (kz2, 'kz2'), (n2, 'n2')):
+        _need(t, c128, nm)
+    _need(wl_norm, torch.float64, 'wl_norm')
     B, npw = kz1.shape
     R12 = torch.empty((B, 2 * npw), dtype=c128, device=kz1.device)
     T12 = torch.empty_like(R12)
@@ -72,7 +89,12 @@ def interface_dense(film_kz, film_n, wl_norm, J, J_dag):
     J complex128 [B, P, M] (divided by the area ratio); J_dag [B, M, P].
     Returns R12 [B,P,P], T12 [B,M,P], R21 [B,M,M], T21 [B,P,M] and info [B].
     """
+    for t, nm in ((film_kz, 'film_kz'), (film_n, 'film_n'), (J, 'J'), (J_dag, 'J_dag')):
+        _need(t, c128, nm)
+    _need(wl_norm, torch.float64, 'wl_norm')
     B, P, M = J.shape
+    if tuple(J_dag.shape) != (B, M, P) or tuple(film_kz.shape) != (B, P // 2):
+        raise ValueError('inconsistent interface shapes')
     dev = J.device
     R12 = torch.empty((B, P, P), dtype=c128, device=dev)
     T12 = torch.empty((B, M, P), dtype=c128, device=dev)
@@ -120,6 +142,10 @@ class DenseStackSolver(object):
         dev = self.device
         arr = (EmuLayer * L)()
         for i, ly in enumerate(layers):
+            for nm in ('R12', 'T12', 'R21', 'T21'):
+                _need(getattr(ly, nm), c128, 'layer %d %s' % (i, nm))
+            if ly.kz is not None:
+                _need(ly.kz, c128, 'layer %d kz' % i)
             e = arr[i]
             e.M = ly.M
             e.dense = int(ly.dense)

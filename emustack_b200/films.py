@@ -158,9 +158,17 @@ class FilmStackSolver(object):
         shears  float64 [L, ncoord] or None
         Returns a dict of device tensors (reused across calls).
         """
-        for t, nm in ((wl_nm, 'wl_nm'), (k_pll, 'k_pll'), (n, 'n')):
-            if not t.is_cuda or not t.is_contiguous():
-                raise ValueError('%s must be a contiguous CUDA tensor' % nm)
+        for t, nm, dt in ((wl_nm, 'wl_nm', torch.float64), (k_pll, 'k_pll', torch.float64),
+                          (n, 'n', torch.complex128)):
+            if not t.is_cuda or not t.is_contiguous() or t.dtype != dt:
+                raise TypeError('%s must be a contiguous CUDA %s tensor' % (nm, dt))
+        if heights_nm is not None and (heights_nm.dtype != torch.float64 or not heights_nm.is_cuda
+                                       or not heights_nm.is_contiguous()):
+            raise TypeError('heights_nm must be a contiguous CUDA float64 tensor')
+        if incoming is not None and (incoming.dtype != torch.complex128 or not incoming.is_cuda):
+            raise TypeError('incoming must be a CUDA complex128 tensor')
+        if shears is not None and (shears.dtype != torch.float64 or not shears.is_cuda):
+            raise TypeError('shears must be a CUDA float64 tensor')
         B = int(wl_nm.shape[0])
         if tuple(n.shape) != (B, self.L) or n.dtype != torch.complex128:
             raise ValueError('n must be complex128 [B, L]')

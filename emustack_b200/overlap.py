@@ -1,0 +1,147 @@
+"""Bloch-mode / plane-wave overlap integrals and Bloch-mode normalisation on
+the GPU (rows a11-a13 of the GSM stage).
+
+``overlap_batch`` computes J (2 Npw x M) and J_dag (M x 2 Npw) for a batch of
+wavelengths on one mesh (backend/fortran/J_overlap.f, J_dagger_overlap.f,
+pw_ordering.f; J divided by the area ratio as backend/mode_calcs.py:384-386
+does).  ``mode_normalisation`` computes the diagonal of the adjoint x prime
+orthogonality matrix and the factors 1/sqrt(ovl)^2 that normalise the
+adjoint modes (backend/fortran/orthogonal.f, normalisation.f).
+``overlap_from_fields`` chains both for a drop-in ``Simmo``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import EmuNormalise, EmuOverlap, check, lib, ptr, stream_ptr
+
+c128 = torch.complex128
+
+
+class DeviceMesh(object):
+    """A Mesh (emustack_b200.mesh) resident on the GPU."""
+
+    def __init__(self, mesh, device='cuda'):
+        self.mesh = mesh
+        self.x, self.table_nod, self.type_el = mesh.to_device(device)
+        self.nel, self.npt = mesh.nel, mesh.npt
+
+
+def _check_sol(sol, nel, name):
+    if sol is None:
+        return
+    if sol.dtype != c128 or not sol.is_cuda or not sol.is_contiguous():
+        raise TypeError('%s must be a contiguous CUDA complex128 tensor' % name)
+    if sol.dim() != 5 or tuple(sol.shape[1:2]) != (nel,) or tuple(sol.shape[3:]) != (13, 3):
+        raise ValueError('%s must be [batch][nel][nval][13][3]' % name)
+
+
+def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, area_norm=1.0,
+                  dy=1.0, scale2=None, perm2=None, elements_per_chunk=0):
+    """J, J_dag (device tensors) and index_pw_inv for a batch of problems.
+
+    px, py     int32 [Npw] plane-wave orders (emustack_b200.films.grating_orders)
+    bloch      float64 [B, 2] k_parallel * period;  k0 float64 [B] = 2 pi / wl_norm
+    sol1/sol2  complex128 [B, nel, M, 13, 3] prime / adjoint fields
+    scale2     complex128 [B, M] adjoint normalisation factors (or None)
+    """
+    dev = dmesh.x.device
+    _check_sol(sol1, dmesh.nel, 'sol1')
+    _check_sol(sol2, dmesh.nel, 'sol2')
+    ref = sol1 if sol1 is not None else sol2
+    B, M = int(ref.shape[0]), int(ref.shape[2])
+    npw = len(px)
+    d_px = torch.as_tensor(np.asarray(px, np.int32), device=dev)
+    d_py = torch.as_tensor(np.asarray(py, np.int32), device=dev)
+    for t, nm, dt in ((bloch, 'bloch', torch.float64), (k0, 'k0', torch.float64)):
+        if t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+            raise TypeError('%s must be a contiguous CUDA %s tensor' % (nm, dt))
+    J = torch.empty((B, 2 * npw, M), dtype=c128, device=dev) if sol1 is not None else None
+    Jd = torch.empty((B, M, 2 * npw), dtype=c128, device=dev) if sol2 is not None else None
+    inv = torch.empty((B, npw), dtype=torch.int32, device=dev)
+    d = EmuOverlap()
+    d.batch, d.nval, d.nel, d.npt = B, M, dmesh.nel, dmesh.npt
+    d.n_pw, d.max_order = npw, int(max_order)
+    d.d_px, d.d_py = ptr(d_px), ptr(d_py)
+    d.d_x, d.d_table_nod = ptr(dmesh.x), ptr(dmesh.table_nod)
+    d.d, d.dy = 1.0, float(dy)
+    d.d_bloch, d.d_k0 = ptr(bloch), ptr(k0)
+    d.d_sol1, d.d_sol2 = ptr(sol1), ptr(sol2)
+    d.d_scale2, d.d_perm2 = ptr(scale2), ptr(perm2)
+    d.area_norm = float(area_norm)
+    d.d_J, d.d_J_dag, d.d_index_pw_inv = ptr(J), ptr(Jd), ptr(inv)
+    d.elements_per_chunk = int(elements_per_chunk)
+    L = lib()
+    nbytes = L.emu_overlap_workspace_size(C.byref(d))
+    ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+    check(L.emu_overlap_batch(C.byref(d), ptr(ws), C.c_size_t(nbytes), stream_ptr()), 'emu_overlap_batch')
+    return J, Jd, inv
+
+
+def mode_normalisation(dmesh, pp, k0, beta1, sol1, sol2):
+    """Diagonal of the orthogonality matrix, normalisation factors and the
+    count of |diag| <= 1e-7 per problem (device tensors)."""
+    dev = dmesh.x.device
+    _check_sol(sol1, dmesh.nel, 'sol1')
+    _check_sol(sol2, dmesh.nel, 'sol2')
+    B, M = int(sol1.shape[0]), int(sol1.shape[2])
+    pp = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
+    if beta1.dtype != c128 or not beta1.is_cuda:
+        raise TypeError('beta1 must be a CUDA complex128 tensor')
+    diag = torch.empty((B, M), dtype=c128, device=dev)
+    scale = torch.empty((B, M), dtype=c128, device=dev)
+    nsmall = torch.empty((B,), dtype=torch.int32, device=dev)
+    d = EmuNormalise()
+    d.batch, d.nval, d.nel, d.npt = B, M, dmesh.nel, dmesh.npt
+    d.d_x, d.d_table_nod, d.d_type_el = ptr(dmesh.x), ptr(dmesh.table_nod), ptr(dmesh.type_el)
+    d.d_pp, d.d_k0, d.d_beta1 = ptr(pp), ptr(k0), ptr(beta1.contiguous())
+    d.d_sol1, d.d_sol2 = ptr(sol1), ptr(sol2)
+    d.d_diag, d.d_scale, d.d_n_small = ptr(diag), ptr(scale), ptr(nsmall)
+    L = lib()
+    nbytes = L.emu_mode_overlap_workspace_size(C.byref(d))
+    ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+    check(L.emu_mode_overlap_diag(C.byref(d), ptr(ws), C.c_size_t(nbytes), stream_ptr()),
+          'emu_mode_overlap_diag')
+    return diag, scale, nsmall
+
+
+def overlap_from_fields(simmo, fields):
+    """J / area_norm and J_dag of a Simmo from its P2 mode fields.
+
+    fields: dict with 'sol1', 'sol2' ([nel][M][13][3], the reference layout
+    of sol(3, 13, M, nel)), 'beta1' (prime propagation constants; default
+    simmo.k_z), 'pp' (per material type; default 1, the E-field
+    formulation) and optionally 'mesh' (else simmo.structure.mesh).
+    The adjoint modes are normalised on the GPU first.
+    """
+    from .films import grating_orders
+    st = simmo.structure
+    mesh = fields.get('mesh', getattr(st, 'mesh', None))
+    if mesh is None:
+        raise ValueError('overlap integrals need the mesh of the mode fields')
+    dev = torch.device('cuda', torch.cuda.current_device())
+    dm = fields.get('_device_mesh') or DeviceMesh(mesh, dev)
+    sol1 = torch.as_tensor(np.ascontiguousarray(fields['sol1'], np.complex128), device=dev).unsqueeze(0)
+    sol2 = torch.as_tensor(np.ascontiguousarray(fields['sol2'], np.complex128), device=dev).unsqueeze(0)
+    M = sol1.shape[2]
+    beta1 = torch.as_tensor(np.asarray(fields.get('beta1', simmo.k_z), np.complex128).reshape(1, M), device=dev)
+    n_types = int(mesh.type_el.max())
+    pp = fields.get('pp', np.ones(n_types, np.complex128))
+    wl_norm = simmo.wl_norm()
+    k0 = torch.tensor([2 * np.pi / wl_norm], dtype=torch.float64, device=dev)
+    bloch = torch.tensor(np.asarray(simmo.k_pll_norm(), np.float64).reshape(1, 2), device=dev)
+    diag, scale, nsmall = mode_normalisation(dm, pp, k0, beta1, sol1, sol2)
+    if int(nsmall[0].item()) != 0:
+        raise NotImplementedError('adjoint modes with |<m|m>| <= 1e-7 need the conjugate-pair '
+                                  'reordering of orthogonal.f, which this path does not run')
+    mo = simmo.max_order_PWs
+    px, py = grating_orders(mo, st.period, st.period_y, False)
+    area_norm = st.period_y / st.period
+    J, Jd, inv = overlap_batch(dm, px, py, mo, bloch, k0, sol1, sol2, area_norm=area_norm,
+                               dy=st.period_y / st.period, scale2=scale)
+    simmo.overlap_diag = diag[0].cpu().numpy()
+    return np.asmatrix(J[0].cpu().numpy()), np.asmatrix(Jd[0].cpu().numpy())

@@ -269,6 +269,74 @@ long long emu_stack_dense_list_stride(const EmuStackDense *p);
 int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace, size_t workspace_bytes,
                           void *stream);
 
+/* ------------------------------------- a11, a12: overlap integrals
+ * J (2 Npw x nval) and J_dag (nval x 2 Npw) of P2 Bloch-mode fields with the
+ * TE ("E") and TM ("K") plane waves, by the 16-point triangle quadrature
+ * over every element with the affine element map, rows in the sorted
+ * plane-wave order (key -Re(kz^2), kz^2 = k0^2 - alpha^2 - beta^2).
+ * Replaces J_overlap (backend/fortran/J_overlap.f:3-246, called from
+ * backend/fortran/py_calc_modes.f:802-806), J_dagger_overlap
+ * (backend/fortran/J_dagger_overlap.f:3-246, py_calc_modes.f:818-822),
+ * pw_ordering (backend/fortran/pw_ordering.f:2-91) and the division
+ * J / area_norm of backend/mode_calcs.py:384-386.
+ * Fields use the reference layout sol(3, 13, nval, nel) (Fortran order),
+ * i.e. [nel][nval][13][3] complex; table_nod is [nel][6], 1-based.
+ * The plane-wave set is the caller's (emu_grating_orders), the set the
+ * films of the same stack use. */
+typedef struct {
+  int batch;               /* problems (wavelengths) on one mesh            */
+  int nval;                /* Bloch modes                                   */
+  int nel, npt;            /* triangles, nodes                              */
+  int n_pw;                /* plane waves per polarisation                  */
+  int max_order;           /* max |px|, |py| of the order set (<= 24)       */
+  const int32_t *d_px, *d_py; /* [Npw]                                      */
+  const double *d_x;       /* [npt][2] coordinates in units of the period   */
+  const int64_t *d_table_nod; /* [nel][6], 1-based                          */
+  double d, dy;            /* lattice vectors (1, period_y/period)          */
+  const double *d_bloch;   /* [batch][2] k_parallel * period                */
+  const double *d_k0;      /* [batch] 2 pi / (wl / period)                  */
+  const emu_c128 *d_sol1;  /* [batch][nel][nval][13][3] or NULL             */
+  const emu_c128 *d_sol2;  /* adjoint fields, same layout, or NULL          */
+  const emu_c128 *d_scale2;/* [batch][nval] normalisation of the adjoint modes or NULL */
+  const int32_t *d_perm2;  /* [batch][nval] adjoint order after pair swaps or NULL */
+  double area_norm;        /* period_y / period                             */
+  emu_c128 *d_J;           /* [batch][2 Npw][nval] (with d_sol1)            */
+  emu_c128 *d_J_dag;       /* [batch][nval][2 Npw] (with d_sol2)            */
+  int32_t *d_index_pw_inv; /* [batch][Npw] 0-based sorted positions or NULL */
+  int elements_per_chunk;  /* 0 = default (4096); bounds the workspace      */
+} EmuOverlap;
+
+size_t emu_overlap_workspace_size(const EmuOverlap *p);
+int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------- a13: Bloch-mode normalisation
+ * Diagonal of the adjoint x prime orthogonality matrix
+ *   ovl(n, n) = sum_el sol2_el(:, n)^T  M_el  (beta1(n) sol1_el(:, n)),
+ * M_el the 12 x 22 P2-mass / P3-gradient element matrix times
+ * pp(type_el) / k0 (backend/fortran/orthogonal.f:84-248), and the
+ * normalisation factors scale(n) = 1 / sqrt(ovl(n, n))^2, or 1 when
+ * |sqrt(ovl(n, n))| <= 1e-8 (backend/fortran/normalisation.f:15-31).
+ * n_small[b] counts |ovl(n, n)| <= 1e-7, the trigger of the reference's
+ * conjugate-pair reordering (orthogonal.f:252-301); the caller runs that
+ * reordering (emu_mode_overlap_matrix gives the full matrix it needs). */
+typedef struct {
+  int batch, nval, nel, npt;
+  const double *d_x;       /* [npt][2]                                      */
+  const int64_t *d_table_nod; /* [nel][6], 1-based                          */
+  const int64_t *d_type_el;/* [nel], 1-based                                */
+  const emu_c128 *d_pp;    /* [n_types] (1 for the E-field formulation)     */
+  const double *d_k0;      /* [batch]                                       */
+  const emu_c128 *d_beta1; /* [batch][nval] prime propagation constants     */
+  const emu_c128 *d_sol1, *d_sol2; /* [batch][nel][nval][13][3]             */
+  emu_c128 *d_diag;        /* [batch][nval]                                 */
+  emu_c128 *d_scale;       /* [batch][nval]                                 */
+  int32_t *d_n_small;      /* [batch]                                       */
+} EmuNormalise;
+
+size_t emu_mode_overlap_workspace_size(const EmuNormalise *p);
+int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t workspace_bytes,
+                          void *stream);
+
 /* ------------------------------------------------------- measurement
  * FP64 FMA throughput probe: blocks x threads threads each run 64 dependent
  * FMA chains of `iters` steps (2*64*iters*threads*blocks flops).  Used as the

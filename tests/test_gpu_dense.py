@@ -60,8 +60,9 @@ def test_interface_dense_matches_reference():
         npw = kz.shape[0]
         dev = 'cuda'
         R12, T12, R21, T21, info = interface_dense(
-            torch.tensor(kz.reshape(1, npw), device=dev), torch.tensor([1.0 + 0j], device=dev),
-            torch.tensor([float(raw['q%d_wl_norm' % q])], device=dev),
+            torch.tensor(kz.reshape(1, npw), device=dev),
+            torch.tensor([1.0 + 0j], dtype=torch.complex128, device=dev),
+            torch.tensor([float(raw['q%d_wl_norm' % q])], dtype=torch.float64, device=dev),
             torch.tensor(J[None], device=dev), torch.tensor(Jd[None], device=dev))
         assert int(info[0]) == 0
         for nm, t in (('R12', R12), ('T12', T12), ('R21', R21), ('T21', T21)):
@@ -99,7 +100,7 @@ def _dropin_stack(pt, use_J):
                 air = sim.air_ref()
                 dev = 'cuda'
                 _interfaces_i_have_known[(id(air), id(sim))] = {'dev': tuple(
-                    torch.tensor(np.asarray(L[m]), device=dev).unsqueeze(0)
+                    torch.tensor(np.ascontiguousarray(L[m]), device=dev).unsqueeze(0)
                     for m in ('R12', 'T12', 'R21', 'T21')) + (True,)}
                 lays.append(sim)
     shears = pt.get('shears')
