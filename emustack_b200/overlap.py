@@ -92,6 +92,8 @@ def mode_normalisation(dmesh, pp, k0, beta1, sol1, sol2):
     pp = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
     if beta1.dtype != c128 or not beta1.is_cuda:
         raise TypeError('beta1 must be a CUDA complex128 tensor')
+    if k0.dtype != torch.float64 or not k0.is_cuda or tuple(k0.shape) != (B,):
+        raise TypeError('k0 must be a CUDA float64 tensor [batch]')
     diag = torch.empty((B, M), dtype=c128, device=dev)
     scale = torch.empty((B, M), dtype=c128, device=dev)
     nsmall = torch.empty((B,), dtype=torch.int32, device=dev)

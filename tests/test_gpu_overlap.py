@@ -59,7 +59,7 @@ def test_normalisation_matches_oracle():
     ovl, perm, scale, warn, s2n, b2 = OV.orthogonal_normalise(mesh.x, mesh.table_nod, mesh.type_el, pp, b1,
                                                               b1, s1, s2, k0)
     dm = DeviceMesh(mesh)
-    diag, sc, ns = mode_normalisation(dm, pp, torch.tensor([k0], device='cuda'),
+    diag, sc, ns = mode_normalisation(dm, pp, torch.tensor([k0], dtype=torch.float64, device='cuda'),
                                       torch.tensor(b1[None], device='cuda'),
                                       torch.tensor(s1[None], device='cuda'), torch.tensor(s2[None], device='cuda'))
     assert int(ns[0]) == 0
