@@ -554,3 +554,52 @@ extern "C" int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspac
   emu::note_launch();
   return emu::check_launch();
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory at the point where they solve:
+// a host thread inside a latency-critical loop (cudaMalloc and cudaFree
+// synchronise the device), code that runs while another framework owns the
+// device heap through its own caching allocator, or an embedding that must
+// not fail on memory pressure after start-up.  For them the film solve can
+// use a fixed scratch array compiled into this library instead of a
+// caller-provided workspace.  The array lives in every GPU that loads the
+// library, for the life of the process.
+#include <mutex>
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_film_scratch[kStaticScratchBytes];
+
+std::mutex g_scratch_mu;
+void *g_scratch_addr[64] = {nullptr};
+
+}  // namespace
+
+extern "C" size_t emu_film_stack_static_scratch_bytes(void) { return kStaticScratchBytes; }
+
+extern "C" int emu_film_stack_batch_noalloc(const EmuFilmStackBatch *p, void *stream) {
+  int st = validate(p);
+  if (st != EMU_OK) return st;
+  if (p->n_points == 0) return EMU_OK;
+  if (emu_film_stack_workspace_size(p) > kStaticScratchBytes) return EMU_E_WORKSPACE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EMU_E_CUDA;
+  void *addr = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+      // the host-side name of the array is not a device address: ask the
+      // runtime for this device's copy once, with the device current
+      if (cudaGetSymbolAddress(&g_scratch_addr[dev], g_film_scratch) != cudaSuccess) {
+        g_scratch_addr[dev] = nullptr;
+        cudaGetLastError();
+        return EMU_E_CUDA;
+      }
+    }
+    addr = g_scratch_addr[dev];
+  }
+  return emu_film_stack_batch(p, addr, kStaticScratchBytes, stream);
+}

@@ -337,6 +337,27 @@ size_t emu_mode_overlap_workspace_size(const EmuNormalise *p);
 int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t workspace_bytes,
                           void *stream);
 
+/* Allocation-free variant of emu_film_stack_batch (no counterpart in the
+ * reference, which has no GPU path).  For callers that cannot allocate
+ * device memory where they solve -- a thread in a latency-critical loop
+ * (cudaMalloc / cudaFree synchronise the device), code running while
+ * another framework's caching allocator owns the device heap, or an
+ * embedding that must not fail on memory pressure after start-up -- the
+ * solve uses a scratch array of emu_film_stack_static_scratch_bytes()
+ * (16 MiB) compiled into the library instead of a caller workspace.  The
+ * caller still passes every input and output buffer.
+ *   - Requests whose emu_film_stack_workspace_size() exceeds that size are
+ *     rejected with EMU_E_WORKSPACE (split the batch).
+ *   - The first call on a device looks up that device's copy of the array
+ *     (cudaGetSymbolAddress); make that first call before any stream
+ *     capture.
+ *   - All calls share the one array per device: calls that can overlap on
+ *     the GPU (different streams, other host threads) race on it; order
+ *     them on one stream.  Nothing in it needs to start at zero.
+ *   - No cudaMalloc, cudaFree or allocating library routine is called. */
+size_t emu_film_stack_static_scratch_bytes(void);
+int emu_film_stack_batch_noalloc(const EmuFilmStackBatch *p, void *stream);
+
 /* ------------------------------------------------------- measurement
  * FP64 FMA throughput probe: blocks x threads threads each run 64 dependent
  * FMA chains of `iters` steps (2*64*iters*threads*blocks flops).  Used as the
