@@ -278,10 +278,11 @@ def run_ours(args, rank, world, local_rank):
         fp64_peak = fp64_peak_tflops()
         tfl = flops / (ms_per_step / 1e3) / 1e12
         traffic = None
-        tf = os.path.join(ROOT, 'profiles', 'film_stack_traffic.json')
+        tf = os.path.join(ROOT, 'profiles', 'film_stack_32768pts.md')
         if os.path.exists(tf):
-            with open(tf) as f:
-                traffic = json.load(f).get('dram_bytes_per_launch')
+            for line in open(tf):
+                if line.startswith('| dram_bytes_per_launch |'):
+                    traffic = int(line.split('|')[2])
         result = {
             'metric': METRIC,
             'value': value,

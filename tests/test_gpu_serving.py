@@ -75,8 +75,9 @@ def test_serving_matches_oracle():
 
 def test_admission_respects_hbm_budget():
     from emustack_b200.serving import GsmServer
-    reqs = _requests(200, seed=2)
-    per = max(r.bytes_on_device() for r in reqs)
+    reqs = _requests(400, seed=2)[::2]   # one stack shape: equal device footprint per request
+    per = reqs[0].bytes_on_device()
+    assert all(r.bytes_on_device() == per for r in reqs)
     with GsmServer(max_batch=1000, hbm_budget_bytes=10 * per) as srv:
         futs = [srv.submit(r) for r in reqs]
         [f.result(timeout=120) for f in futs]
