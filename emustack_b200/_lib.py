@@ -171,7 +171,7 @@ class EmuOverlap(C.Structure):
         ('d', C.c_double), ('dy', C.c_double), ('d_bloch', vp), ('d_k0', vp),
         ('d_sol1', vp), ('d_sol2', vp), ('d_scale2', vp), ('d_perm2', vp),
         ('area_norm', C.c_double), ('d_J', vp), ('d_J_dag', vp), ('d_index_pw_inv', vp),
-        ('elements_per_chunk', C.c_int),
+        ('elements_per_chunk', C.c_int), ('precision', C.c_int), ('d_error', vp),
     ]
 
 
@@ -189,4 +189,6 @@ EXTRA_SIGNATURES.extend([
     ('emu_overlap_batch', C.c_int, [C.POINTER(EmuOverlap), vp, C.c_size_t, vp]),
     ('emu_mode_overlap_workspace_size', C.c_size_t, [C.POINTER(EmuNormalise)]),
     ('emu_mode_overlap_diag', C.c_int, [C.POINTER(EmuNormalise), vp, C.c_size_t, vp]),
+    ('emu_tc_gemm_workspace_size', C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    ('emu_tc_gemm_tf32x3', C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, C.c_size_t, vp]),
 ])

@@ -41,13 +41,14 @@ def _check_sol(sol, nel, name):
 
 
 def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, area_norm=1.0,
-                  dy=1.0, scale2=None, perm2=None, elements_per_chunk=0):
+                  dy=1.0, scale2=None, perm2=None, elements_per_chunk=0, precision='fp64'):
     """J, J_dag (device tensors) and index_pw_inv for a batch of problems.
 
     px, py     int32 [Npw] plane-wave orders (emustack_b200.films.grating_orders)
     bloch      float64 [B, 2] k_parallel * period;  k0 float64 [B] = 2 pi / wl_norm
     sol1/sol2  complex128 [B, nel, M, 13, 3] prime / adjoint fields
     scale2     complex128 [B, M] adjoint normalisation factors (or None)
+    precision  'fp64' (FP64 GEMM) or 'tf32x3' (tensor cores, split-TF32 products)
     """
     dev = dmesh.x.device
     _check_sol(sol1, dmesh.nel, 'sol1')
@@ -75,11 +76,40 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     d.area_norm = float(area_norm)
     d.d_J, d.d_J_dag, d.d_index_pw_inv = ptr(J), ptr(Jd), ptr(inv)
     d.elements_per_chunk = int(elements_per_chunk)
+    if precision not in ('fp64', 'tf32x3'):
+        raise ValueError("precision must be 'fp64' or 'tf32x3'")
+    d.precision = 1 if precision == 'tf32x3' else 0
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    d.d_error = ptr(err)
     L = lib()
     nbytes = L.emu_overlap_workspace_size(C.byref(d))
     ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
     check(L.emu_overlap_batch(C.byref(d), ptr(ws), C.c_size_t(nbytes), stream_ptr()), 'emu_overlap_batch')
+    if d.precision == 1 and int(err.item()) != 0:
+        raise _lib.EmuError(6, 'emu_overlap_batch (tensor-core wait)')
     return J, Jd, inv
+
+
+def tc_gemm(A, B, splits=4):
+    """C = A B^T (float64 CUDA tensors [m, k], [n, k]) on the tensor cores
+    with split-TF32 products (emu_tc_gemm_tf32x3)."""
+    for t, nm in ((A, 'A'), (B, 'B')):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.dim() != 2:
+            raise TypeError('%s must be a contiguous CUDA float64 matrix' % nm)
+    m, k = A.shape
+    n = B.shape[0]
+    if B.shape[1] != k:
+        raise ValueError('inner dimensions differ')
+    Cm = torch.empty((m, n), dtype=torch.float64, device=A.device)
+    err = torch.zeros(1, dtype=torch.int32, device=A.device)
+    L = lib()
+    nbytes = L.emu_tc_gemm_workspace_size(m, n, k, splits)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=A.device)
+    check(L.emu_tc_gemm_tf32x3(m, n, k, ptr(A), ptr(B), ptr(Cm), splits, ptr(err), ptr(ws),
+                               C.c_size_t(nbytes), stream_ptr()), 'emu_tc_gemm_tf32x3')
+    if int(err.item()) != 0:
+        raise _lib.EmuError(6, 'emu_tc_gemm_tf32x3 (bounded wait)')
+    return Cm
 
 
 def mode_normalisation(dmesh, pp, k0, beta1, sol1, sol2):

@@ -304,6 +304,11 @@ typedef struct {
   emu_c128 *d_J_dag;       /* [batch][nval][2 Npw] (with d_sol2)            */
   int32_t *d_index_pw_inv; /* [batch][Npw] 0-based sorted positions or NULL */
   int elements_per_chunk;  /* 0 = default (4096); bounds the workspace      */
+  int precision;           /* 0: FP64 SIMT GEMM; 1: tensor cores, split-TF32
+                              (hi + lo) products, FP32 accumulation per K split,
+                              FP64 sum of the splits                          */
+  int32_t *d_error;        /* [1] set to 1 if a bounded device wait gave up
+                              (tensor-core path), else left untouched; may be NULL */
 } EmuOverlap;
 
 size_t emu_overlap_workspace_size(const EmuOverlap *p);
@@ -357,6 +362,18 @@ int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t works
  *   - No cudaMalloc, cudaFree or allocating library routine is called. */
 size_t emu_film_stack_static_scratch_bytes(void);
 int emu_film_stack_batch_noalloc(const EmuFilmStackBatch *p, void *stream);
+
+/* Tensor-core GEMM used by the overlap integrals, exposed for testing:
+ * C (m x n, FP64) = A (m x k) . B (n x k)^T with both operands split into
+ * TF32 hi + lo parts, three tcgen05 MMAs per step (hi.hi + hi.lo + lo.hi),
+ * FP32 accumulation in tensor memory over each of `splits` K ranges and an
+ * FP64 sum of the ranges.  d_err[0] is set to 1 if a bounded device wait
+ * gave up.  No counterpart in the reference (which has no GPU path); it
+ * stands in for the FP64 contraction of J_overlap.f:162-184. */
+size_t emu_tc_gemm_workspace_size(int m, int n, int k, int splits);
+int emu_tc_gemm_tf32x3(int m, int n, int k, const double *d_A, const double *d_B, double *d_C,
+                       int splits, int32_t *d_err, void *d_workspace, size_t workspace_bytes,
+                       void *stream);
 
 /* ------------------------------------------------------- measurement
  * FP64 FMA throughput probe: blocks x threads threads each run 64 dependent
