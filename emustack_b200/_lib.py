@@ -189,6 +189,8 @@ EXTRA_SIGNATURES.extend([
     ('emu_overlap_batch', C.c_int, [C.POINTER(EmuOverlap), vp, C.c_size_t, vp]),
     ('emu_mode_overlap_workspace_size', C.c_size_t, [C.POINTER(EmuNormalise)]),
     ('emu_mode_overlap_diag', C.c_int, [C.POINTER(EmuNormalise), vp, C.c_size_t, vp]),
+    ('emu_mode_overlap_reorder_workspace_size', C.c_size_t, [C.POINTER(EmuNormalise)]),
+    ('emu_mode_overlap_reorder', C.c_int, [C.POINTER(EmuNormalise), vp, vp, vp, C.c_size_t, vp]),
     ('emu_tc_gemm_workspace_size', C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
     ('emu_tc_gemm_tf32x3', C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, C.c_size_t, vp]),
 ])

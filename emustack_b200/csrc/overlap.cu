@@ -547,6 +547,81 @@ int tc_splits(int npw, int M, long long K2) {
   return sp < 1 ? 1 : sp;
 }
 
+// ---------------------------------------------------------------- pair reordering
+// Full adjoint x prime matrix for the conjugate-pair reordering of
+// orthogonal.f:252-301 (only run when a diagonal entry vanishes).
+__global__ void elem_scal_kernel(const double *x, const int64_t *tn, long nel, double *ms_all) {
+  for (long el = blockIdx.x * (long)blockDim.x + threadIdx.x; el < nel; el += (long)gridDim.x * blockDim.x) {
+    double ms[12][22];
+    element_scal(element_geo(x, tn, el), ms);
+    double *o = ms_all + (size_t)el * 264;
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 22; ++j) o[i * 22 + j] = ms[i][j];
+  }
+}
+
+// ovl[i][j] = sum_el (pp_e / k0) sol2_el(:, i)^T ms_el (beta1(j) sol1_el(:, j)); one thread per (i, j).
+__global__ void ovl_full_kernel(const double *ms_all, int nval, long nel, const int64_t *type_el,
+                                const cd *pp, const double *k0, const cd *beta1, const cd *sol1,
+                                const cd *sol2, cd *ovl) {
+  const long total = (long)nval * nval;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / nval), j = (int)(t % nval);
+    cd acc = cd{0.0, 0.0};
+    for (long el = 0; el < nel; ++el) {
+      const double *ms = ms_all + (size_t)el * 264;
+      const cd *s1 = sol1 + ((size_t)el * nval + j) * 39;
+      const cd *s2 = sol2 + ((size_t)el * nval + i) * 39;
+      cd e = cd{0.0, 0.0};
+      for (int r = 0; r < 12; ++r) {
+        cd v = cd{0.0, 0.0};
+        for (int c = 0; c < 22; ++c) {
+          const cd s = sol1_entry(s1, c);
+          v.x = fma(ms[r * 22 + c], s.x, v.x);
+          v.y = fma(ms[r * 22 + c], s.y, v.y);
+        }
+        e = cadd(e, cmul(v, s2[(r >> 1) * 3 + (r & 1)]));
+      }
+      const cd p = pp[type_el[el] - 1];
+      acc = cadd(acc, cmul(e, cd{p.x / k0[0], p.y / k0[0]}));
+    }
+    ovl[t] = cmul(acc, beta1[j]);
+  }
+}
+
+// The reordering loop itself (one thread): swaps of adjoint modes recorded
+// as a permutation; the recomputed diagonal is ovl[perm[i]][i].
+__global__ void pair_swap_kernel(const cd *ovl, int nval, int32_t *perm, cd *diag, cd *scale, int32_t *warn) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i < nval; ++i) perm[i] = i;
+  int skip = 0, w = 0;
+  for (int j = 0; j < nval; ++j) {
+    const cd djj = ovl[(size_t)j * nval + j];
+    if (hypot(djj.x, djj.y) > 1e-7) continue;
+    if (skip == 0) {
+      if (j == nval - 1) ++w;
+      for (int j2 = j + 1; j2 < nval; ++j2) {
+        const cd o = ovl[(size_t)j2 * nval + j];
+        if (hypot(o.x, o.y) > 1e-7) {
+          const int t = perm[j];
+          perm[j] = perm[j2];
+          perm[j2] = t;
+        }
+      }
+      skip = 1;
+    } else {
+      skip = 0;
+    }
+  }
+  for (int i = 0; i < nval; ++i) {
+    const cd d = ovl[(size_t)perm[i] * nval + i];
+    diag[i] = d;
+    const cd z = csqrt_p(d);
+    scale[i] = (hypot(z.x, z.y) > 1e-8) ? crecip(cmul(z, z)) : cd{1.0, 0.0};
+  }
+  *warn = w;
+}
+
 }  // namespace
 
 // =============================================================== C ABI
@@ -767,6 +842,45 @@ extern "C" int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, s
     diag_finish_kernel<<<(p->nval + 127) / 128, 128, 0, s>>>(
         part, (int)nch, p->nval, a.beta1, (cd *)p->d_diag + (size_t)b * p->nval,
         (cd *)p->d_scale + (size_t)b * p->nval, p->d_n_small + b);
+    emu::note_launch(2);
+  }
+  return emu::check_launch();
+}
+
+extern "C" size_t emu_mode_overlap_reorder_workspace_size(const EmuNormalise *p) {
+  if (!p || p->nval < 1 || p->nel < 1) return 0;
+  return align_up(sizeof(double) * 264 * (size_t)p->nel, 256) +
+         align_up(sizeof(cd) * (size_t)p->nval * p->nval, 256) + 256;
+}
+
+extern "C" int emu_mode_overlap_reorder(const EmuNormalise *p, int32_t *d_perm, int32_t *d_warn,
+                                        void *d_workspace, size_t workspace_bytes, void *stream) {
+  if (!p) return EMU_E_ARG;
+  if (p->batch < 0 || p->nval < 1 || p->nel < 1) return EMU_E_SHAPE;
+  if (!p->d_x || !p->d_table_nod || !p->d_type_el || !p->d_pp || !p->d_k0 || !p->d_beta1 ||
+      !p->d_sol1 || !p->d_sol2 || !p->d_diag || !p->d_scale || !d_perm || !d_warn)
+    return EMU_E_ARG;
+  if (p->batch == 0) return EMU_OK;
+  if (!d_workspace || workspace_bytes < emu_mode_overlap_reorder_workspace_size(p)) return EMU_E_WORKSPACE;
+  int st = upload_tables();
+  if (st != EMU_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *ms_all = (double *)d_workspace;
+  cd *ovl = (cd *)((char *)d_workspace + align_up(sizeof(double) * 264 * (size_t)p->nel, 256));
+  const int sms = emu::sm_count();
+  elem_scal_kernel<<<(int)((p->nel + 127) / 128 < 8 * sms ? (p->nel + 127) / 128 : 8 * sms), 128, 0, s>>>(
+      p->d_x, p->d_table_nod, p->nel, ms_all);
+  emu::note_launch();
+  for (int b = 0; b < p->batch; ++b) {
+    const size_t off = (size_t)b * p->nel * p->nval * 39;
+    const long tot = (long)p->nval * p->nval;
+    ovl_full_kernel<<<(int)((tot + 127) / 128 < 16 * sms ? (tot + 127) / 128 : 16 * sms), 128, 0, s>>>(
+        ms_all, p->nval, p->nel, p->d_type_el, (const cd *)p->d_pp, p->d_k0 + b,
+        (const cd *)p->d_beta1 + (size_t)b * p->nval, (const cd *)p->d_sol1 + off,
+        (const cd *)p->d_sol2 + off, ovl);
+    pair_swap_kernel<<<1, 32, 0, s>>>(ovl, p->nval, d_perm + (size_t)b * p->nval,
+                                       (cd *)p->d_diag + (size_t)b * p->nval,
+                                       (cd *)p->d_scale + (size_t)b * p->nval, d_warn + b);
     emu::note_launch(2);
   }
   return emu::check_launch();

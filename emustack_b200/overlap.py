@@ -141,6 +141,36 @@ def mode_normalisation(dmesh, pp, k0, beta1, sol1, sol2):
     return diag, scale, nsmall
 
 
+def mode_reorder(dmesh, pp, k0, beta1, sol1, sol2):
+    """Conjugate-pair reordering of the adjoint modes (orthogonal.f:252-301)
+    on the GPU: returns (perm, diag, scale, warn) device tensors; perm[b][i]
+    is the adjoint mode at position i after the swaps."""
+    dev = dmesh.x.device
+    _check_sol(sol1, dmesh.nel, 'sol1')
+    _check_sol(sol2, dmesh.nel, 'sol2')
+    B, M = int(sol1.shape[0]), int(sol1.shape[2])
+    pp = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
+    if k0.dtype != torch.float64 or beta1.dtype != c128:
+        raise TypeError('k0 must be float64 and beta1 complex128')
+    diag = torch.empty((B, M), dtype=c128, device=dev)
+    scale = torch.empty((B, M), dtype=c128, device=dev)
+    perm = torch.empty((B, M), dtype=torch.int32, device=dev)
+    warn = torch.empty((B,), dtype=torch.int32, device=dev)
+    nsmall = torch.empty((B,), dtype=torch.int32, device=dev)
+    d = EmuNormalise()
+    d.batch, d.nval, d.nel, d.npt = B, M, dmesh.nel, dmesh.npt
+    d.d_x, d.d_table_nod, d.d_type_el = ptr(dmesh.x), ptr(dmesh.table_nod), ptr(dmesh.type_el)
+    d.d_pp, d.d_k0, d.d_beta1 = ptr(pp), ptr(k0), ptr(beta1.contiguous())
+    d.d_sol1, d.d_sol2 = ptr(sol1), ptr(sol2)
+    d.d_diag, d.d_scale, d.d_n_small = ptr(diag), ptr(scale), ptr(nsmall)
+    L = lib()
+    nbytes = L.emu_mode_overlap_reorder_workspace_size(C.byref(d))
+    ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+    check(L.emu_mode_overlap_reorder(C.byref(d), ptr(perm), ptr(warn), ptr(ws), C.c_size_t(nbytes),
+                                     stream_ptr()), 'emu_mode_overlap_reorder')
+    return perm, diag, scale, warn
+
+
 def overlap_from_fields(simmo, fields):
     """J / area_norm and J_dag of a Simmo from its P2 mode fields.
 
@@ -167,13 +197,17 @@ def overlap_from_fields(simmo, fields):
     k0 = torch.tensor([2 * np.pi / wl_norm], dtype=torch.float64, device=dev)
     bloch = torch.tensor(np.asarray(simmo.k_pll_norm(), np.float64).reshape(1, 2), device=dev)
     diag, scale, nsmall = mode_normalisation(dm, pp, k0, beta1, sol1, sol2)
+    perm = None
     if int(nsmall[0].item()) != 0:
-        raise NotImplementedError('adjoint modes with |<m|m>| <= 1e-7 need the conjugate-pair '
-                                  'reordering of orthogonal.f, which this path does not run')
+        # a vanishing <m|m>: the reference reorders conjugate pairs first
+        perm, diag, scale, warn = mode_reorder(dm, pp, k0, beta1, sol1, sol2)
+        if int(warn[0].item()) != 0 and M <= 20:
+            print('Warning found 1 BM of cmplx conj pair, increase num_BMs to include the other.')
     mo = simmo.max_order_PWs
     px, py = grating_orders(mo, st.period, st.period_y, False)
     area_norm = st.period_y / st.period
     J, Jd, inv = overlap_batch(dm, px, py, mo, bloch, k0, sol1, sol2, area_norm=area_norm,
-                               dy=st.period_y / st.period, scale2=scale)
+                               dy=st.period_y / st.period, scale2=scale, perm2=perm,
+                               precision=fields.get('precision', 'fp64'))
     simmo.overlap_diag = diag[0].cpu().numpy()
     return np.asmatrix(J[0].cpu().numpy()), np.asmatrix(Jd[0].cpu().numpy())

@@ -342,6 +342,19 @@ size_t emu_mode_overlap_workspace_size(const EmuNormalise *p);
 int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t workspace_bytes,
                           void *stream);
 
+/* The conjugate-pair reordering of the adjoint modes
+ * (backend/fortran/orthogonal.f:252-301), for problems whose diagonal has
+ * entries |ovl(j, j)| <= 1e-7: computes the full matrix, runs the reference's
+ * swap loop (each such adjoint mode j, unless it is the second of a pair just
+ * handled, is exchanged with every later mode j2 with |ovl(j2, j)| > 1e-7),
+ * and writes perm[b][i] (adjoint mode now at position i, to pass as
+ * EmuOverlap.d_perm2), the recomputed diagonal ovl(perm[i], i) to d_diag,
+ * its normalisation factors to d_scale and the reference's pair-warning
+ * count to warn[b]. */
+size_t emu_mode_overlap_reorder_workspace_size(const EmuNormalise *p);
+int emu_mode_overlap_reorder(const EmuNormalise *p, int32_t *d_perm, int32_t *d_warn,
+                             void *d_workspace, size_t workspace_bytes, void *stream);
+
 /* Allocation-free variant of emu_film_stack_batch (no counterpart in the
  * reference, which has no GPU path).  For callers that cannot allocate
  * device memory where they solve -- a thread in a latency-critical loop

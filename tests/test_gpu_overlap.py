@@ -102,3 +102,41 @@ def test_simmo_from_fields_stack_matches_oracle():
     r = O.calc_scat(layers, air, period, pol='TE', heights_nm=[90.0])
     np.testing.assert_allclose(st.R_net, r.R_net, rtol=1e-8, atol=1e-9)
     np.testing.assert_allclose(np.asarray(st.a_list, float), np.asarray(r.a_list, float), rtol=1e-8, atol=1e-9)
+
+
+def test_pair_reordering_on_gpu_matches_oracle():
+    """A vanishing <m|m> triggers the conjugate-pair swap loop of
+    orthogonal.f:252-301 on the GPU: permutation, recomputed diagonal,
+    normalisation factors and the J_dag built from them match the oracle."""
+    from emustack_b200.films import grating_orders
+    from emustack_b200.overlap import DeviceMesh, mode_normalisation, mode_reorder, overlap_batch
+    rng = np.random.default_rng(21)
+    mesh = square_cell(4, radius=0.3)
+    nval = 5
+    s1, s2 = _fields(rng, mesh.nel, nval), _fields(rng, mesh.nel, nval)
+    s2[:, 1] = 0.0
+    b1 = rng.uniform(1, 3, nval) + 0j
+    k0 = 2 * np.pi / 0.95
+    pp = [1.0 + 0j, 1.0 + 0j]
+    ovl, perm, scale, warn, s2n, b2 = OV.orthogonal_normalise(mesh.x, mesh.table_nod, mesh.type_el, pp, b1, b1,
+                                                              s1, s2, k0)
+    assert list(perm) != list(range(nval))
+    dm = DeviceMesh(mesh)
+    args = (dm, pp, torch.tensor([k0], dtype=torch.float64, device='cuda'), torch.tensor(b1[None], device='cuda'),
+            torch.tensor(s1[None], device='cuda'), torch.tensor(s2[None], device='cuda'))
+    diag, sc, ns = mode_normalisation(*args)
+    assert int(ns[0]) >= 1
+    gperm, gdiag, gscale, gwarn = mode_reorder(*args)
+    np.testing.assert_array_equal(gperm[0].cpu().numpy(), perm)
+    np.testing.assert_allclose(gdiag[0].cpu().numpy(), np.diag(ovl), rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(gscale[0].cpu().numpy(), scale, rtol=1e-10)
+    assert int(gwarn[0]) == warn
+    mo = 1
+    px, py = grating_orders(mo, 600.0, 600.0)
+    bl = np.array([0.11, 0.07])
+    J, Jd, inv = overlap_batch(dm, px, py, mo, torch.tensor(bl[None], device='cuda'),
+                               torch.tensor([k0], dtype=torch.float64, device='cuda'), None,
+                               torch.tensor(s2[None], device='cuda'), scale2=gscale, perm2=gperm)
+    oinv, _, _ = OV.pw_ordering(mo, 1.0, 1.0, bl, k0)
+    Jdo = OV.J_dagger_overlap(mesh.x, mesh.table_nod, s2n, 1.0, 1.0, bl, oinv, mo)
+    np.testing.assert_allclose(Jd[0].cpu().numpy(), Jdo, rtol=1e-9, atol=1e-11)
