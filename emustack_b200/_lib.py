@@ -194,3 +194,37 @@ EXTRA_SIGNATURES.extend([
     ('emu_tc_gemm_workspace_size', C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
     ('emu_tc_gemm_tf32x3', C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, C.c_size_t, vp]),
 ])
+
+PT_BAD_POINT = 32
+
+
+class EmuFilmPoint(C.Structure):
+    _fields_ = [
+        ('n_layers', C.c_int32), ('n_pw', C.c_int32), ('world_1d', C.c_int32), ('pol', C.c_int32),
+        ('order_off', C.c_int64), ('n_off', C.c_int64), ('h_off', C.c_int64),
+        ('inc_off', C.c_int64), ('rt_off', C.c_int64), ('list_off', C.c_int64),
+        ('np_off', C.c_int64), ('ws_off', C.c_int64),
+        ('period', C.c_double), ('period_y', C.c_double), ('wl_nm', C.c_double),
+        ('kx', C.c_double), ('ky', C.c_double),
+    ]
+
+
+class EmuFilmVarBatch(C.Structure):
+    _fields_ = [
+        ('n_points', C.c_int), ('max_layers', C.c_int), ('max_pw', C.c_int),
+        ('d_points', vp), ('d_order', vp), ('d_px', vp), ('d_py', vp), ('d_n', vp),
+        ('d_heights_nm', vp), ('d_incoming', vp), ('d_R_net', vp), ('d_T_net', vp),
+        ('d_a_list', vp), ('d_t_list', vp), ('d_r_list', vp), ('d_flags', vp),
+        ('d_specular', vp), ('d_num_prop', vp),
+        ('order_len', C.c_int64), ('n_len', C.c_int64), ('h_len', C.c_int64),
+        ('inc_len', C.c_int64), ('rt_len', C.c_int64), ('list_len', C.c_int64),
+        ('np_len', C.c_int64),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_film_var_plan', C.c_int, [vp, C.c_int, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ('emu_film_var_batch', C.c_int, [C.POINTER(EmuFilmVarBatch), vp, C.c_size_t, vp]),
+])

@@ -1,0 +1,455 @@
+// Per-order film recursion shared by the film kernels (uniform batches in
+// film_stack.cu, heterogeneous batches in film_varlen.cu): impedances,
+// Fresnel interfaces, the bottom-to-top cascade of one plane-wave order for
+// both polarisations and, for orders carrying incident light, the
+// top-to-bottom flux pass (backend/mode_calcs.py:199-218, 451-477;
+// backend/stack.py:196-366).
+#pragma once
+#include "emu_cplx.cuh"
+#include "emu_fastmath.cuh"
+#include "emu_internal.h"
+#include "emu_modes.cuh"
+
+namespace emu {
+
+constexpr int kSave = 5;  // saved scalars per (layer, polarisation)
+
+struct LayerC {
+  cd k, zcr, ik;  // wavenumber, 1/n, 1/k
+};
+
+// Shared-memory layout of one point's slot (byte offsets); a slot sized for
+// (npw, L) also holds any point with fewer orders and layers.
+struct SlotSmem {
+  int keys, rank, wood, nprop, acc, lay, h, misc, stride;
+};
+
+__host__ __device__ inline SlotSmem slot_layout(int npw, int L) {
+  SlotSmem s;
+  int o = 0;
+  s.lay = o; o += (int)sizeof(LayerC) * L;
+  s.acc = o; o += 16 * (L + 1);
+  s.keys = o; o += 8 * npw;
+  s.h = o; o += 8 * (L > 2 ? L - 2 : 1);
+  s.rank = o; o += 4 * npw;
+  s.nprop = o; o += 4 * (L + 1);
+  s.wood = o; o += 4 * ((L + 1 + 31) / 32);
+  s.misc = o; o += 16;  // [0] specular order, [1] layer-Wood flag
+  s.stride = (o + 15) / 16 * 16;
+  return s;
+}
+
+// Thread teams that solve one point together: a whole CTA's slot (uniform
+// batches, barriers over the CTA) or one warp (heterogeneous batches).
+struct CtaTeam {
+  int lt, size;
+  __device__ void sync() const { __syncthreads(); }
+  __device__ bool any(bool v) const { return __syncthreads_or(v) != 0; }
+};
+struct WarpTeam {
+  int lt;
+  static constexpr int size = 32;
+  __device__ void sync() const { __syncwarp(); }
+  __device__ bool any(bool v) const { return __any_sync(0xffffffffu, v) != 0; }
+};
+
+// A point accessor P (FilmPointCtx-like) exposes, as member functions:
+//   L() npw() world_1d() pol() ncoord() slot_per_order() dy() period()
+//   inv_sqrt2(), px() py() (order lists), incoming() ([P] or unused),
+//   shears() ([L][2] or NULL), ws() ([n_slots][L][2][kSave] workspace),
+//   R_net() T_net() ([P]), kz() ([L][npw] or NULL), layer_rt() ([L][2][P]
+//   or NULL), vcd() vcu() ([L][P], [L-1][P] or NULL).
+// Accessors compute these from kernel parameters on demand, so the
+// recursion holds no per-point pointers in registers.
+template <class Pt>
+__device__ __forceinline__ cd incidence(const Pt &c, int pos, int spec) {
+  const int pol = c.pol(), npw = c.npw();
+  if (pol == EMU_POL_INCOMING) {
+    const emu_c128 v = c.incoming()[pos];
+    return cd{v.re, v.im};
+  }
+  const bool te = (pos == spec), tm = (pos == spec + npw);
+  switch (pol) {
+    case EMU_POL_TE: return te ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    case EMU_POL_TM: return tm ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    case EMU_POL_UN: return (te || tm) ? cd{c.inv_sqrt2(), 0.0} : cd{0.0, 0.0};
+    case EMU_POL_RCIRC: return te ? cd{c.inv_sqrt2(), 0.0} : (tm ? cd{0.0, c.inv_sqrt2()} : cd{0.0, 0.0});
+    case EMU_POL_LCIRC: return te ? cd{c.inv_sqrt2(), 0.0} : (tm ? cd{0.0, -c.inv_sqrt2()} : cd{0.0, 0.0});
+  }
+  return cd{0.0, 0.0};
+}
+
+__device__ __forceinline__ void store_c(emu_c128 *p, size_t i, cd v) {
+  p[i] = emu_c128{v.x, v.y};
+}
+
+// U-weighted flux contribution of one order and polarisation
+// (backend/stack.py:311-321, 351): propagating orders give |f-|^2 - |f+|^2,
+// evanescent ones the cross terms with -+i.
+__device__ __forceinline__ cd flux_term(cd fm, cd fp, bool prop, bool tm) {
+  if (prop) return cd{cabs2(fm) - cabs2(fp), 0.0};
+  // TE: conj(fm)(-i)fp + conj(fp)(i)fm ; TM: conj(fm)(i)fp + conj(fp)(-i)fm
+  const cd a = cmul(cconj(fm), fp);
+  const cd b = cmul(cconj(fp), fm);
+  const cd d = csub(b, a);
+  const cd te = cd{-d.y, d.x};
+  return tm ? cneg(te) : te;
+}
+
+// Cascade of one order (both polarisations) bottom to top, then, if the
+// order carries incident light, its flux pass top to bottom.
+template <class Pt>
+__device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec, const LayerC *lay,
+                            const double *hsm, const unsigned *wood, bool wood_air, double a0,
+                            double b0, double sa0, double sb0, double wln, int np_air, int np_in,
+                            int np_out, cd *acc, int *nprop, bool count) {
+  const int L = p.L(), npw = p.npw(), P = 2 * npw;
+  const int px = p.px()[u], py = p.py()[u];
+  double al_air, be_air;
+  order_ab(p.world_1d(), p.dy(), px, py, wood_air ? sa0 : a0, wood_air ? sb0 : b0, al_air, be_air);
+  const cd kair = wavenumber(cd{1.0, 0.0}, wln);
+  const cd kz_air = csqrt_p(kz_arg(kair, al_air, be_air));
+  // air impedances (1/n = 1): Z_TE = k/kz, Z_TM = kz/k
+  const cd z1[2] = {cmul(kair, crcp_nr(kz_air)), cmul(kz_air, crcp_nr(kair))};
+  const cd sz1[2] = {csqrt_nr(z1[0]), csqrt_nr(z1[1])};
+  const double *sh = p.shears();
+  double al_sh = 0.0, be_sh = 0.0;
+  if (sh)
+    order_ab(p.world_1d(), p.dy(), p.px()[j], p.py()[j], wood_air ? sa0 : a0, wood_air ? sb0 : b0, al_sh,
+             be_sh);
+  const cd din[2] = {incidence(p, j, spec), incidence(p, j + npw, spec)};
+  const bool active = !cis_zero(din[0]) || !cis_zero(din[1]);
+  const int aslot = p.slot_per_order() ? u : 0;
+  cd *wsv = p.ws() + ((size_t)aslot * L) * 2 * kSave;
+  cd tnet[2], rnet[2];
+  for (int l = 0; l < L; ++l) {
+    const bool wl_l = (wood[l >> 5] >> (l & 31)) & 1u;
+    double al, be;
+    order_ab(p.world_1d(), p.dy(), px, py, wl_l ? sa0 : a0, wl_l ? sb0 : b0, al, be);
+    const LayerC c = lay[l];
+    const cd kz = csqrt_p(kz_arg(c.k, al, be));
+    const bool fin = (l >= 1 && l < L - 1);
+    if (count && fin && kz.y == 0.0) atomicAdd(&nprop[l], 1);
+    if (p.kz()) store_c(p.kz(), (size_t)l * npw + j, kz);
+    // Z_TE = (1/n) k / kz ; Z_TM = (1/n) kz / k
+    const cd z2[2] = {cmul(c.zcr, cmul(c.k, crcp_nr(kz))), cmul(c.zcr, cmul(kz, c.ik))};
+    const cd pr = fin ? cexp_ikh(kz, hsm[l - 1] / p.period()) : cd{1.0, 0.0};
+    cd Q = cd{1.0, 0.0}, Qi = cd{1.0, 0.0};
+    if (sh && l >= 1) {
+      double c0, c1;
+      if (l < L - 1) {
+        c0 = sh[2 * (l - 1)] - sh[2 * l];
+        c1 = sh[2 * (l - 1) + 1] - sh[2 * l + 1];
+      } else {
+        c0 = sh[2 * l];
+        c1 = sh[2 * l + 1];
+      }
+      Q = shear_phase(al_sh, be_sh, c0, c1, p.ncoord());
+      Qi = shear_phase(al_sh, be_sh, -1 * c0, -1 * c1, p.ncoord());
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const cd is = crcp_nr(cadd(z2[q], z1[q]));
+      const cd R12 = cmul(csub(z2[q], z1[q]), is);
+      const cd T12 = cmul(cscale(cmul(csqrt_nr(z2[q]), sz1[q]), 2.0), is);
+      const cd R21 = cneg(R12), T21 = T12;
+      if (p.layer_rt()) {
+        const size_t o = (size_t)l * 2 * P;
+        store_c(p.layer_rt(), o + j + q * npw, R12);
+        store_c(p.layer_rt(), o + P + j + q * npw, T12);
+      }
+      cd *sv = wsv + ((size_t)l * 2 + q) * kSave;
+      if (l == 0) {
+        tnet[q] = T12;
+        rnet[q] = R12;
+        if (active) {
+          sv[0] = rnet[q];
+          sv[1] = tnet[q];
+        }
+        continue;
+      }
+      // air gap below layer l (backend/stack.py:229-247, 263-278)
+      cd x1;
+      if (sh) {
+        const cd rq = cmul(cmul(Qi, rnet[q]), Q);
+        x1 = cmul(T21, crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rq))));
+        tnet[q] = cmul(cmul(tnet[q], Q), x1);
+        rnet[q] = cadd(R21, cmul(cmul(T12, rq), x1));
+      } else {
+        x1 = cmul(T21, crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rnet[q]))));
+        tnet[q] = cmul(tnet[q], x1);
+        rnet[q] = cadd(R21, cmul(cmul(T12, rnet[q]), x1));
+      }
+      if (active) {
+        sv[0] = x1;
+        sv[1] = rnet[q];
+      }
+      if (!fin) continue;
+      // through layer l (backend/stack.py:249-262)
+      const cd x2 = cmul(T12, crcp_nr(csub(cd{1.0, 0.0}, cmul(cmul(cmul(R21, pr), rnet[q]), pr))));
+      const cd px2 = cmul(pr, x2);
+      tnet[q] = cmul(tnet[q], px2);
+      rnet[q] = cadd(R12, cmul(cmul(cmul(T21, pr), rnet[q]), px2));
+      if (active) {
+        sv[2] = pr;
+        sv[3] = x2;
+        sv[4] = rnet[q];
+      }
+    }
+  }
+  store_c(p.R_net(), j, rnet[0]);
+  store_c(p.R_net(), j + npw, rnet[1]);
+  store_c(p.T_net(), j, tnet[0]);
+  store_c(p.T_net(), j + npw, tnet[1]);
+
+  // ---- flux pass (backend/stack.py:323-366)
+  const bool want_vec = p.vcd() != nullptr;
+  if (!active) {
+    if (want_vec) {
+      for (int lv = 0; lv < L; ++lv)
+        for (int q = 0; q < 2; ++q) store_c(p.vcd(), (size_t)lv * P + j + q * npw, cd{0.0, 0.0});
+      for (int lv = 0; lv < L - 1; ++lv)
+        for (int q = 0; q < 2; ++q) store_c(p.vcu(), (size_t)lv * P + j + q * npw, cd{0.0, 0.0});
+    }
+    return;
+  }
+  const bool prop = j < np_air;
+  double in_sum = 0.0, up_sum = 0.0, out_sum = 0.0;
+  for (int q = 0; q < 2; ++q) {
+    const int pos = j + q * npw;
+    const cd *top = wsv + ((size_t)(L - 1) * 2 + q) * kSave;
+    const cd dp = cmul(top[1], din[q]);  // d_plus = r_top d
+    if (j < np_in) {
+      in_sum += cabs2(din[q]);
+      up_sum += cabs2(dp);
+    }
+    if (want_vec) {
+      store_c(p.vcd(), pos, din[q]);
+      store_c(p.vcu(), pos, dp);
+    }
+    cd f1m = cmul(top[0], din[q]);
+    for (int i = 0; i < L - 2; ++i) {
+      const int k = L - 2 - i;
+      const cd *s = wsv + ((size_t)k * 2 + q) * kSave;
+      const cd f1p = cmul(s[4], f1m);
+      const cd fl = flux_term(f1m, f1p, prop, q == 1);
+      atomicAdd(&acc[1 + i].x, fl.x);
+      atomicAdd(&acc[1 + i].y, fl.y);
+      const cd f2m = cmul(s[3], f1m);
+      const cd f2p = cmul(cmul(s[1], s[2]), f2m);
+      if (want_vec) {
+        store_c(p.vcd(), (size_t)(1 + i) * P + pos, f2m);
+        store_c(p.vcu(), (size_t)(1 + i) * P + pos, f2p);
+      }
+      f1m = cmul(cmul(s[0], s[2]), f2m);
+    }
+    const cd *s0 = wsv + ((size_t)0 * 2 + q) * kSave;
+    const cd f2m = cmul(s0[1], f1m);
+    if (want_vec) store_c(p.vcd(), (size_t)(L - 1) * P + pos, f2m);
+    if (j < np_out) out_sum += cabs2(f2m);
+  }
+  atomicAdd(&acc[0].x, in_sum);
+  atomicAdd(&acc[L].x, up_sum);
+  atomicAdd(&acc[L - 1].x, out_sum);
+}
+
+// One point, phases 0-6 (the film kernels' header comments describe them).
+// Every thread of the team calls this with the same `valid`, and with
+// `valid` false takes the same barriers without touching memory.  The point
+// accessor adds, to the fields solve_order uses: wl_nm() kx() ky() (k_pll),
+// n(i), height(i), and the optional outputs sort_order() specular()
+// num_prop() fluxes() (NULL to skip), and the required a_list() t_list()
+// r_list() flags().
+template <class Team, class Pt>
+__device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool valid,
+                                           unsigned char *base, const SlotSmem &S) {
+  LayerC *lay = (LayerC *)(base + S.lay);
+  cd *acc = (cd *)(base + S.acc);
+  double *keys = (double *)(base + S.keys);
+  double *hsm = (double *)(base + S.h);
+  int *rank = (int *)(base + S.rank);
+  int *nprop = (int *)(base + S.nprop);
+  unsigned *wood = (unsigned *)(base + S.wood);
+  int *misc = (int *)(base + S.misc);
+  const int lt = tm.lt, team = tm.size;
+  const int L = valid ? p.L() : 2, npw = valid ? p.npw() : 1;
+  const int wood_words = (L + 1 + 31) / 32;
+  const bool count = valid && p.num_prop() != nullptr;
+  double wln = 1.0, a0 = 0.0, b0 = 0.0;
+  if (valid) {
+    wln = wl_norm(p.wl_nm(), p.period());
+    a0 = p.kx() * p.period();
+    b0 = p.ky() * p.period();
+  }
+  const double sa0 = (1 - 1e-9) * a0, sb0 = (1 - 1e-9) * b0;
+  // ---------------------------------------------------------- phase 0
+  if (valid) {
+    for (int i = lt; i < L; i += team) {
+      const emu_c128 v = p.n(i);
+      const cd n = cd{v.re, v.im};
+      LayerC c;
+      c.k = wavenumber(n, wln);
+      c.zcr = crecip(n);
+      c.ik = crecip(c.k);
+      lay[i] = c;
+    }
+    for (int i = lt; i < L - 2; i += team) hsm[i] = p.height(i);
+    for (int i = lt; i < L + 1; i += team) {
+      acc[i] = cd{0.0, 0.0};
+      nprop[i] = 0;
+    }
+    for (int i = lt; i < wood_words; i += team) wood[i] = 0u;
+    if (lt == 0) {
+      misc[0] = -1;
+      misc[1] = 0;
+    }
+  }
+  tm.sync();
+  // ---------------------------------------------------------- phase 1
+  if (valid) {
+    const cd kair = wavenumber(cd{1.0, 0.0}, wln);
+    for (int u = lt; u < npw; u += team) {
+      double al, be;
+      order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], a0, b0, al, be);
+      const cd kz = csqrt_p(kz_arg(kair, al, be));
+      if (cis_zero(kz)) atomicOr(&wood[L >> 5], 1u << (L & 31));
+      keys[u] = -1 * kz.x + kz.y;
+      if (kz.y == 0.0) atomicAdd(&nprop[L], 1);
+    }
+  }
+  tm.sync();
+  // ---------------------------------------------------------- phase 2
+  const bool wood_air = valid && ((wood[L >> 5] >> (L & 31)) & 1u);
+  if (tm.any(wood_air)) {
+    if (wood_air && lt == 0) nprop[L] = 0;
+    tm.sync();
+    if (wood_air) {
+      const cd kair = wavenumber(cd{1.0, 0.0}, wln);
+      for (int u = lt; u < npw; u += team) {
+        double al, be;
+        order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], sa0, sb0, al, be);
+        const cd kz = csqrt_p(kz_arg(kair, al, be));
+        keys[u] = -1 * kz.x + kz.y;
+        if (kz.y == 0.0) atomicAdd(&nprop[L], 1);
+      }
+    }
+    tm.sync();
+  }
+  // ---------------------------------------------------------- phase 3
+  if (valid) {
+    int32_t *so = p.sort_order();
+    for (int u = lt; u < npw; u += team) {
+      const double ku = keys[u];
+      int r = 0;
+      for (int v = 0; v < npw; ++v) {
+        const double kv = keys[v];
+        r += (kv < ku) || (kv == ku && v < u);
+      }
+      rank[u] = r;
+      const int pxu = p.px()[u], pyu = p.py()[u];
+      const bool zero_order = (pxu == 0) && (p.world_1d() || pyu == 0);
+      if (zero_order) misc[0] = r;
+      if (so) so[r] = u;
+      double al, be;
+      order_ab(p.world_1d(), p.dy(), pxu, pyu, a0, b0, al, be);
+      if (csqrt_p(kz_arg(lay[0].k, al, be)).y == 0.0) atomicAdd(&nprop[0], 1);
+      if (csqrt_p(kz_arg(lay[L - 1].k, al, be)).y == 0.0) atomicAdd(&nprop[L - 1], 1);
+      // Wood check of every layer: k_z == 0 exactly iff its argument is 0
+      for (int l = 0; l < L; ++l) {
+        const cd arg = kz_arg(lay[l].k, al, be);
+        if (arg.x == 0.0 && arg.y == 0.0) {
+          atomicOr(&wood[l >> 5], 1u << (l & 31));
+          misc[1] = 1;
+        }
+      }
+    }
+  }
+  tm.sync();
+  // ---------------------------------------------------------- phase 4
+  const bool layer_wood = valid && misc[1] != 0;
+  if (valid && !layer_wood) {
+    const int spec = misc[0];
+    const int np_air = nprop[L], np_in = nprop[L - 1], np_out = nprop[0];
+    for (int u = lt; u < npw; u += team)
+      solve_order(p, u, rank[u], spec, lay, hsm, wood, wood_air, a0, b0, sa0, sb0, wln, np_air,
+                  np_in, np_out, acc, nprop, count);
+  }
+  // ---------------------------------------------------------- phase 5
+  if (tm.any(layer_wood)) {
+    // recount substrate / superstrate with the scaled k_parallel where marked
+    if (layer_wood && lt == 0) {
+      nprop[0] = 0;
+      nprop[L - 1] = 0;
+    }
+    tm.sync();
+    if (layer_wood) {
+      for (int u = lt; u < npw; u += team) {
+        for (int t = 0; t < 2; ++t) {
+          const int l = t ? L - 1 : 0;
+          const bool wl_l = (wood[l >> 5] >> (l & 31)) & 1u;
+          double al, be;
+          order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], wl_l ? sa0 : a0, wl_l ? sb0 : b0,
+                   al, be);
+          if (csqrt_p(kz_arg(lay[l].k, al, be)).y == 0.0) atomicAdd(&nprop[l], 1);
+        }
+      }
+    }
+    tm.sync();
+    if (layer_wood) {
+      const int spec = misc[0];
+      const int np_air = nprop[L], np_in = nprop[L - 1], np_out = nprop[0];
+      for (int u = lt; u < npw; u += team)
+        solve_order(p, u, rank[u], spec, lay, hsm, wood, wood_air, a0, b0, sa0, sb0, wln, np_air,
+                    np_in, np_out, acc, nprop, count);
+    }
+  }
+  tm.sync();
+  // ---------------------------------------------------------- phase 6
+  if (valid && lt == 0) {
+    uint32_t flags = 0;
+    if (wood_air) flags |= EMU_PT_WOOD_AIR;
+    if (layer_wood) flags |= EMU_PT_WOOD_LAYER;
+    const int np_in = nprop[L - 1], np_out = nprop[0];
+    if (np_out == 0) flags |= EMU_PT_NO_PROP_SUB;
+    if (np_in == 0) flags |= EMU_PT_NO_PROP_SUP;
+    double *al = p.a_list();
+    double *tl = p.t_list();
+    const double df0 = acc[0].x, up0 = acc[L].x, dsub = acc[L - 1].x;
+    // |down_fluxes[i]| with down_fluxes = [df0, gap_1..gap_{L-2}, dsub]
+    auto dfa = [&](int i) -> double {
+      if (i == 0) return fabs(df0);
+      if (i == L - 1) return fabs(dsub);
+      return hypot(acc[i].x, acc[i].y);
+    };
+    double rr = 0.0;
+    if (np_out != 0) {
+      for (int i = 1; i <= L - 2; ++i) al[i - 1] = fabs(dfa(i) - dfa(i + 1));
+      al[L - 2] = fabs(df0 - dsub - up0);
+      for (int i = 0; i <= L - 3; ++i) tl[i] = fabs(dfa(i + 2) / dfa(i));
+      tl[L - 2] = fabs(dsub / df0);
+      rr = fabs(up0 / df0);
+    } else {
+      for (int i = 0; i < L - 1; ++i) {
+        al[i] = 0.0;
+        tl[i] = 0.0;
+      }
+    }
+    *p.r_list() = rr;
+    bool fin = isfinite(rr);
+    for (int i = 0; i < L - 1; ++i) fin = fin && isfinite(al[i]) && isfinite(tl[i]);
+    if (!fin) flags |= EMU_PT_NONFINITE;
+    *p.flags() = flags;
+    if (p.specular()) *p.specular() = misc[0];
+    if (int32_t *np = p.num_prop())
+      for (int i = 0; i <= L; ++i) np[i] = nprop[i];
+    if (double *fo = p.fluxes()) {
+      for (int i = 0; i <= L; ++i) {
+        fo[2 * i] = acc[i].x;
+        fo[2 * i + 1] = acc[i].y;
+      }
+    }
+  }
+  tm.sync();
+}
+
+}  // namespace emu

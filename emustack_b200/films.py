@@ -182,3 +182,209 @@ class FilmStackSolver(object):
         check(L.emu_film_stack_batch(C.byref(d), ptr(ws), C.c_size_t(ws.numel()), stream_ptr(stream)),
               'emu_film_stack_batch')
         return out
+
+
+# ---------------------------------------------------------------- uneven batches
+_POINT_DTYPE = np.dtype([
+    ('n_layers', np.int32), ('n_pw', np.int32), ('world_1d', np.int32), ('pol', np.int32),
+    ('order_off', np.int64), ('n_off', np.int64), ('h_off', np.int64), ('inc_off', np.int64),
+    ('rt_off', np.int64), ('list_off', np.int64), ('np_off', np.int64), ('ws_off', np.int64),
+    ('period', np.float64), ('period_y', np.float64), ('wl_nm', np.float64),
+    ('kx', np.float64), ('ky', np.float64),
+])
+assert _POINT_DTYPE.itemsize == C.sizeof(_lib.EmuFilmPoint)
+
+
+class FilmPoint(object):
+    """One spectral point of an all-film stack, any shape.
+
+    The arguments are what the reference's Stack(layers).calc_scat(pol)
+    reads from its ThinFilm layers and Light: refractive indices bottom to
+    top with each layer's ``loss`` flag already applied, finite-layer
+    heights, wavelength, k_parallel (nm^-1), period(s), ``max_order_PWs``,
+    the polarisation ('TE', 'TM', 'un', 'R Circ', 'L Circ') or a full
+    incoming amplitude vector of length 2 Npw (sorted order).
+    """
+
+    __slots__ = ('n', 'heights', 'wl_nm', 'k_pll', 'period', 'period_y', 'max_order', 'pol',
+                 'world_1d', 'incoming')
+
+    def __init__(self, n, heights, wl_nm, k_pll, period, max_order, pol='TE', period_y=None,
+                 world_1d=False, incoming=None):
+        self.n = np.asarray(n, np.complex128).reshape(-1)
+        self.heights = np.asarray(heights, np.float64).reshape(-1)
+        if len(self.n) < 2:
+            raise ValueError('a stack needs at least a substrate and a superstrate')
+        if self.heights.shape != (len(self.n) - 2,):
+            raise ValueError('need one height per finite layer')
+        self.wl_nm = float(wl_nm)
+        self.k_pll = np.asarray(k_pll, np.float64).reshape(2)
+        self.period = float(period)
+        self.period_y = float(period if period_y is None else period_y)
+        self.max_order = int(max_order)
+        self.world_1d = bool(world_1d)
+        self.incoming = None if incoming is None else np.asarray(incoming, np.complex128).reshape(-1)
+        if self.incoming is None and pol not in _lib.POL:
+            raise NotImplementedError('Must select from the currently implemented polarisations; '
+                                      'TE, TM, R Circ, L Circ.')
+        self.pol = pol
+
+
+class FilmVarSolver(object):
+    """All-film points of mixed shapes in one launch (``emu_film_var_batch``).
+
+    ``plan(points)`` packs the points on the host (pinned memory),
+    ``solve(plan)`` copies them to the device, launches once and returns the
+    packed device outputs, ``unpack(plan, out)`` splits host copies of them
+    per point.  Order sets are built once per (max_order, period, period_y,
+    world_1d) and shared by every point that uses them.
+    """
+
+    def __init__(self, device='cuda'):
+        self.device = torch.device(device)
+        self._orders = {}
+        self._px, self._py = [], []
+        self._n_orders = 0
+        self._d_orders = None
+        self._ws = None
+
+    def _order_off(self, key):
+        hit = self._orders.get(key)
+        if hit is None:
+            px, py = grating_orders(key[0], key[1], key[2], key[3])
+            hit = (self._n_orders, len(px))
+            self._orders[key] = hit
+            self._px.append(px)
+            self._py.append(py)
+            self._n_orders += len(px)
+            self._d_orders = None
+        return hit
+
+    def _device_orders(self):
+        if self._d_orders is None:
+            px = np.concatenate(self._px).astype(np.int32)
+            py = np.concatenate(self._py).astype(np.int32)
+            self._d_orders = (torch.from_numpy(px).to(self.device),
+                              torch.from_numpy(py).to(self.device))
+        return self._d_orders
+
+    def plan(self, points):
+        B = len(points)
+        desc = np.zeros(B, _POINT_DTYPE)
+        n_parts, h_parts, inc_parts = [], [], []
+        n_off = h_off = inc_off = 0
+        for i, p in enumerate(points):
+            o_off, npw = self._order_off((p.max_order, p.period, p.period_y, p.world_1d))
+            L = len(p.n)
+            d = desc[i]
+            d['n_layers'], d['n_pw'], d['world_1d'] = L, npw, int(p.world_1d)
+            d['order_off'], d['n_off'], d['h_off'] = o_off, n_off, h_off
+            d['period'], d['period_y'], d['wl_nm'] = p.period, p.period_y, p.wl_nm
+            d['kx'], d['ky'] = p.k_pll[0], p.k_pll[1]
+            n_parts.append(p.n)
+            n_off += L
+            h_parts.append(p.heights)
+            h_off += L - 2
+            if p.incoming is not None:
+                if p.incoming.shape != (2 * npw,):
+                    raise ValueError('incoming must have 2 Npw = %d entries' % (2 * npw))
+                d['pol'] = _lib.POL_INCOMING
+                d['inc_off'] = inc_off
+                inc_parts.append(p.incoming)
+                inc_off += 2 * npw
+            else:
+                d['pol'] = _lib.POL[p.pol]
+        order = np.zeros(B, np.int32)
+        rt_len, list_len, np_len = C.c_int64(), C.c_int64(), C.c_int64()
+        ws_bytes, max_l, max_pw = C.c_size_t(), C.c_int(), C.c_int()
+        check(lib().emu_film_var_plan(desc.ctypes.data_as(C.c_void_p), B,
+                                      order.ctypes.data_as(C.c_void_p), C.byref(rt_len),
+                                      C.byref(list_len), C.byref(np_len), C.byref(ws_bytes),
+                                      C.byref(max_l), C.byref(max_pw)), 'emu_film_var_plan')
+
+        def pinned(parts, dtype, npdtype):
+            a = np.concatenate(parts).astype(npdtype) if parts else np.zeros(0, npdtype)
+            t = torch.empty(max(a.size, 1), dtype=dtype).pin_memory()
+            t.numpy()[:a.size] = a
+            return t, a.size
+
+        pl = {
+            'B': B, 'desc': desc, 'max_layers': max_l.value, 'max_pw': max_pw.value,
+            'rt_len': rt_len.value, 'list_len': list_len.value, 'np_len': np_len.value,
+            'ws_bytes': ws_bytes.value,
+        }
+        pl['h_desc'] = torch.from_numpy(desc.view(np.uint8).copy()).pin_memory()
+        pl['h_order'] = torch.from_numpy(order).pin_memory()
+        pl['h_n'], pl['n_len'] = pinned(n_parts, torch.complex128, np.complex128)
+        pl['h_h'], pl['h_len'] = pinned(h_parts, torch.float64, np.float64)
+        pl['h_inc'], pl['inc_len'] = pinned(inc_parts, torch.complex128, np.complex128)
+        return pl
+
+    def workspace(self, nbytes):
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def solve(self, pl, stream=None, want_num_prop=False):
+        """Copy a plan to the device and solve it in one launch; returns
+        device tensors R_net/T_net [rt_len], a_list/t_list [list_len],
+        r_list/flags/specular [B] (and num_prop [np_len])."""
+        dev = self.device
+        px, py = self._device_orders()
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        with torch.cuda.stream(s):
+            d_desc = pl['h_desc'].to(dev, non_blocking=True)
+            d_order = pl['h_order'].to(dev, non_blocking=True)
+            d_n = pl['h_n'].to(dev, non_blocking=True)
+            d_h = pl['h_h'].to(dev, non_blocking=True)
+            d_inc = pl['h_inc'].to(dev, non_blocking=True)
+            B = pl['B']
+            out = {
+                'R_net': torch.empty(max(pl['rt_len'], 1), dtype=torch.complex128, device=dev),
+                'T_net': torch.empty(max(pl['rt_len'], 1), dtype=torch.complex128, device=dev),
+                'a_list': torch.empty(max(pl['list_len'], 1), dtype=torch.float64, device=dev),
+                't_list': torch.empty(max(pl['list_len'], 1), dtype=torch.float64, device=dev),
+                'r_list': torch.empty(max(B, 1), dtype=torch.float64, device=dev),
+                'flags': torch.empty(max(B, 1), dtype=torch.int32, device=dev),
+                'specular': torch.empty(max(B, 1), dtype=torch.int32, device=dev),
+            }
+            if want_num_prop:
+                out['num_prop'] = torch.empty(max(pl['np_len'], 1), dtype=torch.int32, device=dev)
+            ws = self.workspace(pl['ws_bytes'])
+            d = _lib.EmuFilmVarBatch()
+            d.n_points = B
+            d.max_layers, d.max_pw = pl['max_layers'], pl['max_pw']
+            d.d_points, d.d_order = ptr(d_desc), ptr(d_order)
+            d.d_px, d.d_py = ptr(px), ptr(py)
+            d.d_n, d.d_heights_nm, d.d_incoming = ptr(d_n), ptr(d_h), ptr(d_inc)
+            d.d_R_net, d.d_T_net = ptr(out['R_net']), ptr(out['T_net'])
+            d.d_a_list, d.d_t_list = ptr(out['a_list']), ptr(out['t_list'])
+            d.d_r_list, d.d_flags = ptr(out['r_list']), ptr(out['flags'])
+            d.d_specular = ptr(out['specular'])
+            d.d_num_prop = ptr(out.get('num_prop'))
+            d.order_len = self._n_orders
+            d.n_len, d.h_len, d.inc_len = pl['n_len'], pl['h_len'], pl['inc_len']
+            d.rt_len, d.list_len, d.np_len = pl['rt_len'], pl['list_len'], pl['np_len']
+            check(lib().emu_film_var_batch(C.byref(d), ptr(ws), C.c_size_t(ws.numel()),
+                                           stream_ptr(s)), 'emu_film_var_batch')
+            out['_keep'] = (d_desc, d_order, d_n, d_h, d_inc)
+        return out
+
+    @staticmethod
+    def unpack(pl, host):
+        """Split host copies (numpy) of the packed outputs per point."""
+        res = []
+        for i, d in enumerate(pl['desc']):
+            P, L = 2 * int(d['n_pw']), int(d['n_layers'])
+            ro, lo = int(d['rt_off']), int(d['list_off'])
+            r = {
+                'R_net': host['R_net'][ro:ro + P], 'T_net': host['T_net'][ro:ro + P],
+                'a_list': host['a_list'][lo:lo + L - 1], 't_list': host['t_list'][lo:lo + L - 1],
+                'r_list': host['r_list'][i], 'flags': int(host['flags'][i]),
+                'specular': int(host['specular'][i]),
+            }
+            if 'num_prop' in host:
+                no = int(d['np_off'])
+                r['num_prop'] = host['num_prop'][no:no + L + 1]
+            res.append(r)
+        return res

@@ -376,6 +376,73 @@ int emu_mode_overlap_reorder(const EmuNormalise *p, int32_t *d_perm, int32_t *d_
 size_t emu_film_stack_static_scratch_bytes(void);
 int emu_film_stack_batch_noalloc(const EmuFilmStackBatch *p, void *stream);
 
+/* --------------------------------- a2-a4, a7, a9, a10: uneven film batches
+ * The film solve of emu_film_stack_batch for a batch whose points differ in
+ * shape: each point brings its own layer count, order set (Npw, 1D or 2D),
+ * periods, polarisation, wavelength and k_parallel -- in the reference, one
+ * Stack(layers).calc_scat(pol) call each (backend/stack.py:162-426), made in
+ * a loop or a process pool over wavelengths and structures.  One warp
+ * solves one point; points of any mix of shapes share one launch.
+ *
+ * Every per-point array is packed: the point's slices start at its offsets
+ * (counted in elements of the array they index).  Offsets and sizes come
+ * from emu_film_var_plan, which also sizes the workspace.  Outputs match
+ * emu_film_stack_batch's for the same point (sorted-order R_net / T_net
+ * diagonals, a_list / t_list / r_list, EMU_PT_* flags).  A point whose
+ * descriptor is out of range (L < 2, Npw < 1, L or Npw above the batch
+ * bounds, bad pol, a slice outside its array) is not solved and gets
+ * EMU_PT_BAD_POINT. */
+#define EMU_PT_BAD_POINT 32u     /* descriptor out of range: point skipped  */
+
+typedef struct {
+  int32_t n_layers;      /* L >= 2                                          */
+  int32_t n_pw;          /* Npw of this point's order set                   */
+  int32_t world_1d;
+  int32_t pol;           /* EMU_POL_*                                       */
+  int64_t order_off;     /* d_px / d_py: Npw orders (emu_grating_orders)    */
+  int64_t n_off;         /* d_n: L indices, substrate first                 */
+  int64_t h_off;         /* d_heights_nm: L-2 heights                       */
+  int64_t inc_off;       /* d_incoming: 2 Npw (pol == EMU_POL_INCOMING)     */
+  int64_t rt_off;        /* d_R_net / d_T_net: 2 Npw        (set by plan)   */
+  int64_t list_off;      /* d_a_list / d_t_list: L-1        (set by plan)   */
+  int64_t np_off;        /* d_num_prop: L+1                 (set by plan)   */
+  int64_t ws_off;        /* workspace, bytes                (set by plan)   */
+  double period, period_y; /* nm                                            */
+  double wl_nm;          /* wavelength (nm)                                 */
+  double kx, ky;         /* k_parallel (nm^-1)                              */
+} EmuFilmPoint;
+
+typedef struct {
+  int n_points;                /* B                                         */
+  int max_layers, max_pw;      /* bounds over the points (from the plan)    */
+  const EmuFilmPoint *d_points;/* [B]                                       */
+  const int32_t *d_order;      /* [B] solve order (costliest first) or NULL */
+  const int32_t *d_px, *d_py;
+  const emu_c128 *d_n;
+  const double *d_heights_nm;
+  const emu_c128 *d_incoming;  /* NULL unless some pol == EMU_POL_INCOMING  */
+  emu_c128 *d_R_net, *d_T_net; /* sum of 2 Npw                              */
+  double *d_a_list, *d_t_list; /* sum of L-1                                */
+  double *d_r_list;            /* [B]                                       */
+  uint32_t *d_flags;           /* [B]                                       */
+  int32_t *d_specular;         /* [B] or NULL                               */
+  int32_t *d_num_prop;         /* sum of L+1 or NULL                        */
+  /* lengths (elements) of the packed arrays above: a point whose slices
+   * fall outside them, or outside the workspace, gets EMU_PT_BAD_POINT */
+  int64_t order_len, n_len, h_len, inc_len, rt_len, list_len, np_len;
+} EmuFilmVarBatch;
+
+/* Host-side plan over the host copy of the descriptors: fills rt_off,
+ * list_off, np_off and ws_off, returns the output lengths (elements) and
+ * the workspace bytes, the bounds for max_layers / max_pw, and (when
+ * h_order is not NULL) a costliest-first solve order.  Returns EMU_E_SHAPE
+ * for a point out of range. */
+int emu_film_var_plan(EmuFilmPoint *h_points, int n_points, int32_t *h_order,
+                      int64_t *rt_len, int64_t *list_len, int64_t *np_len,
+                      size_t *workspace_bytes, int *max_layers, int *max_pw);
+int emu_film_var_batch(const EmuFilmVarBatch *p, void *d_workspace, size_t workspace_bytes,
+                       void *stream);
+
 /* Tensor-core GEMM used by the overlap integrals, exposed for testing:
  * C (m x n, FP64) = A (m x k) . B (n x k)^T with both operands split into
  * TF32 hi + lo parts, three tcgen05 MMAs per step (hi.hi + hi.lo + lo.hi),

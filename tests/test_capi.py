@@ -64,3 +64,64 @@ def test_grating_orders_1d_and_errors():
     import ctypes as C
     n = C.c_int(0)
     assert _lib.lib().emu_grating_orders(-1, 1.0, 1.0, 0, None, None, 0, C.byref(n)) == 1
+
+
+def test_film_var_struct_layout_matches_header(tmp_path):
+    """ctypes mirrors of EmuFilmPoint / EmuFilmVarBatch have the C layout."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    from emustack_b200 import _lib
+    gcc = shutil.which('gcc')
+    if gcc is None:
+        pytest.skip('gcc not available')
+    src = tmp_path / 'layout.c'
+    fields = [f for f, _ in _lib.EmuFilmVarBatch._fields_]
+    pfields = [f for f, _ in _lib.EmuFilmPoint._fields_]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "emustack_gsm.h"', 'int main(void){',
+             'printf("%zu %zu\\n", sizeof(EmuFilmPoint), sizeof(EmuFilmVarBatch));']
+    lines += ['printf("%%zu ", offsetof(EmuFilmPoint, %s));' % f for f in pfields]
+    lines += ['printf("\\n");']
+    lines += ['printf("%%zu ", offsetof(EmuFilmVarBatch, %s));' % f for f in fields]
+    lines += ['printf("\\n"); return 0; }']
+    src.write_text('\n'.join(lines))
+    exe = tmp_path / 'layout'
+    subprocess.check_call([gcc, '-I' + os.path.join(ROOT, 'include'), str(src), '-o', str(exe)])
+    out = subprocess.check_output([str(exe)]).decode().split('\n')
+    sp, sb = map(int, out[0].split())
+    assert sp == C.sizeof(_lib.EmuFilmPoint) and sb == C.sizeof(_lib.EmuFilmVarBatch)
+    assert list(map(int, out[1].split())) == [getattr(_lib.EmuFilmPoint, f).offset for f in pfields]
+    assert list(map(int, out[2].split())) == [getattr(_lib.EmuFilmVarBatch, f).offset for f in fields]
+
+
+def test_film_var_plan_offsets_and_order():
+    """emu_film_var_plan packs outputs point after point, sizes the workspace
+    (one slot per point, Npw slots for caller-given incoming vectors) and
+    orders points costliest first (stable on ties)."""
+    import ctypes as C
+    from emustack_b200 import _lib, films
+    shapes = [(3, 5, 0), (12, 25, 0), (2, 1, 0), (12, 25, -1), (5, 9, 2)]
+    desc = np.zeros(len(shapes), films._POINT_DTYPE)
+    for i, (L, npw, pol) in enumerate(shapes):
+        desc[i]['n_layers'], desc[i]['n_pw'], desc[i]['pol'] = L, npw, pol
+        desc[i]['period'] = desc[i]['period_y'] = 600.0
+    order = np.zeros(len(shapes), np.int32)
+    rt, li, npl = C.c_int64(), C.c_int64(), C.c_int64()
+    ws, ml, mp = C.c_size_t(), C.c_int(), C.c_int()
+    st = _lib.lib().emu_film_var_plan(desc.ctypes.data_as(C.c_void_p), len(shapes),
+                                      order.ctypes.data_as(C.c_void_p), C.byref(rt), C.byref(li),
+                                      C.byref(npl), C.byref(ws), C.byref(ml), C.byref(mp))
+    assert st == 0
+    assert rt.value == sum(2 * s[1] for s in shapes)
+    assert li.value == sum(s[0] - 1 for s in shapes)
+    assert npl.value == sum(s[0] + 1 for s in shapes)
+    assert (ml.value, mp.value) == (12, 25)
+    np.testing.assert_array_equal(desc['rt_off'], np.cumsum([0] + [2 * s[1] for s in shapes])[:-1])
+    np.testing.assert_array_equal(desc['list_off'], np.cumsum([0] + [s[0] - 1 for s in shapes])[:-1])
+    per = [(s[1] if s[2] == -1 else 1) * s[0] * 2 * 5 * 16 for s in shapes]
+    np.testing.assert_array_equal(desc['ws_off'], np.cumsum([0] + per)[:-1])
+    assert ws.value == sum(per)
+    assert list(order[:2]) == [1, 3] and order[-1] == 2
+    desc[2]['n_layers'] = 1
+    assert _lib.lib().emu_film_var_plan(desc.ctypes.data_as(C.c_void_p), len(shapes), None,
+                                        None, None, None, None, None, None) == 2
