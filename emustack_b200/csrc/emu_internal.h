@@ -24,10 +24,12 @@ int sm_count();
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Tensor-core split-TF32 GEMM (tc_gemm.cu): C64[Mp][Np] = A[Mp][Kp] . B[Np][Kp]^T
-// from hi/lo FP32 operands; Cpart is scratch of splits * Mp * Np floats.
-int tc_gemm_tf32x3(const float *Ahi, const float *Alo, const float *Bhi, const float *Blo, int Mp,
-                   int Np, int Kp, int splits, float *Cpart, double *C64, int *d_err,
-                   cudaStream_t s);
+// from FP32 operands (split into TF32 hi/lo inside the kernel); Cpart is
+// scratch of splits * Mp * Np floats.
+int tc_gemm_tf32x3(const float *A, const float *B, int Mp, int Np, int Kp, int splits, float *Cpart,
+                   double *C64, int *d_err, cudaStream_t s);
+// output tiles of one K split
+int tc_tiles(int Mp, int Np);
 size_t tc_smem_bytes();
 
 }  // namespace emu

@@ -486,18 +486,11 @@ __global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, const 
 // B (2M x 2K) with B[c*M + n][half*K + el*6 + node] = Re/Im sol(c, node, n, el),
 // both split into TF32 hi + lo.  C = A B^T then holds Re G (rows 0..npw-1) and
 // Im G (rows npw..2npw-1).
-__device__ __forceinline__ void tf32_split(double x, float &hi, float &lo) {
-  const float f = (float)x;
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
-  hi = __uint_as_float(h);
-  const float r = (float)(x - (double)hi);
-  uint32_t l;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
-  lo = __uint_as_float(l);
-}
-
-__global__ void make_A_kernel(const cd *E, int npw, long long K, int conj, float *Ahi, float *Alo) {
+// Real embedding of the complex contraction G = E~ . S as one real GEMM
+// C[2 npw][2 M] = A[2 npw][2 K] . B[2 M][2 K]^T, operands in FP32:
+//   A rows s (Re) and npw + s (Im): [Re E, -Im E] and [Im E, Re E]
+//   B rows c * M + m: [Re S, Im S]
+__global__ void make_A_kernel(const cd *E, int npw, long long K, int conj, float *A) {
   const long long total = 2LL * npw * 2 * K;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
@@ -508,11 +501,11 @@ __global__ void make_A_kernel(const cd *E, int npw, long long K, int conj, float
     cd e = E[(size_t)s * K + kk];
     if (conj) e.y = -e.y;
     const double v = (part == 0) ? (half == 0 ? e.x : -e.y) : (half == 0 ? e.y : e.x);
-    tf32_split(v, Ahi[i], Alo[i]);
+    A[i] = (float)v;
   }
 }
 
-__global__ void make_B_kernel(const cd *sol, int nval, long e0, long ne, float *Bhi, float *Blo) {
+__global__ void make_B_kernel(const cd *sol, int nval, long e0, long ne, float *B) {
   const long long K = 6LL * ne;
   const long long total = 2LL * nval * 2 * K;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
@@ -524,7 +517,7 @@ __global__ void make_B_kernel(const cd *sol, int nval, long e0, long ne, float *
     const long el = (long)(kk / 6);
     const int node = (int)(kk % 6);
     const cd v = sol[((size_t)(e0 + el) * nval + mode) * 39 + node * 3 + c];
-    tf32_split(half == 0 ? v.x : v.y, Bhi[i], Blo[i]);
+    B[i] = (float)(half == 0 ? v.x : v.y);
   }
 }
 
@@ -538,9 +531,10 @@ __global__ void pack_G_kernel(const double *C64, int npw, int n2, cd *acc, int f
   }
 }
 
+// K splits so that tiles x splits fills one wave of CTAs (one per SM)
 int tc_splits(int npw, int M, long long K2) {
-  const int tiles = (int)(((2LL * M + 127) / 128) * ((2LL * npw + 127) / 128));
-  int sp = (2 * emu::sm_count() + tiles - 1) / tiles;
+  const int tiles = emu::tc_tiles(2 * npw, 2 * M);
+  int sp = emu::sm_count() / tiles;
   const int maxsp = (int)(K2 / 256 > 0 ? K2 / 256 : 1);
   if (sp > maxsp) sp = maxsp;
   if (sp > 64) sp = 64;
@@ -640,8 +634,8 @@ extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
   b += align_up(sizeof(cd) * nparts * npw * 2 * M, 256);     // partials
   if (p->precision == 1) {
     const long long K2 = 12 * ne;
-    b += align_up(sizeof(float) * 2 * (2 * npw) * K2, 256);   // A hi, lo
-    b += align_up(sizeof(float) * 2 * (2 * M) * K2, 256);     // B hi, lo
+    b += align_up(sizeof(float) * (2 * npw) * K2, 256);       // A (FP32)
+    b += align_up(sizeof(float) * (2 * M) * K2, 256);         // B (FP32)
     b += align_up(sizeof(float) * 64 * (2 * npw) * (2 * M), 256);  // split partials
     b += align_up(sizeof(double) * (2 * npw) * (2 * M), 256);  // C64
     b += 256;                                                   // error flag
@@ -682,15 +676,13 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   cd *parts = (cd *)take(sizeof(cd) * (size_t)nparts * npw * 2 * M);
   const long long gsz = (long long)npw * 2 * M;
   if (p->precision != 0 && p->precision != 1) return EMU_E_ARG;
-  float *Ahi = nullptr, *Alo = nullptr, *Bhi = nullptr, *Blo = nullptr, *Cpart = nullptr;
+  float *A32 = nullptr, *B32 = nullptr, *Cpart = nullptr;
   double *C64 = nullptr;
   int *terr = nullptr;
   if (p->precision == 1) {
     const long long K2 = 12 * nec;
-    Ahi = (float *)take(sizeof(float) * 2 * (2 * (size_t)npw) * K2);
-    Alo = Ahi + (2 * (size_t)npw) * K2;
-    Bhi = (float *)take(sizeof(float) * 2 * (2 * (size_t)M) * K2);
-    Blo = Bhi + (2 * (size_t)M) * K2;
+    A32 = (float *)take(sizeof(float) * (2 * (size_t)npw) * K2);
+    B32 = (float *)take(sizeof(float) * (2 * (size_t)M) * K2);
     Cpart = (float *)take(sizeof(float) * 64 * (2 * (size_t)npw) * (2 * M));
     C64 = (double *)take(sizeof(double) * (2 * (size_t)npw) * (2 * M));
     terr = p->d_error ? (int *)p->d_error : (int *)take(256);
@@ -747,13 +739,13 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
           const long long K = 6 * ne;
           const long long na = 2LL * npw * 2 * K, nb = 2LL * M * 2 * K;
           make_A_kernel<<<(int)((na + 255) / 256 < 16 * sms ? (na + 255) / 256 : 16 * sms), 256, 0, s>>>(
-              E, npw, K, pass, Ahi, Alo);
+              E, npw, K, pass, A32);
           make_B_kernel<<<(int)((nb + 255) / 256 < 16 * sms ? (nb + 255) / 256 : 16 * sms), 256, 0, s>>>(
-              sol, M, e0, ne, Bhi, Blo);
+              sol, M, e0, ne, B32);
           emu::note_launch(2);
           const int sp = tc_splits(npw, M, 2 * K);
-          const int tst = emu::tc_gemm_tf32x3(Ahi, Alo, Bhi, Blo, 2 * npw, 2 * M, (int)(2 * K), sp, Cpart,
-                                              C64, terr, s);
+          const int tst = emu::tc_gemm_tf32x3(A32, B32, 2 * npw, 2 * M, (int)(2 * K), sp, Cpart, C64,
+                                              terr, s);
           if (tst != EMU_OK) return tst;
           const long long rgs = (gsz + 255) / 256;
           pack_G_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(C64, npw, 2 * M, acc, first);
