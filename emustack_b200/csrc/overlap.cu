@@ -171,6 +171,9 @@ struct EtArgs {
   const double *bloch;  // this problem's k_parallel * period (2 values)
   cd *E;
   long long ldE;
+  // tensor-core path: instead of E, the real embedding A (FP32,
+  // [2 npw][2 K], K = 6 ne): row s = [Re E, -Im E], row npw + s = [Im E, Re E]
+  float *A32;
 };
 
 constexpr int kEtWarps = 4;
@@ -236,9 +239,22 @@ __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
             acc[k].y = fma(e.y, c_phi2[q][k], acc[k].y);
           }
         }
-        cd *row = a.E + (size_t)a.pos[s] * a.ldE + (size_t)el * 6;
+        if (a.A32) {
+          const long long K = 6LL * a.ne;
+          float *r0 = a.A32 + (size_t)a.pos[s] * 2 * K + (size_t)el * 6;
+          float *r1 = r0 + (size_t)a.npw * 2 * K;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) row[k] = acc[k];
+          for (int k = 0; k < 6; ++k) {
+            r0[k] = (float)acc[k].x;
+            r0[K + k] = (float)(-acc[k].y);
+            r1[k] = (float)acc[k].y;
+            r1[K + k] = (float)acc[k].x;
+          }
+        } else {
+          cd *row = a.E + (size_t)a.pos[s] * a.ldE + (size_t)el * 6;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) row[k] = acc[k];
+        }
       }
     }
     __syncwarp();
@@ -486,54 +502,74 @@ __global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, const 
 // B (2M x 2K) with B[c*M + n][half*K + el*6 + node] = Re/Im sol(c, node, n, el),
 // both split into TF32 hi + lo.  C = A B^T then holds Re G (rows 0..npw-1) and
 // Im G (rows npw..2npw-1).
-// Real embedding of the complex contraction G = E~ . S as one real GEMM
-// C[2 npw][2 M] = A[2 npw][2 K] . B[2 M][2 K]^T, operands in FP32:
-//   A rows s (Re) and npw + s (Im): [Re E, -Im E] and [Im E, Re E]
-//   B rows c * M + m: [Re S, Im S]
-__global__ void make_A_kernel(const cd *E, int npw, long long K, int conj, float *A) {
-  const long long total = 2LL * npw * 2 * K;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long r = i / (2 * K), kp = i % (2 * K);
-    const int s = (int)(r % npw), part = (int)(r / npw);
-    const long long kk = kp % K;
-    const int half = (int)(kp / K);
-    cd e = E[(size_t)s * K + kk];
-    if (conj) e.y = -e.y;
-    const double v = (part == 0) ? (half == 0 ? e.x : -e.y) : (half == 0 ? e.y : e.x);
-    A[i] = (float)v;
-  }
-}
+// Tensor-core path: the complex contractions G = E~ . S1 and
+// G_dag = conj(E~) . S2 = conj(E~ . conj(S2)) share one real GEMM
+//   C[2 npw][Nb] = A[2 npw][2 K] . B[Nb][2 K]^T
+// with A from etable_kernel (A32 output) and B rows
+//   c * M + m          = [Re S1, Im S1]   (c = 0, 1: x, y component)
+//   off1 + c * M + m   = [Re S2, -Im S2]  (off1 = 2 M when S1 is present)
+// B tile builder: 8 modes x 16 elements per CTA; the 12 transverse values
+// (node 0-5, component 0-1) of each (element, mode) record are read with
+// consecutive lanes, staged in shared memory and written as rows of
+// 96 contiguous floats per half.
+constexpr int kBModes = 8, kBElems = 16;
 
-__global__ void make_B_kernel(const cd *sol, int nval, long e0, long ne, float *B) {
+__global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, long e0, long ne,
+                                                     int conj, int row0, float *B) {
+  __shared__ cd v[kBModes][kBElems][12];
   const long long K = 6LL * ne;
-  const long long total = 2LL * nval * 2 * K;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long n = i / (2 * K), kp = i % (2 * K);
-    const int c = (int)(n / nval), mode = (int)(n % nval);
-    const long long kk = kp % K;
-    const int half = (int)(kp / K);
-    const long el = (long)(kk / 6);
-    const int node = (int)(kk % 6);
-    const cd v = sol[((size_t)(e0 + el) * nval + mode) * 39 + node * 3 + c];
-    B[i] = (float)(half == 0 ? v.x : v.y);
+  const int m0 = blockIdx.x * kBModes;
+  const long el0 = (long)blockIdx.y * kBElems;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // load: warp w takes mode m0 + w, two elements per step (lanes 0-23)
+  const int m = m0 + w;
+  if (lane < 24) {
+    const int j = lane % 12, eo = lane / 12;
+    const int node = j >> 1, c = j & 1;
+    for (int e = eo; e < kBElems; e += 2) {
+      const long el = el0 + e;
+      cd x = cd{0.0, 0.0};
+      if (m < nval && el < ne) x = sol[((size_t)(e0 + el) * nval + m) * 39 + node * 3 + c];
+      v[w][e][j] = x;
+    }
+  }
+  __syncthreads();
+  // write: 16 rows (c, mode) x 2 halves x 96 floats (element-major, node-minor)
+  const int nel_here = (int)(ne - el0 < kBElems ? ne - el0 : kBElems);
+  for (int i = threadIdx.x; i < 2 * kBModes * 2 * 96; i += 256) {
+    const int within = i % 96, rh = i / 96;
+    const int half = rh & 1, r = rh >> 1;
+    const int c = r / kBModes, mm = r % kBModes;
+    const int e = within / 6, node = within % 6;
+    if (m0 + mm >= nval || e >= nel_here) continue;
+    const cd x = v[mm][e][node * 2 + c];
+    const float val = half == 0 ? (float)x.x : (float)(conj ? -x.y : x.y);
+    B[(size_t)(row0 + c * nval + m0 + mm) * 2 * K + (size_t)half * K + (size_t)(el0 + e) * 6 + node] = val;
   }
 }
 
-__global__ void pack_G_kernel(const double *C64, int npw, int n2, cd *acc, int first) {
+// G (+)= C[:, 0:2M] ; G_dag (+)= conj(C[:, off1:off1+2M])
+__global__ void pack_G_kernel(const double *C64, int npw, int nb, int n2, cd *G, cd *Gd, int off1,
+                              int first) {
   const long long total = (long long)npw * n2;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const long long s = i / n2, n = i % n2;
-    const cd g = cd{C64[(size_t)s * n2 + n], C64[(size_t)(npw + s) * n2 + n]};
-    acc[i] = first ? g : cadd(acc[i], g);
+    const int s = (int)(i / n2), n = (int)(i % n2);
+    const double *r0 = C64 + (size_t)s * nb, *r1 = C64 + (size_t)(npw + s) * nb;
+    if (G) {
+      const cd g = cd{r0[n], r1[n]};
+      G[i] = first ? g : cadd(G[i], g);
+    }
+    if (Gd) {
+      const cd g = cd{r0[off1 + n], -r1[off1 + n]};
+      Gd[i] = first ? g : cadd(Gd[i], g);
+    }
   }
 }
 
 // K splits so that tiles x splits fills one wave of CTAs (one per SM)
-int tc_splits(int npw, int M, long long K2) {
-  const int tiles = emu::tc_tiles(2 * npw, 2 * M);
+int tc_splits(int npw, int nb, long long K2) {
+  const int tiles = emu::tc_tiles(2 * npw, nb);
   int sp = emu::sm_count() / tiles;
   const int maxsp = (int)(K2 / 256 > 0 ? K2 / 256 : 1);
   if (sp > maxsp) sp = maxsp;
@@ -635,9 +671,9 @@ extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
   if (p->precision == 1) {
     const long long K2 = 12 * ne;
     b += align_up(sizeof(float) * (2 * npw) * K2, 256);       // A (FP32)
-    b += align_up(sizeof(float) * (2 * M) * K2, 256);         // B (FP32)
-    b += align_up(sizeof(float) * 64 * (2 * npw) * (2 * M), 256);  // split partials
-    b += align_up(sizeof(double) * (2 * npw) * (2 * M), 256);  // C64
+    b += align_up(sizeof(float) * (4 * M) * K2, 256);         // B (FP32), both field sets
+    b += align_up(sizeof(float) * 64 * (2 * npw) * (4 * M), 256);  // split partials
+    b += align_up(sizeof(double) * (2 * npw) * (4 * M), 256);  // C64
     b += 256;                                                   // error flag
   }
   return b + 256;
@@ -682,9 +718,9 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   if (p->precision == 1) {
     const long long K2 = 12 * nec;
     A32 = (float *)take(sizeof(float) * (2 * (size_t)npw) * K2);
-    B32 = (float *)take(sizeof(float) * (2 * (size_t)M) * K2);
-    Cpart = (float *)take(sizeof(float) * 64 * (2 * (size_t)npw) * (2 * M));
-    C64 = (double *)take(sizeof(double) * (2 * (size_t)npw) * (2 * M));
+    B32 = (float *)take(sizeof(float) * (4 * (size_t)M) * K2);
+    Cpart = (float *)take(sizeof(float) * 64 * (2 * (size_t)npw) * (4 * M));
+    C64 = (double *)take(sizeof(double) * (2 * (size_t)npw) * (4 * M));
     terr = p->d_error ? (int *)p->d_error : (int *)take(256);
     if (!p->d_error && cudaMemsetAsync(terr, 0, sizeof(int), (cudaStream_t)stream) != cudaSuccess)
       return EMU_E_CUDA;
@@ -710,49 +746,64 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
     pa.out_inv = p->d_index_pw_inv ? p->d_index_pw_inv + (size_t)b * npw : nullptr;
     pw_setup_kernel<<<1, 256, sizeof(double) * npw, s>>>(pa);
     emu::note_launch();
-    for (int pass = 0; pass < 2; ++pass) {
-      const cd *sol = (const cd *)(pass == 0 ? p->d_sol1 : p->d_sol2);
-      if (!sol) continue;
-      sol += (size_t)b * p->nel * M * 39;
-      cd *acc = pass == 0 ? G : Gd;
+    auto et_args = [&](long e0, long ne) {
+      EtArgs ea;
+      ea.npw = npw;
+      ea.mo = p->max_order;
+      ea.e0 = (int)e0;
+      ea.ne = (int)ne;
+      ea.px = p->d_px;
+      ea.py = p->d_py;
+      ea.pos = pos;
+      ea.x = p->d_x;
+      ea.tn = p->d_table_nod;
+      ea.d = p->d;
+      ea.dy = p->dy;
+      ea.bloch = p->d_bloch + 2 * b;
+      ea.E = E;
+      ea.ldE = 6 * ne;
+      ea.A32 = nullptr;
+      return ea;
+    };
+    const cd *sol1 = p->d_sol1 ? (const cd *)p->d_sol1 + (size_t)b * p->nel * M * 39 : nullptr;
+    const cd *sol2 = p->d_sol2 ? (const cd *)p->d_sol2 + (size_t)b * p->nel * M * 39 : nullptr;
+    if (p->precision == 1) {
+      // both contractions per element chunk: one E~ table (as the FP32 A
+      // operand), one B with the two field sets, one tensor-core GEMM
+      const int nb = (sol1 ? 2 * M : 0) + (sol2 ? 2 * M : 0);
+      const int off1 = sol1 ? 2 * M : 0;
       int first = 1;
       for (long e0 = 0; e0 < p->nel; e0 += nec) {
         const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
-        EtArgs ea;
-        ea.npw = npw;
-        ea.mo = p->max_order;
-        ea.e0 = (int)e0;
-        ea.ne = (int)ne;
-        ea.px = p->d_px;
-        ea.py = p->d_py;
-        ea.pos = pos;
-        ea.x = p->d_x;
-        ea.tn = p->d_table_nod;
-        ea.d = p->d;
-        ea.dy = p->dy;
-        ea.bloch = p->d_bloch + 2 * b;
-        ea.E = E;
-        ea.ldE = 6 * ne;
+        const long long K = 6 * ne;
+        EtArgs ea = et_args(e0, ne);
+        ea.A32 = A32;
         const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
         etable_kernel<<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
-        if (p->precision == 1) {
-          const long long K = 6 * ne;
-          const long long na = 2LL * npw * 2 * K, nb = 2LL * M * 2 * K;
-          make_A_kernel<<<(int)((na + 255) / 256 < 16 * sms ? (na + 255) / 256 : 16 * sms), 256, 0, s>>>(
-              E, npw, K, pass, A32);
-          make_B_kernel<<<(int)((nb + 255) / 256 < 16 * sms ? (nb + 255) / 256 : 16 * sms), 256, 0, s>>>(
-              sol, M, e0, ne, B32);
-          emu::note_launch(2);
-          const int sp = tc_splits(npw, M, 2 * K);
-          const int tst = emu::tc_gemm_tf32x3(A32, B32, 2 * npw, 2 * M, (int)(2 * K), sp, Cpart, C64,
-                                              terr, s);
-          if (tst != EMU_OK) return tst;
-          const long long rgs = (gsz + 255) / 256;
-          pack_G_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(C64, npw, 2 * M, acc, first);
-          emu::note_launch();
-          first = 0;
-          continue;
-        }
+        const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems));
+        if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1, M, e0, ne, 0, 0, B32);
+        if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2, M, e0, ne, 1, off1, B32);
+        emu::note_launch(1 + (sol1 ? 1 : 0) + (sol2 ? 1 : 0));
+        const int sp = tc_splits(npw, nb, 2 * K);
+        const int tst = emu::tc_gemm_tf32x3(A32, B32, 2 * npw, nb, (int)(2 * K), sp, Cpart, C64, terr, s);
+        if (tst != EMU_OK) return tst;
+        const long long rgs = (gsz + 255) / 256;
+        pack_G_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(
+            C64, npw, nb, 2 * M, sol1 ? G : nullptr, sol2 ? Gd : nullptr, off1, first);
+        emu::note_launch();
+        first = 0;
+      }
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      const cd *sol = pass == 0 ? sol1 : sol2;
+      if (!sol) continue;
+      cd *acc = pass == 0 ? G : Gd;
+      int first = 1;
+      for (long e0 = 0; e0 < p->nel && p->precision == 0; e0 += nec) {
+        const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
+        EtArgs ea = et_args(e0, ne);
+        const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
+        etable_kernel<<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
         const long long rn = ne * 6 * 2 * (long long)M;
         const long long rg = (rn + 255) / 256;
         repack_kernel<<<(int)(rg < 16 * sms ? rg : 16 * sms), 256, 0, s>>>(sol, M, e0, ne, S);
