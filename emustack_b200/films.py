@@ -207,7 +207,7 @@ class FilmPoint(object):
     """
 
     __slots__ = ('n', 'heights', 'wl_nm', 'k_pll', 'period', 'period_y', 'max_order', 'pol',
-                 'world_1d', 'incoming')
+                 'world_1d', 'incoming', '_rec')
 
     def __init__(self, n, heights, wl_nm, k_pll, period, max_order, pol='TE', period_y=None,
                  world_1d=False, incoming=None):
@@ -228,16 +228,48 @@ class FilmPoint(object):
             raise NotImplementedError('Must select from the currently implemented polarisations; '
                                       'TE, TM, R Circ, L Circ.')
         self.pol = pol
+        # packing record: order-set key, then the descriptor scalars
+        self._rec = ((self.max_order, self.period, self.period_y, self.world_1d), len(self.n),
+                     int(self.world_1d), _lib.POL_INCOMING if self.incoming is not None else _lib.POL[pol],
+                     self.period, self.period_y, self.wl_nm, float(self.k_pll[0]), float(self.k_pll[1]))
+
+
+class _Grow(object):
+    """A growable buffer (pinned host or device) handing out views."""
+
+    def __init__(self, dtype, device=None, pinned=False):
+        self.dtype, self.device, self.pinned = dtype, device, pinned
+        self.t = None
+
+    def get(self, n):
+        n = max(int(n), 1)
+        if self.t is None or self.t.numel() < n:
+            cap = max(n, 2 * (self.t.numel() if self.t is not None else 0))
+            if self.pinned:
+                self.t = torch.empty(cap, dtype=self.dtype).pin_memory()
+            else:
+                self.t = torch.empty(cap, dtype=self.dtype, device=self.device)
+        return self.t[:n]
+
+
+class FilmVarPlan(object):
+    """Host side of one uneven batch: descriptors and packed inputs in the
+    solver's pinned staging buffers (valid until the solver plans again)."""
+
+    __slots__ = ('B', 'desc', 'max_layers', 'max_pw', 'rt_len', 'list_len', 'np_len', 'ws_bytes',
+                 'n_len', 'h_len', 'inc_len', 'h_desc', 'h_order', 'h_n', 'h_h', 'h_inc')
 
 
 class FilmVarSolver(object):
     """All-film points of mixed shapes in one launch (``emu_film_var_batch``).
 
-    ``plan(points)`` packs the points on the host (pinned memory),
+    ``plan(points)`` packs the points into pinned host staging buffers,
     ``solve(plan)`` copies them to the device, launches once and returns the
-    packed device outputs, ``unpack(plan, out)`` splits host copies of them
-    per point.  Order sets are built once per (max_order, period, period_y,
-    world_1d) and shared by every point that uses them.
+    packed device outputs, ``fetch(plan, out)`` copies those back into pinned
+    host buffers, ``unpack(plan, host)`` splits host arrays per point.
+    Order sets are built once per (max_order, period, period_y, world_1d)
+    and shared by every point that uses them.  Staging, device and
+    workspace buffers grow and are reused: one solver serves one stream.
     """
 
     def __init__(self, device='cuda'):
@@ -246,7 +278,17 @@ class FilmVarSolver(object):
         self._px, self._py = [], []
         self._n_orders = 0
         self._d_orders = None
-        self._ws = None
+        self._ws = _Grow(torch.uint8, self.device)
+        self._hs = {k: _Grow(dt, pinned=True) for k, dt in (
+            ('desc', torch.uint8), ('order', torch.int32), ('n', torch.complex128),
+            ('h', torch.float64), ('inc', torch.complex128))}
+        self._ds = {k: _Grow(g.dtype, self.device) for k, g in self._hs.items()}
+        self._out = {k: _Grow(dt, self.device) for k, dt in self._OUT}
+        self._hout = {k: _Grow(dt, pinned=True) for k, dt in self._OUT}
+
+    _OUT = (('R_net', torch.complex128), ('T_net', torch.complex128), ('a_list', torch.float64),
+            ('t_list', torch.float64), ('r_list', torch.float64), ('flags', torch.int32),
+            ('specular', torch.int32), ('num_prop', torch.int32))
 
     def _order_off(self, key):
         hit = self._orders.get(key)
@@ -268,113 +310,121 @@ class FilmVarSolver(object):
                               torch.from_numpy(py).to(self.device))
         return self._d_orders
 
+    _REC = np.dtype([('n_layers', np.int64), ('world_1d', np.int32), ('pol', np.int32),
+                     ('period', np.float64), ('period_y', np.float64), ('wl_nm', np.float64),
+                     ('kx', np.float64), ('ky', np.float64)])
+
     def plan(self, points):
         B = len(points)
+        orders = self._orders
+        recs = [p._rec for p in points]
+        oo = [orders.get(r[0]) or self._order_off(r[0]) for r in recs]
+        sc = np.array([r[1:] for r in recs], self._REC) if B else np.zeros(0, self._REC)
+        Ls = sc['n_layers']
+        npw = np.fromiter((o[1] for o in oo), np.int64, B)
         desc = np.zeros(B, _POINT_DTYPE)
-        n_parts, h_parts, inc_parts = [], [], []
-        n_off = h_off = inc_off = 0
-        for i, p in enumerate(points):
-            o_off, npw = self._order_off((p.max_order, p.period, p.period_y, p.world_1d))
-            L = len(p.n)
-            d = desc[i]
-            d['n_layers'], d['n_pw'], d['world_1d'] = L, npw, int(p.world_1d)
-            d['order_off'], d['n_off'], d['h_off'] = o_off, n_off, h_off
-            d['period'], d['period_y'], d['wl_nm'] = p.period, p.period_y, p.wl_nm
-            d['kx'], d['ky'] = p.k_pll[0], p.k_pll[1]
-            n_parts.append(p.n)
-            n_off += L
-            h_parts.append(p.heights)
-            h_off += L - 2
-            if p.incoming is not None:
-                if p.incoming.shape != (2 * npw,):
-                    raise ValueError('incoming must have 2 Npw = %d entries' % (2 * npw))
-                d['pol'] = _lib.POL_INCOMING
-                d['inc_off'] = inc_off
+        for f in ('n_layers', 'world_1d', 'pol', 'period', 'period_y', 'wl_nm', 'kx', 'ky'):
+            desc[f] = sc[f]
+        desc['n_pw'] = npw
+        desc['order_off'] = np.fromiter((o[0] for o in oo), np.int64, B)
+        desc['n_off'] = np.cumsum(Ls) - Ls
+        desc['h_off'] = np.cumsum(Ls - 2) - (Ls - 2)
+        inc_parts, inc_off = [], 0
+        if B and (sc['pol'] == _lib.POL_INCOMING).any():
+            inc_offs = np.zeros(B, np.int64)
+            for i in np.nonzero(sc['pol'] == _lib.POL_INCOMING)[0]:
+                p = points[i]
+                if p.incoming.shape != (2 * npw[i],):
+                    raise ValueError('incoming must have 2 Npw = %d entries' % (2 * npw[i]))
+                inc_offs[i] = inc_off
                 inc_parts.append(p.incoming)
-                inc_off += 2 * npw
-            else:
-                d['pol'] = _lib.POL[p.pol]
-        order = np.zeros(B, np.int32)
+                inc_off += 2 * int(npw[i])
+            desc['inc_off'] = inc_offs
+        pl = FilmVarPlan()
+        pl.B = B
+        h_order = self._hs['order'].get(B)
         rt_len, list_len, np_len = C.c_int64(), C.c_int64(), C.c_int64()
         ws_bytes, max_l, max_pw = C.c_size_t(), C.c_int(), C.c_int()
         check(lib().emu_film_var_plan(desc.ctypes.data_as(C.c_void_p), B,
-                                      order.ctypes.data_as(C.c_void_p), C.byref(rt_len),
+                                      C.c_void_p(h_order.data_ptr()), C.byref(rt_len),
                                       C.byref(list_len), C.byref(np_len), C.byref(ws_bytes),
                                       C.byref(max_l), C.byref(max_pw)), 'emu_film_var_plan')
-
-        def pinned(parts, dtype, npdtype):
-            a = np.concatenate(parts).astype(npdtype) if parts else np.zeros(0, npdtype)
-            t = torch.empty(max(a.size, 1), dtype=dtype).pin_memory()
-            t.numpy()[:a.size] = a
-            return t, a.size
-
-        pl = {
-            'B': B, 'desc': desc, 'max_layers': max_l.value, 'max_pw': max_pw.value,
-            'rt_len': rt_len.value, 'list_len': list_len.value, 'np_len': np_len.value,
-            'ws_bytes': ws_bytes.value,
-        }
-        pl['h_desc'] = torch.from_numpy(desc.view(np.uint8).copy()).pin_memory()
-        pl['h_order'] = torch.from_numpy(order).pin_memory()
-        pl['h_n'], pl['n_len'] = pinned(n_parts, torch.complex128, np.complex128)
-        pl['h_h'], pl['h_len'] = pinned(h_parts, torch.float64, np.float64)
-        pl['h_inc'], pl['inc_len'] = pinned(inc_parts, torch.complex128, np.complex128)
+        pl.desc = desc
+        pl.max_layers, pl.max_pw = max_l.value, max_pw.value
+        pl.rt_len, pl.list_len, pl.np_len = rt_len.value, list_len.value, np_len.value
+        pl.ws_bytes = ws_bytes.value
+        pl.h_order = h_order
+        pl.h_desc = self._hs['desc'].get(desc.nbytes)
+        pl.h_desc.numpy()[:] = desc.view(np.uint8)
+        pl.n_len = int(Ls.sum())
+        pl.h_n = self._hs['n'].get(pl.n_len)
+        pl.h_n.numpy()[:pl.n_len] = np.concatenate([p.n for p in points]) if B else []
+        pl.h_len = int((Ls - 2).sum())
+        pl.h_h = self._hs['h'].get(pl.h_len)
+        if pl.h_len:
+            pl.h_h.numpy()[:pl.h_len] = np.concatenate([p.heights for p in points])
+        pl.inc_len = inc_off
+        pl.h_inc = self._hs['inc'].get(inc_off)
+        if inc_off:
+            pl.h_inc.numpy()[:inc_off] = np.concatenate(inc_parts)
         return pl
-
-    def workspace(self, nbytes):
-        if self._ws is None or self._ws.numel() < nbytes:
-            self._ws = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
-        return self._ws
 
     def solve(self, pl, stream=None, want_num_prop=False):
         """Copy a plan to the device and solve it in one launch; returns
         device tensors R_net/T_net [rt_len], a_list/t_list [list_len],
-        r_list/flags/specular [B] (and num_prop [np_len])."""
+        r_list/flags/specular [B] (and num_prop [np_len]), views of buffers
+        this solver reuses."""
         dev = self.device
         px, py = self._device_orders()
         s = stream if stream is not None else torch.cuda.current_stream(dev)
+        B = pl.B
         with torch.cuda.stream(s):
-            d_desc = pl['h_desc'].to(dev, non_blocking=True)
-            d_order = pl['h_order'].to(dev, non_blocking=True)
-            d_n = pl['h_n'].to(dev, non_blocking=True)
-            d_h = pl['h_h'].to(dev, non_blocking=True)
-            d_inc = pl['h_inc'].to(dev, non_blocking=True)
-            B = pl['B']
-            out = {
-                'R_net': torch.empty(max(pl['rt_len'], 1), dtype=torch.complex128, device=dev),
-                'T_net': torch.empty(max(pl['rt_len'], 1), dtype=torch.complex128, device=dev),
-                'a_list': torch.empty(max(pl['list_len'], 1), dtype=torch.float64, device=dev),
-                't_list': torch.empty(max(pl['list_len'], 1), dtype=torch.float64, device=dev),
-                'r_list': torch.empty(max(B, 1), dtype=torch.float64, device=dev),
-                'flags': torch.empty(max(B, 1), dtype=torch.int32, device=dev),
-                'specular': torch.empty(max(B, 1), dtype=torch.int32, device=dev),
-            }
-            if want_num_prop:
-                out['num_prop'] = torch.empty(max(pl['np_len'], 1), dtype=torch.int32, device=dev)
-            ws = self.workspace(pl['ws_bytes'])
-            d = _lib.EmuFilmVarBatch()
-            d.n_points = B
-            d.max_layers, d.max_pw = pl['max_layers'], pl['max_pw']
-            d.d_points, d.d_order = ptr(d_desc), ptr(d_order)
-            d.d_px, d.d_py = ptr(px), ptr(py)
-            d.d_n, d.d_heights_nm, d.d_incoming = ptr(d_n), ptr(d_h), ptr(d_inc)
-            d.d_R_net, d.d_T_net = ptr(out['R_net']), ptr(out['T_net'])
-            d.d_a_list, d.d_t_list = ptr(out['a_list']), ptr(out['t_list'])
-            d.d_r_list, d.d_flags = ptr(out['r_list']), ptr(out['flags'])
-            d.d_specular = ptr(out['specular'])
-            d.d_num_prop = ptr(out.get('num_prop'))
-            d.order_len = self._n_orders
-            d.n_len, d.h_len, d.inc_len = pl['n_len'], pl['h_len'], pl['inc_len']
-            d.rt_len, d.list_len, d.np_len = pl['rt_len'], pl['list_len'], pl['np_len']
-            check(lib().emu_film_var_batch(C.byref(d), ptr(ws), C.c_size_t(ws.numel()),
+            d = {}
+            for k, h in (('desc', pl.h_desc), ('order', pl.h_order), ('n', pl.h_n), ('h', pl.h_h),
+                         ('inc', pl.h_inc)):
+                d[k] = self._ds[k].get(h.numel())
+                d[k].copy_(h, non_blocking=True)
+            lens = dict(R_net=pl.rt_len, T_net=pl.rt_len, a_list=pl.list_len, t_list=pl.list_len,
+                        r_list=B, flags=B, specular=B, num_prop=pl.np_len)
+            out = {k: self._out[k].get(lens[k]) for k, _ in self._OUT
+                   if k != 'num_prop' or want_num_prop}
+            ws = self._ws.get(pl.ws_bytes)
+            e = _lib.EmuFilmVarBatch()
+            e.n_points = B
+            e.max_layers, e.max_pw = pl.max_layers, pl.max_pw
+            e.d_points, e.d_order = ptr(d['desc']), ptr(d['order'])
+            e.d_px, e.d_py = ptr(px), ptr(py)
+            e.d_n, e.d_heights_nm, e.d_incoming = ptr(d['n']), ptr(d['h']), ptr(d['inc'])
+            e.d_R_net, e.d_T_net = ptr(out['R_net']), ptr(out['T_net'])
+            e.d_a_list, e.d_t_list = ptr(out['a_list']), ptr(out['t_list'])
+            e.d_r_list, e.d_flags = ptr(out['r_list']), ptr(out['flags'])
+            e.d_specular = ptr(out['specular'])
+            e.d_num_prop = ptr(out.get('num_prop'))
+            e.order_len = self._n_orders
+            e.n_len, e.h_len, e.inc_len = pl.n_len, pl.h_len, pl.inc_len
+            e.rt_len, e.list_len, e.np_len = pl.rt_len, pl.list_len, pl.np_len
+            check(lib().emu_film_var_batch(C.byref(e), ptr(ws), C.c_size_t(ws.numel()),
                                            stream_ptr(s)), 'emu_film_var_batch')
-            out['_keep'] = (d_desc, d_order, d_n, d_h, d_inc)
         return out
+
+    def fetch(self, out, stream=None):
+        """Asynchronous copies of packed device outputs into pinned host
+        buffers of this solver; returns numpy views (valid once the stream
+        reaches this point, until the next fetch)."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        host = {}
+        with torch.cuda.stream(s):
+            for k, t in out.items():
+                h = self._hout[k].get(t.numel())
+                h.copy_(t, non_blocking=True)
+                host[k] = h.numpy()
+        return host
 
     @staticmethod
     def unpack(pl, host):
         """Split host copies (numpy) of the packed outputs per point."""
         res = []
-        for i, d in enumerate(pl['desc']):
+        for i, d in enumerate(pl.desc):
             P, L = 2 * int(d['n_pw']), int(d['n_layers'])
             ro, lo = int(d['rt_off']), int(d['list_off'])
             r = {

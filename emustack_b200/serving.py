@@ -1,82 +1,159 @@
 """Continuous-batching server for GSM solves on one GPU.
 
-Requests (one spectral point of a stack each) arrive at any time; a
-scheduler thread groups the waiting ones by shape signature, admits as many
-as fit the HBM budget into one device batch, and launches it on a free
-stream while earlier batches are still running.  Each batch is one fused
-launch of the film kernel (``emu_film_stack_batch``) between an async
-host-to-device copy of its inputs and a device-to-host copy of its results;
-a request's latency runs from ``submit`` to the moment the scheduler sees
-its batch's completion event.  Results do not depend on the batch a point
-lands in (the film kernel treats every point independently, in a fixed
-order of operations), which ``tests/test_gpu_serving.py`` checks.
+Requests (one spectral point of an all-film stack each, any shape) arrive at
+any time; a scheduler thread admits waiting requests into a device batch as
+long as the batch fits the HBM budget left by the batches still in flight,
+and launches it on a free stream while earlier batches are still running.
+
+Two batching modes:
+
+* ``'mixed'`` (default): a batch takes requests in arrival order whatever
+  their shape (layer count, order set, periods, polarisation) and runs as one
+  launch of the uneven-batch film kernel (``emu_film_var_batch``, one warp
+  per point);
+* ``'grouped'``: requests are grouped by shape signature and each batch is
+  one launch of the uniform film kernel (``emu_film_stack_batch``).
+
+Each batch is an async host-to-device copy of its packed inputs, one kernel,
+and an async device-to-host copy of its packed outputs on the slot's
+stream.  A request's latency runs from its arrival (``t_arrival`` if the
+caller scheduled one, else ``submit``) to the moment the scheduler sees its
+batch's completion event.  Results do not depend on the batch a point lands
+in: the kernels treat every point independently, with one fixed order of
+operations per point.
 """
 from __future__ import annotations
 
 import collections
-import concurrent.futures as cf
-import queue
 import threading
 import time
 
 import numpy as np
 import torch
 
-from .films import FilmStackSolver
+from .films import FilmPoint, FilmStackSolver, FilmVarSolver, grating_orders
+
+_NPW = {}
 
 
-class FilmRequest(object):
+def _npw(max_order, period, period_y, world_1d):
+    key = (max_order, period, period_y, world_1d)
+    n = _NPW.get(key)
+    if n is None:
+        n = len(grating_orders(max_order, period, period_y, world_1d)[0])
+        _NPW[key] = n
+    return n
+
+
+class FilmRequest(FilmPoint):
     """One spectral point of an all-film stack (bottom-to-top indices n)."""
 
-    __slots__ = ('n', 'heights', 'wl_nm', 'k_pll', 'period', 'period_y', 'max_order', 'pol',
-                 'world_1d', 'signature', 't_submit', 'future')
+    __slots__ = ('signature', 't_submit', 't_arrival', 'future', 'npw')
 
     def __init__(self, n, heights, wl_nm, k_pll, period, max_order, pol='TE', period_y=None,
-                 world_1d=False):
-        self.n = np.asarray(n, np.complex128)
-        self.heights = np.asarray(heights, np.float64)
-        if self.heights.shape != (len(self.n) - 2,):
-            raise ValueError('need one height per finite layer')
-        self.wl_nm = float(wl_nm)
-        self.k_pll = np.asarray(k_pll, np.float64).reshape(2)
-        self.period = float(period)
-        self.period_y = float(period if period_y is None else period_y)
-        self.max_order = int(max_order)
-        self.pol = pol
-        self.world_1d = bool(world_1d)
+                 world_1d=False, incoming=None, t_arrival=None):
+        super().__init__(n, heights, wl_nm, k_pll, period, max_order, pol=pol, period_y=period_y,
+                         world_1d=world_1d, incoming=incoming)
+        self.npw = _npw(self.max_order, self.period, self.period_y, self.world_1d)
         self.signature = ('film', len(self.n), self.max_order, self.period, self.period_y,
-                          self.world_1d, pol)
+                          self.world_1d, pol if incoming is None else None)
+        self.t_arrival = t_arrival
 
     def bytes_on_device(self):
-        L = len(self.n)
-        npw_est = (2 * self.max_order + 1) ** 2
-        P = 2 * npw_est
-        return 8 + 16 + 16 * L + 8 * (L - 2) + 2 * 16 * P + 2 * 8 * (L - 1) + 12 + L * 160
+        """Inputs, outputs and workspace of this point on the device."""
+        L, P = len(self.n), 2 * self.npw
+        slots = self.npw if self.incoming is not None else 1
+        return (120 + 16 * L + 8 * (L - 2) + (16 * P if self.incoming is not None else 0)
+                + 2 * 16 * P + 2 * 8 * (L - 1) + 4 * (L + 1) + 16 + slots * L * 160)
+
+
+class FilmResult(object):
+    """Outputs of one request: dict-like view into its batch's host arrays
+    (keys R_net, T_net, a_list, t_list, r_list, flags, specular)."""
+
+    __slots__ = ('_h', '_ro', '_P', '_lo', '_L', '_i')
+
+    def __init__(self, host, ro, P, lo, L, i):
+        self._h, self._ro, self._P, self._lo, self._L, self._i = host, ro, P, lo, L, i
+
+    def __getitem__(self, k):
+        h = self._h
+        if k in ('R_net', 'T_net'):
+            return h[k][self._ro:self._ro + self._P]
+        if k in ('a_list', 't_list'):
+            return h[k][self._lo:self._lo + self._L - 1]
+        if k == 'r_list':
+            return h['r_list'][self._i]
+        if k in ('flags', 'specular'):
+            return int(h[k][self._i])
+        raise KeyError(k)
+
+    def keys(self):
+        return ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags', 'specular')
+
+
+class RequestFuture(object):
+    """Completion handle of one request (the subset of concurrent.futures.
+    Future the server needs, without a lock per request: completions are
+    published per batch under the server's one condition variable)."""
+
+    __slots__ = ('_value', '_exc', '_done', '_cv')
+
+    def __init__(self, cv):
+        self._cv = cv
+        self._done = False
+        self._value = self._exc = None
+
+    def done(self):
+        return self._done
+
+    def result(self, timeout=None):
+        if not self._done:
+            end = None if timeout is None else time.monotonic() + timeout
+            with self._cv:
+                while not self._done:
+                    left = None if end is None else end - time.monotonic()
+                    if left is not None and left <= 0:
+                        raise TimeoutError('request not finished')
+                    self._cv.wait(left)
+        if self._exc is not None:
+            raise self._exc
+        return self._value
 
 
 class _Batch(object):
-    def __init__(self, reqs, slot, event, outs, nbytes):
-        self.reqs, self.slot, self.event, self.outs, self.nbytes = reqs, slot, event, outs, nbytes
+    __slots__ = ('reqs', 'slot', 'event', 'nbytes', 'finish', 'keep')
+
+    def __init__(self, reqs, slot, event, nbytes, finish, keep):
+        self.reqs, self.slot, self.event = reqs, slot, event
+        self.nbytes, self.finish, self.keep = nbytes, finish, keep
 
 
 class GsmServer(object):
     """Continuous batching of GSM solve requests on one GPU.
 
     hbm_budget_bytes bounds the device memory of batches in flight;
-    n_streams batches may run at once; max_batch caps one launch.
+    n_streams batches may run at once; max_batch caps one launch;
+    batching is 'mixed' (any shapes in one launch) or 'grouped'.
     """
 
     def __init__(self, device=None, hbm_budget_bytes=150 << 30, max_batch=32768, n_streams=2,
-                 poll_s=2e-4):
+                 poll_s=2e-4, batching='mixed'):
+        if batching not in ('mixed', 'grouped'):
+            raise ValueError("batching must be 'mixed' or 'grouped'")
         self.device = (torch.device('cuda', torch.cuda.current_device()) if device is None
                        else torch.device(device))
+        self.batching = batching
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
         self.poll_s = poll_s
-        self.q = queue.Queue()
+        self.q = collections.deque()      # submit -> scheduler (append / popleft are atomic)
+        self._wake = threading.Event()
+        self._idle = False
+        self._cv = threading.Condition()
         self.pending = collections.OrderedDict()
-        self.slots = [dict(stream=torch.cuda.Stream(device=self.device), solvers={}, busy=False)
-                      for _ in range(n_streams)]
+        self.slots = [dict(stream=torch.cuda.Stream(device=self.device), solvers={}, busy=False,
+                           var=None) for _ in range(n_streams)]
         self.inflight = []
         self.inflight_bytes = 0
         self.latencies = []
@@ -86,14 +163,21 @@ class GsmServer(object):
         self._thread = None
         self.t_first = None
         self.t_last = None
+        self.error = None
+        # host seconds spent packing, launching and finishing batches, and
+        # device seconds from the H2D copy to the end of the D2H copy
+        self.prof = dict(plan_s=0.0, launch_s=0.0, finish_s=0.0, device_s=0.0)
 
     # ---------------------------------------------------------------- API
     def submit(self, req):
-        req.future = cf.Future()
+        req.future = RequestFuture(self._cv)
         req.t_submit = time.perf_counter()
-        if self.t_first is None:
-            self.t_first = req.t_submit
-        self.q.put(req)
+        t0 = req.t_arrival if req.t_arrival is not None else req.t_submit
+        if self.t_first is None or t0 < self.t_first:
+            self.t_first = t0
+        self.q.append(req)
+        if self._idle:
+            self._wake.set()
         return req.future
 
     def start(self):
@@ -103,6 +187,7 @@ class GsmServer(object):
 
     def stop(self):
         self._stop.set()
+        self._wake.set()
         if self._thread is not None:
             self._thread.join()
 
@@ -126,30 +211,61 @@ class GsmServer(object):
         }
 
     # ---------------------------------------------------------------- loop
+    def _key(self, r):
+        return 'all' if self.batching == 'mixed' else r.signature
+
+    def _take(self, block):
+        if block and not self.q:
+            self._idle = True
+            if not self.q:
+                self._wake.wait(0.01)
+            self._idle = False
+            self._wake.clear()
+        got = False
+        q, pend = self.q, self.pending
+        while q:
+            r = q.popleft()
+            k = self._key(r)
+            d = pend.get(k)
+            if d is None:
+                d = pend[k] = collections.deque()
+            d.append(r)
+            got = True
+        return got
+
     def _loop(self):
         torch.cuda.set_device(self.device)
-        while True:
-            got = False
+        try:
             while True:
-                try:
-                    r = self.q.get_nowait()
-                except queue.Empty:
+                got = self._take(block=False)
+                done_any = self._retire()
+                launched = self._launch()
+                if self._stop.is_set() and not self.pending and not self.inflight and not self.q:
                     break
-                self.pending.setdefault(r.signature, collections.deque()).append(r)
-                got = True
-            done_any = self._retire()
-            launched = self._launch()
-            if self._stop.is_set() and not self.pending and not self.inflight and self.q.empty():
-                break
-            if not (got or done_any or launched):
-                if self.inflight:
-                    time.sleep(self.poll_s)
+                if not (got or done_any or launched):
+                    if self.inflight:
+                        time.sleep(self.poll_s)
+                    else:
+                        self._take(block=True)
+        except Exception as e:  # fail every waiting request instead of hanging them
+            self.error = e
+            waiting = [r for b in self.inflight for r in b.reqs]
+            waiting += [r for dq in self.pending.values() for r in dq]
+            while self.q:
+                waiting.append(self.q.popleft())
+            self._publish([r for r in waiting if not r.future.done()], exc=e)
+
+    def _publish(self, reqs, values=None, exc=None):
+        """Complete a batch of requests and wake their waiters once."""
+        with self._cv:
+            for i, r in enumerate(reqs):
+                f = r.future
+                if exc is not None:
+                    f._exc = exc
                 else:
-                    try:
-                        r = self.q.get(timeout=0.01)
-                        self.pending.setdefault(r.signature, collections.deque()).append(r)
-                    except queue.Empty:
-                        pass
+                    f._value = values[i]
+                f._done = True
+            self._cv.notify_all()
 
     def _retire(self):
         done_any = False
@@ -157,11 +273,7 @@ class GsmServer(object):
         for b in self.inflight:
             if b.event.query():
                 t = time.perf_counter()
-                host = {k: v.numpy() for k, v in b.outs.items()}
-                for i, r in enumerate(b.reqs):
-                    res = {k: v[i].copy() for k, v in host.items()}
-                    self.latencies.append(t - r.t_submit)
-                    r.future.set_result(res)
+                b.finish(b, t)
                 self.t_last = t
                 self.inflight_bytes -= b.nbytes
                 b.slot['busy'] = False
@@ -176,28 +288,65 @@ class GsmServer(object):
         for slot in self.slots:
             if slot['busy'] or not self.pending:
                 continue
-            sig = next(iter(self.pending))
-            dq = self.pending[sig]
+            key = next(iter(self.pending))
+            dq = self.pending[key]
             reqs, nbytes = [], 0
             while dq and len(reqs) < self.max_batch:
                 nb = dq[0].bytes_on_device()
-                if self.inflight_bytes + nbytes + nb > self.budget and reqs:
-                    break
-                if self.inflight_bytes + nbytes + nb > self.budget and self.inflight:
+                if self.inflight_bytes + nbytes + nb > self.budget and (reqs or self.inflight):
                     break
                 reqs.append(dq.popleft())
                 nbytes += nb
             if not dq:
-                del self.pending[sig]
+                del self.pending[key]
             else:
-                self.pending.move_to_end(sig)
+                self.pending.move_to_end(key)
             if not reqs:
                 continue
-            self._run_batch(slot, sig, reqs, nbytes)
+            if self.batching == 'mixed':
+                self._run_mixed(slot, reqs, nbytes)
+            else:
+                self._run_grouped(slot, reqs[0].signature, reqs, nbytes)
             launched = True
         return launched
 
-    def _run_batch(self, slot, sig, reqs, nbytes):
+    def _record(self, reqs, t):
+        self.latencies.extend([t - (r.t_arrival if r.t_arrival is not None else r.t_submit)
+                               for r in reqs])
+
+    def _run_mixed(self, slot, reqs, nbytes):
+        if slot['var'] is None:
+            slot['var'] = FilmVarSolver(self.device)
+        solver = slot['var']
+        s = slot['stream']
+        t0 = time.perf_counter()
+        pl = solver.plan(reqs)
+        t1 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        out = solver.solve(pl, stream=s)
+        host = solver.fetch(out, stream=s)
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(s)
+        self.prof['plan_s'] += t1 - t0
+        self.prof['launch_s'] += time.perf_counter() - t1
+        desc = pl.desc
+
+        def finish(b, t):
+            # copy out of the slot's staging buffers before the slot is reused
+            t2 = time.perf_counter()
+            h = {k: v.copy() for k, v in host.items()}
+            ro, lo = desc['rt_off'].tolist(), desc['list_off'].tolist()
+            P, L = (2 * desc['n_pw']).tolist(), desc['n_layers'].tolist()
+            vals = [FilmResult(h, ro[i], P[i], lo[i], L[i], i) for i in range(len(b.reqs))]
+            self._publish(b.reqs, vals)
+            self._record(b.reqs, t)
+            self.prof['finish_s'] += time.perf_counter() - t2
+            self.prof['device_s'] += e0.elapsed_time(b.event) / 1e3
+
+        self._submit(_Batch(reqs, slot, ev, nbytes, finish, None))
+
+    def _run_grouped(self, slot, sig, reqs, nbytes):
         _, L, mo, per, per_y, w1d, pol = sig
         B = len(reqs)
         solver = slot['solvers'].get(sig)
@@ -219,19 +368,27 @@ class GsmServer(object):
             dkp = kp.to(self.device, non_blocking=True)
             dn = n.to(self.device, non_blocking=True)
             dh = h.to(self.device, non_blocking=True) if L > 2 else None
-            o = solver.solve(dwl, dkp, dn, dh, pol=pol, stream=s)
+            o = solver.solve(dwl, dkp, dn, dh, pol=pol, stream=s, want=('specular',))
             outs = {}
-            for k in ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags'):
+            for k in ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags', 'specular'):
                 t = torch.empty(o[k].shape, dtype=o[k].dtype).pin_memory()
                 t.copy_(o[k], non_blocking=True)
                 outs[k] = t
             ev = torch.cuda.Event()
             ev.record(s)
-        # keep the device inputs alive until the batch retires
-        outs_keep = _Batch(reqs, slot, ev, outs, nbytes)
-        outs_keep.keep = (dwl, dkp, dn, dh)
-        slot['busy'] = True
-        self.inflight.append(outs_keep)
-        self.inflight_bytes += nbytes
+
+        def finish(b, t):
+            host = {k: v.numpy() for k, v in outs.items()}
+            vals = [{k: (v[i].copy() if v.ndim > 1 else v[i]) for k, v in host.items()}
+                    for i in range(len(b.reqs))]
+            self._publish(b.reqs, vals)
+            self._record(b.reqs, t)
+
+        self._submit(_Batch(reqs, slot, ev, nbytes, finish, (dwl, dkp, dn, dh)))
+
+    def _submit(self, batch):
+        batch.slot['busy'] = True
+        self.inflight.append(batch)
+        self.inflight_bytes += batch.nbytes
         self.n_batches += 1
-        self.batch_sizes.append(B)
+        self.batch_sizes.append(len(batch.reqs))

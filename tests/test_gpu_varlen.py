@@ -22,7 +22,7 @@ TOL = dict(rtol=1e-9, atol=1e-10)
 
 
 def _host(out):
-    return {k: v.cpu().numpy() for k, v in out.items() if not k.startswith('_')}
+    return {k: v.cpu().numpy() for k, v in out.items()}
 
 
 def _solve(points, **kw):
@@ -143,10 +143,10 @@ def test_bad_descriptor_is_flagged_and_skipped():
     pl = s.plan(pts)
     good = s.unpack(pl, _host(s.solve(pl)))
     torch.cuda.synchronize()
-    desc = pl['desc'].copy()
-    desc[5]['n_off'] = pl['n_len']          # past the end of d_n
-    desc[8]['n_layers'] = pl['max_layers'] + 1
-    pl['h_desc'] = torch.from_numpy(desc.view(np.uint8).copy()).pin_memory()
+    desc = pl.desc.copy()
+    desc[5]['n_off'] = pl.n_len              # past the end of d_n
+    desc[8]['n_layers'] = pl.max_layers + 1
+    pl.h_desc.numpy()[:] = desc.view(np.uint8)
     out = _host(s.solve(pl))
     torch.cuda.synchronize()
     assert out['flags'][5] == _lib.PT_BAD_POINT and out['flags'][8] == _lib.PT_BAD_POINT
