@@ -27,6 +27,7 @@ using namespace emu;
 
 __constant__ double c_wq[16], c_xq[16], c_yq[16];
 __constant__ double c_phi2[16][6];       // P2 basis at the quadrature points
+__constant__ float c_phi2f[16][6];       // the same, rounded to FP32 (tensor-core operand path)
 __constant__ double c_g3[16][2][10];     // P3 gradients (reference triangle)
 
 // 16-point symmetric rule of Lyness & Jespersen (J. Inst. Math. Appl. 15,
@@ -55,6 +56,7 @@ int upload_tables() {
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && done[dev]) return EMU_OK;
   double w[16], x[16], y[16], phi[16][6], g[16][2][10];
+  float phif[16][6];
   quad_table(w, x, y);
   for (int q = 0; q < 16; ++q) {
     const double x0 = x[q], y0 = y[q];
@@ -65,6 +67,7 @@ int upload_tables() {
     phi[q][3] = -4 * x0 * (-1 + x0 + y0);
     phi[q][4] = 4 * x0 * y0;
     phi[q][5] = -4 * y0 * (-1 + x0 + y0);
+    for (int k = 0; k < 6; ++k) phif[q][k] = (float)phi[q][k];
     // P3 gradients (backend/fortran/phi3_2d_mat.f:17-64)
     const double t = (-11 - 27 * x0 * x0 + x0 * (36 - 54 * y0) + 36 * y0 - 27 * y0 * y0) / 2.;
     g[q][0][0] = t; g[q][1][0] = t;
@@ -89,6 +92,7 @@ int upload_tables() {
       cudaMemcpyToSymbol(c_xq, x, sizeof(x)) != cudaSuccess ||
       cudaMemcpyToSymbol(c_yq, y, sizeof(y)) != cudaSuccess ||
       cudaMemcpyToSymbol(c_phi2, phi, sizeof(phi)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_phi2f, phif, sizeof(phif)) != cudaSuccess ||
       cudaMemcpyToSymbol(c_g3, g, sizeof(g)) != cudaSuccess)
     return EMU_E_CUDA;
   if (dev >= 0 && dev < 64) done[dev] = true;
@@ -184,6 +188,11 @@ __host__ __device__ inline size_t et_warp_bytes(int mo) {
   return sizeof(cd) * (16 + 2 * 16 * (size_t)(2 * mo + 1)) + sizeof(double) * 16;
 }
 
+// kF32: tensor-core operand path.  The phase factor of each quadrature point
+// is formed in FP64 (base x tx x ty, the argument and powers in FP64) and
+// rounded to FP32 (relative 6e-8); the 16-point x 6-node sums then run in
+// FP32, below the ~2^-21 relative error of the split-TF32 products they feed.
+template <bool kF32>
 __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
   extern __shared__ __align__(16) unsigned char et_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -227,30 +236,43 @@ __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
     if (ok) {
       for (int s = lane; s < a.npw; s += 32) {
         const int ix = a.px[s] + a.mo, iy = a.py[s] + a.mo;
-        cd acc[6];
+        if constexpr (kF32) {
+          float2 acc[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) acc[k] = cd{0.0, 0.0};
+          for (int k = 0; k < 6; ++k) acc[k] = make_float2(0.f, 0.f);
 #pragma unroll 4
-        for (int q = 0; q < 16; ++q) {
-          const cd e = cscale(cmul(cmul(base[q], tx[q * no + ix]), ty[q * no + iy]), cq[q]);
+          for (int q = 0; q < 16; ++q) {
+            const cd e = cscale(cmul(cmul(base[q], tx[q * no + ix]), ty[q * no + iy]), cq[q]);
+            const float ex = (float)e.x, ey = (float)e.y;
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            acc[k].x = fma(e.x, c_phi2[q][k], acc[k].x);
-            acc[k].y = fma(e.y, c_phi2[q][k], acc[k].y);
+            for (int k = 0; k < 6; ++k) {
+              acc[k].x = fmaf(ex, c_phi2f[q][k], acc[k].x);
+              acc[k].y = fmaf(ey, c_phi2f[q][k], acc[k].y);
+            }
           }
-        }
-        if (a.A32) {
           const long long K = 6LL * a.ne;
           float *r0 = a.A32 + (size_t)a.pos[s] * 2 * K + (size_t)el * 6;
           float *r1 = r0 + (size_t)a.npw * 2 * K;
 #pragma unroll
           for (int k = 0; k < 6; ++k) {
-            r0[k] = (float)acc[k].x;
-            r0[K + k] = (float)(-acc[k].y);
-            r1[k] = (float)acc[k].y;
-            r1[K + k] = (float)acc[k].x;
+            r0[k] = acc[k].x;
+            r0[K + k] = -acc[k].y;
+            r1[k] = acc[k].y;
+            r1[K + k] = acc[k].x;
           }
         } else {
+          cd acc[6];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) acc[k] = cd{0.0, 0.0};
+#pragma unroll 4
+          for (int q = 0; q < 16; ++q) {
+            const cd e = cscale(cmul(cmul(base[q], tx[q * no + ix]), ty[q * no + iy]), cq[q]);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+              acc[k].x = fma(e.x, c_phi2[q][k], acc[k].x);
+              acc[k].y = fma(e.y, c_phi2[q][k], acc[k].y);
+            }
+          }
           cd *row = a.E + (size_t)a.pos[s] * a.ldE + (size_t)el * 6;
 #pragma unroll
           for (int k = 0; k < 6; ++k) row[k] = acc[k];
@@ -728,8 +750,10 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   const int sms = emu::sm_count();
   const size_t et_smem = kEtWarps * et_warp_bytes(p->max_order);
   if (et_smem > 48 * 1024 &&
-      cudaFuncSetAttribute(etable_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)et_smem) !=
-          cudaSuccess)
+      (cudaFuncSetAttribute(etable_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)et_smem) != cudaSuccess ||
+       cudaFuncSetAttribute(etable_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)et_smem) != cudaSuccess))
     return EMU_E_CUDA;
   for (int b = 0; b < p->batch; ++b) {
     PwArgs pa;
@@ -779,7 +803,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
         EtArgs ea = et_args(e0, ne);
         ea.A32 = A32;
         const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
-        etable_kernel<<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
+        etable_kernel<true><<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
         const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems));
         if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1, M, e0, ne, 0, 0, B32);
         if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2, M, e0, ne, 1, off1, B32);
@@ -803,7 +827,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
         const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
         EtArgs ea = et_args(e0, ne);
         const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
-        etable_kernel<<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
+        etable_kernel<false><<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
         const long long rn = ne * 6 * 2 * (long long)M;
         const long long rg = (rn + 255) / 256;
         repack_kernel<<<(int)(rg < 16 * sms ? rg : 16 * sms), 256, 0, s>>>(sol, M, e0, ne, S);
