@@ -176,7 +176,8 @@ struct EtArgs {
   cd *E;
   long long ldE;
   // tensor-core path: instead of E, the real embedding A (FP32,
-  // [2 npw][2 K], K = 6 ne): row s = [Re E, -Im E], row npw + s = [Im E, Re E]
+  // [2 npw][2 K], K = 6 ne), columns in (element, node, re/im) order:
+  // row s = (Re E, -Im E) pairs, row npw + s = (Im E, Re E) pairs
   float *A32;
 };
 
@@ -188,15 +189,89 @@ __host__ __device__ inline size_t et_warp_bytes(int mo) {
   return sizeof(cd) * (16 + 2 * 16 * (size_t)(2 * mo + 1)) + sizeof(double) * 16;
 }
 
-// kF32: tensor-core operand path.  The phase factor of each quadrature point
-// is formed in FP64 (base x tx x ty, the argument and powers in FP64) and
-// rounded to FP32 (relative 6e-8); the 16-point x 6-node sums then run in
-// FP32, below the ~2^-21 relative error of the split-TF32 products they feed.
+// FP32 tables of the tensor-core operand path: bc[16] (base x weight),
+// tx[16][no], ty[16][no] as float2
+__host__ __device__ inline size_t et_warp_bytes_f32(int mo) {
+  return sizeof(float2) * (16 + 2 * 16 * (size_t)(2 * mo + 1));
+}
+
+// kF32: tensor-core operand path.  The phase tables of each element are
+// computed in FP64 (arguments, sincos, powers) and stored rounded to FP32
+// (relative 6e-8 per entry); the phase products and the 16-point x 6-node
+// sums then run in FP32 (~3e-7 relative), below the ~2^-21 relative error of
+// the split-TF32 products they feed.  Half the table bytes of the FP64 path,
+// so twice the resident warps.
 template <bool kF32>
 __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
   extern __shared__ __align__(16) unsigned char et_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int no = 2 * a.mo + 1;
+  if constexpr (kF32) {
+    float2 *bc = (float2 *)(et_smem + (size_t)w * et_warp_bytes_f32(a.mo));  // [16]
+    float2 *fx = bc + 16;                                                      // [16][no]
+    float2 *fy = fx + 16 * no;                                                 // [16][no]
+    const double bx = a.bloch[0], by = a.bloch[1];
+    const long long K = 6LL * a.ne;
+    for (long el0 = (long)blockIdx.x * kEtWarps; el0 < a.ne; el0 += (long)gridDim.x * kEtWarps) {
+      const long el = el0 + w;
+      const bool ok = el < a.ne;
+      if (ok && lane < 16) {
+        const Geo g = element_geo(a.x, a.tn, a.e0 + el);
+        const int q = lane;
+        const double xg = g.x1 + g.B00 * c_xq[q] + g.B01 * c_yq[q];
+        const double yg = g.y1 + g.B10 * c_xq[q] + g.B11 * c_yq[q];
+        const double wq = c_wq[q] * g.adet;
+        double s, c;
+        sincos(-(bx * xg + by * yg), &s, &c);
+        bc[q] = make_float2((float)(c * wq), (float)(s * wq));
+        double sx, cx, sy, cy;
+        sincos(-2.0 * 3.141592653589793 / a.d * xg, &sx, &cx);
+        sincos(-2.0 * 3.141592653589793 / a.dy * yg, &sy, &cy);
+        const cd ux = cd{cx, sx}, uy = cd{cy, sy};
+        cd px = cd{1.0, 0.0}, py = cd{1.0, 0.0};
+        fx[q * no + a.mo] = make_float2(1.f, 0.f);
+        fy[q * no + a.mo] = make_float2(1.f, 0.f);
+        for (int p = 1; p <= a.mo; ++p) {
+          px = cmul(px, ux);
+          py = cmul(py, uy);
+          fx[q * no + a.mo + p] = make_float2((float)px.x, (float)px.y);
+          fx[q * no + a.mo - p] = make_float2((float)px.x, (float)-px.y);
+          fy[q * no + a.mo + p] = make_float2((float)py.x, (float)py.y);
+          fy[q * no + a.mo - p] = make_float2((float)py.x, (float)-py.y);
+        }
+      }
+      __syncwarp();
+      if (ok) {
+        for (int s = lane; s < a.npw; s += 32) {
+          const int ix = a.px[s] + a.mo, iy = a.py[s] + a.mo;
+          float2 acc[6];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) acc[k] = make_float2(0.f, 0.f);
+#pragma unroll 4
+          for (int q = 0; q < 16; ++q) {
+            const float2 b = bc[q], u = fx[q * no + ix], v = fy[q * no + iy];
+            const float2 t = make_float2(b.x * u.x - b.y * u.y, b.x * u.y + b.y * u.x);
+            const float ex = t.x * v.x - t.y * v.y, ey = t.x * v.y + t.y * v.x;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+              acc[k].x = fmaf(ex, c_phi2f[q][k], acc[k].x);
+              acc[k].y = fmaf(ey, c_phi2f[q][k], acc[k].y);
+            }
+          }
+          // K order (element, node, re/im): 12 contiguous floats per row
+          float4 *r0 = (float4 *)(a.A32 + (size_t)a.pos[s] * 2 * K + (size_t)el * 12);
+          float4 *r1 = (float4 *)((float *)r0 + (size_t)a.npw * 2 * K);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            r0[k] = make_float4(acc[2 * k].x, -acc[2 * k].y, acc[2 * k + 1].x, -acc[2 * k + 1].y);
+            r1[k] = make_float4(acc[2 * k].y, acc[2 * k].x, acc[2 * k + 1].y, acc[2 * k + 1].x);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    return;
+  }
   cd *wb = (cd *)(et_smem + (size_t)w * et_warp_bytes(a.mo));
   cd *base = wb;                 // [16]
   cd *tx = base + 16;            // [16][no]
@@ -236,31 +311,7 @@ __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
     if (ok) {
       for (int s = lane; s < a.npw; s += 32) {
         const int ix = a.px[s] + a.mo, iy = a.py[s] + a.mo;
-        if constexpr (kF32) {
-          float2 acc[6];
-#pragma unroll
-          for (int k = 0; k < 6; ++k) acc[k] = make_float2(0.f, 0.f);
-#pragma unroll 4
-          for (int q = 0; q < 16; ++q) {
-            const cd e = cscale(cmul(cmul(base[q], tx[q * no + ix]), ty[q * no + iy]), cq[q]);
-            const float ex = (float)e.x, ey = (float)e.y;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-              acc[k].x = fmaf(ex, c_phi2f[q][k], acc[k].x);
-              acc[k].y = fmaf(ey, c_phi2f[q][k], acc[k].y);
-            }
-          }
-          const long long K = 6LL * a.ne;
-          float *r0 = a.A32 + (size_t)a.pos[s] * 2 * K + (size_t)el * 6;
-          float *r1 = r0 + (size_t)a.npw * 2 * K;
-#pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            r0[k] = acc[k].x;
-            r0[K + k] = -acc[k].y;
-            r1[k] = acc[k].y;
-            r1[K + k] = acc[k].x;
-          }
-        } else {
+        {
           cd acc[6];
 #pragma unroll
           for (int k = 0; k < 6; ++k) acc[k] = cd{0.0, 0.0};
@@ -527,13 +578,14 @@ __global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, const 
 // Tensor-core path: the complex contractions G = E~ . S1 and
 // G_dag = conj(E~) . S2 = conj(E~ . conj(S2)) share one real GEMM
 //   C[2 npw][Nb] = A[2 npw][2 K] . B[Nb][2 K]^T
-// with A from etable_kernel (A32 output) and B rows
-//   c * M + m          = [Re S1, Im S1]   (c = 0, 1: x, y component)
-//   off1 + c * M + m   = [Re S2, -Im S2]  (off1 = 2 M when S1 is present)
+// with A from etable_kernel (A32 output) and B rows, K in (element, node,
+// re/im) order,
+//   c * M + m          = (Re S1, Im S1) pairs   (c = 0, 1: x, y component)
+//   off1 + c * M + m   = (Re S2, -Im S2) pairs  (off1 = 2 M when S1 is present)
 // B tile builder: 8 modes x 16 elements per CTA; the 12 transverse values
 // (node 0-5, component 0-1) of each (element, mode) record are read with
 // consecutive lanes, staged in shared memory and written as rows of
-// 96 contiguous floats per half.
+// 192 contiguous floats.
 constexpr int kBModes = 8, kBElems = 16;
 
 __global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, long e0, long ne,
@@ -548,6 +600,7 @@ __global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, lo
   if (lane < 24) {
     const int j = lane % 12, eo = lane / 12;
     const int node = j >> 1, c = j & 1;
+#pragma unroll
     for (int e = eo; e < kBElems; e += 2) {
       const long el = el0 + e;
       cd x = cd{0.0, 0.0};
@@ -556,17 +609,16 @@ __global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, lo
     }
   }
   __syncthreads();
-  // write: 16 rows (c, mode) x 2 halves x 96 floats (element-major, node-minor)
+  // write: 16 rows (c, mode) x 192 floats (element, node, re/im)
   const int nel_here = (int)(ne - el0 < kBElems ? ne - el0 : kBElems);
-  for (int i = threadIdx.x; i < 2 * kBModes * 2 * 96; i += 256) {
-    const int within = i % 96, rh = i / 96;
-    const int half = rh & 1, r = rh >> 1;
+  for (int i = threadIdx.x; i < 2 * kBModes * 192; i += 256) {
+    const int within = i % 192, r = i / 192;
     const int c = r / kBModes, mm = r % kBModes;
-    const int e = within / 6, node = within % 6;
+    const int e = within / 12, node = (within % 12) >> 1, ri = within & 1;
     if (m0 + mm >= nval || e >= nel_here) continue;
     const cd x = v[mm][e][node * 2 + c];
-    const float val = half == 0 ? (float)x.x : (float)(conj ? -x.y : x.y);
-    B[(size_t)(row0 + c * nval + m0 + mm) * 2 * K + (size_t)half * K + (size_t)(el0 + e) * 6 + node] = val;
+    const float val = ri == 0 ? (float)x.x : (float)(conj ? -x.y : x.y);
+    B[(size_t)(row0 + c * nval + m0 + mm) * 2 * K + (size_t)(el0 + e) * 12 + node * 2 + ri] = val;
   }
 }
 
@@ -749,11 +801,12 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   }
   const int sms = emu::sm_count();
   const size_t et_smem = kEtWarps * et_warp_bytes(p->max_order);
+  const size_t et_smem32 = kEtWarps * et_warp_bytes_f32(p->max_order);
   if (et_smem > 48 * 1024 &&
       (cudaFuncSetAttribute(etable_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)et_smem) != cudaSuccess ||
        cudaFuncSetAttribute(etable_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)et_smem) != cudaSuccess))
+                            (int)et_smem32) != cudaSuccess))
     return EMU_E_CUDA;
   for (int b = 0; b < p->batch; ++b) {
     PwArgs pa;
@@ -803,7 +856,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
         EtArgs ea = et_args(e0, ne);
         ea.A32 = A32;
         const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
-        etable_kernel<true><<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
+        etable_kernel<true><<<eg < 16 * sms ? eg : 16 * sms, 32 * kEtWarps, et_smem32, s>>>(ea);
         const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems));
         if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1, M, e0, ne, 0, 0, B32);
         if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2, M, e0, ne, 1, off1, B32);
