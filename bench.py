@@ -312,8 +312,18 @@ def run_ours(args, rank, world, local_rank):
                         'peak_source': 'DFMA probe kernel (emu_probe_fp64), measured in this run',
                         'flops_per_step': flops},
             'clocks': clk.summary(),
+            'autotune': _tuned(),
         }
     return result
+
+
+def _tuned():
+    """Launch choices the autotuner made for the kernels timed here (chosen
+    during warm-up from CUDA-event timings of every candidate)."""
+    from emustack_b200.autotune import default_tuner
+    return [{'kernel': k.split('|')[1], 'shape': json.loads(k.split('|')[2]), 'choice': e['choice'],
+             'candidate_ms': {c: round(t, 4) for c, t in e['ms'].items()}}
+            for k, e in default_tuner().log]
 
 
 def film_flops(B, L, P):

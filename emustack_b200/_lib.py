@@ -41,7 +41,10 @@ class EmuFilmStackBatch(C.Structure):
         ('d_flags', vp),
         ('d_kz', vp), ('d_layer_rt', vp), ('d_vec_coef_down', vp), ('d_vec_coef_up', vp),
         ('d_fluxes', vp), ('d_sort_order', vp), ('d_specular', vp), ('d_num_prop', vp),
+        ('variant', C.c_int),
     ]
+
+FILM_VARIANTS = (0, 1, 2, 3)
 
 
 class EmuError(RuntimeError):
@@ -172,6 +175,7 @@ class EmuOverlap(C.Structure):
         ('d_sol1', vp), ('d_sol2', vp), ('d_scale2', vp), ('d_perm2', vp),
         ('area_norm', C.c_double), ('d_J', vp), ('d_J_dag', vp), ('d_index_pw_inv', vp),
         ('elements_per_chunk', C.c_int), ('precision', C.c_int), ('d_error', vp),
+        ('tc_splits', C.c_int),
     ]
 
 
@@ -218,7 +222,7 @@ class EmuFilmVarBatch(C.Structure):
         ('d_specular', vp), ('d_num_prop', vp),
         ('order_len', C.c_int64), ('n_len', C.c_int64), ('h_len', C.c_int64),
         ('inc_len', C.c_int64), ('rt_len', C.c_int64), ('list_len', C.c_int64),
-        ('np_len', C.c_int64),
+        ('np_len', C.c_int64), ('warps_per_cta', C.c_int),
     ]
 
 

@@ -46,7 +46,12 @@ namespace {
 
 using namespace emu;
 
-constexpr int kThreads = 256;
+// Launch variants (EmuFilmStackBatch.variant): threads per CTA and the
+// minimum resident CTAs per SM given to the compiler (which sets the
+// register cap: 65536 / (threads * min CTAs), at most 255).
+constexpr int kVariants = 4;
+constexpr int kMaxCtaSmem = 200 * 1024;
+constexpr int kVarThreadsTab[kVariants] = {256, 128, 512, 256};
 
 struct FilmArgs {
   EmuFilmStackBatch p;
@@ -115,7 +120,8 @@ struct UniformPoint {
   __device__ uint32_t *flags() const { return a.p.d_flags + b; }
 };
 
-__global__ void __launch_bounds__(kThreads, 2) film_stack_kernel(FilmArgs a) {
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) film_stack_kernel(FilmArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const EmuFilmStackBatch &p = a.p;
   const int B = p.n_points;
@@ -136,10 +142,20 @@ struct Launch {
   size_t smem;
 };
 
+using FilmKernel = void (*)(FilmArgs);
+// 0: 256 threads x 2 CTAs (128 registers), 1: 128 x 4 (128), 2: 512 x 1
+// (128), 3: 256 x 1 (255 registers, no spills, half the resident warps)
+const FilmKernel kVarKernels[kVariants] = {film_stack_kernel<256, 2>, film_stack_kernel<128, 4>,
+                                           film_stack_kernel<512, 1>, film_stack_kernel<256, 1>};
+
 Launch plan(const EmuFilmStackBatch *p) {
   Launch l;
-  l.team = p->n_pw <= kThreads ? p->n_pw : kThreads;
-  l.ppc = kThreads / l.team;
+  const int threads = kVarThreadsTab[p->variant];
+  l.team = p->n_pw <= threads ? p->n_pw : threads;
+  l.ppc = threads / l.team;
+  // at most kMaxCtaSmem of slots per CTA (small order sets, many points)
+  const int stride = slot_layout(p->n_pw, p->n_layers).stride;
+  if (l.ppc * stride > kMaxCtaSmem) l.ppc = kMaxCtaSmem / stride > 0 ? kMaxCtaSmem / stride : 1;
   l.n_act = (p->pol == EMU_POL_INCOMING) ? p->n_pw : 1;
   l.smem = (size_t)slot_layout(p->n_pw, p->n_layers).stride * l.ppc;
   return l;
@@ -158,7 +174,8 @@ int validate(const EmuFilmStackBatch *p) {
   if (p->n_layers > 2 && p->n_points > 0 && !p->d_heights_nm) return EMU_E_ARG;
   if ((p->d_vec_coef_down == nullptr) != (p->d_vec_coef_up == nullptr)) return EMU_E_ARG;
   if (p->d_shears && p->shear_ncoord != 1 && p->shear_ncoord != 2) return EMU_E_ARG;
-  if (slot_layout(p->n_pw, p->n_layers).stride > 200 * 1024) return EMU_E_SHAPE;
+  if (p->variant < 0 || p->variant >= kVariants) return EMU_E_ARG;
+  if (slot_layout(p->n_pw, p->n_layers).stride > kMaxCtaSmem) return EMU_E_SHAPE;
   return EMU_OK;
 }
 
@@ -186,20 +203,21 @@ extern "C" int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspac
   a.ws = (cd *)d_workspace;
   a.dy = p->period_y / p->period;
   a.inv_sqrt2 = 1.0 / sqrt(2.0);
+  const FilmKernel kern = kVarKernels[p->variant];
+  const int threads = kVarThreadsTab[p->variant];
   if (l.smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(film_stack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)l.smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem) !=
+        cudaSuccess)
       return EMU_E_CUDA;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, film_stack_kernel, kThreads, l.smem) !=
-          cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, l.smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const long long groups = ((long long)p->n_points + l.ppc - 1) / l.ppc;
   long long grid = (long long)emu::sm_count() * per_sm;
   if (grid > groups) grid = groups;
-  film_stack_kernel<<<(int)grid, kThreads, l.smem, (cudaStream_t)stream>>>(a);
+  kern<<<(int)grid, threads, l.smem, (cudaStream_t)stream>>>(a);
   emu::note_launch();
   return emu::check_launch();
 }

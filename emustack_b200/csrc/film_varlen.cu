@@ -198,7 +198,9 @@ extern "C" int emu_film_var_batch(const EmuFilmVarBatch *p, void *d_workspace,
   a.ws = (unsigned char *)d_workspace;
   a.ws_bytes = (int64_t)workspace_bytes;
   a.inv_sqrt2_ = 1.0 / sqrt(2.0);
+  if (p->warps_per_cta < 0 || p->warps_per_cta > kVarThreads / 32) return EMU_E_ARG;
   a.warps = std::max(1, std::min(kVarThreads / 32, kMaxSlotBytes / stride));
+  if (p->warps_per_cta > 0) a.warps = std::min(a.warps, p->warps_per_cta);
   const size_t smem = (size_t)stride * a.warps;
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(film_var_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -206,14 +208,14 @@ extern "C" int emu_film_var_batch(const EmuFilmVarBatch *p, void *d_workspace,
       return EMU_E_CUDA;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, film_var_kernel, kVarThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, film_var_kernel, 32 * a.warps, smem) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const long long groups = ((long long)p->n_points + a.warps - 1) / a.warps;
   long long grid = (long long)emu::sm_count() * per_sm;
   if (grid > groups) grid = groups;
-  film_var_kernel<<<(int)grid, kVarThreads, smem, (cudaStream_t)stream>>>(a);
+  film_var_kernel<<<(int)grid, 32 * a.warps, smem, (cudaStream_t)stream>>>(a);
   emu::note_launch();
   return emu::check_launch();
 }

@@ -786,6 +786,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   cd *parts = (cd *)take(sizeof(cd) * (size_t)nparts * npw * 2 * M);
   const long long gsz = (long long)npw * 2 * M;
   if (p->precision != 0 && p->precision != 1) return EMU_E_ARG;
+  if (p->tc_splits < 0) return EMU_E_ARG;
   float *A32 = nullptr, *B32 = nullptr, *Cpart = nullptr;
   double *C64 = nullptr;
   int *terr = nullptr;
@@ -861,7 +862,8 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
         if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1, M, e0, ne, 0, 0, B32);
         if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2, M, e0, ne, 1, off1, B32);
         emu::note_launch(1 + (sol1 ? 1 : 0) + (sol2 ? 1 : 0));
-        const int sp = tc_splits(npw, nb, 2 * K);
+        int sp = tc_splits(npw, nb, 2 * K);
+        if (p->tc_splits > 0) sp = p->tc_splits < 64 ? p->tc_splits : 64;
         const int tst = emu::tc_gemm_tf32x3(A32, B32, 2 * npw, nb, (int)(2 * K), sp, Cpart, C64, terr, s);
         if (tst != EMU_OK) return tst;
         const long long rgs = (gsz + 255) / 256;

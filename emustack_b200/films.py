@@ -147,7 +147,7 @@ class FilmStackSolver(object):
         return self._ws
 
     def solve(self, wl_nm, k_pll, n, heights_nm=None, pol='TE', incoming=None, shears=None,
-              want=(), stream=None):
+              want=(), stream=None, variant=None):
         """Solve a batch on the device.
 
         wl_nm   float64 [B]           k_pll float64 [B, 2] (nm^-1)
@@ -156,6 +156,9 @@ class FilmStackSolver(object):
         incoming complex128 [B, P] or None (then ``pol`` selects the
         specular incidence of backend/mode_calcs.py:220-250)
         shears  float64 [L, ncoord] or None
+        variant launch variant of the film kernel (``EmuFilmStackBatch.variant``);
+                None: the autotuner's choice for this shape (timed on first
+                use), results do not depend on it
         Returns a dict of device tensors (reused across calls).
         """
         for t, nm, dt in ((wl_nm, 'wl_nm', torch.float64), (k_pll, 'k_pll', torch.float64),
@@ -179,8 +182,19 @@ class FilmStackSolver(object):
         L = lib()
         nbytes = L.emu_film_stack_workspace_size(C.byref(d))
         ws = self.workspace(nbytes)
-        check(L.emu_film_stack_batch(C.byref(d), ptr(ws), C.c_size_t(ws.numel()), stream_ptr(stream)),
-              'emu_film_stack_batch')
+
+        def run(v):
+            d.variant = int(v)
+            check(L.emu_film_stack_batch(C.byref(d), ptr(ws), C.c_size_t(ws.numel()),
+                                         stream_ptr(stream)), 'emu_film_stack_batch')
+
+        if variant is None:
+            from .autotune import default_tuner, size_bucket
+            shape = dict(L=self.L, npw=self.npw, B=size_bucket(B), inc=incoming is not None,
+                         opt=sorted(want))
+            variant = default_tuner().choose('film_stack', shape, list(_lib.FILM_VARIANTS), run, 0,
+                                             stream=stream)
+        run(variant)
         return out
 
 
@@ -369,11 +383,12 @@ class FilmVarSolver(object):
             pl.h_inc.numpy()[:inc_off] = np.concatenate(inc_parts)
         return pl
 
-    def solve(self, pl, stream=None, want_num_prop=False):
+    def solve(self, pl, stream=None, want_num_prop=False, warps=None):
         """Copy a plan to the device and solve it in one launch; returns
         device tensors R_net/T_net [rt_len], a_list/t_list [list_len],
         r_list/flags/specular [B] (and num_prop [np_len]), views of buffers
-        this solver reuses."""
+        this solver reuses.  warps: points (warps) per CTA, 1-8; None takes
+        the autotuner's choice for batches of 1024 points or more, else 8."""
         dev = self.device
         px, py = self._device_orders()
         s = stream if stream is not None else torch.cuda.current_stream(dev)
@@ -403,8 +418,19 @@ class FilmVarSolver(object):
             e.order_len = self._n_orders
             e.n_len, e.h_len, e.inc_len = pl.n_len, pl.h_len, pl.inc_len
             e.rt_len, e.list_len, e.np_len = pl.rt_len, pl.list_len, pl.np_len
-            check(lib().emu_film_var_batch(C.byref(e), ptr(ws), C.c_size_t(ws.numel()),
-                                           stream_ptr(s)), 'emu_film_var_batch')
+
+            def run(w):
+                e.warps_per_cta = int(w)
+                check(lib().emu_film_var_batch(C.byref(e), ptr(ws), C.c_size_t(ws.numel()),
+                                               stream_ptr(s)), 'emu_film_var_batch')
+
+            if warps is None:
+                warps = 0
+                if B >= 1024:
+                    from .autotune import default_tuner, size_bucket
+                    shape = dict(B=size_bucket(B), max_pw=size_bucket(pl.max_pw), max_L=pl.max_layers)
+                    warps = default_tuner().choose('film_var', shape, [2, 4, 8], run, 0, stream=s)
+            run(warps)
         return out
 
     def fetch(self, out, stream=None):

@@ -41,7 +41,8 @@ def _check_sol(sol, nel, name):
 
 
 def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, area_norm=1.0,
-                  dy=1.0, scale2=None, perm2=None, elements_per_chunk=0, precision='fp64'):
+                  dy=1.0, scale2=None, perm2=None, elements_per_chunk=0, precision='fp64',
+                  tc_splits=0, tune=True):
     """J, J_dag (device tensors) and index_pw_inv for a batch of problems.
 
     px, py     int32 [Npw] plane-wave orders (emustack_b200.films.grating_orders)
@@ -49,6 +50,9 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     sol1/sol2  complex128 [B, nel, M, 13, 3] prime / adjoint fields
     scale2     complex128 [B, M] adjoint normalisation factors (or None)
     precision  'fp64' (FP64 GEMM) or 'tf32x3' (tensor cores, split-TF32 products)
+    elements_per_chunk, tc_splits: launch choices (0 = defaults); with
+               tune=True and both 0 the tensor-core path takes the
+               autotuner's choice for this shape (timed on first use)
     """
     dev = dmesh.x.device
     _check_sol(sol1, dmesh.nel, 'sol1')
@@ -81,10 +85,31 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     d.precision = 1 if precision == 'tf32x3' else 0
     err = torch.zeros(1, dtype=torch.int32, device=dev)
     d.d_error = ptr(err)
+    d.tc_splits = int(tc_splits)
     L = lib()
-    nbytes = L.emu_overlap_workspace_size(C.byref(d))
+    cands = None
+    if d.precision == 1 and tune and not elements_per_chunk and not tc_splits:
+        chunks = sorted({min(c, dmesh.nel) for c in (4096, 8192, 16384)})
+        cands = [(c, s) for c in chunks for s in (0, 8)]
+    sizes = []
+    for c in (cands or [(d.elements_per_chunk, d.tc_splits)]):
+        d.elements_per_chunk = c[0]
+        sizes.append(L.emu_overlap_workspace_size(C.byref(d)))
+    nbytes = max(sizes)
     ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
-    check(L.emu_overlap_batch(C.byref(d), ptr(ws), C.c_size_t(nbytes), stream_ptr()), 'emu_overlap_batch')
+
+    def run(c):
+        d.elements_per_chunk, d.tc_splits = int(c[0]), int(c[1])
+        check(L.emu_overlap_batch(C.byref(d), ptr(ws), C.c_size_t(nbytes), stream_ptr()),
+              'emu_overlap_batch')
+
+    choice = (int(elements_per_chunk), int(tc_splits))
+    if cands:
+        from .autotune import default_tuner, size_bucket
+        shape = dict(npw=npw, M=M, nel=size_bucket(dmesh.nel), B=B, J=sol1 is not None,
+                     Jd=sol2 is not None)
+        choice = default_tuner().choose('overlap_tc', shape, cands, run, (0, 0))
+    run(choice)
     if d.precision == 1 and int(err.item()) != 0:
         raise _lib.EmuError(6, 'emu_overlap_batch (tensor-core wait)')
     return J, Jd, inv

@@ -61,8 +61,11 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
+        from emustack_b200.autotune import default_tuner
+        tuned = [e['choice'] for k, e in default_tuner().log if '|overlap_tc|' in k]
         print(json.dumps({'precision': prec, 'nel': nel, 'nval': M, 'npw': npw, 'ms_per_J_pair': ms,
-                          'tflops': flops / (ms / 1e3) / 1e12, 'flops': flops}))
+                          'tflops': flops / (ms / 1e3) / 1e12, 'flops': flops,
+                          'tuned_chunk_splits': tuned[-1] if tuned else None}))
 
 
 if __name__ == '__main__':

@@ -172,6 +172,10 @@ typedef struct {
   int32_t *d_sort_order; /* [B][Npw] air sort order (argsort result)        */
   int32_t *d_specular;   /* [B] specular order index                        */
   int32_t *d_num_prop;   /* [B][L+1] propagating orders per layer, air last */
+  /* launch variant (threads per CTA x minimum CTAs per SM): 0 = 256 x 2
+   * (default), 1 = 128 x 4, 2 = 512 x 1, 3 = 256 x 1 (up to 255 registers);
+   * results are identical, only speed differs (chosen by an autotuner) */
+  int variant;
 } EmuFilmStackBatch;
 
 size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p);
@@ -309,6 +313,8 @@ typedef struct {
                               FP64 sum of the splits                          */
   int32_t *d_error;        /* [1] set to 1 if a bounded device wait gave up
                               (tensor-core path), else left untouched; may be NULL */
+  int tc_splits;           /* tensor-core path: K splits per GEMM (1-64), 0 = one
+                              wave of CTAs; results differ only in FP32 rounding */
 } EmuOverlap;
 
 size_t emu_overlap_workspace_size(const EmuOverlap *p);
@@ -430,6 +436,8 @@ typedef struct {
   /* lengths (elements) of the packed arrays above: a point whose slices
    * fall outside them, or outside the workspace, gets EMU_PT_BAD_POINT */
   int64_t order_len, n_len, h_len, inc_len, rt_len, list_len, np_len;
+  int warps_per_cta;           /* 1-8 warps (points) per CTA, 0 = 8 (fewer if
+                                  the shared-memory slots do not fit); speed only */
 } EmuFilmVarBatch;
 
 /* Host-side plan over the host copy of the descriptors: fills rt_off,
