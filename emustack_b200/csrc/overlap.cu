@@ -505,76 +505,81 @@ __device__ __forceinline__ cd sol1_entry(const cd *s1, int j) {
   return s1[(t < 3 ? t : t + 3) * 3 + 2];
 }
 
+// Diagonal of the orthogonality matrix for a batch: block (chunk c, problem
+// b) stages the element matrices of kDiagChunk elements in shared memory
+// (precomputed once per mesh by elem_scal_kernel), then each thread takes
+// modes n = tid, tid + 128, ... and sums its chunk's contribution.
+constexpr int kDiagChunk = 16;
+
 struct DiagArgs {
   int nval;
-  long nel, chunk;
-  const double *x;
-  const int64_t *tn, *type_el;
-  const cd *pp, *beta1, *sol1, *sol2;
-  const double *k0;
-  cd *part;  // [nchunks][nval]
+  long nel;
+  const double *ms_all;  // [nel][12][22]
+  const int64_t *type_el;
+  const cd *pp, *sol1, *sol2;  // sol: [B][nel][nval][13][3]
+  const double *k0;            // [B]
+  cd *part;                    // [B][nchunks][nval]
 };
 
 __global__ void __launch_bounds__(128) diag_kernel(DiagArgs a) {
-  __shared__ double ms[12][22];
-  __shared__ cd ppk;
-  const long c = blockIdx.x;
-  const long e0 = c * a.chunk, e1 = min(a.nel, e0 + a.chunk);
-  for (int n0 = 0; n0 < a.nval; n0 += blockDim.x) {
-    const int n = n0 + threadIdx.x;
+  __shared__ double ms[kDiagChunk][264];
+  __shared__ cd ppk[kDiagChunk];
+  const long c = blockIdx.x, nch = gridDim.x;
+  const int b = blockIdx.y;
+  const long e0 = c * kDiagChunk;
+  const int ne = (int)min((long)kDiagChunk, a.nel - e0);
+  for (int i = threadIdx.x; i < ne * 264; i += blockDim.x)
+    ms[i / 264][i % 264] = a.ms_all[(size_t)e0 * 264 + i];
+  if (threadIdx.x < ne) {
+    const cd p = a.pp[a.type_el[e0 + threadIdx.x] - 1];
+    ppk[threadIdx.x] = cd{p.x / a.k0[b], p.y / a.k0[b]};
+  }
+  __syncthreads();
+  const size_t sb = (size_t)b * a.nel * a.nval * 39;
+  for (int n = threadIdx.x; n < a.nval; n += blockDim.x) {
     cd acc = cd{0.0, 0.0};
-    for (long el = e0; el < e1; ++el) {
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        const Geo g = element_geo(a.x, a.tn, el);
-        element_scal(g, ms);
-        const cd p = a.pp[a.type_el[el] - 1];
-        ppk = cd{p.x / a.k0[0], p.y / a.k0[0]};
-      }
-      __syncthreads();
-      if (n < a.nval) {
-        const cd *s1 = a.sol1 + ((size_t)el * a.nval + n) * 39;
-        const cd *s2 = a.sol2 + ((size_t)el * a.nval + n) * 39;
-        cd s1v[22];
+    for (int e = 0; e < ne; ++e) {
+      const cd *s1 = a.sol1 + sb + ((size_t)(e0 + e) * a.nval + n) * 39;
+      const cd *s2 = a.sol2 + sb + ((size_t)(e0 + e) * a.nval + n) * 39;
+      cd s1v[22];
 #pragma unroll
-        for (int j = 0; j < 22; ++j) s1v[j] = sol1_entry(s1, j);
-        cd e = cd{0.0, 0.0};
+      for (int j = 0; j < 22; ++j) s1v[j] = sol1_entry(s1, j);
+      const double *m = ms[e];
+      cd v_e = cd{0.0, 0.0};
 #pragma unroll
-        for (int i = 0; i < 12; ++i) {
-          cd v = cd{0.0, 0.0};
+      for (int i = 0; i < 12; ++i) {
+        cd v = cd{0.0, 0.0};
 #pragma unroll
-          for (int j = 0; j < 22; ++j) {
-            v.x = fma(ms[i][j], s1v[j].x, v.x);
-            v.y = fma(ms[i][j], s1v[j].y, v.y);
-          }
-          e = cadd(e, cmul(v, s2[(i >> 1) * 3 + (i & 1)]));
+        for (int j = 0; j < 22; ++j) {
+          v.x = fma(m[i * 22 + j], s1v[j].x, v.x);
+          v.y = fma(m[i * 22 + j], s1v[j].y, v.y);
         }
-        acc = cadd(acc, cmul(e, ppk));
+        v_e = cadd(v_e, cmul(v, s2[(i >> 1) * 3 + (i & 1)]));
       }
+      acc = cadd(acc, cmul(v_e, ppk[e]));
     }
-    if (n < a.nval) a.part[(size_t)c * a.nval + n] = acc;
+    a.part[((size_t)b * nch + c) * a.nval + n] = acc;
   }
 }
 
-// diag(n) = beta1(n) sum_chunks part ; scale = 1/sqrt(diag)^2 (or 1)
-__global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, const cd *beta1, cd *diag,
-                                   cd *scale, int *n_small) {
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nval; n += gridDim.x * blockDim.x) {
+// diag(n) = beta1(n) sum_chunks part ; scale = 1/sqrt(diag)^2 (or 1); one
+// thread per (problem, mode)
+__global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, int batch, const cd *beta1,
+                                   cd *diag, cd *scale, int *n_small) {
+  const long total = (long)batch * nval;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / nval), n = (int)(t % nval);
     cd s = cd{0.0, 0.0};
-    for (int c = 0; c < nchunks; ++c) s = cadd(s, part[(size_t)c * nval + n]);
-    s = cmul(s, beta1[n]);
-    diag[n] = s;
-    if (hypot(s.x, s.y) <= 1e-7) atomicAdd(n_small, 1);
+    for (int c = 0; c < nchunks; ++c) s = cadd(s, part[((size_t)b * nchunks + c) * nval + n]);
+    s = cmul(s, beta1[t]);
+    diag[t] = s;
+    if (hypot(s.x, s.y) <= 1e-7) atomicAdd(n_small + b, 1);
     const cd z = csqrt_p(s);
-    scale[n] = (hypot(z.x, z.y) > 1e-8) ? crecip(cmul(z, z)) : cd{1.0, 0.0};
+    scale[t] = (hypot(z.x, z.y) > 1e-8) ? crecip(cmul(z, z)) : cd{1.0, 0.0};
   }
 }
 
 // ---------------------------------------------------------------- tensor-core operands
-// A = [[Er, -Ei], [Ei, Er]] (2 npw x 2K) from E~ (conjugated for J_dag), and
-// B (2M x 2K) with B[c*M + n][half*K + el*6 + node] = Re/Im sol(c, node, n, el),
-// both split into TF32 hi + lo.  C = A B^T then holds Re G (rows 0..npw-1) and
-// Im G (rows npw..2npw-1).
 // Tensor-core path: the complex contractions G = E~ . S1 and
 // G_dag = conj(E~) . S2 = conj(E~ . conj(S2)) share one real GEMM
 //   C[2 npw][Nb] = A[2 npw][2 K] . B[Nb][2 K]^T
@@ -729,12 +734,21 @@ __global__ void pair_swap_kernel(const cd *ovl, int nval, int32_t *perm, cd *dia
 }  // namespace
 
 // =============================================================== C ABI
+// K splits of the FP64 overlap GEMM: 4, or enough CTAs for two waves when
+// the output has few 64 x 64 tiles (few plane waves or modes)
+static int ov_nparts(int npw, int M) {
+  const int tiles = ((2 * M + kTN - 1) / kTN) * ((npw + kTM - 1) / kTM);
+  if (tiles >= 32) return 4;
+  const int n = (2 * emu::sm_count() + tiles - 1) / tiles;
+  return n < 4 ? 4 : (n > 64 ? 64 : n);
+}
+
 extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
   if (!p || p->n_pw < 1 || p->nval < 1 || p->nel < 1) return 0;
   const long long npw = p->n_pw, M = p->nval;
   const long long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
   const long long ne = chunk < p->nel ? chunk : p->nel;
-  const long long nparts = 4;
+  const long long nparts = ov_nparts(p->n_pw, p->nval);
   size_t b = 0;
   b += align_up(sizeof(int32_t) * npw, 256);                 // pos
   b += align_up(sizeof(double) * 3 * npw, 256);              // tab
@@ -770,7 +784,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   const int npw = p->n_pw, M = p->nval;
   const long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
   const long nec = chunk < p->nel ? chunk : p->nel;
-  const int nparts = 4;
+  const int nparts = ov_nparts(npw, M);
   char *w = (char *)d_workspace;
   auto take = [&](size_t bytes) {
     char *r = w;
@@ -924,10 +938,11 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
 
 // ---------------------------------------------------------------- normalisation
 extern "C" size_t emu_mode_overlap_workspace_size(const EmuNormalise *p) {
-  if (!p || p->nval < 1 || p->nel < 1) return 0;
-  const long long chunk = 64;
-  const long long nch = (p->nel + chunk - 1) / chunk;
-  return align_up(sizeof(cd) * nch * p->nval, 256) + 256;
+  if (!p || p->nval < 1 || p->nel < 1 || p->batch < 0) return 0;
+  const long long nch = (p->nel + kDiagChunk - 1) / kDiagChunk;
+  const long long B = p->batch > 0 ? p->batch : 1;
+  return align_up(sizeof(double) * 264 * (size_t)p->nel, 256) +
+         align_up(sizeof(cd) * B * nch * p->nval, 256) + 256;
 }
 
 extern "C" int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, size_t workspace_bytes,
@@ -938,34 +953,35 @@ extern "C" int emu_mode_overlap_diag(const EmuNormalise *p, void *d_workspace, s
       !p->d_sol1 || !p->d_sol2 || !p->d_diag || !p->d_scale || !p->d_n_small)
     return EMU_E_ARG;
   if (p->batch == 0) return EMU_OK;
+  if (p->batch > 65535) return EMU_E_SHAPE;
   if (!d_workspace || workspace_bytes < emu_mode_overlap_workspace_size(p)) return EMU_E_WORKSPACE;
   int st = upload_tables();
   if (st != EMU_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
-  const long chunk = 64;
-  const long nch = (p->nel + chunk - 1) / chunk;
-  cd *part = (cd *)d_workspace;
+  const long nch = (p->nel + kDiagChunk - 1) / kDiagChunk;
+  double *ms_all = (double *)d_workspace;
+  cd *part = (cd *)((char *)d_workspace + align_up(sizeof(double) * 264 * (size_t)p->nel, 256));
   if (cudaMemsetAsync(p->d_n_small, 0, sizeof(int32_t) * p->batch, s) != cudaSuccess) return EMU_E_CUDA;
-  for (int b = 0; b < p->batch; ++b) {
-    DiagArgs a;
-    a.nval = p->nval;
-    a.nel = p->nel;
-    a.chunk = chunk;
-    a.x = p->d_x;
-    a.tn = p->d_table_nod;
-    a.type_el = p->d_type_el;
-    a.pp = (const cd *)p->d_pp;
-    a.beta1 = (const cd *)p->d_beta1 + (size_t)b * p->nval;
-    a.sol1 = (const cd *)p->d_sol1 + (size_t)b * p->nel * p->nval * 39;
-    a.sol2 = (const cd *)p->d_sol2 + (size_t)b * p->nel * p->nval * 39;
-    a.k0 = p->d_k0 + b;
-    a.part = part;
-    diag_kernel<<<(int)nch, 128, 0, s>>>(a);
-    diag_finish_kernel<<<(p->nval + 127) / 128, 128, 0, s>>>(
-        part, (int)nch, p->nval, a.beta1, (cd *)p->d_diag + (size_t)b * p->nval,
-        (cd *)p->d_scale + (size_t)b * p->nval, p->d_n_small + b);
-    emu::note_launch(2);
-  }
+  const int sms = emu::sm_count();
+  const long eb = (p->nel + 127) / 128;
+  elem_scal_kernel<<<(int)(eb < 8 * sms ? eb : 8 * sms), 128, 0, s>>>(p->d_x, p->d_table_nod, p->nel, ms_all);
+  DiagArgs a;
+  a.nval = p->nval;
+  a.nel = p->nel;
+  a.ms_all = ms_all;
+  a.type_el = p->d_type_el;
+  a.pp = (const cd *)p->d_pp;
+  a.sol1 = (const cd *)p->d_sol1;
+  a.sol2 = (const cd *)p->d_sol2;
+  a.k0 = p->d_k0;
+  a.part = part;
+  diag_kernel<<<dim3((unsigned)nch, (unsigned)p->batch), 128, 0, s>>>(a);
+  const long nt = (long)p->batch * p->nval;
+  const long fb = (nt + 127) / 128;
+  diag_finish_kernel<<<(int)(fb < 8 * sms ? fb : 8 * sms), 128, 0, s>>>(
+      part, (int)nch, p->nval, p->batch, (const cd *)p->d_beta1, (cd *)p->d_diag, (cd *)p->d_scale,
+      p->d_n_small);
+  emu::note_launch(3);
   return emu::check_launch();
 }
 

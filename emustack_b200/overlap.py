@@ -31,6 +31,14 @@ class DeviceMesh(object):
         self.nel, self.npt = mesh.nel, mesh.npt
 
 
+def _dev_int32(a, dev):
+    """Device int32 copy of an order list (kept as is if it already is one,
+    so callers inside CUDA-graph capture make no host copies)."""
+    if isinstance(a, torch.Tensor) and a.is_cuda and a.dtype == torch.int32:
+        return a
+    return torch.as_tensor(np.asarray(a, np.int32), device=dev)
+
+
 def _check_sol(sol, nel, name):
     if sol is None:
         return
@@ -42,7 +50,7 @@ def _check_sol(sol, nel, name):
 
 def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, area_norm=1.0,
                   dy=1.0, scale2=None, perm2=None, elements_per_chunk=0, precision='fp64',
-                  tc_splits=0, tune=True):
+                  tc_splits=0, tune=True, check_error=True):
     """J, J_dag (device tensors) and index_pw_inv for a batch of problems.
 
     px, py     int32 [Npw] plane-wave orders (emustack_b200.films.grating_orders)
@@ -53,6 +61,8 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     elements_per_chunk, tc_splits: launch choices (0 = defaults); with
                tune=True and both 0 the tensor-core path takes the
                autotuner's choice for this shape (timed on first use)
+    check_error: read the tensor-core wait flag back (a host synchronisation);
+               False inside CUDA-graph capture (the flag stays on the device)
     """
     dev = dmesh.x.device
     _check_sol(sol1, dmesh.nel, 'sol1')
@@ -60,8 +70,7 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     ref = sol1 if sol1 is not None else sol2
     B, M = int(ref.shape[0]), int(ref.shape[2])
     npw = len(px)
-    d_px = torch.as_tensor(np.asarray(px, np.int32), device=dev)
-    d_py = torch.as_tensor(np.asarray(py, np.int32), device=dev)
+    d_px, d_py = _dev_int32(px, dev), _dev_int32(py, dev)
     for t, nm, dt in ((bloch, 'bloch', torch.float64), (k0, 'k0', torch.float64)):
         if t.dtype != dt or not t.is_cuda or not t.is_contiguous():
             raise TypeError('%s must be a contiguous CUDA %s tensor' % (nm, dt))
@@ -110,7 +119,7 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
                      Jd=sol2 is not None)
         choice = default_tuner().choose('overlap_tc', shape, cands, run, (0, 0))
     run(choice)
-    if d.precision == 1 and int(err.item()) != 0:
+    if check_error and d.precision == 1 and int(err.item()) != 0:
         raise _lib.EmuError(6, 'emu_overlap_batch (tensor-core wait)')
     return J, Jd, inv
 
@@ -144,7 +153,8 @@ def mode_normalisation(dmesh, pp, k0, beta1, sol1, sol2):
     _check_sol(sol1, dmesh.nel, 'sol1')
     _check_sol(sol2, dmesh.nel, 'sol2')
     B, M = int(sol1.shape[0]), int(sol1.shape[2])
-    pp = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
+    if not (isinstance(pp, torch.Tensor) and pp.is_cuda and pp.dtype == c128):
+        pp = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
     if beta1.dtype != c128 or not beta1.is_cuda:
         raise TypeError('beta1 must be a CUDA complex128 tensor')
     if k0.dtype != torch.float64 or not k0.is_cuda or tuple(k0.shape) != (B,):
