@@ -143,6 +143,7 @@ class EmuStackDense(C.Structure):
         ('d_vec_coef_down', vp), ('d_vec_coef_up', vp),
         ('vec_coef_down_stride', C.c_longlong), ('vec_coef_up_stride', C.c_longlong),
         ('save_lists', C.c_int), ('d_tnet_list', vp), ('d_rnet_list', vp),
+        ('mode', C.c_int),
     ]
 
 

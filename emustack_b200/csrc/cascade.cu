@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include "dense_la.cuh"
+#include "dense_multi.cuh"
 #include "emu_internal.h"
 
 namespace {
@@ -43,6 +44,7 @@ struct StackArgs {
   long long ws_stride;
   int *ipiv;
   double inv_sqrt2;
+  int flux_only;  // the cascade was run by stack_dense_multi: outputs and fluxes only
 };
 
 struct Smem {
@@ -142,6 +144,11 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
 
   auto lay_ptr = [&](const cd *p, long long s) { return p + (size_t)b * s; };
 
+  int slot = 0;       // index of the current rnet in Rl
+  int tcols = P;      // columns of tnet
+  if (a.flux_only) {
+    slot = 2 * L - 3;
+  } else {
   // ---- substrate: tnet = T12_0, rnet = R12_0
   {
     const DLayer &l0 = a.lay[0];
@@ -158,8 +165,6 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
       copy_mat(a.rnl + (size_t)b * (2 * L - 2) * DD, P, Rl, P, P, P);
     }
   }
-  int slot = 0;       // index of the current rnet in Rl
-  int tcols = P;      // columns of tnet
   for (int i = 1; i < L; ++i) {
     const DLayer &ly = a.lay[i];
     const int M = ly.M;
@@ -299,12 +304,13 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
       copy_mat(a.rnl + ((size_t)b * (2 * L - 2) + slot) * DD, P, rn2, P, P, P);
     }
   }
+  }  // cascade
   // outputs R_net (P x P), T_net (M0 x P)
   const cd *Rtop = Rl + (size_t)slot * DD;
   copy_mat(a.R_net + (size_t)b * P * P, P, Rtop, P, P, P);
   copy_mat(a.T_net + (size_t)b * M0 * P, P, tnet, P, M0, P);
   __syncthreads();
-  if (tid == 0 && a.info) a.info[b] = info;
+  if (tid == 0 && a.info && !a.flux_only) a.info[b] = info;
   if (!a.calc_fluxes) return;
 
   // ---------------- fluxes, top to bottom (stack.py:289-426)
@@ -432,6 +438,266 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Multi-CTA cascade.  The same steps as stack_dense_kernel, in the same
+// order and with the same arithmetic (results are bit-identical), but each
+// step is a launch over all solves of the batch that spreads the matrices
+// over many CTAs: batched tiled GEMMs, getrf_multi / getrs_multi and
+// elementwise kernels.  The workspace holds exactly what the one-CTA kernel
+// keeps (rnet / inv_t21 / inv_t12 lists, propagation vectors, tnet and
+// scratch), so the flux pass runs afterwards as stack_dense_kernel with
+// flux_only set.  Large matrices (P, M in the hundreds) then use the whole
+// GPU even for a handful of solves.
+
+struct MultiWs {
+  long long stride, DD;
+  int D, L;
+  cd *ws;
+  __host__ __device__ cd *base(long long b) const { return ws + b * stride; }
+  __host__ __device__ cd *Rl(int slot) const { return ws + (long long)slot * DD; }  // add b * stride
+  __host__ __device__ cd *X1(int i) const { return ws + (long long)(2 * L - 2 + i) * DD; }
+  __host__ __device__ cd *X2(int i) const { return ws + (long long)(2 * L - 2 + L - 1 + i) * DD; }
+  __host__ __device__ cd *Pl(int i) const {
+    return ws + (long long)(2 * L - 2 + L - 1 + (L > 2 ? L - 2 : 0)) * DD + (long long)i * D;
+  }
+  __host__ __device__ cd *tnet() const {
+    return ws + (long long)(2 * L - 2 + L - 1 + (L > 2 ? L - 2 : 0)) * DD + (long long)(L > 2 ? L - 2 : 0) * D;
+  }
+  __host__ __device__ cd *T() const { return tnet() + DD; }
+  __host__ __device__ cd *Y() const { return tnet() + 2 * DD; }
+  __host__ __device__ cd *Z() const { return tnet() + 3 * DD; }
+};
+
+#define EW_LOOP(total)                                                                        \
+  const long long b = blockIdx.y;                                                             \
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (total);           \
+       e += (long long)gridDim.x * blockDim.x)
+
+inline dim3 ew_grid(long long n, int batch) {
+  long long g = (n + 255) / 256;
+  if (g > 1024) g = 1024;
+  return dim3((unsigned)(g < 1 ? 1 : g), (unsigned)batch);
+}
+
+// dst[b] (rows x cols, ldd) = src[b] (lds)
+__global__ void ew_copy(cd *dst, long long sd, int ldd, const cd *src, long long ss, int lds, int rows, int cols) {
+  EW_LOOP((long long)rows * cols) {
+    const int r = (int)(e / cols), c = (int)(e % cols);
+    dst[b * sd + (long long)r * ldd + c] = src[b * ss + (long long)r * lds + c];
+  }
+}
+
+// dst[b] = diag(d[b]) (n x n)
+__global__ void ew_diag(cd *dst, long long sd, const cd *d, long long sdd, int n) {
+  EW_LOOP((long long)n * n) {
+    const int r = (int)(e / n), c = (int)(e % n);
+    dst[b * sd + e] = (r == c) ? d[b * sdd + r] : cd{0.0, 0.0};
+  }
+}
+
+// dst[b] = I (n x n)
+__global__ void ew_eye(cd *dst, long long sd, int n) {
+  EW_LOOP((long long)n * n) dst[b * sd + e] = cd{(e / n == e % n) ? 1.0 : 0.0, 0.0};
+}
+
+// shear: Z = Qinv rnet Q (P x P), tnet[:, c] *= Q(c) (M0 x tcols)
+__global__ void ew_shear(StackArgs a, MultiWs w, int slot, double c0, double c1, int M0, int tcols) {
+  const int P = a.P;
+  EW_LOOP((long long)P * P + (long long)M0 * tcols) {
+    cd *base = w.base(b);
+    if (e < (long long)P * P) {
+      const int r = (int)(e / P), c = (int)(e % P);
+      const cd *rnet = base + (w.Rl(slot) - w.ws);
+      cd *Z = base + (w.Z() - w.ws);
+      Z[e] = cmul(cmul(shear_q(a, (int)b, r, -1 * c0, -1 * c1), rnet[e]), shear_q(a, (int)b, c, c0, c1));
+    } else {
+      const long long f = e - (long long)P * P;
+      const int c = (int)(f % tcols);
+      cd *tn = base + (w.tnet() - w.ws);
+      tn[f] = cmul(tn[f], shear_q(a, (int)b, c, c0, c1));
+    }
+  }
+}
+
+// T = I - diag(r12) rg  (P x P)
+__global__ void ew_t_gap_diag(cd *T, long long sT, const cd *r12, long long sr, const cd *rg, long long sg, int P) {
+  EW_LOOP((long long)P * P) {
+    const int r = (int)(e / P), c = (int)(e % P);
+    T[b * sT + e] = csub(cd{(r == c) ? 1.0 : 0.0, 0.0}, cmul(r12[b * sr + r], rg[b * sg + e]));
+  }
+}
+
+// rn1 = diag(t12) Y + diag(r21)  (P x P)
+__global__ void ew_rn_gap_diag(cd *rn, long long sn, const cd *t12, long long st, const cd *Y, long long sy,
+                               const cd *r21, long long sr, int P) {
+  EW_LOOP((long long)P * P) {
+    const int r = (int)(e / P), c = (int)(e % P);
+    const cd v = cmul(t12[b * st + r], Y[b * sy + e]);
+    rn[b * sn + e] = (r == c) ? cadd(r21[b * sr + r], v) : v;
+  }
+}
+
+// pd = exp(i kz h)  (M)
+__global__ void ew_prop(cd *pd, long long sp, const cd *kz, long long skz, double hn, int M) {
+  EW_LOOP(M) pd[b * sp + e] = cexp_ikh(kz[b * skz + e], hn);
+}
+
+// Z = diag(pd) rn1 diag(pd), T = I  (M x M)
+__global__ void ew_layer_dense(cd *Z, cd *T, long long sw, const cd *pd, long long sp, const cd *rn1, int M) {
+  EW_LOOP((long long)M * M) {
+    const int r = (int)(e / M), c = (int)(e % M);
+    const cd *p = pd + b * sp;
+    Z[b * sw + e] = cmul(cmul(p[r], rn1[b * sw + e]), p[c]);
+    T[b * sw + e] = cd{(r == c) ? 1.0 : 0.0, 0.0};
+  }
+}
+
+// T = I - diag(r21) diag(pd) rn1 diag(pd)  (M x M)
+__global__ void ew_t_layer_diag(cd *T, long long sw, const cd *r21, long long sr, const cd *pd, long long sp,
+                                const cd *rn1, int M) {
+  EW_LOOP((long long)M * M) {
+    const int r = (int)(e / M), c = (int)(e % M);
+    const cd *p = pd + b * sp;
+    T[b * sw + e] = csub(cd{(r == c) ? 1.0 : 0.0, 0.0},
+                         cmul(cmul(cmul(r21[b * sr + r], p[r]), rn1[b * sw + e]), p[c]));
+  }
+}
+
+// Z = diag(pd) X2  (M x P)
+__global__ void ew_rowscale(cd *Z, long long sw, const cd *pd, long long sp, const cd *X2, int M, int P) {
+  EW_LOOP((long long)M * P) Z[b * sw + e] = cmul(pd[b * sp + e / P], X2[b * sw + e]);
+}
+
+// rn2 = diag(t21) diag(pd) Y + diag(r12)  (P x P)
+__global__ void ew_rn_layer_diag(cd *rn, long long sw, const cd *t21, long long st, const cd *pd, long long sp,
+                                 const cd *Y, const cd *r12, long long sr, int P) {
+  EW_LOOP((long long)P * P) {
+    const int r = (int)(e / P), c = (int)(e % P);
+    const cd v = cmul(cmul(t21[b * st + r], pd[b * sp + r]), Y[b * sw + e]);
+    rn[b * sw + e] = (r == c) ? cadd(r12[b * sr + r], v) : v;
+  }
+}
+
+int stack_dense_multi(const StackArgs &a, cudaStream_t s) {
+  const int B = a.B, L = a.L, P = a.P, D = a.D;
+  MultiWs w;
+  w.stride = a.ws_stride;
+  w.DD = (long long)D * D;
+  w.D = D;
+  w.L = L;
+  w.ws = a.ws;
+  const long long S = w.stride;       // batch stride of every workspace object
+  const long long sip = D;            // ipiv batch stride
+  const int M0 = a.lay[0].M;
+  const cd one{1.0, 0.0}, zero{0.0, 0.0}, mone{-1.0, 0.0};
+  const long long DD = w.DD, LS = (long long)(2 * L - 2) * DD;  // saved-list stride in tnl / rnl
+  int n_launch = 0;
+  auto ew = [&](long long n) {
+    ++n_launch;
+    return ew_grid(n, B);
+  };
+  if (a.info && cudaMemsetAsync(a.info, 0, sizeof(int) * B, s) != cudaSuccess) return EMU_E_CUDA;
+  cd *tnet = w.tnet(), *T = w.T(), *Y = w.Y(), *Z = w.Z();
+  // ---- substrate
+  {
+    const DLayer &l0 = a.lay[0];
+    if (l0.dense) {
+      ew_copy<<<ew(M0 * P), 256, 0, s>>>(tnet, S, P, l0.T12, l0.sT12, P, M0, P);
+      ew_copy<<<ew(P * P), 256, 0, s>>>(w.Rl(0), S, P, l0.R12, l0.sR12, P, P, P);
+    } else {
+      ew_diag<<<ew(P * P), 256, 0, s>>>(tnet, S, l0.T12, l0.sT12, P);
+      ew_diag<<<ew(P * P), 256, 0, s>>>(w.Rl(0), S, l0.R12, l0.sR12, P);
+    }
+    if (a.save_lists) {
+      ew_copy<<<ew(M0 * P), 256, 0, s>>>(a.tnl, LS, P, tnet, S, P, M0, P);
+      ew_copy<<<ew(P * P), 256, 0, s>>>(a.rnl, LS, P, w.Rl(0), S, P, P, P);
+    }
+  }
+  int slot = 0, tcols = P;
+  for (int i = 1; i < L; ++i) {
+    const DLayer &ly = a.lay[i];
+    const int M = ly.M;
+    cd *rnet = w.Rl(slot), *X1 = w.X1(i - 1), *rn1 = w.Rl(slot + 1);
+    const cd *rg = rnet;
+    if (a.has_shear) {
+      double c0, c1;
+      if (i < L - 1) {
+        c0 = a.lay[i - 1].sh0 - ly.sh0;
+        c1 = a.lay[i - 1].sh1 - ly.sh1;
+      } else {
+        c0 = ly.sh0;
+        c1 = ly.sh1;
+      }
+      ew_shear<<<ew((long long)P * P + (long long)M0 * tcols), 256, 0, s>>>(a, w, slot, c0, c1, M0, tcols);
+      rg = Z;
+    }
+    if (ly.dense) {
+      ew_eye<<<ew(P * P), 256, 0, s>>>(T, S, P);
+      bgemm(P, P, P, mone, ly.R12, ly.sR12, P, rg, S, P, one, T, S, P, B, s);
+      ew_copy<<<ew(P * M), 256, 0, s>>>(X1, S, M, ly.T21, ly.sT21, M, P, M);
+    } else {
+      ew_t_gap_diag<<<ew(P * P), 256, 0, s>>>(T, S, ly.R12, ly.sR12, rg, S, P);
+      ew_diag<<<ew(P * P), 256, 0, s>>>(X1, S, ly.T21, ly.sT21, P);
+    }
+    getrf_multi(P, T, S, P, a.ipiv, sip, a.info, (2 * i - 1) * 100000, B, s);
+    getrs_multi(P, M, T, S, P, a.ipiv, sip, X1, S, M, B, s);
+    bgemm(M0, M, P, one, tnet, S, tcols, X1, S, M, zero, Y, S, M, B, s);
+    ew_copy<<<ew(M0 * M), 256, 0, s>>>(tnet, S, M, Y, S, M, M0, M);
+    tcols = M;
+    if (ly.dense) {
+      bgemm(M, P, P, one, ly.T12, ly.sT12, P, rg, S, P, zero, Y, S, P, B, s);
+      ew_copy<<<ew(M * M), 256, 0, s>>>(rn1, S, M, ly.R21, ly.sR21, M, M, M);
+      bgemm(M, M, P, one, Y, S, P, X1, S, M, one, rn1, S, M, B, s);
+    } else {
+      bgemm(P, P, P, one, rg, S, P, X1, S, P, zero, Y, S, P, B, s);
+      ew_rn_gap_diag<<<ew(P * P), 256, 0, s>>>(rn1, S, ly.T12, ly.sT12, Y, S, ly.R21, ly.sR21, P);
+    }
+    slot += 1;
+    if (a.save_lists) {
+      ew_copy<<<ew(M0 * tcols), 256, 0, s>>>(a.tnl + slot * DD, LS, tcols, tnet, S, tcols, M0, tcols);
+      ew_copy<<<ew(M * M), 256, 0, s>>>(a.rnl + slot * DD, LS, M, rn1, S, M, M, M);
+    }
+    if (i == L - 1) break;
+    cd *pd = w.Pl(i - 1);
+    ew_prop<<<ew(M), 256, 0, s>>>(pd, S, ly.kz, ly.skz, ly.hn, M);
+    cd *X2 = w.X2(i - 1), *rn2 = w.Rl(slot + 1);
+    if (ly.dense) {
+      ew_layer_dense<<<ew(M * M), 256, 0, s>>>(Z, T, S, pd, S, rn1, M);
+      bgemm(M, M, M, mone, ly.R21, ly.sR21, M, Z, S, M, one, T, S, M, B, s);
+      ew_copy<<<ew(M * P), 256, 0, s>>>(X2, S, P, ly.T12, ly.sT12, P, M, P);
+    } else {
+      ew_t_layer_diag<<<ew(M * M), 256, 0, s>>>(T, S, ly.R21, ly.sR21, pd, S, rn1, M);
+      ew_diag<<<ew(P * P), 256, 0, s>>>(X2, S, ly.T12, ly.sT12, P);
+    }
+    getrf_multi(M, T, S, M, a.ipiv, sip, a.info, (2 * i) * 100000, B, s);
+    getrs_multi(M, P, T, S, M, a.ipiv, sip, X2, S, P, B, s);
+    ew_rowscale<<<ew(M * P), 256, 0, s>>>(Z, S, pd, S, X2, M, P);
+    bgemm(M0, P, M, one, tnet, S, tcols, Z, S, P, zero, Y, S, P, B, s);
+    ew_copy<<<ew(M0 * P), 256, 0, s>>>(tnet, S, P, Y, S, P, M0, P);
+    tcols = P;
+    if (ly.dense) {
+      bgemm(P, M, M, one, ly.T21, ly.sT21, M, rn1, S, M, zero, Y, S, M, B, s, pd, S);
+      ew_copy<<<ew(P * P), 256, 0, s>>>(rn2, S, P, ly.R12, ly.sR12, P, P, P);
+      bgemm(P, P, M, one, Y, S, M, Z, S, P, one, rn2, S, P, B, s);
+    } else {
+      bgemm(P, P, P, one, rn1, S, P, Z, S, P, zero, Y, S, P, B, s);
+      ew_rn_layer_diag<<<ew(P * P), 256, 0, s>>>(rn2, S, ly.T21, ly.sT21, pd, S, Y, ly.R12, ly.sR12, P);
+    }
+    slot += 1;
+    if (a.save_lists) {
+      ew_copy<<<ew(M0 * P), 256, 0, s>>>(a.tnl + slot * DD, LS, P, tnet, S, P, M0, P);
+      ew_copy<<<ew(P * P), 256, 0, s>>>(a.rnl + slot * DD, LS, P, rn2, S, P, P, P);
+    }
+  }
+  note_launch(n_launch);
+  // outputs and fluxes from the saved state
+  StackArgs f = a;
+  f.flux_only = 1;
+  stack_dense_kernel<<<B, kDLThreads, 0, s>>>(f);
+  note_launch();
+  return check_launch();
+}
+
 }  // namespace
 
 namespace {
@@ -469,6 +735,8 @@ int validate(const EmuStackDense *p) {
   }
   if (p->h_shears && (!p->d_air_alphas || (p->shear_ncoord == 2 && !p->d_air_betas))) return EMU_E_ARG;
   if (p->save_lists && (!p->d_tnet_list || !p->d_rnet_list)) return EMU_E_ARG;
+  if (p->mode < 0 || p->mode > 2) return EMU_E_ARG;
+  if (p->batch > 65535) return EMU_E_SHAPE;
   return EMU_OK;
 }
 
@@ -546,6 +814,12 @@ extern "C" int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace,
   a.ws_stride = per_solve_elems(p);
   a.ipiv = (int *)((char *)d_workspace + align_up((size_t)p->batch * a.ws_stride * sizeof(cd), 16));
   a.inv_sqrt2 = 1.0 / sqrt(2.0);
+  a.flux_only = 0;
+  // one CTA per solve while the batch fills the GPU and matrices are small;
+  // the multi-CTA cascade for large matrices or few solves
+  int mode = p->mode;
+  if (mode == 0) mode = (a.D >= 256 || (a.D >= 96 && p->batch < emu::sm_count())) ? 2 : 1;
+  if (mode == 2) return stack_dense_multi(a, (cudaStream_t)stream);
   stack_dense_kernel<<<p->batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);
   emu::note_launch();
   return emu::check_launch();

@@ -136,7 +136,9 @@ class DenseStackSolver(object):
 
     def solve(self, layers, P, pol='TE', incoming=None, specular=None, num_prop=None,
               calc_fluxes=True, shears=None, air_alphas=None, air_betas=None,
-              want_vec_coef=False, save_lists=False):
+              want_vec_coef=False, save_lists=False, mode=0):
+        """mode: 0 automatic, 1 one CTA per solve, 2 every step spread over
+        many CTAs (emu_stack_dense_batch); results are identical."""
         L = len(layers)
         B = int(layers[0].R12.shape[0])
         dev = self.device
@@ -159,6 +161,7 @@ class DenseStackSolver(object):
             e.height_norm = ly.height_norm
         d = EmuStackDense()
         d.batch, d.n_layers, d.P = B, L, P
+        d.mode = int(mode)
         d.h_layers = C.cast(arr, C.POINTER(EmuLayer))
         sh_arr = None
         if shears is not None:

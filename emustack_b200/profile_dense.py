@@ -45,6 +45,7 @@ def main():
     ap.add_argument('--batch', type=int, default=148)
     ap.add_argument('--steps', type=int, default=2)
     ap.add_argument('--warmup', type=int, default=1)
+    ap.add_argument('--mode', type=int, default=0, help='cascade: 0 auto, 1 one CTA per solve, 2 multi-CTA')
     args = ap.parse_args()
     from emustack_b200.dense import DenseLayer, DenseStackSolver, film_interface, interface_dense
     from emustack_b200.films import grating_orders
@@ -106,7 +107,7 @@ def main():
             R12, T12, R21, T21, _ = ifs[k]
             lay.append(DenseLayer(R12, T12, R21, T21, True, kzs[k], hs[k]))
         lay.append(DenseLayer(Ra, Ta, -Ra, Ta, False))
-        return solver.solve(lay, P, pol='TE', specular=spec, num_prop=nprop)
+        return solver.solve(lay, P, pol='TE', specular=spec, num_prop=nprop, mode=args.mode)
 
     for _ in range(args.warmup):
         ifs = interfaces()
@@ -132,7 +133,7 @@ def main():
     info = out['info'].cpu().numpy()
     rate = lambda f, ms: B * f / (ms / 1e3) / 1e12
     print(json.dumps({
-        'P': P, 'M': M, 'layers': K, 'batch': B,
+        'P': P, 'M': M, 'layers': K, 'batch': B, 'mode': args.mode,
         'interfaces_ms_per_wl': t_if / B, 'cascade_ms_per_wl': t_cs / B,
         'total_ms_per_wl': (t_if + t_cs) / B, 'wl_per_s': B / ((t_if + t_cs) / 1e3),
         'interfaces_tflops': rate(f_if, t_if), 'cascade_tflops': rate(f_cs, t_cs),

@@ -266,6 +266,9 @@ typedef struct {
   int save_lists;              /* 1: fill d_tnet_list / d_rnet_list         */
   emu_c128 *d_tnet_list;       /* [batch][2L-2][list_stride]                */
   emu_c128 *d_rnet_list;
+  int mode;                    /* 0 auto; 1 one CTA per solve; 2 each step
+                                  spread over many CTAs (large matrices, few
+                                  solves); identical results                 */
 } EmuStackDense;
 
 size_t emu_stack_dense_workspace_size(const EmuStackDense *p);

@@ -155,3 +155,73 @@ def test_film_stack_through_dense_path_matches_film_kernel():
     st.calc_scat(pol=pt['pol'], save_scat_list=True)
     np.testing.assert_allclose(st.R_net, pt['R_net'], **TOL)
     np.testing.assert_allclose(np.asarray(st.a_list, float), pt['a_list'], **TOL)
+
+
+def _random_dense_stack(rng, B, P, Ms, dense_flags, dev):
+    """Substrate film, finite layers (dense with M modes or films), air
+    superstrate film: random interface matrices of moderate norm."""
+    from emustack_b200.dense import DenseLayer
+    c = lambda *s: torch.tensor(_rand(s, rng), device=dev)
+    layers = [DenseLayer(*(0.4 * c(B, P) for _ in range(4)), False)]
+    for M, dense in zip(Ms, dense_flags):
+        kz = torch.tensor(rng.uniform(0, 3, (B, M)) + 1j * rng.uniform(0, 0.3, (B, M)), device=dev)
+        if dense:
+            R12, T12 = 0.3 * c(B, P, P) / np.sqrt(P), 0.3 * c(B, M, P) / np.sqrt(P)
+            R21, T21 = 0.3 * c(B, M, M) / np.sqrt(M), 0.3 * c(B, P, M) / np.sqrt(M)
+            layers.append(DenseLayer(R12, T12, R21, T21, True, kz, rng.uniform(0.05, 0.4)))
+        else:
+            kz = kz[:, :P].contiguous() if M >= P else torch.cat([kz, kz], 1)[:, :P].contiguous()
+            layers.append(DenseLayer(*(0.4 * c(B, P) for _ in range(4)), False, kz, rng.uniform(0.05, 0.4)))
+    layers.append(DenseLayer(*(0.4 * c(B, P) for _ in range(4)), False))
+    return layers
+
+
+@pytest.mark.parametrize('B,P,Ms,dense,shear,inc', [
+    (3, 18, [26, 18], [True, False], False, False),
+    (2, 40, [56, 40, 30], [True, False, True], True, False),
+    (4, 26, [30], [True], False, True),
+    (1, 130, [150, 130], [True, True], True, True),
+])
+def test_multi_cta_cascade_equals_one_cta_cascade(B, P, Ms, dense, shear, inc):
+    """The multi-CTA cascade (each step spread over many CTAs) runs the same
+    arithmetic as the one-CTA-per-solve kernel: all outputs are bit-identical."""
+    from emustack_b200.dense import DenseStackSolver
+    rng = np.random.default_rng(P + len(Ms))
+    dev = torch.device('cuda')
+    Ms = [M if d else P for M, d in zip(Ms, dense)]
+    layers = _random_dense_stack(rng, B, P, Ms, dense, dev)
+    npw = P // 2
+    spec = torch.tensor(rng.integers(0, npw, B), dtype=torch.int32, device=dev)
+    nprop = torch.tensor(rng.integers(1, npw, (B, 3)), dtype=torch.int32, device=dev)
+    kw = dict(specular=spec, num_prop=nprop, want_vec_coef=True, save_lists=True)
+    if inc:
+        kw['incoming'] = torch.tensor(_rand((B, P), rng), device=dev)
+    if shear:
+        kw['shears'] = [rng.uniform(-0.3, 0.3, 2) for _ in range(len(layers))]
+        kw['air_alphas'] = torch.tensor(rng.uniform(-3, 3, (B, npw)), device=dev)
+        kw['air_betas'] = torch.tensor(rng.uniform(-3, 3, (B, npw)), device=dev)
+    outs = []
+    for mode in (1, 2):
+        o = DenseStackSolver(dev).solve(layers, P, pol='TM', mode=mode, **kw)
+        torch.cuda.synchronize()
+        outs.append({k: v.cpu() for k, v in o.items() if isinstance(v, torch.Tensor)})
+    assert int(outs[0]['info'].abs().sum()) == 0
+    for k in outs[0]:
+        assert torch.equal(outs[0][k], outs[1][k]), k
+
+
+def test_multi_cta_cascade_reports_singular_solve():
+    """A gap solve with an exactly singular matrix reports the same info code
+    in both cascades (first zero pivot, continuing as LAPACK does)."""
+    from emustack_b200.dense import DenseLayer, DenseStackSolver
+    dev = torch.device('cuda')
+    B, P = 2, 6
+    one = torch.ones((B, P), dtype=torch.complex128, device=dev)
+    z = torch.zeros((B, P), dtype=torch.complex128, device=dev)
+    # substrate reflects fully, superstrate R12 = 1: I - R12 rnet = 0
+    layers = [DenseLayer(one, one, -one, one, False), DenseLayer(one, one, -one, one, False)]
+    infos = []
+    for mode in (1, 2):
+        o = DenseStackSolver(dev).solve(layers, P, calc_fluxes=False, mode=mode)
+        infos.append(o['info'].cpu().numpy())
+    assert (infos[0] != 0).all() and np.array_equal(infos[0], infos[1])
