@@ -69,6 +69,8 @@ def lib():
     L.emu_status_string.restype = C.c_char_p
     L.emu_status_string.argtypes = [C.c_int]
     L.emu_launch_count.restype = C.c_longlong
+    L.emu_set_dense_mode.restype = C.c_int
+    L.emu_set_dense_mode.argtypes = [C.c_int]
     L.emu_grating_orders.restype = C.c_int
     L.emu_grating_orders.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, vp, vp, C.c_int,
                                      C.POINTER(C.c_int)]

@@ -817,7 +817,7 @@ extern "C" int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace,
   a.flux_only = 0;
   // one CTA per solve while the batch fills the GPU and matrices are small;
   // the multi-CTA cascade for large matrices or few solves
-  int mode = p->mode;
+  int mode = p->mode ? p->mode : emu::dense_mode();
   if (mode == 0) mode = (a.D >= 256 || (a.D >= 96 && p->batch < emu::sm_count())) ? 2 : 1;
   if (mode == 2) return stack_dense_multi(a, (cudaStream_t)stream);
   stack_dense_kernel<<<p->batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);

@@ -8,8 +8,11 @@
 namespace emu {
 
 static std::atomic<long long> g_launches{0};
+static std::atomic<int> g_dense_mode{0};
 
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int dense_mode() { return g_dense_mode.load(std::memory_order_relaxed); }
 
 int sm_count() {
   static int cache[64] = {0};
@@ -31,6 +34,11 @@ extern "C" {
 int emu_version(void) { return 100; }
 
 long long emu_launch_count(void) { return emu::g_launches.load(); }
+
+int emu_set_dense_mode(int mode) {
+  if (mode < 0 || mode > 2) return -1;
+  return emu::g_dense_mode.exchange(mode);
+}
 
 const char *emu_status_string(int s) {
   switch (s) {

@@ -30,6 +30,10 @@ int tc_gemm_tf32x3(const float *A, const float *B, int Mp, int Np, int Kp, int s
                    double *C64, int *d_err, cudaStream_t s);
 // output tiles of one K split
 int tc_tiles(int Mp, int Np);
+
+// process-wide choice for the dense interface / cascade paths (0 automatic,
+// 1 one CTA per problem, 2 multi-CTA), set by emu_set_dense_mode
+int dense_mode();
 size_t tc_smem_bytes();
 
 }  // namespace emu

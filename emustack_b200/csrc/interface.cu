@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "dense_la.cuh"
+#include "dense_multi.cuh"
 #include "emu_internal.h"
 #include "emu_modes.cuh"
 
@@ -107,6 +108,112 @@ __global__ void __launch_bounds__(kDLThreads) interface_dense_kernel(IfArgs a) {
   if (tid == 0 && a.info) a.info[b] = info;
 }
 
+// ---------------------------------------------------------------------------
+// Multi-CTA interfaces: interface_dense_kernel's steps, in the same order and
+// with the same arithmetic (bit-identical results), each a launch over all
+// interfaces of the batch with the matrices spread over many CTAs.
+
+// z = sqrt(1 / Z_film) (both polarisations), A = z o J, B = J_dag o z
+__global__ void ifm_prep(IfArgs a) {
+  const int P = a.P, M = a.M, npw = a.npw;
+  const long long b = blockIdx.y;
+  cd *ws = a.ws + b * a.ws_stride;
+  cd *A = ws, *B = A + (size_t)P * M;
+  const cd n = a.n[b];
+  const cd k = wavenumber(n, a.wln[b]);
+  // every thread recomputes the z it needs (cheap), so no grid-wide sync
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 2LL * P * M;
+       e += (long long)gridDim.x * blockDim.x) {
+    const bool isA = e < (long long)P * M;
+    const long long f = isA ? e : e - (long long)P * M;
+    const int i = isA ? (int)(f / M) : (int)(f % P);
+    const int j = i % npw;
+    cd zte, ztm;
+    film_Z(n, k, a.kz[b * npw + j], zte, ztm);
+    const cd zi = (i < npw) ? csqrt_p(crecip(zte)) : csqrt_p(crecip(ztm));
+    if (isA) {
+      A[f] = cmul(zi, a.J[b * P * M + f]);
+    } else {
+      B[f] = cmul(a.Jd[b * M * P + f], zi);
+    }
+  }
+}
+
+// S = I + G, R21 = I - G, T12 = B
+__global__ void ifm_sg(IfArgs a) {
+  const int P = a.P, M = a.M;
+  const long long b = blockIdx.y;
+  cd *ws = a.ws + b * a.ws_stride;
+  cd *B = ws + (size_t)P * M, *S = B + (size_t)M * P, *G = S + (size_t)M * M;
+  cd *R21 = a.R21 + b * M * M, *T12 = a.T12 + b * M * P;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)M * M + (long long)M * P;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < (long long)M * M) {
+      const int r = (int)(e / M), c = (int)(e % M);
+      const cd g = G[e];
+      const double one = (r == c) ? 1.0 : 0.0;
+      S[e] = cd{one + g.x, 0.0 + g.y};
+      R21[e] = cd{one - g.x, 0.0 - g.y};
+    } else {
+      const long long f = e - (long long)M * M;
+      T12[f] = B[f];
+    }
+  }
+}
+
+// G = I (M x M), R12 = -I (P x P)
+__global__ void ifm_eyes(IfArgs a) {
+  const int P = a.P, M = a.M;
+  const long long b = blockIdx.y;
+  cd *G = a.ws + b * a.ws_stride + (size_t)2 * P * M + (size_t)M * M;
+  cd *R12 = a.R12 + b * P * P;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)M * M + (long long)P * P;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < (long long)M * M) {
+      G[e] = cd{(e / M == e % M) ? 1.0 : 0.0, 0.0};
+    } else {
+      const long long f = e - (long long)M * M;
+      R12[f] = cd{(f / P == f % P) ? -1.0 : 0.0, 0.0};
+    }
+  }
+}
+
+__global__ void ifm_t12x2(IfArgs a) {
+  const long long b = blockIdx.y, n = (long long)a.M * a.P;
+  cd *T12 = a.T12 + b * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    T12[e] = cscale(T12[e], 2.0);
+}
+
+inline dim3 ifm_grid(long long n, int batch) {
+  long long g = (n + 255) / 256;
+  if (g > 1024) g = 1024;
+  return dim3((unsigned)(g < 1 ? 1 : g), (unsigned)batch);
+}
+
+int interface_dense_multi(const IfArgs &a, int batch, cudaStream_t s) {
+  const int P = a.P, M = a.M;
+  const long long S_ = (long long)a.ws_stride;
+  cd *A = a.ws, *B = A + (size_t)P * M, *S = B + (size_t)M * P, *G = S + (size_t)M * M;
+  const cd one{1.0, 0.0}, zero{0.0, 0.0}, two{2.0, 0.0};
+  if (a.info && cudaMemsetAsync(a.info, 0, sizeof(int) * batch, s) != cudaSuccess) return EMU_E_CUDA;
+  ifm_prep<<<ifm_grid(2LL * P * M, batch), 256, 0, s>>>(a);
+  bgemm(M, M, P, one, B, S_, P, A, S_, M, zero, G, S_, M, batch, s);
+  ifm_sg<<<ifm_grid((long long)M * M + (long long)M * P, batch), 256, 0, s>>>(a);
+  note_launch(2);
+  getrf_multi(M, S, S_, M, a.ipiv, M, a.info, 0, batch, s);
+  getrs_multi(M, P, S, S_, M, a.ipiv, M, a.T12, (long long)M * P, P, batch, s);
+  getrs_multi(M, M, S, S_, M, a.ipiv, M, a.R21, (long long)M * M, M, batch, s);
+  ifm_eyes<<<ifm_grid((long long)M * M + (long long)P * P, batch), 256, 0, s>>>(a);
+  note_launch();
+  getrs_multi(M, M, S, S_, M, a.ipiv, M, G, S_, M, batch, s);
+  bgemm(P, M, M, two, A, S_, M, G, S_, M, zero, a.T21, (long long)P * M, M, batch, s);
+  bgemm(P, P, M, two, A, S_, M, a.T12, (long long)M * P, P, one, a.R12, (long long)P * P, P, batch, s);
+  ifm_t12x2<<<ifm_grid((long long)M * P, batch), 256, 0, s>>>(a);
+  note_launch();
+  return check_launch();
+}
+
 struct FiArgs {
   int B, npw;
   const cd *kz1, *n1, *kz2, *n2;
@@ -173,6 +280,12 @@ extern "C" int emu_interface_dense_batch(int batch, int P, int M, const emu_c128
   a.ws_stride = (size_t)2 * P * M + (size_t)2 * M * M + (size_t)P;
   a.ws = (cd *)d_workspace;
   a.ipiv = (int *)((char *)d_workspace + align_up((size_t)batch * a.ws_stride * sizeof(cd), 16));
+  int mode = emu::dense_mode();
+  // measured at P = 618, M = 400: one CTA per interface wins once the batch
+  // fills the GPU (2.0 vs 4.6 ms per interface at 148), the multi-CTA path
+  // below half of it (4.7 vs 15.9 ms at 16)
+  if (mode == 0) mode = (M >= 96 && 2 * batch <= emu::sm_count()) ? 2 : 1;
+  if (mode == 2) return interface_dense_multi(a, batch, (cudaStream_t)stream);
   interface_dense_kernel<<<batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);
   emu::note_launch();
   return emu::check_launch();

@@ -67,6 +67,13 @@ typedef struct {
 /* Library version (major*10000 + minor*100 + patch). */
 int emu_version(void);
 
+/* Process-wide choice of the dense interface and cascade paths (no
+ * counterpart in the reference): 0 automatic (by matrix size and batch),
+ * 1 one CTA per problem, 2 every step spread over many CTAs.  Results are
+ * bit-identical; only speed differs.  Returns the previous value, or -1 for
+ * an invalid mode.  An EmuStackDense.mode other than 0 takes precedence. */
+int emu_set_dense_mode(int mode);
+
 /* Human-readable name of a status code. */
 const char *emu_status_string(int status);
 
