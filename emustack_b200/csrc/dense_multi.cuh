@@ -60,10 +60,17 @@ inline void bgemm(int m, int n, int k, cd alpha, const cd *A, long long sA, int 
 // inner loop of cta_getrf): pivot search, full-row swap, column scaling,
 // rank-1 update of the rest of the panel.  info[b] = code + j + 1 for the
 // first exactly-zero pivot of this factorisation if info[b] is still 0.
-__global__ void __launch_bounds__(kDLThreads) panel_kernel(cd *A_, long long sA, int lda, int n, int j0,
-                                                           int jb, int *ipiv_, long long sip,
-                                                           int *info, int code) {
-  __shared__ LuSmem ls;
+constexpr int kPanelThreads = 1024;
+struct PanelSmem {
+  double val[kPanelThreads / 32];
+  int idx[kPanelThreads / 32];
+  int piv;
+};
+
+__global__ void __launch_bounds__(kPanelThreads) panel_kernel(cd *A_, long long sA, int lda, int n, int j0,
+                                                              int jb, int *ipiv_, long long sip,
+                                                              int *info, int code) {
+  __shared__ PanelSmem ls;
   const int tid = threadIdx.x, nt = blockDim.x;
   const long long b = blockIdx.x;
   cd *A = A_ + b * sA;
@@ -133,36 +140,73 @@ __global__ void __launch_bounds__(kDLThreads) panel_kernel(cd *A_, long long sA,
   }
 }
 
-// X rows r0 .. r0+rb-1 := L11^{-1} X rows (unit lower L11 = L[r0.., r0..]),
-// one thread per column c in [c0, c0 + ncols).
-__global__ void trsm_lower_kernel(const cd *L_, long long sL, int ldl, int r0, int rb, cd *X_, long long sX,
-                                  int ldx, int c0, int ncols) {
+// X rows r0 .. r0+rb-1 := L11^{-1} X rows (unit lower L11 = L[r0.., r0..],
+// rb <= kNB), one thread per column c in [c0, c0 + ncols): the block's L11 is
+// staged in shared memory, each column's rb values are held in registers,
+// and the substitution runs in the order of cta_getrf / cta_getrs.
+__global__ void __launch_bounds__(128) trsm_lower_kernel(const cd *L_, long long sL, int ldl, int r0, int rb,
+                                                         cd *X_, long long sX, int ldx, int c0, int ncols) {
+  __shared__ cd Ls[kNB][kNB];
   const long long b = blockIdx.y;
   const cd *L = L_ + b * sL;
   cd *X = X_ + b * sX;
-  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < ncols; cc += gridDim.x * blockDim.x) {
-    const int c = c0 + cc;
-    for (int r = 1; r < rb; ++r) {
-      cd s = X[(size_t)(r0 + r) * ldx + c];
-      for (int t = 0; t < r; ++t) s = csub(s, cmul(L[(size_t)(r0 + r) * ldl + r0 + t], X[(size_t)(r0 + t) * ldx + c]));
-      X[(size_t)(r0 + r) * ldx + c] = s;
+  for (int e = threadIdx.x; e < rb * rb; e += blockDim.x) {
+    const int r = e / rb, t = e % rb;
+    Ls[r][t] = L[(size_t)(r0 + r) * ldl + r0 + t];
+  }
+  __syncthreads();
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= ncols) return;
+  const int c = c0 + cc;
+  cd x[kNB];
+#pragma unroll
+  for (int r = 0; r < kNB; ++r)
+    if (r < rb) x[r] = X[(size_t)(r0 + r) * ldx + c];
+#pragma unroll
+  for (int r = 1; r < kNB; ++r) {
+    if (r < rb) {
+      cd s = x[r];
+#pragma unroll
+      for (int t = 0; t < r; ++t) s = csub(s, cmul(Ls[r][t], x[t]));
+      x[r] = s;
     }
   }
+#pragma unroll
+  for (int r = 1; r < kNB; ++r)
+    if (r < rb) X[(size_t)(r0 + r) * ldx + c] = x[r];
 }
 
 // X rows r0 .. r0+rb-1 := U11^{-1} X rows (upper U11 with its diagonal).
-__global__ void trsm_upper_kernel(const cd *U_, long long sU, int ldu, int r0, int rb, cd *X_, long long sX,
-                                  int ldx, int ncols) {
+__global__ void __launch_bounds__(128) trsm_upper_kernel(const cd *U_, long long sU, int ldu, int r0, int rb,
+                                                         cd *X_, long long sX, int ldx, int ncols) {
+  __shared__ cd Us[kNB][kNB];
   const long long b = blockIdx.y;
   const cd *U = U_ + b * sU;
   cd *X = X_ + b * sX;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) {
-    for (int r = rb - 1; r >= 0; --r) {
-      cd s = X[(size_t)(r0 + r) * ldx + c];
-      for (int t = r + 1; t < rb; ++t) s = csub(s, cmul(U[(size_t)(r0 + r) * ldu + r0 + t], X[(size_t)(r0 + t) * ldx + c]));
-      X[(size_t)(r0 + r) * ldx + c] = cdiv(s, U[(size_t)(r0 + r) * ldu + r0 + r]);
+  for (int e = threadIdx.x; e < rb * rb; e += blockDim.x) {
+    const int r = e / rb, t = e % rb;
+    Us[r][t] = U[(size_t)(r0 + r) * ldu + r0 + t];
+  }
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  cd x[kNB];
+#pragma unroll
+  for (int r = 0; r < kNB; ++r)
+    if (r < rb) x[r] = X[(size_t)(r0 + r) * ldx + c];
+#pragma unroll
+  for (int r = kNB - 1; r >= 0; --r) {
+    if (r < rb) {
+      cd s = x[r];
+#pragma unroll
+      for (int t = r + 1; t < kNB; ++t)
+        if (t < rb) s = csub(s, cmul(Us[r][t], x[t]));
+      x[r] = cdiv(s, Us[r][r]);
     }
   }
+#pragma unroll
+  for (int r = 0; r < kNB; ++r)
+    if (r < rb) X[(size_t)(r0 + r) * ldx + c] = x[r];
 }
 
 // row interchanges ipiv[0..n) applied in order to the columns of X
@@ -191,7 +235,9 @@ inline void getrf_multi(int n, cd *A, long long sA, int lda, int *ipiv, long lon
                         int batch, cudaStream_t s) {
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int jb = min(kNB, n - j0);
-    panel_kernel<<<batch, kDLThreads, 0, s>>>(A, sA, lda, n, j0, jb, ipiv, sip, info, code);
+    // a panel is a latency-bound chain of column steps: the widest CTA keeps
+    // each step short (the arithmetic does not depend on the width)
+    panel_kernel<<<batch, kPanelThreads, 0, s>>>(A, sA, lda, n, j0, jb, ipiv, sip, info, code);
     note_launch();
     const int rest = n - (j0 + jb);
     if (rest > 0) {
