@@ -1,7 +1,8 @@
 """Time an uneven batch of all-film solves in one launch against per-solve
-and per-shape launches.
+and per-shape launches (and, with --arrays N, N nanostructured-array stacks
+grouped by shape against one call per stack).
 
-    python -m emustack_b200.profile_uneven [--points 4096] [--steps 5]
+    python -m emustack_b200.profile_uneven [--points 4096] [--steps 5] [--arrays 2048]
 
 The batch follows the uneven-batch distribution (the film half of it):
 P = 2 Npw log-uniform in [50, 900] (the order set of the max order whose Npw
@@ -30,12 +31,131 @@ import torch
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 
+def array_stacks(n, seed=0, period=500.0):
+    """Nanostructured-array stacks of the uneven distribution: P = 2 Npw
+    log-uniform in [50, 900] (nearest order set), M = P + 20 Bloch modes per
+    array layer, 2-12 array layers between a film substrate (n = 1.46) and
+    air.  Interfaces come from synthetic J (P x M), J_dag (M x P), complex
+    N(0,1)/sqrt(P), Bloch k_z Re U(0, 2 k0), Im U(0, 0.1 k0), heights
+    U(50, 200) nm; wavelength U(350, 1100) nm, normal incidence, TE."""
+    from emustack_b200.serve_bench import order_table
+    rng = np.random.default_rng(seed)
+    tab = order_table(period)
+    P = np.exp(rng.uniform(np.log(50), np.log(900), n))
+    out = []
+    for i in range(n):
+        mo = int(np.argmin(np.abs(tab - P[i] / 2)))
+        out.append(dict(mo=mo, npw=int(tab[mo]), K=int(rng.integers(2, 13)), wl=float(rng.uniform(350, 1100)),
+                        seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def time_array_groups(stacks, period=500.0, group=True, n_streams=1):
+    """Solve array stacks (interfaces + cascade + fluxes) grouped by shape
+    (P, number of layers) into batched calls, or one call per stack; groups
+    are dealt round-robin to n_streams CUDA streams (independent solves
+    overlap on the device).  Returns (ms, groups).  Inputs are built on the
+    device before timing."""
+    from emustack_b200.dense import DenseLayer, DenseStackSolver, film_interface, interface_dense
+    from emustack_b200.films import grating_orders
+    from emustack_b200.profile_dense import air_kz
+    dev = torch.device('cuda')
+    keyf = (lambda s: (s['mo'], s['K'])) if group else (lambda s: id(s))
+    groups = collections.defaultdict(list)
+    for s in stacks:
+        groups[keyf(s)].append(s)
+    prepared = []
+    for _, ss in groups.items():
+        mo, K = ss[0]['mo'], ss[0]['K']
+        px, py = grating_orders(mo, period, period)
+        npw = len(px)
+        P, M, B = 2 * npw, 2 * npw + 20, len(ss)
+        wl = np.array([s['wl'] for s in ss])
+        wln = wl / period
+        kza = np.stack([air_kz(px, py, w, period) for w in wl])
+        order = np.argsort(-kza.real + kza.imag, axis=1, kind='stable')
+        kza = np.take_along_axis(kza, order, 1)
+        kzs = np.take_along_axis(np.stack([air_kz(px, py, w, period, 1.46) for w in wl]), order, 1)
+        g = torch.Generator(device='cuda').manual_seed(ss[0]['seed'])
+        cr = lambda *sh: torch.complex(torch.randn(sh, dtype=torch.float64, device=dev, generator=g),
+                                       torch.randn(sh, dtype=torch.float64, device=dev, generator=g))
+        k0 = torch.tensor(2 * np.pi / wln, device=dev)
+        lay = dict(B=B, P=P, M=M, K=K, kza=torch.tensor(kza, device=dev), kzs=torch.tensor(kzs, device=dev),
+                   wln=torch.tensor(wln, device=dev),
+                   J=[cr(B, P, M) / np.sqrt(P) for _ in range(K)], Jd=[cr(B, M, P) / np.sqrt(P) for _ in range(K)],
+                   kz=[torch.complex(2 * torch.rand(B, M, dtype=torch.float64, device=dev, generator=g),
+                                     0.1 * torch.rand(B, M, dtype=torch.float64, device=dev, generator=g))
+                       * k0[:, None] for _ in range(K)],
+                   h=[float(x) for x in np.random.default_rng(ss[0]['seed']).uniform(50, 200, K) / period],
+                   spec=torch.zeros(B, dtype=torch.int32, device=dev),
+                   nprop=torch.tensor([[int((kza[b].imag == 0).sum())] * 2 + [int((kzs[b].imag == 0).sum())]
+                                       for b in range(B)], dtype=torch.int32, device=dev))
+        prepared.append(lay)
+    streams = [torch.cuda.Stream(dev) for _ in range(n_streams)]
+    solvers = [DenseStackSolver(dev) for _ in range(n_streams)]
+    n_air = {}
+    for B in sorted({lay['B'] for lay in prepared}):
+        n_air[B] = (torch.ones(B, dtype=torch.complex128, device=dev),
+                    torch.full((B,), 1.46 + 0j, dtype=torch.complex128, device=dev))
+
+    def run(lay, solver):
+        na, ns = n_air[lay['B']]
+        Rs, Ts = film_interface(lay['kza'], na, lay['kzs'], ns, lay['wln'])
+        Ra, Ta = film_interface(lay['kza'], na, lay['kza'], na, lay['wln'])
+        layers = [DenseLayer(Rs, Ts, -Rs, Ts, False)]
+        for k in range(lay['K']):
+            R12, T12, R21, T21, _ = interface_dense(lay['kza'], na, lay['wln'], lay['J'][k], lay['Jd'][k])
+            layers.append(DenseLayer(R12, T12, R21, T21, True, lay['kz'][k], lay['h'][k]))
+        layers.append(DenseLayer(Ra, Ta, -Ra, Ta, False))
+        return solver.solve(layers, lay['P'], pol='TE', specular=lay['spec'], num_prop=lay['nprop'])
+
+    for lay in prepared[:3]:
+        run(lay, solvers[0])
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(main)
+    for st in streams:
+        st.wait_stream(main)
+    for i, lay in enumerate(prepared):
+        with torch.cuda.stream(streams[i % n_streams]):
+            run(lay, solvers[i % n_streams])
+    for st in streams:
+        main.wait_stream(st)
+    b.record(main)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b), len(prepared)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--points', type=int, default=4096)
     ap.add_argument('--steps', type=int, default=5)
     ap.add_argument('--per-solve', type=int, default=512, help='points timed one launch each')
+    ap.add_argument('--arrays', type=int, default=0, help='also time this many array stacks')
+    ap.add_argument('--array-sample', type=int, default=32, help='array stacks timed one call each')
+    ap.add_argument('--streams', type=int, default=4, help='streams for the array groups')
     args = ap.parse_args()
+    if args.arrays:
+        stacks = array_stacks(args.arrays)
+        ms_g, ng = time_array_groups(stacks, n_streams=args.streams)
+        sample = stacks[:args.array_sample]
+        ms_s, _ = time_array_groups(sample, group=False)
+        flops = 0.0
+        for s in stacks:
+            P = 2 * s['npw']
+            M = P + 20
+            flops += s['K'] * 8.0 * ((3 * M * M * P + P * P * M + 4.0 / 3 * M ** 3)
+                                     + (4.0 / 3 * P ** 3 + 5 * P * P * M + 3 * M * M * P + 4.0 / 3 * M ** 3))
+        print(json.dumps({
+            'array_stacks': len(stacks), 'shape_groups': ng, 'streams': args.streams,
+            'mean_P': float(np.mean([2 * s['npw'] for s in stacks])),
+            'mean_array_layers': float(np.mean([s['K'] for s in stacks])),
+            'grouped_ms': ms_g, 'grouped_solves_per_s': len(stacks) / (ms_g / 1e3),
+            'grouped_tflops': flops / (ms_g / 1e3) / 1e12,
+            'per_solve_sample': len(sample), 'per_solve_ms_sample': ms_s,
+            'per_solve_solves_per_s': len(sample) / (ms_s / 1e3),
+        }), flush=True)
     from emustack_b200.films import FilmStackSolver, FilmVarSolver
     from emustack_b200.serve_bench import make_requests
     dev = torch.device('cuda')
