@@ -28,8 +28,13 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // scratch of splits * Mp * Np floats.
 int tc_gemm_tf32x3(const float *A, const float *B, int Mp, int Np, int Kp, int splits, float *Cpart,
                    double *C64, int *d_err, cudaStream_t s);
+// Batched form: Cpart[b][split][Mp][Np] partial sums for b < batch (operand
+// batch strides sA, sB in floats); *used = number of K splits taken.
+int tc_gemm_tf32x3_parts(const float *A, long long sA, const float *B, long long sB, int Mp, int Np, int Kp,
+                         int batch, int splits, float *Cpart, int *d_err, int *used, cudaStream_t s);
 // output tiles of one K split
 int tc_tiles(int Mp, int Np);
+
 
 // process-wide choice for the dense interface / cascade paths (0 automatic,
 // 1 one CTA per problem, 2 multi-CTA), set by emu_set_dense_mode

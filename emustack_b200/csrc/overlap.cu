@@ -179,6 +179,10 @@ struct EtArgs {
   // [2 npw][2 K], K = 6 ne), columns in (element, node, re/im) order:
   // row s = (Re E, -Im E) pairs, row npw + s = (Im E, Re E) pairs
   float *A32;
+  // tensor-core path, several problems per launch (blockIdx.y = problem):
+  // per-problem strides of pos (ints) and A32 (floats); bloch advances by 2
+  int spos;
+  long long sA32;
 };
 
 constexpr int kEtWarps = 4;
@@ -210,7 +214,10 @@ __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
     float2 *bc = (float2 *)(et_smem + (size_t)w * et_warp_bytes_f32(a.mo));  // [16]
     float2 *fx = bc + 16;                                                      // [16][no]
     float2 *fy = fx + 16 * no;                                                 // [16][no]
-    const double bx = a.bloch[0], by = a.bloch[1];
+    const int prob = blockIdx.y;
+    const double bx = a.bloch[2 * prob], by = a.bloch[2 * prob + 1];
+    const int32_t *pos = a.pos + (size_t)prob * a.spos;
+    float *A32 = a.A32 + (size_t)prob * a.sA32;
     const long long K = 6LL * a.ne;
     for (long el0 = (long)blockIdx.x * kEtWarps; el0 < a.ne; el0 += (long)gridDim.x * kEtWarps) {
       const long el = el0 + w;
@@ -259,7 +266,7 @@ __global__ void __launch_bounds__(32 * kEtWarps) etable_kernel(EtArgs a) {
             }
           }
           // K order (element, node, re/im): 12 contiguous floats per row
-          float4 *r0 = (float4 *)(a.A32 + (size_t)a.pos[s] * 2 * K + (size_t)el * 12);
+          float4 *r0 = (float4 *)(A32 + (size_t)pos[s] * 2 * K + (size_t)el * 12);
           float4 *r1 = (float4 *)((float *)r0 + (size_t)a.npw * 2 * K);
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
@@ -447,6 +454,13 @@ __global__ void reduce_parts_kernel(const cd *parts, int nparts, long long strid
 // by area_norm; J_dag[i][row] uses adjoint column perm[i] scaled by scale[i].
 __global__ void epilogue_kernel(const cd *G, const double *tab, int npw, int nval, double inv_area,
                                 int dagger, const cd *scale, const int32_t *perm, cd *out) {
+  // problem blockIdx.y: every array advances by its per-problem size
+  const long long y = blockIdx.y;
+  G += y * 2 * npw * (long long)nval;
+  tab += y * 3 * npw;
+  if (scale) scale += y * nval;
+  if (perm) perm += y * nval;
+  out += y * 2 * npw * (long long)nval;
   const long total = (long)npw * nval;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
     const int r = (int)(i / nval), n = (int)(i % nval);
@@ -593,9 +607,11 @@ __global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, int ba
 // 192 contiguous floats.
 constexpr int kBModes = 8, kBElems = 16;
 
-__global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, long e0, long ne,
-                                                     int conj, int row0, float *B) {
+__global__ void __launch_bounds__(256) make_B_kernel(const cd *sol_, long long ssol, int nval, long e0, long ne,
+                                                     int conj, int row0, float *B_, long long sB) {
   __shared__ cd v[kBModes][kBElems][12];
+  const cd *sol = sol_ + (size_t)blockIdx.z * ssol;  // problem blockIdx.z
+  float *B = B_ + (size_t)blockIdx.z * sB;
   const long long K = 6LL * ne;
   const int m0 = blockIdx.x * kBModes;
   const long el0 = (long)blockIdx.y * kBElems;
@@ -627,34 +643,36 @@ __global__ void __launch_bounds__(256) make_B_kernel(const cd *sol, int nval, lo
   }
 }
 
-// G (+)= C[:, 0:2M] ; G_dag (+)= conj(C[:, off1:off1+2M])
-__global__ void pack_G_kernel(const double *C64, int npw, int nb, int n2, cd *G, cd *Gd, int off1,
-                              int first) {
-  const long long total = (long long)npw * n2;
+// G (+)= C[:, 0:2M] ; G_dag (+)= conj(C[:, off1:off1+2M]), C = FP64 sum of
+// the tensor-core K-split partials Cp[prob][split][2 npw][nb]; problem
+// blockIdx.y; G, Gd advance by gsz per problem.
+__global__ void pack_G_parts_kernel(const float *Cp, int nsplit, int npw, int nb, int n2, cd *G_, cd *Gd_,
+                                    long long gsz, int off1, int first) {
+  const long long prob = blockIdx.y;
+  const float *C = Cp + prob * nsplit * (long long)2 * npw * nb;
+  cd *G = G_ ? G_ + prob * gsz : nullptr;
+  cd *Gd = Gd_ ? Gd_ + prob * gsz : nullptr;
+  const long long total = (long long)npw * n2, step = (long long)2 * npw * nb;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const int s = (int)(i / n2), n = (int)(i % n2);
-    const double *r0 = C64 + (size_t)s * nb, *r1 = C64 + (size_t)(npw + s) * nb;
-    if (G) {
-      const cd g = cd{r0[n], r1[n]};
-      G[i] = first ? g : cadd(G[i], g);
+    double a0 = 0.0, a1 = 0.0, d0 = 0.0, d1 = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) {
+      const float *r0 = C + sp * step + (size_t)s * nb, *r1 = C + sp * step + (size_t)(npw + s) * nb;
+      if (G) {
+        a0 += (double)r0[n];
+        a1 += (double)r1[n];
+      }
+      if (Gd) {
+        d0 += (double)r0[off1 + n];
+        d1 += (double)r1[off1 + n];
+      }
     }
-    if (Gd) {
-      const cd g = cd{r0[off1 + n], -r1[off1 + n]};
-      Gd[i] = first ? g : cadd(Gd[i], g);
-    }
+    if (G) G[i] = first ? cd{a0, a1} : cadd(G[i], cd{a0, a1});
+    if (Gd) Gd[i] = first ? cd{d0, -d1} : cadd(Gd[i], cd{d0, -d1});
   }
 }
 
-// K splits so that tiles x splits fills one wave of CTAs (one per SM)
-int tc_splits(int npw, int nb, long long K2) {
-  const int tiles = emu::tc_tiles(2 * npw, nb);
-  int sp = emu::sm_count() / tiles;
-  const int maxsp = (int)(K2 / 256 > 0 ? K2 / 256 : 1);
-  if (sp > maxsp) sp = maxsp;
-  if (sp > 64) sp = 64;
-  return sp < 1 ? 1 : sp;
-}
 
 // ---------------------------------------------------------------- pair reordering
 // Full adjoint x prime matrix for the conjugate-pair reordering of
@@ -743,9 +761,59 @@ static int ov_nparts(int npw, int M) {
   return n < 4 ? 4 : (n > 64 ? 64 : n);
 }
 
+// ---- tensor-core path: problems in groups, one launch per step for a group
+struct TcPlan {
+  long nec;        // elements per chunk
+  long long K2;    // 12 nec: GEMM K of one chunk
+  int nb, off1;    // B rows (2M per field set), row of the adjoint set
+  int group;       // problems per launch
+  int splits;      // K splits of the GEMM
+};
+
+constexpr size_t kTcGroupBytes = (size_t)4 << 30;  // scratch budget of one group
+
+static size_t tc_problem_bytes(const EmuOverlap *p, const TcPlan &t) {
+  const size_t npw = p->n_pw, M = p->nval;
+  return align_up(sizeof(int32_t) * npw, 16) + align_up(sizeof(double) * 3 * npw, 16) +
+         2 * align_up(sizeof(cd) * npw * 2 * M, 16) + sizeof(float) * 2 * npw * t.K2 +
+         sizeof(float) * t.nb * t.K2 + sizeof(float) * t.splits * 2 * npw * t.nb;
+}
+
+static TcPlan tc_plan(const EmuOverlap *p) {
+  TcPlan t;
+  const long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
+  t.nec = chunk < p->nel ? chunk : p->nel;
+  t.K2 = 12 * (long long)t.nec;
+  t.nb = (p->d_sol1 ? 2 * p->nval : 0) + (p->d_sol2 ? 2 * p->nval : 0);
+  if (t.nb == 0) t.nb = 2 * p->nval;
+  t.off1 = p->d_sol1 ? 2 * p->nval : 0;
+  // largest group within the budget (at one split), then splits so that
+  // tiles x splits x group fills one wave of CTAs
+  t.splits = 1;
+  const size_t per = tc_problem_bytes(p, t);
+  long long g = (long long)(kTcGroupBytes / (per > 0 ? per : 1));
+  if (g < 1) g = 1;
+  if (g > p->batch) g = p->batch;
+  if (g > 1024) g = 1024;
+  t.group = (int)g;
+  const int tiles = emu::tc_tiles(2 * p->n_pw, t.nb) * t.group;
+  int sp = (emu::sm_count() + tiles - 1) / tiles;
+  const int maxsp = (int)(t.K2 / 256 > 0 ? t.K2 / 256 : 1);
+  if (sp > maxsp) sp = maxsp;
+  if (p->tc_splits > 0) sp = p->tc_splits;
+  if (sp > 64) sp = 64;
+  if (sp * t.group > 65535) sp = 65535 / t.group;
+  t.splits = sp < 1 ? 1 : sp;
+  return t;
+}
+
 extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
-  if (!p || p->n_pw < 1 || p->nval < 1 || p->nel < 1) return 0;
+  if (!p || p->n_pw < 1 || p->nval < 1 || p->nel < 1 || p->batch < 0) return 0;
   const long long npw = p->n_pw, M = p->nval;
+  if (p->precision == 1) {
+    const TcPlan t = tc_plan(p);
+    return (size_t)t.group * tc_problem_bytes(p, t) + 16 * 256 + 256;
+  }
   const long long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
   const long long ne = chunk < p->nel ? chunk : p->nel;
   const long long nparts = ov_nparts(p->n_pw, p->nval);
@@ -756,15 +824,113 @@ extern "C" size_t emu_overlap_workspace_size(const EmuOverlap *p) {
   b += align_up(sizeof(cd) * 6 * ne * 2 * M, 256);           // S chunk
   b += 2 * align_up(sizeof(cd) * npw * 2 * M, 256);          // G, Gd
   b += align_up(sizeof(cd) * nparts * npw * 2 * M, 256);     // partials
-  if (p->precision == 1) {
-    const long long K2 = 12 * ne;
-    b += align_up(sizeof(float) * (2 * npw) * K2, 256);       // A (FP32)
-    b += align_up(sizeof(float) * (4 * M) * K2, 256);         // B (FP32), both field sets
-    b += align_up(sizeof(float) * 64 * (2 * npw) * (4 * M), 256);  // split partials
-    b += align_up(sizeof(double) * (2 * npw) * (4 * M), 256);  // C64
-    b += 256;                                                   // error flag
-  }
   return b + 256;
+}
+
+// Tensor-core J / J_dag for all problems, `group` problems per launch: plane
+// waves, per element chunk the E~ table (as the FP32 A operand) and B (both
+// field sets), one batched tcgen05 GEMM, the split sums folded into G / G_dag,
+// then the epilogues.
+static int overlap_tc(const EmuOverlap *p, void *ws, cudaStream_t s) {
+  const TcPlan t = tc_plan(p);
+  const int npw = p->n_pw, M = p->nval, Gp = t.group;
+  const long long gsz = (long long)npw * 2 * M;
+  char *w = (char *)ws;
+  auto take = [&](size_t bytes) {
+    char *r = w;
+    w += align_up(bytes, 256);
+    return (void *)r;
+  };
+  int32_t *pos = (int32_t *)take(sizeof(int32_t) * npw * Gp);
+  double *tab = (double *)take(sizeof(double) * 3 * npw * Gp);
+  cd *G = (cd *)take(sizeof(cd) * gsz * Gp);
+  cd *Gd = (cd *)take(sizeof(cd) * gsz * Gp);
+  float *A32 = (float *)take(sizeof(float) * 2 * npw * t.K2 * Gp);
+  float *B32 = (float *)take(sizeof(float) * t.nb * t.K2 * Gp);
+  float *Cpart = (float *)take(sizeof(float) * t.splits * 2 * npw * (size_t)t.nb * Gp);
+  int *terr = p->d_error ? (int *)p->d_error : (int *)take(256);
+  if (!p->d_error && cudaMemsetAsync(terr, 0, sizeof(int), s) != cudaSuccess) return EMU_E_CUDA;
+  const int sms = emu::sm_count();
+  const size_t et_smem32 = kEtWarps * et_warp_bytes_f32(p->max_order);
+  if (et_smem32 > 48 * 1024 &&
+      cudaFuncSetAttribute(etable_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)et_smem32) !=
+          cudaSuccess)
+    return EMU_E_CUDA;
+  const long long ssol = (long long)p->nel * M * 39;
+  const cd *sol1 = (const cd *)p->d_sol1, *sol2 = (const cd *)p->d_sol2;
+  for (int g0 = 0; g0 < p->batch; g0 += Gp) {
+    const int ng = (p->batch - g0) < Gp ? (p->batch - g0) : Gp;
+    PwArgs pa;
+    pa.batch = ng;
+    pa.npw = npw;
+    pa.px = p->d_px;
+    pa.py = p->d_py;
+    pa.d = p->d;
+    pa.dy = p->dy;
+    pa.bloch = p->d_bloch + 2 * (size_t)g0;
+    pa.k0 = p->d_k0 + g0;
+    pa.pos = pos;
+    pa.tab = tab;
+    pa.out_inv = p->d_index_pw_inv ? p->d_index_pw_inv + (size_t)g0 * npw : nullptr;
+    pw_setup_kernel<<<ng, 256, sizeof(double) * npw, s>>>(pa);
+    emu::note_launch();
+    int first = 1;
+    for (long e0 = 0; e0 < p->nel; e0 += t.nec) {
+      const long ne = (p->nel - e0) < t.nec ? (p->nel - e0) : t.nec;
+      const long long K2 = 12 * (long long)ne;
+      EtArgs ea;
+      ea.npw = npw;
+      ea.mo = p->max_order;
+      ea.e0 = (int)e0;
+      ea.ne = (int)ne;
+      ea.px = p->d_px;
+      ea.py = p->d_py;
+      ea.pos = pos;
+      ea.x = p->d_x;
+      ea.tn = p->d_table_nod;
+      ea.d = p->d;
+      ea.dy = p->dy;
+      ea.bloch = p->d_bloch + 2 * (size_t)g0;
+      ea.E = nullptr;
+      ea.ldE = 6 * ne;
+      ea.A32 = A32;
+      ea.spos = npw;
+      ea.sA32 = 2LL * npw * K2;
+      long long eg = (ne + kEtWarps - 1) / kEtWarps;
+      const long long egmax = (16LL * sms + ng - 1) / ng;
+      if (eg > egmax) eg = egmax;
+      etable_kernel<true><<<dim3((unsigned)eg, (unsigned)ng), 32 * kEtWarps, et_smem32, s>>>(ea);
+      const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems), (unsigned)ng);
+      const long long sB = (long long)t.nb * K2;
+      if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1 + (size_t)g0 * ssol, ssol, M, e0, ne, 0, 0, B32, sB);
+      if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2 + (size_t)g0 * ssol, ssol, M, e0, ne, 1, t.off1, B32, sB);
+      emu::note_launch(1 + (sol1 ? 1 : 0) + (sol2 ? 1 : 0));
+      int used = 0;
+      const int tst = emu::tc_gemm_tf32x3_parts(A32, 2LL * npw * K2, B32, sB, 2 * npw, t.nb, (int)K2, ng, t.splits,
+                                                Cpart, terr, &used, s);
+      if (tst != EMU_OK) return tst;
+      long long rgs = (gsz + 255) / 256;
+      if (rgs > 1024) rgs = 1024;
+      pack_G_parts_kernel<<<dim3((unsigned)rgs, (unsigned)ng), 256, 0, s>>>(
+          Cpart, used, npw, t.nb, 2 * M, sol1 ? G : nullptr, sol2 ? Gd : nullptr, gsz, t.off1, first);
+      emu::note_launch();
+      first = 0;
+    }
+    long long eb = ((long long)npw * M + 255) / 256;
+    if (eb > 1024) eb = 1024;
+    if (sol1) {
+      epilogue_kernel<<<dim3((unsigned)eb, (unsigned)ng), 256, 0, s>>>(
+          G, tab, npw, M, 1.0 / p->area_norm, 0, nullptr, nullptr, (cd *)p->d_J + (size_t)g0 * 2 * npw * M);
+      emu::note_launch();
+    }
+    if (sol2) {
+      epilogue_kernel<<<dim3((unsigned)eb, (unsigned)ng), 256, 0, s>>>(
+          Gd, tab, npw, M, 1.0, 1, p->d_scale2 ? (const cd *)p->d_scale2 + (size_t)g0 * M : nullptr,
+          p->d_perm2 ? p->d_perm2 + (size_t)g0 * M : nullptr, (cd *)p->d_J_dag + (size_t)g0 * 2 * npw * M);
+      emu::note_launch();
+    }
+  }
+  return emu::check_launch();
 }
 
 extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t workspace_bytes,
@@ -776,11 +942,14 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   if ((p->d_sol1 == nullptr) != (p->d_J == nullptr) || (p->d_sol2 == nullptr) != (p->d_J_dag == nullptr))
     return EMU_E_ARG;
   if (p->max_order < 0 || p->max_order > kMaxOrd) return EMU_E_UNSUPPORTED;
+  if (p->precision != 0 && p->precision != 1) return EMU_E_ARG;
+  if (p->tc_splits < 0) return EMU_E_ARG;
   if (p->batch == 0) return EMU_OK;
   if (!d_workspace || workspace_bytes < emu_overlap_workspace_size(p)) return EMU_E_WORKSPACE;
   int st = upload_tables();
   if (st != EMU_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
+  if (p->precision == 1) return overlap_tc(p, d_workspace, s);
   const int npw = p->n_pw, M = p->nval;
   const long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
   const long nec = chunk < p->nel ? chunk : p->nel;
@@ -799,29 +968,11 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   cd *Gd = (cd *)take(sizeof(cd) * (size_t)npw * 2 * M);
   cd *parts = (cd *)take(sizeof(cd) * (size_t)nparts * npw * 2 * M);
   const long long gsz = (long long)npw * 2 * M;
-  if (p->precision != 0 && p->precision != 1) return EMU_E_ARG;
-  if (p->tc_splits < 0) return EMU_E_ARG;
-  float *A32 = nullptr, *B32 = nullptr, *Cpart = nullptr;
-  double *C64 = nullptr;
-  int *terr = nullptr;
-  if (p->precision == 1) {
-    const long long K2 = 12 * nec;
-    A32 = (float *)take(sizeof(float) * (2 * (size_t)npw) * K2);
-    B32 = (float *)take(sizeof(float) * (4 * (size_t)M) * K2);
-    Cpart = (float *)take(sizeof(float) * 64 * (2 * (size_t)npw) * (4 * M));
-    C64 = (double *)take(sizeof(double) * (2 * (size_t)npw) * (4 * M));
-    terr = p->d_error ? (int *)p->d_error : (int *)take(256);
-    if (!p->d_error && cudaMemsetAsync(terr, 0, sizeof(int), (cudaStream_t)stream) != cudaSuccess)
-      return EMU_E_CUDA;
-  }
   const int sms = emu::sm_count();
   const size_t et_smem = kEtWarps * et_warp_bytes(p->max_order);
-  const size_t et_smem32 = kEtWarps * et_warp_bytes_f32(p->max_order);
   if (et_smem > 48 * 1024 &&
-      (cudaFuncSetAttribute(etable_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)et_smem) != cudaSuccess ||
-       cudaFuncSetAttribute(etable_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)et_smem32) != cudaSuccess))
+      cudaFuncSetAttribute(etable_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)et_smem) !=
+          cudaSuccess)
     return EMU_E_CUDA;
   for (int b = 0; b < p->batch; ++b) {
     PwArgs pa;
@@ -838,63 +989,33 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
     pa.out_inv = p->d_index_pw_inv ? p->d_index_pw_inv + (size_t)b * npw : nullptr;
     pw_setup_kernel<<<1, 256, sizeof(double) * npw, s>>>(pa);
     emu::note_launch();
-    auto et_args = [&](long e0, long ne) {
-      EtArgs ea;
-      ea.npw = npw;
-      ea.mo = p->max_order;
-      ea.e0 = (int)e0;
-      ea.ne = (int)ne;
-      ea.px = p->d_px;
-      ea.py = p->d_py;
-      ea.pos = pos;
-      ea.x = p->d_x;
-      ea.tn = p->d_table_nod;
-      ea.d = p->d;
-      ea.dy = p->dy;
-      ea.bloch = p->d_bloch + 2 * b;
-      ea.E = E;
-      ea.ldE = 6 * ne;
-      ea.A32 = nullptr;
-      return ea;
-    };
     const cd *sol1 = p->d_sol1 ? (const cd *)p->d_sol1 + (size_t)b * p->nel * M * 39 : nullptr;
     const cd *sol2 = p->d_sol2 ? (const cd *)p->d_sol2 + (size_t)b * p->nel * M * 39 : nullptr;
-    if (p->precision == 1) {
-      // both contractions per element chunk: one E~ table (as the FP32 A
-      // operand), one B with the two field sets, one tensor-core GEMM
-      const int nb = (sol1 ? 2 * M : 0) + (sol2 ? 2 * M : 0);
-      const int off1 = sol1 ? 2 * M : 0;
-      int first = 1;
-      for (long e0 = 0; e0 < p->nel; e0 += nec) {
-        const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
-        const long long K = 6 * ne;
-        EtArgs ea = et_args(e0, ne);
-        ea.A32 = A32;
-        const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
-        etable_kernel<true><<<eg < 16 * sms ? eg : 16 * sms, 32 * kEtWarps, et_smem32, s>>>(ea);
-        const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems));
-        if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1, M, e0, ne, 0, 0, B32);
-        if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2, M, e0, ne, 1, off1, B32);
-        emu::note_launch(1 + (sol1 ? 1 : 0) + (sol2 ? 1 : 0));
-        int sp = tc_splits(npw, nb, 2 * K);
-        if (p->tc_splits > 0) sp = p->tc_splits < 64 ? p->tc_splits : 64;
-        const int tst = emu::tc_gemm_tf32x3(A32, B32, 2 * npw, nb, (int)(2 * K), sp, Cpart, C64, terr, s);
-        if (tst != EMU_OK) return tst;
-        const long long rgs = (gsz + 255) / 256;
-        pack_G_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(
-            C64, npw, nb, 2 * M, sol1 ? G : nullptr, sol2 ? Gd : nullptr, off1, first);
-        emu::note_launch();
-        first = 0;
-      }
-    }
     for (int pass = 0; pass < 2; ++pass) {
       const cd *sol = pass == 0 ? sol1 : sol2;
       if (!sol) continue;
       cd *acc = pass == 0 ? G : Gd;
       int first = 1;
-      for (long e0 = 0; e0 < p->nel && p->precision == 0; e0 += nec) {
+      for (long e0 = 0; e0 < p->nel; e0 += nec) {
         const long ne = (p->nel - e0) < nec ? (p->nel - e0) : nec;
-        EtArgs ea = et_args(e0, ne);
+        EtArgs ea;
+        ea.npw = npw;
+        ea.mo = p->max_order;
+        ea.e0 = (int)e0;
+        ea.ne = (int)ne;
+        ea.px = p->d_px;
+        ea.py = p->d_py;
+        ea.pos = pos;
+        ea.x = p->d_x;
+        ea.tn = p->d_table_nod;
+        ea.d = p->d;
+        ea.dy = p->dy;
+        ea.bloch = p->d_bloch + 2 * b;
+        ea.E = E;
+        ea.ldE = 6 * ne;
+        ea.A32 = nullptr;
+        ea.spos = 0;
+        ea.sA32 = 0;
         const int eg = (int)((ne + kEtWarps - 1) / kEtWarps);
         etable_kernel<false><<<eg < 8 * sms ? eg : 8 * sms, 32 * kEtWarps, et_smem, s>>>(ea);
         const long long rn = ne * 6 * 2 * (long long)M;

@@ -138,10 +138,12 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+// box at (x = K, y = row, z = problem) of a 3D [batch][rows][Kp] map
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z,
+                                            uint32_t mbar) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-      ::"r"(dst), "l"((uint64_t)map), "r"(mbar), "r"(x), "r"(y)
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(dst), "l"((uint64_t)map), "r"(mbar), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
 
@@ -170,8 +172,8 @@ __device__ __forceinline__ void split_tile(float4 *x, float4 *lo, int n4, int t)
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    tc_tf32x3_kernel(const __grid_constant__ TmaMaps maps, int Mp, int Np, int Kp, int kper, float *C,
-                     int *err) {
+    tc_tf32x3_kernel(const __grid_constant__ TmaMaps maps, int Mp, int Np, int Kp, int kper, int nsplit,
+                     float *C, int *err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   // 128-byte swizzled tiles need 1024-byte aligned shared addresses
   const uint32_t raw = smem_u32(sm_raw);
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint32_t *tslot = (uint32_t *)(bars + 3 * kStages + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
-  const int split = blockIdx.z;
+  const int split = blockIdx.z % nsplit, prob = blockIdx.z / nsplit;
   const int kbeg = split * kper;
   const int kend = min(Kp, kbeg + kper);
   const int nst = kend > kbeg ? (kend - kbeg + kTcK - 1) / kTcK : 0;
@@ -219,8 +221,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_expect_tx(fb, (uint32_t)(kATileBytes + kBTileBytes));
         const uint32_t base = smem_u32(buf + (size_t)b * kStageBytes);
         const int k0 = kbeg + t * kTcK;
-        tma_load_2d(base, &maps.a, k0, m0, fb);
-        tma_load_2d(base + 2 * kATileBytes, &maps.b, k0, n0, fb);
+        tma_load_3d(base, &maps.a, k0, m0, prob, fb);
+        tma_load_3d(base + 2 * kATileBytes, &maps.b, k0, n0, prob, fb);
       }
     }
   } else if (warp == 1) {
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp >= 2) {
     const int q = warp & 3;  // TMEM lane quarter this warp may read
     const int row = m0 + q * 32 + lane;
-    float *Cs = C + (size_t)split * Mp * Np;
+    float *Cs = C + ((size_t)prob * nsplit + split) * Mp * Np;
     if (nst > 0 && all_ok) {
       for (int c0 = 0; c0 < kTcN; c0 += 32) {
         float v[32];
@@ -340,16 +342,18 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 2D map over a row-major [rows][Kp] FP32 matrix, box = 32 (K, 128 bytes) x
-// box_rows, 128-byte swizzle (the UMMA SWIZZLE_128B K-major layout).
-static bool make_map(CUtensorMap *m, const float *ptr, int rows, int Kp, int box_rows) {
+// 3D map over `batch` row-major [rows][Kp] FP32 matrices `sbatch` floats
+// apart, box = 32 (K, 128 bytes) x box_rows x 1, 128-byte swizzle (the UMMA
+// SWIZZLE_128B K-major layout).
+static bool make_map(CUtensorMap *m, const float *ptr, int rows, int Kp, int box_rows, int batch,
+                     long long sbatch) {
   auto fn = encode_fn();
   if (!fn) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)Kp * 4};
-  const cuuint32_t box[2] = {(cuuint32_t)kTcK, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)ptr, dims, strides, box, estr,
+  const cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)batch};
+  const cuuint64_t strides[2] = {(cuuint64_t)Kp * 4, (cuuint64_t)sbatch * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)kTcK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)ptr, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -358,29 +362,48 @@ size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + 1024 + 256; }
 
 int tc_tiles(int Mp, int Np) { return ((Mp + kTcM - 1) / kTcM) * ((Np + kTcN - 1) / kTcN); }
 
-// C64[Mp][Np] = A[Mp][Kp] . B[Np][Kp]^T with split-TF32 tensor-core MMAs.
-// Operands FP32 (16-byte aligned rows, Kp % 4 == 0); Cpart scratch
-// [splits][Mp][Np] floats.
-int tc_gemm_tf32x3(const float *A, const float *B, int Mp, int Np, int Kp, int splits, float *Cpart,
-                   double *C64, int *d_err, cudaStream_t s) {
-  if (Mp < 1 || Np < 1 || Kp < 4 || splits < 1 || (Kp % 4)) return EMU_E_SHAPE;
-  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15)) return EMU_E_ARG;
+// Cpart[b][split][Mp][Np] = partial sums over K splits of A_b[Mp][Kp] .
+// B_b[Np][Kp]^T for b < batch, split-TF32 tensor-core MMAs.  Operands FP32,
+// 16-byte aligned, Kp % 4 == 0, batch strides sA, sB (floats, multiples of
+// 4).  Returns the number of splits used in *used.
+int tc_gemm_tf32x3_parts(const float *A, long long sA, const float *B, long long sB, int Mp, int Np, int Kp,
+                         int batch, int splits, float *Cpart, int *d_err, int *used, cudaStream_t s) {
+  if (Mp < 1 || Np < 1 || Kp < 4 || splits < 1 || batch < 1 || (Kp % 4)) return EMU_E_SHAPE;
+  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (sA % 4) || (sB % 4)) return EMU_E_ARG;
+  if (batch > 1 && (sA < (long long)Mp * Kp || sB < (long long)Np * Kp)) return EMU_E_ARG;
   TmaMaps maps;
-  if (!make_map(&maps.a, A, Mp, Kp, kTcM) || !make_map(&maps.b, B, Np, Kp, kTcN)) return EMU_E_CUDA;
+  if (!make_map(&maps.a, A, Mp, Kp, kTcM, batch, batch > 1 ? sA : (long long)Mp * Kp) ||
+      !make_map(&maps.b, B, Np, Kp, kTcN, batch, batch > 1 ? sB : (long long)Np * Kp))
+    return EMU_E_CUDA;
   const size_t smem = tc_smem_bytes();
   if (cudaFuncSetAttribute(tc_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return EMU_E_CUDA;
   int kper = (Kp + splits - 1) / splits;
   kper = (kper + kTcK - 1) / kTcK * kTcK;
-  const int used = (Kp + kper - 1) / kper;
-  dim3 grid((Np + kTcN - 1) / kTcN, (Mp + kTcM - 1) / kTcM, used);
-  tc_tf32x3_kernel<<<grid, kTcThreads, smem, s>>>(maps, Mp, Np, Kp, kper, Cpart, d_err);
+  const int nsplit = (Kp + kper - 1) / kper;
+  if ((long long)nsplit * batch > 65535) return EMU_E_SHAPE;
+  dim3 grid((Np + kTcN - 1) / kTcN, (Mp + kTcM - 1) / kTcM, nsplit * batch);
+  tc_tf32x3_kernel<<<grid, kTcThreads, smem, s>>>(maps, Mp, Np, Kp, kper, nsplit, Cpart, d_err);
+  note_launch();
+  *used = nsplit;
+  return check_launch();
+}
+
+// C64[Mp][Np] = A[Mp][Kp] . B[Np][Kp]^T with split-TF32 tensor-core MMAs.
+// Operands FP32 (16-byte aligned rows, Kp % 4 == 0); Cpart scratch
+// [splits][Mp][Np] floats.
+int tc_gemm_tf32x3(const float *A, const float *B, int Mp, int Np, int Kp, int splits, float *Cpart,
+                   double *C64, int *d_err, cudaStream_t s) {
+  int used = 0;
+  const int st = tc_gemm_tf32x3_parts(A, (long long)Mp * Kp, B, (long long)Np * Kp, Mp, Np, Kp, 1, splits, Cpart,
+                                      d_err, &used, s);
+  if (st != EMU_OK) return st;
   const long long n = (long long)Mp * Np;
   int g = (int)((n + 255) / 256);
   if (g > 8 * sm_count()) g = 8 * sm_count();
   sum_splits_kernel<<<g, 256, 0, s>>>(Cpart, used, n, C64);
-  note_launch(2);
+  note_launch(1);
   return check_launch();
 }
 
