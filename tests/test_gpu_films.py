@@ -186,3 +186,41 @@ def test_full_size_batch_properties():
                   n_lossy[sub].contiguous(), torch.tensor(h, device=dev), pol='TE')
     assert torch.equal(o2['R_net'], full['R_net'][sub])
     assert torch.equal(o2['a_list'], full['a_list'][sub])
+
+
+@pytest.mark.parametrize('pol', ['un', 'incoming'])
+def test_launch_variants_agree(pol):
+    """Every launch variant of the film kernel gives the same result: the
+    per-order quantities (R_net, T_net, k_z, interface r/t, mode vectors)
+    bit for bit, the flux sums (a/t/r lists, fluxes) to rounding, since the
+    teams add them up with shared-memory atomics in no fixed order."""
+    from emustack_b200 import _lib
+    from emustack_b200.films import FilmStackSolver
+    h, nl = _config2_stack(seed=5, L=6)
+    B = 40
+    wl, kp = _points(B, seed=9)
+    s = FilmStackSolver(len(nl), 4, 500.0)
+    dev = s.device
+    inc = None
+    if pol == 'incoming':
+        rng = np.random.default_rng(2)
+        inc = rng.normal(size=(B, 2 * s.npw)) + 1j * rng.normal(size=(B, 2 * s.npw))
+        inc[:, rng.random(2 * s.npw) < 0.6] = 0
+        inc = torch.tensor(inc, device=dev)
+    shears = torch.tensor(np.linspace(0, 0.4, 2 * len(nl)).reshape(len(nl), 2), device=dev)
+    want = ('kz', 'layer_rt', 'vec_coef', 'fluxes', 'num_prop')
+    args = (torch.tensor(wl, device=dev), torch.tensor(kp, device=dev),
+            torch.tensor(np.tile(nl, (B, 1)), device=dev), torch.tensor(h, device=dev))
+    res = {}
+    for v in _lib.FILM_VARIANTS:
+        out = s.solve(*args, pol='un' if inc is None else 'incoming', incoming=inc, shears=shears,
+                      want=want, variant=v)
+        res[v] = {k: t.cpu().numpy().copy() for k, t in out.items()}
+    exact = ('R_net', 'T_net', 'kz', 'layer_rt', 'vec_coef_down', 'vec_coef_up', 'flags', 'num_prop')
+    for v in _lib.FILM_VARIANTS[1:]:
+        for k, x in res[v].items():
+            if k in exact:
+                np.testing.assert_array_equal(x, res[0][k], err_msg='variant %d %s' % (v, k))
+            else:
+                np.testing.assert_allclose(x, res[0][k], rtol=1e-12, atol=1e-14,
+                                           err_msg='variant %d %s' % (v, k))
