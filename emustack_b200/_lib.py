@@ -131,6 +131,7 @@ class EmuLayer(C.Structure):
         ('stride_R12', C.c_longlong), ('stride_T12', C.c_longlong),
         ('stride_R21', C.c_longlong), ('stride_T21', C.c_longlong),
         ('d_kz', vp), ('stride_kz', C.c_longlong), ('height_norm', C.c_double),
+        ('d_height_norm', vp),
     ]
 
 

@@ -25,6 +25,7 @@ struct DLayer {
   long long sR12, sT12, sR21, sT21, skz;
   int M, dense;
   double hn, sh0, sh1;
+  const double *hnp;  // per-point height / period [b], or null: hn for all
 };
 
 struct StackArgs {
@@ -244,7 +245,8 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
     // ---------------- through layer i (stack.py:249-262)
     cd *pd = Pl + (size_t)(i - 1) * D;
     const cd *kz = lay_ptr(ly.kz, ly.skz);
-    for (int r = tid; r < M; r += nt) pd[r] = cexp_ikh(kz[r], ly.hn);
+    const double hn = ly.hnp ? ly.hnp[b] : ly.hn;
+    for (int r = tid; r < M; r += nt) pd[r] = cexp_ikh(kz[r], hn);
     __syncthreads();
     cd *X2 = X2l + (size_t)(i - 1) * DD;      // M x P
     cd *rn2 = Rl + (size_t)(slot + 1) * DD;   // P x P
@@ -538,8 +540,9 @@ __global__ void ew_rn_gap_diag(cd *rn, long long sn, const cd *t12, long long st
 }
 
 // pd = exp(i kz h)  (M)
-__global__ void ew_prop(cd *pd, long long sp, const cd *kz, long long skz, double hn, int M) {
-  EW_LOOP(M) pd[b * sp + e] = cexp_ikh(kz[b * skz + e], hn);
+__global__ void ew_prop(cd *pd, long long sp, const cd *kz, long long skz, double hn, const double *hnp,
+                        int M) {
+  EW_LOOP(M) pd[b * sp + e] = cexp_ikh(kz[b * skz + e], hnp ? hnp[b] : hn);
 }
 
 // Z = diag(pd) rn1 diag(pd), T = I  (M x M)
@@ -659,7 +662,7 @@ int stack_dense_multi(const StackArgs &a, cudaStream_t s) {
     }
     if (i == L - 1) break;
     cd *pd = w.Pl(i - 1);
-    ew_prop<<<ew(M), 256, 0, s>>>(pd, S, ly.kz, ly.skz, ly.hn, M);
+    ew_prop<<<ew(M), 256, 0, s>>>(pd, S, ly.kz, ly.skz, ly.hn, ly.hnp, M);
     cd *X2 = w.X2(i - 1), *rn2 = w.Rl(slot + 1);
     if (ly.dense) {
       ew_layer_dense<<<ew(M * M), 256, 0, s>>>(Z, T, S, pd, S, rn1, M);
@@ -783,6 +786,7 @@ extern "C" int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace,
     d.M = l.M;
     d.dense = l.dense;
     d.hn = l.height_norm;
+    d.hnp = l.d_height_norm;
     d.sh0 = p->h_shears ? p->h_shears[2 * i] : 0.0;
     d.sh1 = p->h_shears ? p->h_shears[2 * i + 1] : 0.0;
   }

@@ -115,15 +115,21 @@ class DenseLayer(object):
     """One layer of a dense batch: device interface matrices with air.
 
     dense=False: film, R12..T21 are diagonals [B, P]; dense=True: full
-    matrices [B, P, P], [B, M, P], [B, M, M], [B, P, M].  kz [B, M] and
-    height_norm (height / period) for finite layers.
+    matrices [B, P, P], [B, M, P], [B, M, M], [B, P, M] (a leading 1 instead
+    of B shares one matrix across the batch).  kz [B, M] and height_norm
+    (height / period) for finite layers: one float for the whole batch, or a
+    CUDA float64 tensor [B] of per-point heights.
     """
 
     def __init__(self, R12, T12, R21, T21, dense, kz=None, height_norm=0.0):
         self.R12, self.T12, self.R21, self.T21 = R12, T12, R21, T21
         self.dense = bool(dense)
         self.kz = kz
-        self.height_norm = float(height_norm)
+        if torch.is_tensor(height_norm):
+            _need(height_norm, torch.float64, 'height_norm', 1)
+            self.height_norm = height_norm
+        else:
+            self.height_norm = float(height_norm)
         self.M = int(T12.shape[1]) if dense else int(R12.shape[1])
 
 
@@ -157,8 +163,13 @@ class DenseStackSolver(object):
                 setattr(e, 'stride_' + nm, int(t[0].numel()) if t.shape[0] == B and B > 1 else 0)
             if ly.kz is not None:
                 e.d_kz = ptr(ly.kz)
-                e.stride_kz = int(ly.kz[0].numel()) if B > 1 else 0
-            e.height_norm = ly.height_norm
+                e.stride_kz = int(ly.kz[0].numel()) if ly.kz.shape[0] == B and B > 1 else 0
+            if torch.is_tensor(ly.height_norm):
+                if ly.height_norm.numel() != B:
+                    raise ValueError('layer %d: height_norm must have one entry per point' % i)
+                e.d_height_norm = ptr(ly.height_norm)
+            else:
+                e.height_norm = ly.height_norm
         d = EmuStackDense()
         d.batch, d.n_layers, d.P = B, L, P
         d.mode = int(mode)

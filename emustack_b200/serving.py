@@ -1,11 +1,15 @@
 """Continuous-batching server for GSM solves on one GPU.
 
-Requests (one spectral point of an all-film stack each, any shape) arrive at
-any time; a scheduler thread admits waiting requests into a device batch as
-long as the batch fits the HBM budget left by the batches still in flight,
-and launches it on a free stream while earlier batches are still running.
+Requests -- one spectral point each, of an all-film stack of any shape
+(``FilmRequest``) or of a stack with nanostructured array layers
+(``ArrayRequest``, emustack_b200.array_serving) -- arrive at any time; a
+scheduler thread admits waiting requests into a device batch as long as the
+batch fits the HBM budget left by the batches still in flight, and launches
+it on a free stream while earlier batches are still running.  Array layers'
+interfaces with the air reference are cached on the device (``SMatrixCache``)
+and reused by every later request that names the same layer.
 
-Two batching modes:
+Film requests have two batching modes:
 
 * ``'mixed'`` (default): a batch takes requests in arrival order whatever
   their shape (layer count, order set, periods, polarisation) and runs as one
@@ -13,6 +17,10 @@ Two batching modes:
   per point);
 * ``'grouped'``: requests are grouped by shape signature and each batch is
   one launch of the uniform film kernel (``emu_film_stack_batch``).
+
+Array requests are always grouped by shape signature (order set,
+polarisation, layer kinds and Bloch-mode counts): a batch is the chain of
+``ArrayBatcher.launch`` (film modes, missing interfaces, cascade + fluxes).
 
 Each batch is an async host-to-device copy of its packed inputs, one kernel,
 and an async device-to-host copy of its packed outputs on the slot's
@@ -31,6 +39,7 @@ import time
 import numpy as np
 import torch
 
+from .array_serving import ArrayBatcher, ArrayLayer, ArrayRequest, SMatrixCache  # noqa: F401
 from .films import FilmPoint, FilmStackSolver, FilmVarSolver, grating_orders
 
 _NPW = {}
@@ -132,19 +141,25 @@ class _Batch(object):
 class GsmServer(object):
     """Continuous batching of GSM solve requests on one GPU.
 
-    hbm_budget_bytes bounds the device memory of batches in flight;
+    hbm_budget_bytes bounds the device memory of the server: the layer
+    interface cache (smatrix_cache_bytes of it) plus the batches in flight;
     n_streams batches may run at once; max_batch caps one launch;
-    batching is 'mixed' (any shapes in one launch) or 'grouped'.
+    batching of film requests is 'mixed' (any shapes in one launch) or
+    'grouped'.
     """
 
     def __init__(self, device=None, hbm_budget_bytes=150 << 30, max_batch=32768, n_streams=2,
-                 poll_s=2e-4, batching='mixed'):
+                 poll_s=2e-4, batching='mixed', smatrix_cache_bytes=16 << 30):
         if batching not in ('mixed', 'grouped'):
             raise ValueError("batching must be 'mixed' or 'grouped'")
         self.device = (torch.device('cuda', torch.cuda.current_device()) if device is None
                        else torch.device(device))
         self.batching = batching
-        self.budget = int(hbm_budget_bytes)
+        if smatrix_cache_bytes >= hbm_budget_bytes:
+            raise ValueError('the layer interface cache must leave room for batches in the budget')
+        self.cache = SMatrixCache(smatrix_cache_bytes)
+        self._arrays = None
+        self.budget = int(hbm_budget_bytes) - int(smatrix_cache_bytes)
         self.max_batch = int(max_batch)
         self.poll_s = poll_s
         self.q = collections.deque()      # submit -> scheduler (append / popleft are atomic)
@@ -208,11 +223,14 @@ class GsmServer(object):
             'throughput_per_s': n / span if n and span > 0 else float('nan'),
             'p50_ms': float(np.percentile(lat, 50)) if n else float('nan'),
             'p99_ms': float(np.percentile(lat, 99)) if n else float('nan'),
+            'smatrix_cache': self.cache.stats(),
         }
 
     # ---------------------------------------------------------------- loop
     def _key(self, r):
-        return 'all' if self.batching == 'mixed' else r.signature
+        if self.batching == 'mixed' and not isinstance(r, ArrayRequest):
+            return 'all'
+        return r.signature
 
     def _take(self, block):
         if block and not self.q:
@@ -303,7 +321,9 @@ class GsmServer(object):
                 self.pending.move_to_end(key)
             if not reqs:
                 continue
-            if self.batching == 'mixed':
+            if isinstance(reqs[0], ArrayRequest):
+                self._run_arrays(slot, reqs, nbytes)
+            elif self.batching == 'mixed':
                 self._run_mixed(slot, reqs, nbytes)
             else:
                 self._run_grouped(slot, reqs[0].signature, reqs, nbytes)
@@ -385,6 +405,26 @@ class GsmServer(object):
             self._record(b.reqs, t)
 
         self._submit(_Batch(reqs, slot, ev, nbytes, finish, (dwl, dkp, dn, dh)))
+
+    def _run_arrays(self, slot, reqs, nbytes):
+        if self._arrays is None:
+            self._arrays = ArrayBatcher(self.device, self.cache)
+        t1 = time.perf_counter()
+        ev, fin = self._arrays.launch(reqs, slot['stream'], id(slot))
+        self.prof['launch_s'] += time.perf_counter() - t1
+
+        def finish(b, t):
+            t2 = time.perf_counter()
+            vals = fin()
+            ok = [i for i, v in enumerate(vals) if not isinstance(v, Exception)]
+            self._publish([b.reqs[i] for i in ok], [vals[i] for i in ok])
+            for i, v in enumerate(vals):
+                if isinstance(v, Exception):
+                    self._publish([b.reqs[i]], exc=v)
+            self._record(b.reqs, t)
+            self.prof['finish_s'] += time.perf_counter() - t2
+
+        self._submit(_Batch(reqs, slot, ev, nbytes, finish, None))
 
     def _submit(self, batch):
         batch.slot['busy'] = True

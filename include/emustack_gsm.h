@@ -246,6 +246,8 @@ typedef struct {
   const emu_c128 *d_kz;  /* [b][M] k_z (finite layers)                      */
   long long stride_kz;
   double height_norm;    /* height / period (finite layers)                 */
+  const double *d_height_norm; /* [b] per-point height / period, or NULL:
+                                * height_norm for every point               */
 } EmuLayer;
 
 typedef struct {

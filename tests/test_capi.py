@@ -66,8 +66,13 @@ def test_grating_orders_1d_and_errors():
     assert _lib.lib().emu_grating_orders(-1, 1.0, 1.0, 0, None, None, 0, C.byref(n)) == 1
 
 
-def test_film_var_struct_layout_matches_header(tmp_path):
-    """ctypes mirrors of EmuFilmPoint / EmuFilmVarBatch have the C layout."""
+STRUCTS = ('EmuFilmStackBatch', 'EmuAnalloModes', 'EmuLayer', 'EmuStackDense', 'EmuOverlap',
+           'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch')
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror of a descriptor struct has the C layout of
+    include/emustack_gsm.h (size and the offset of every field)."""
     import ctypes as C
     import shutil
     import subprocess
@@ -76,22 +81,22 @@ def test_film_var_struct_layout_matches_header(tmp_path):
     if gcc is None:
         pytest.skip('gcc not available')
     src = tmp_path / 'layout.c'
-    fields = [f for f, _ in _lib.EmuFilmVarBatch._fields_]
-    pfields = [f for f, _ in _lib.EmuFilmPoint._fields_]
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "emustack_gsm.h"', 'int main(void){',
-             'printf("%zu %zu\\n", sizeof(EmuFilmPoint), sizeof(EmuFilmVarBatch));']
-    lines += ['printf("%%zu ", offsetof(EmuFilmPoint, %s));' % f for f in pfields]
-    lines += ['printf("\\n");']
-    lines += ['printf("%%zu ", offsetof(EmuFilmVarBatch, %s));' % f for f in fields]
-    lines += ['printf("\\n"); return 0; }']
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "emustack_gsm.h"', 'int main(void){']
+    for name in STRUCTS:
+        lines.append('printf("%%zu", sizeof(%s));' % name)
+        lines += ['printf(" %%zu", offsetof(%s, %s));' % (name, f) for f, _ in getattr(_lib, name)._fields_]
+        lines.append('printf("\\n");')
+    lines.append('return 0; }')
     src.write_text('\n'.join(lines))
     exe = tmp_path / 'layout'
     subprocess.check_call([gcc, '-I' + os.path.join(ROOT, 'include'), str(src), '-o', str(exe)])
-    out = subprocess.check_output([str(exe)]).decode().split('\n')
-    sp, sb = map(int, out[0].split())
-    assert sp == C.sizeof(_lib.EmuFilmPoint) and sb == C.sizeof(_lib.EmuFilmVarBatch)
-    assert list(map(int, out[1].split())) == [getattr(_lib.EmuFilmPoint, f).offset for f in pfields]
-    assert list(map(int, out[2].split())) == [getattr(_lib.EmuFilmVarBatch, f).offset for f in fields]
+    out = subprocess.check_output([str(exe)]).decode().strip().split('\n')
+    assert len(out) == len(STRUCTS)
+    for name, line in zip(STRUCTS, out):
+        st = getattr(_lib, name)
+        got = list(map(int, line.split()))
+        assert got[0] == C.sizeof(st), name
+        assert got[1:] == [getattr(st, f).offset for f, _ in st._fields_], name
 
 
 def test_film_var_plan_offsets_and_order():
