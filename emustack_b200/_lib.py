@@ -236,3 +236,41 @@ EXTRA_SIGNATURES.extend([
                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ('emu_film_var_batch', C.c_int, [C.POINTER(EmuFilmVarBatch), vp, C.c_size_t, vp]),
 ])
+
+
+class EmuVarLayer(C.Structure):
+    _fields_ = [
+        ('M', C.c_int), ('dense', C.c_int),
+        ('d_R12', vp), ('d_T12', vp), ('d_R21', vp), ('d_T21', vp), ('d_kz', vp),
+        ('height_norm', C.c_double),
+    ]
+
+
+class EmuStackPoint(C.Structure):
+    _fields_ = [
+        ('n_layers', C.c_int32), ('P', C.c_int32), ('pol', C.c_int32), ('spec', C.c_int32),
+        ('num_prop', C.c_int32 * 3), ('_pad', C.c_int32),
+        ('layer_off', C.c_int64), ('inc_off', C.c_int64), ('rnet_off', C.c_int64),
+        ('tnet_off', C.c_int64), ('list_off', C.c_int64), ('flux_off', C.c_int64),
+    ]
+
+
+class EmuStackVarBatch(C.Structure):
+    _fields_ = [
+        ('n_stacks', C.c_int), ('d_points', vp), ('d_order', vp), ('d_layers', vp),
+        ('n_layer_desc', C.c_int64),
+        ('d_incoming', vp), ('incoming_len', C.c_int64),
+        ('d_R_net', vp), ('rnet_len', C.c_int64),
+        ('d_T_net', vp), ('tnet_len', C.c_int64),
+        ('d_a_list', vp), ('d_t_list', vp), ('list_len', C.c_int64),
+        ('d_fluxes', vp), ('flux_len', C.c_int64),
+        ('d_r_list', vp), ('d_flags', vp), ('d_info', vp),
+        ('max_P', C.c_int), ('max_D', C.c_int), ('max_L', C.c_int), ('n_slots', C.c_int),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_stack_var_slots', C.c_int, [C.POINTER(EmuStackVarBatch)]),
+    ('emu_stack_var_workspace_size', C.c_size_t, [C.POINTER(EmuStackVarBatch)]),
+    ('emu_stack_var_batch', C.c_int, [C.POINTER(EmuStackVarBatch), vp, C.c_size_t, vp]),
+])

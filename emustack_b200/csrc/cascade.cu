@@ -123,9 +123,11 @@ __device__ __forceinline__ cd incidence(const StackArgs &a, int b, int pos, int 
   return cd{0.0, 0.0};
 }
 
-__global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
-  __shared__ Smem sm;
-  const int b = blockIdx.x;
+// One spectral point, the whole cascade and flux pass, by one CTA.  `a` is
+// the uniform batch's kernel parameter (point b) or, for the uneven batch,
+// a per-stack copy in shared memory whose pointers are already offset to the
+// stack (b = 0).
+__device__ __forceinline__ void stack_body(const StackArgs &a, const int b, Smem &sm) {
   const int L = a.L, P = a.P, D = a.D, npw = a.npw;
   const int tid = threadIdx.x, nt = blockDim.x;
   const size_t DD = (size_t)D * D;
@@ -438,6 +440,11 @@ __global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
       if (a.flags) a.flags[b] = flags;
     }
   }
+}
+
+__global__ void __launch_bounds__(kDLThreads) stack_dense_kernel(StackArgs a) {
+  __shared__ Smem sm;
+  stack_body(a, blockIdx.x, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -825,6 +832,221 @@ extern "C" int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace,
   if (mode == 0) mode = (a.D >= 256 || (a.D >= 96 && p->batch < emu::sm_count())) ? 2 : 1;
   if (mode == 2) return stack_dense_multi(a, (cudaStream_t)stream);
   stack_dense_kernel<<<p->batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);
+  emu::note_launch();
+  return emu::check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Uneven batch of dense stacks in one launch (emu_stack_var_batch).
+//
+// A persistent kernel: each CTA owns one workspace slot and repeatedly takes
+// the next stack from an atomic counter (in the caller's processing order),
+// copies the stack's descriptor into a StackArgs in shared memory with every
+// pointer offset to the stack, checks it against the packed arrays, and runs
+// stack_body on it -- the one-CTA cascade and flux pass of the uniform batch,
+// so a stack gives the same result here as in emu_stack_dense_batch.  No CTA
+// waits on another: a CTA that finds the counter past the end returns.
+
+namespace {
+
+struct VarStackArgs {
+  int n;
+  const EmuStackPoint *pts;
+  const int *order;
+  const EmuVarLayer *lays;
+  long long n_lays;
+  const cd *inc;
+  long long inc_len;
+  cd *R_net, *T_net;
+  long long rnet_len, tnet_len;
+  double *a_list, *t_list, *fluxes, *r_list;
+  long long list_len, flux_len;
+  unsigned *flags;
+  int *info;
+  int max_P, max_D, max_L;
+  int *counter;
+  cd *ws;
+  long long ws_stride;
+  int *ipiv;
+  double inv_sqrt2;
+};
+
+__global__ void __launch_bounds__(kDLThreads) stack_var_kernel(VarStackArgs v) {
+  __shared__ Smem sm;
+  __shared__ StackArgs sa;
+  __shared__ int s_next, s_bad;
+  const int tid = threadIdx.x;
+  cd *ws = v.ws + (size_t)blockIdx.x * v.ws_stride;
+  int *ipiv = v.ipiv + (size_t)blockIdx.x * v.max_D;
+  for (;;) {
+    if (tid == 0) {
+      s_next = atomicAdd(v.counter, 1);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int k = s_next;
+    if (k >= v.n) break;
+    const int s = v.order ? v.order[k] : k;
+    if (s < 0 || s >= v.n) {  // a bad order entry: nothing to flag
+      __syncthreads();
+      continue;
+    }
+    const EmuStackPoint &pt = v.pts[s];
+    const int L = pt.n_layers, P = pt.P;
+    bool ok = L >= 2 && L <= v.max_L && L <= kMaxLayers && P >= 2 && (P % 2) == 0 && P <= v.max_P &&
+              pt.pol >= EMU_POL_INCOMING && pt.pol <= EMU_POL_LCIRC && pt.spec >= 0 && pt.spec < P / 2 &&
+              pt.layer_off >= 0 && pt.layer_off + L <= v.n_lays;
+    for (int q = 0; q < 3; ++q) ok = ok && pt.num_prop[q] >= 0 && pt.num_prop[q] <= P / 2;
+    ok = ok && pt.rnet_off >= 0 && pt.rnet_off + (long long)P * P <= v.rnet_len;
+    ok = ok && pt.tnet_off >= 0 && pt.tnet_off + (long long)P * P <= v.tnet_len;
+    ok = ok && pt.list_off >= 0 && pt.list_off + L - 1 <= v.list_len;
+    ok = ok && (!v.fluxes || (pt.flux_off >= 0 && pt.flux_off + 2LL * (L + 1) <= v.flux_len));
+    ok = ok && (pt.pol != EMU_POL_INCOMING || (v.inc && pt.inc_off >= 0 && pt.inc_off + P <= v.inc_len));
+    if (!ok && tid == 0) s_bad = 1;
+    __syncthreads();
+    if (!s_bad && tid < L) {
+      const EmuVarLayer &l = v.lays[pt.layer_off + tid];
+      const bool fin = tid > 0 && tid < L - 1;
+      bool lok = l.M >= 1 && l.M <= v.max_D && l.d_R12 && l.d_T12 && l.d_R21 && l.d_T21 &&
+                 (!fin || l.d_kz) && (l.dense || l.M == P) && (fin || !l.dense);
+      if (!lok) atomicOr(&s_bad, 1);
+      DLayer &d = sa.lay[tid];
+      d.R12 = (const cd *)l.d_R12;
+      d.T12 = (const cd *)l.d_T12;
+      d.R21 = (const cd *)l.d_R21;
+      d.T21 = (const cd *)l.d_T21;
+      d.kz = (const cd *)l.d_kz;
+      d.sR12 = d.sT12 = d.sR21 = d.sT21 = d.skz = 0;
+      d.M = l.M;
+      d.dense = l.dense;
+      d.hn = l.height_norm;
+      d.sh0 = d.sh1 = 0.0;
+      d.hnp = nullptr;
+    }
+    __syncthreads();
+    if (s_bad) {
+      if (tid == 0) {
+        v.flags[s] = EMU_PT_BAD_POINT;
+        v.info[s] = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (tid == 0) {
+      int D = P;
+      for (int i = 0; i < L; ++i) D = sa.lay[i].M > D ? sa.lay[i].M : D;
+      sa.B = 1;
+      sa.L = L;
+      sa.P = P;
+      sa.npw = P / 2;
+      sa.D = D;
+      sa.ncoord = 1;
+      sa.has_shear = 0;
+      sa.calc_fluxes = 1;
+      sa.pol = pt.pol;
+      sa.save_lists = 0;
+      sa.alphas = sa.betas = nullptr;
+      sa.incoming = pt.pol == EMU_POL_INCOMING ? v.inc + pt.inc_off : nullptr;
+      sa.spec = &pt.spec;
+      sa.nprop = pt.num_prop;
+      sa.R_net = v.R_net + pt.rnet_off;
+      sa.T_net = v.T_net + pt.tnet_off;
+      sa.fluxes = v.fluxes ? v.fluxes + pt.flux_off : nullptr;
+      sa.a_list = v.a_list + pt.list_off;
+      sa.t_list = v.t_list + pt.list_off;
+      sa.r_list = v.r_list + s;
+      sa.flags = v.flags + s;
+      sa.info = v.info + s;
+      sa.vcd = sa.vcu = nullptr;
+      sa.vcd_stride = sa.vcu_stride = 0;
+      sa.tnl = sa.rnl = nullptr;
+      sa.ws = ws;
+      sa.ws_stride = 0;
+      sa.ipiv = ipiv;
+      sa.inv_sqrt2 = v.inv_sqrt2;
+      sa.flux_only = 0;
+    }
+    __syncthreads();
+    stack_body(sa, 0, sm);
+    __syncthreads();
+  }
+}
+
+long long var_slot_elems(int L, int D) {
+  const long long Lf = L > 2 ? L - 2 : 0, DD = (long long)D * D;
+  return (2LL * L - 2 + L - 1 + Lf + 4) * DD + Lf * D + 6LL * D;
+}
+
+int var_validate(const EmuStackVarBatch *p) {
+  if (!p) return EMU_E_ARG;
+  if (p->n_stacks < 0 || p->n_slots < 0) return EMU_E_SHAPE;
+  if (p->n_stacks == 0) return EMU_OK;
+  if (p->max_P < 2 || p->max_D < p->max_P || p->max_L < 2 || p->max_L > kMaxLayers) return EMU_E_SHAPE;
+  if (!p->d_points || !p->d_layers || !p->d_R_net || !p->d_T_net || !p->d_a_list || !p->d_t_list ||
+      !p->d_r_list || !p->d_flags || !p->d_info)
+    return EMU_E_ARG;
+  return EMU_OK;
+}
+
+}  // namespace
+
+extern "C" int emu_stack_var_slots(const EmuStackVarBatch *p) {
+  if (var_validate(p) != EMU_OK) return 0;
+  if (p->n_slots > 0) return p->n_slots < p->n_stacks ? p->n_slots : p->n_stacks;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stack_var_kernel, kDLThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long slots = (long long)emu::sm_count() * per_sm;
+  return (int)(slots < p->n_stacks ? slots : p->n_stacks);
+}
+
+extern "C" size_t emu_stack_var_workspace_size(const EmuStackVarBatch *p) {
+  if (var_validate(p) != EMU_OK) return 0;
+  const long long slots = emu_stack_var_slots(p);
+  return 256 + (size_t)slots * var_slot_elems(p->max_L, p->max_D) * sizeof(cd) +
+         align_up((size_t)slots * p->max_D * sizeof(int), 16);
+}
+
+extern "C" int emu_stack_var_batch(const EmuStackVarBatch *p, void *d_workspace, size_t workspace_bytes,
+                                   void *stream) {
+  const int st = var_validate(p);
+  if (st != EMU_OK) return st;
+  if (p->n_stacks == 0) return EMU_OK;
+  const size_t need = emu_stack_var_workspace_size(p);
+  if (!d_workspace || workspace_bytes < need) return EMU_E_WORKSPACE;
+  const int slots = emu_stack_var_slots(p);
+  cudaStream_t s = (cudaStream_t)stream;
+  VarStackArgs v;
+  v.n = p->n_stacks;
+  v.pts = p->d_points;
+  v.order = p->d_order;
+  v.lays = p->d_layers;
+  v.n_lays = p->n_layer_desc;
+  v.inc = (const cd *)p->d_incoming;
+  v.inc_len = p->incoming_len;
+  v.R_net = (cd *)p->d_R_net;
+  v.T_net = (cd *)p->d_T_net;
+  v.rnet_len = p->rnet_len;
+  v.tnet_len = p->tnet_len;
+  v.a_list = p->d_a_list;
+  v.t_list = p->d_t_list;
+  v.list_len = p->list_len;
+  v.fluxes = p->d_fluxes;
+  v.flux_len = p->flux_len;
+  v.r_list = p->d_r_list;
+  v.flags = p->d_flags;
+  v.info = p->d_info;
+  v.max_P = p->max_P;
+  v.max_D = p->max_D;
+  v.max_L = p->max_L;
+  v.counter = (int *)d_workspace;
+  v.ws = (cd *)((char *)d_workspace + 256);
+  v.ws_stride = var_slot_elems(p->max_L, p->max_D);
+  v.ipiv = (int *)((char *)d_workspace + 256 + (size_t)slots * v.ws_stride * sizeof(cd));
+  v.inv_sqrt2 = 1.0 / sqrt(2.0);
+  if (cudaMemsetAsync(v.counter, 0, sizeof(int), s) != cudaSuccess) return EMU_E_CUDA;
+  stack_var_kernel<<<slots, kDLThreads, 0, s>>>(v);
   emu::note_launch();
   return emu::check_launch();
 }

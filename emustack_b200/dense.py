@@ -380,3 +380,159 @@ def calc_scat_dense(stack, pol='TE', incoming_amplitudes=None, calc_fluxes=True,
         stack.a_list, stack.t_list, stack.r_list = a_list, t_list, [abs(up0 / df[0])]
     stack.down_fluxes = df
     stack.up_flux = [up0]
+
+
+# ---------------------------------------------------------------------------
+# uneven batch of dense stacks in one launch
+# ---------------------------------------------------------------------------
+
+_POINT_DTYPE = np.dtype([
+    ('n_layers', np.int32), ('P', np.int32), ('pol', np.int32), ('spec', np.int32),
+    ('num_prop', np.int32, 3), ('_pad', np.int32),
+    ('layer_off', np.int64), ('inc_off', np.int64), ('rnet_off', np.int64),
+    ('tnet_off', np.int64), ('list_off', np.int64), ('flux_off', np.int64),
+])
+_LAYER_DTYPE = np.dtype([
+    ('M', np.int32), ('dense', np.int32), ('R12', np.uint64), ('T12', np.uint64), ('R21', np.uint64),
+    ('T21', np.uint64), ('kz', np.uint64), ('height_norm', np.float64),
+])
+assert _POINT_DTYPE.itemsize == C.sizeof(_lib.EmuStackPoint)
+assert _LAYER_DTYPE.itemsize == C.sizeof(_lib.EmuVarLayer)
+
+
+class VarStack(object):
+    """One stack of an uneven dense batch (one spectral point).
+
+    layers: bottom to top, each (R12, T12, R21, T21, dense, kz, height_norm)
+    with device tensors of ONE point (film: diagonals [P]; dense: [P, P],
+    [M, P], [M, M], [P, M]; kz [M] for finite layers, else None); the
+    substrate and the superstrate are films.  pol: a polarisation name, or
+    incoming [P] (device) amplitudes.  spec / num_prop (air, superstrate,
+    substrate) may be left None and given to ``StackVarSolver.solve`` as
+    device tensors.
+    """
+
+    __slots__ = ('layers', 'P', 'pol', 'incoming', 'spec', 'num_prop', 'M', 'D', 'cost')
+
+    def __init__(self, layers, P, pol='TE', incoming=None, spec=None, num_prop=None):
+        self.layers = layers
+        self.P = int(P)
+        self.incoming = incoming
+        self.pol = _lib.POL_INCOMING if incoming is not None else _lib.POL[pol]
+        self.spec = spec
+        self.num_prop = num_prop
+        self.M = [int(ly[3].shape[-1]) if ly[4] else self.P for ly in layers]
+        self.D = max([self.P] + self.M)
+        # the one-CTA cascade's work grows as D^3 per layer
+        self.cost = float(len(layers)) * self.D ** 3
+
+
+class StackVarSolver(object):
+    """Cascade + fluxes of an uneven batch of dense stacks in one launch
+    (emu_stack_var_batch): each stack is the one-CTA path of
+    ``DenseStackSolver`` with its own shapes, taken costliest first by a
+    persistent kernel."""
+
+    def __init__(self, device=None):
+        self.device = device or _dev()
+        self._ws = None
+
+    def solve(self, stacks, spec=None, num_prop=None, n_slots=0, ws_budget_bytes=None, want_fluxes=False):
+        """Returns a dict of packed device outputs (R_net, T_net [sum P^2],
+        a_list, t_list [sum (L-1)], r_list, flags, info [n], fluxes [sum
+        2(L+1)] if asked) and the host offsets (rnet_off, list_off,
+        flux_off).  spec [n] / num_prop [n, 3] int32 device tensors override
+        the stacks' own values."""
+        n = len(stacks)
+        dev = self.device
+        pts = np.zeros(n, _POINT_DTYPE)
+        n_lay = sum(len(s.layers) for s in stacks)
+        lays = np.zeros(n_lay, _LAYER_DTYPE)
+        keep = []
+        lo = ro = li = fo = io = 0
+        inc_parts = []
+        for i, s in enumerate(stacks):
+            L, P = len(s.layers), s.P
+            p = pts[i]
+            p['n_layers'], p['P'], p['pol'] = L, P, s.pol
+            if s.spec is not None:
+                p['spec'] = int(s.spec)
+            if s.num_prop is not None:
+                p['num_prop'] = [int(x) for x in s.num_prop]
+            p['layer_off'], p['rnet_off'], p['tnet_off'] = lo, ro, ro
+            p['list_off'], p['flux_off'] = li, fo
+            p['inc_off'] = -1
+            if s.incoming is not None:
+                p['inc_off'] = io
+                inc_parts.append(s.incoming.reshape(-1))
+                io += P
+            for j, (R12, T12, R21, T21, dense, kz, hn) in enumerate(s.layers):
+                e = lays[lo + j]
+                e['M'], e['dense'] = s.M[j], int(bool(dense))
+                for nm, t in (('R12', R12), ('T12', T12), ('R21', R21), ('T21', T21), ('kz', kz)):
+                    if t is not None:
+                        if not t.is_cuda or t.dtype != c128 or not t.is_contiguous():
+                            raise TypeError('stack %d layer %d %s must be a contiguous CUDA complex128 '
+                                            'tensor' % (i, j, nm))
+                        e[nm] = t.data_ptr()
+                        keep.append(t)
+                e['height_norm'] = float(hn)
+            lo += L
+            ro += P * P
+            li += L - 1
+            fo += 2 * (L + 1)
+        out = {
+            'R_net': torch.empty(ro, dtype=c128, device=dev),
+            'T_net': torch.empty(ro, dtype=c128, device=dev),
+            'a_list': torch.empty(li, dtype=torch.float64, device=dev),
+            't_list': torch.empty(li, dtype=torch.float64, device=dev),
+            'r_list': torch.empty(n, dtype=torch.float64, device=dev),
+            'flags': torch.zeros(n, dtype=torch.int32, device=dev),
+            'info': torch.zeros(n, dtype=torch.int32, device=dev),
+        }
+        if want_fluxes:
+            out['fluxes'] = torch.empty(fo, dtype=torch.float64, device=dev)
+        order = np.argsort([-s.cost for s in stacks], kind='stable').astype(np.int32)
+        h_pts = torch.from_numpy(pts.view(np.uint8)).pin_memory()
+        h_lays = torch.from_numpy(lays.view(np.uint8)).pin_memory()
+        h_ord = torch.from_numpy(order).pin_memory()
+        d_pts = h_pts.to(dev, non_blocking=True)
+        d_lays = h_lays.to(dev, non_blocking=True)
+        d_ord = h_ord.to(dev, non_blocking=True)
+        iv = d_pts.view(torch.int32).view(n, _POINT_DTYPE.itemsize // 4)
+        if spec is not None:
+            iv[:, 3] = spec.to(torch.int32)
+        if num_prop is not None:
+            iv[:, 4:7] = num_prop.to(torch.int32)
+        inc = torch.cat(inc_parts) if inc_parts else None
+        d = _lib.EmuStackVarBatch()
+        d.n_stacks = n
+        d.d_points, d.d_order, d.d_layers = ptr(d_pts), ptr(d_ord), ptr(d_lays)
+        d.n_layer_desc = n_lay
+        d.d_incoming, d.incoming_len = ptr(inc), io
+        d.d_R_net, d.rnet_len = ptr(out['R_net']), ro
+        d.d_T_net, d.tnet_len = ptr(out['T_net']), ro
+        d.d_a_list, d.d_t_list, d.list_len = ptr(out['a_list']), ptr(out['t_list']), li
+        d.d_fluxes, d.flux_len = ptr(out.get('fluxes')), fo
+        d.d_r_list, d.d_flags, d.d_info = ptr(out['r_list']), ptr(out['flags']), ptr(out['info'])
+        d.max_P = max(s.P for s in stacks)
+        d.max_D = max(s.D for s in stacks)
+        d.max_L = max(len(s.layers) for s in stacks)
+        L_ = lib()
+        d.n_slots = int(n_slots)
+        if ws_budget_bytes is not None:
+            d.n_slots = 0
+            auto = L_.emu_stack_var_slots(C.byref(d))
+            per = (L_.emu_stack_var_workspace_size(C.byref(d)) - 256) / max(auto, 1)
+            d.n_slots = max(1, min(auto, int(ws_budget_bytes // max(per, 1))))
+        nbytes = L_.emu_stack_var_workspace_size(C.byref(d))
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        check(L_.emu_stack_var_batch(C.byref(d), ptr(self._ws), C.c_size_t(self._ws.numel()), stream_ptr()),
+              'emu_stack_var_batch')
+        out['_keep'] = (keep, d_pts, d_lays, d_ord, inc, h_pts, h_lays, h_ord)
+        out['rnet_off'] = pts['rnet_off']
+        out['list_off'] = pts['list_off']
+        out['flux_off'] = pts['flux_off']
+        out['n_slots'] = int(L_.emu_stack_var_slots(C.byref(d)))
+        return out

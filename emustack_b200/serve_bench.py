@@ -13,6 +13,16 @@ advance (exponential gaps at the offered rate); a submitter thread hands
 each request to the server at its arrival time and latency is measured from
 that scheduled time (so a slow submitter cannot hide queueing).  One JSON
 line per rate: offered and achieved throughput, p50 / p99 latency, batches.
+
+With --array-frac F a fraction F of the requests are array stacks
+(``ArrayRequest``): a film substrate (n = 1.46), 2-12 finite layers each a
+film or one of the nanostructured layers of the request's spectral point,
+and air.  Spectral points come from a pool (--array-pool of them, P log-
+uniform in [50, 900] like the films, M = P + 20 Bloch modes, two array
+layers per point with synthetic J, J_dag complex N(0, 1)/sqrt(P) made on the
+device and Bloch k_z Re U(0, 2 k0), Im U(0, 0.1 k0)), so requests share
+layers as a sweep over heights and layer orders does; the server computes
+each layer's interface once and serves the rest from its device cache.
 """
 from __future__ import annotations
 
@@ -54,21 +64,75 @@ def make_requests(n, seed=0, period=500.0):
     return reqs
 
 
-def run_rate(rate, seconds, batching, max_batch, seed):
+def make_array_pool(n_points, seed=0, period=500.0, device='cuda'):
+    """Spectral points with two synthetic array layers each."""
+    import torch
+    from emustack_b200.array_serving import ArrayLayer
+    rng = np.random.default_rng(seed)
+    tab = order_table(period)
+    g = torch.Generator(device=device).manual_seed(seed)
+    pool = []
+    for i in range(n_points):
+        P = float(np.exp(rng.uniform(np.log(50), np.log(900))))
+        mo = int(np.argmin(np.abs(tab - P / 2)))
+        P = 2 * int(tab[mo])
+        M = P + 20
+        wl = float(rng.uniform(350, 1100))
+        th, ph = np.radians(rng.uniform(0, 60)), np.radians(rng.uniform(0, 90))
+        k = 2 * np.pi / wl
+        kp = np.array([k * np.sin(th) * np.cos(ph), k * np.sin(th) * np.sin(ph)])
+        k0 = 2 * np.pi / (wl / period)
+        cr = lambda *sh: torch.complex(torch.randn(sh, dtype=torch.float64, device=device, generator=g),
+                                       torch.randn(sh, dtype=torch.float64, device=device, generator=g))
+        lays = []
+        for _ in range(2):
+            kz = rng.uniform(0, 2, M) * k0 + 1j * rng.uniform(0, 0.1, M) * k0
+            lays.append(ArrayLayer(kz, J=cr(P, M) / np.sqrt(P), J_dag=cr(M, P) / np.sqrt(P)))
+        pool.append((mo, wl, kp, lays))
+    return pool
+
+
+def make_array_requests(n, pool, seed=0, period=500.0):
+    from emustack_b200.array_serving import ArrayRequest
+    rng = np.random.default_rng(seed)
+    pols = ('TE', 'TM', 'un', 'R Circ')
+    reqs = []
+    for i in range(n):
+        mo, wl, kp, lays = pool[int(rng.integers(len(pool)))]
+        K = int(rng.integers(2, 13))
+        mid = [lays[int(rng.integers(2))] if rng.random() < 0.5
+               else complex(rng.uniform(1.3, 4.0), rng.uniform(0, 0.5)) for _ in range(K)]
+        reqs.append(ArrayRequest([1.46 + 0j] + mid + [1.0 + 0j], rng.uniform(20, 300, K), wl, kp, period, mo,
+                                 pol=pols[i % 4]))
+    return reqs
+
+
+def mixed_requests(n, seed, array_frac, pool):
+    """n requests, a fraction array_frac of them array stacks, in random order."""
+    na = int(round(n * array_frac)) if pool else 0
+    reqs = make_requests(n - na, seed) + (make_array_requests(na, pool, seed + 7) if na else [])
+    order = np.random.default_rng(seed + 3).permutation(len(reqs))
+    return [reqs[i] for i in order]
+
+
+def run_rate(rate, seconds, batching, max_batch, seed, array_frac=0.0, pool=None, n_streams=2):
     import torch
     from emustack_b200.serving import GsmServer
     n = max(int(rate * seconds), 200)
-    reqs = make_requests(n, seed)
+    reqs = mixed_requests(n, seed, array_frac, pool)
     rng = np.random.default_rng(seed + 1)
     gaps = rng.exponential(1.0 / rate, n)
-    srv = GsmServer(max_batch=max_batch, batching=batching).start()
+    srv = GsmServer(max_batch=max_batch, batching=batching, n_streams=n_streams).start()
     # warm the server: bursts as large as the batches this rate will form, so
     # that staging and device buffers have grown before the timed run
-    burst = make_requests(max(64, min(max_batch, int(rate * 0.2))), seed + 2)
+    burst = mixed_requests(max(64, min(max_batch, int(rate * 0.2))), seed + 2, array_frac, pool)
     for _ in range(2):
         for f in [srv.submit(r) for r in burst]:
-            f.result(timeout=120)
+            f.result(timeout=300)
     srv.latencies.clear()
+    srv.array_latencies.clear()
+    c = srv.cache
+    c.hits = c.misses = c.evictions = 0
     srv.batch_sizes.clear()
     srv.n_batches = 0
     srv.t_first = srv.t_last = None
@@ -109,14 +173,22 @@ def run_rate(rate, seconds, batching, max_batch, seed):
     srv.stop()
     st = srv.stats()
     torch.cuda.synchronize()
-    return {
+    out = {
         'offered_per_s': rate, 'requests': n, 'batching': batching, 'max_batch': max_batch,
+        'streams': n_streams,
         'achieved_per_s': st['throughput_per_s'], 'p50_ms': st['p50_ms'], 'p99_ms': st['p99_ms'],
         'batches': st['batches'], 'mean_batch': st['mean_batch'],
         'host_ms_per_batch': {k[:-2]: 1e3 * v / max(st['batches'], 1) for k, v in srv.prof.items()},
         'mean_P': float(np.mean([2 * r.npw for r in reqs])),
-        'mean_layers': float(np.mean([len(r.n) for r in reqs])),
+        'mean_layers': float(np.mean([len(r.layers) if hasattr(r, 'air_key') else len(r.n) for r in reqs])),
     }
+    if array_frac:
+        c = st['smatrix_cache']
+        out.update(array_frac=array_frac, array_requests=st['array_requests'],
+                   array_p50_ms=st['array_p50_ms'], array_p99_ms=st['array_p99_ms'],
+                   cache_hits=c['hits'], cache_misses=c['misses'], cache_entries=c['entries'],
+                   cache_gb=c['bytes'] / 1e9)
+    return out
 
 
 def main():
@@ -126,9 +198,14 @@ def main():
     ap.add_argument('--batching', default='mixed')
     ap.add_argument('--max-batch', type=int, default=32768)
     ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--array-frac', type=float, default=0.0, help='fraction of array-stack requests')
+    ap.add_argument('--array-pool', type=int, default=32, help='spectral points of the array layers')
+    ap.add_argument('--streams', type=int, default=2, help='batches in flight at once')
     args = ap.parse_args()
+    pool = make_array_pool(args.array_pool, args.seed + 11) if args.array_frac > 0 else None
     for r in [float(x) for x in args.rates.split(',')]:
-        print(json.dumps(run_rate(r, args.seconds, args.batching, args.max_batch, args.seed)), flush=True)
+        print(json.dumps(run_rate(r, args.seconds, args.batching, args.max_batch, args.seed,
+                                  args.array_frac, pool, args.streams)), flush=True)
 
 
 if __name__ == '__main__':

@@ -172,6 +172,7 @@ class GsmServer(object):
         self.inflight = []
         self.inflight_bytes = 0
         self.latencies = []
+        self.array_latencies = []         # the array requests' share of latencies
         self.n_batches = 0
         self.batch_sizes = []
         self._stop = threading.Event()
@@ -216,13 +217,18 @@ class GsmServer(object):
         lat = np.array(self.latencies) * 1e3
         n = len(lat)
         span = (self.t_last - self.t_first) if n and self.t_last else float('nan')
+        alat = np.array(self.array_latencies) * 1e3
+        pct = lambda a, q: float(np.percentile(a, q)) if len(a) else float('nan')
         return {
             'requests': n,
             'batches': self.n_batches,
             'mean_batch': float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
             'throughput_per_s': n / span if n and span > 0 else float('nan'),
-            'p50_ms': float(np.percentile(lat, 50)) if n else float('nan'),
-            'p99_ms': float(np.percentile(lat, 99)) if n else float('nan'),
+            'p50_ms': pct(lat, 50),
+            'p99_ms': pct(lat, 99),
+            'array_requests': len(alat),
+            'array_p50_ms': pct(alat, 50),
+            'array_p99_ms': pct(alat, 99),
             'smatrix_cache': self.cache.stats(),
         }
 
@@ -331,8 +337,10 @@ class GsmServer(object):
         return launched
 
     def _record(self, reqs, t):
-        self.latencies.extend([t - (r.t_arrival if r.t_arrival is not None else r.t_submit)
-                               for r in reqs])
+        lat = [t - (r.t_arrival if r.t_arrival is not None else r.t_submit) for r in reqs]
+        self.latencies.extend(lat)
+        if reqs and isinstance(reqs[0], ArrayRequest):
+            self.array_latencies.extend(lat)
 
     def _run_mixed(self, slot, reqs, nbytes):
         if slot['var'] is None:

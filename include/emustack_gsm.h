@@ -285,6 +285,63 @@ long long emu_stack_dense_list_stride(const EmuStackDense *p);
 int emu_stack_dense_batch(const EmuStackDense *p, void *d_workspace, size_t workspace_bytes,
                           void *stream);
 
+/* ------------------- a9, a10: uneven batch of dense stacks, one launch
+ * Stacks of different shapes -- plane-wave count P, layer count, Bloch-mode
+ * counts, polarisation -- each the whole Stack.calc_scat of one spectral
+ * point (backend/stack.py:162-426) with a film substrate and a film
+ * superstrate, solved in ONE launch: a persistent kernel whose CTAs take
+ * stacks in the given order (costliest first) from an atomic counter and
+ * run the cascade and the flux pass of emu_stack_dense_batch's one-CTA path
+ * (same arithmetic, same results).  Layer matrices are read where they lie
+ * (any device pointers, e.g. a cache of layer interfaces); descriptors live
+ * in device memory and are bounds-checked against the packed arrays: a bad
+ * one marks its stack EMU_PT_BAD_POINT in d_flags and is skipped.
+ * No counterpart call in the reference (it solves one Stack per call). */
+typedef struct {
+  int M, dense;                /* as EmuLayer (film: dense = 0, M = P)      */
+  const emu_c128 *d_R12, *d_T12, *d_R21, *d_T21; /* this stack's matrices */
+  const emu_c128 *d_kz;        /* [M] (finite layers)                       */
+  double height_norm;          /* height / period (finite layers)           */
+} EmuVarLayer;
+
+typedef struct {
+  int n_layers, P, pol, spec;  /* pol EMU_POL_*; spec: superstrate specular */
+  int num_prop[3];             /* propagating orders: air, superstrate, substrate */
+  int _pad;
+  long long layer_off;         /* first of n_layers entries in d_layers     */
+  long long inc_off;           /* [P] in d_incoming (EMU_POL_INCOMING)      */
+  long long rnet_off;          /* [P][P] in d_R_net                         */
+  long long tnet_off;          /* [P][P] in d_T_net                         */
+  long long list_off;          /* [L-1] in d_a_list / d_t_list              */
+  long long flux_off;          /* [L+1][2] in d_fluxes                      */
+} EmuStackPoint;
+
+typedef struct {
+  int n_stacks;
+  const EmuStackPoint *d_points;   /* [n_stacks]                            */
+  const int32_t *d_order;          /* [n_stacks] processing order, or NULL  */
+  const EmuVarLayer *d_layers;     /* packed layer descriptors              */
+  long long n_layer_desc;          /* entries in d_layers                   */
+  const emu_c128 *d_incoming;  long long incoming_len;
+  emu_c128 *d_R_net;           long long rnet_len;
+  emu_c128 *d_T_net;           long long tnet_len;
+  double *d_a_list, *d_t_list; long long list_len;
+  double *d_fluxes;            long long flux_len;   /* or NULL              */
+  double *d_r_list;            /* [n_stacks]                                */
+  uint32_t *d_flags;           /* [n_stacks] EMU_PT_*                       */
+  int32_t *d_info;             /* [n_stacks] 0 or the first singular solve  */
+  int max_P, max_D, max_L;     /* bounds of every stack: P, max(P, M), L    */
+  int n_slots;                 /* CTAs (each with its own workspace); 0: as
+                                  many as fit on the GPU at once             */
+} EmuStackVarBatch;
+
+/* Workspace for the batch: n_slots x the workspace of the largest stack.
+ * emu_stack_var_slots gives the CTA count that n_slots = 0 selects. */
+int emu_stack_var_slots(const EmuStackVarBatch *p);
+size_t emu_stack_var_workspace_size(const EmuStackVarBatch *p);
+int emu_stack_var_batch(const EmuStackVarBatch *p, void *d_workspace, size_t workspace_bytes,
+                        void *stream);
+
 /* ------------------------------------- a11, a12: overlap integrals
  * J (2 Npw x nval) and J_dag (nval x 2 Npw) of P2 Bloch-mode fields with the
  * TE ("E") and TM ("K") plane waves, by the 16-point triangle quadrature

@@ -67,7 +67,8 @@ def test_grating_orders_1d_and_errors():
 
 
 STRUCTS = ('EmuFilmStackBatch', 'EmuAnalloModes', 'EmuLayer', 'EmuStackDense', 'EmuOverlap',
-           'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch')
+           'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch', 'EmuVarLayer', 'EmuStackPoint',
+           'EmuStackVarBatch')
 
 
 def test_struct_layouts_match_header(tmp_path):
