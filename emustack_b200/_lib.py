@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libemustack_gsm.so')
 
 EMU_OK = 0
+EMU_E_SHAPE = 2
 STATUS_NAMES = {
     0: 'EMU_OK', 1: 'EMU_E_ARG', 2: 'EMU_E_SHAPE', 3: 'EMU_E_SINGULAR',
     4: 'EMU_E_NONFINITE', 5: 'EMU_E_WORKSPACE', 6: 'EMU_E_TIMEOUT',

@@ -179,6 +179,10 @@ class ArrayRequest(object):
         self.t_arrival = t_arrival
         self._nbytes = None
 
+    def max_dim(self):
+        """D = max(P, M of every array layer): the size of the cascade's matrices."""
+        return max([2 * self.npw] + [ly.M for ly in self.layers if isinstance(ly, ArrayLayer)])
+
     def wl_norm(self):
         """wl / period, nudged off exact multiples (backend/mode_calcs.py:45-49)."""
         w = self.wl_nm / self.period
@@ -321,39 +325,40 @@ class ArrayBatcher(object):
         check(lib().emu_anallo_modes(C.byref(d), stream_ptr()), 'emu_anallo_modes')
         return kz, sort_out, spec, nprop
 
-    def _fill(self, reqs, pos, kz_air, n_air, wln, stream):
-        """Cache entries of the array layers at every position; computes and
-        inserts the missing ones.  Returns {pos: [entry per request]} and the
-        distinct entries used."""
+    def _fill(self, reqs, pos_of, air_of, stream):
+        """Cache entries of the array layers of every request; computes and
+        inserts the missing ones.  pos_of(b) lists request b's array
+        positions; air_of(b) = (kz_air, wln, row) locates its air reference
+        in the device tensors of its order set.  Returns {(b, pos): cache
+        key} and the distinct entries used {key: entry}."""
         cache = self.cache
-        per_pos = {}
+        key_at = {}
         used = {}
-        missing = collections.OrderedDict()   # cache key -> (layer, first request index)
-        for j in pos:
-            es = []
-            for b, r in enumerate(reqs):
+        missing = collections.OrderedDict()   # cache key -> (layer, request index)
+        for b, r in enumerate(reqs):
+            for j in pos_of(b):
                 ly = r.layers[j]
                 key = (ly.key, r.air_key)
-                e = used.get(key)
-                if e is None and key not in missing:
+                if key not in used and key not in missing:
                     e = cache.get(key)
                     if e is None:
                         missing[key] = (ly, b)
                     else:
                         used[key] = e
-                es.append(key)
-            per_pos[j] = es
-        # compute the misses, batched by (source, M)
+                key_at[(b, j)] = key
+        # compute the misses, batched by (source, P, M, air tensors)
         groups = collections.defaultdict(list)
         for key, (ly, b) in missing.items():
-            groups[(ly.J is not None, ly.M)].append((key, ly, b))
-        for (from_J, M), items in groups.items():
+            kz_air, wln, _ = air_of(b)
+            groups[(ly.J is not None, ly.P, ly.M, id(kz_air))].append((key, ly, b))
+        for (from_J, _, M, _), items in groups.items():
             nm = len(items)
             kz = self._upload([ly.k_z for _, ly, _ in items])
             if from_J:
                 J = self._upload([ly.J for _, ly, _ in items])
                 Jd = self._upload([ly.J_dag for _, ly, _ in items])
-                idx = torch.tensor([b for _, _, b in items], dtype=torch.long, device=self.device)
+                kz_air, wln, _ = air_of(items[0][2])
+                idx = torch.tensor([air_of(b)[2] for _, _, b in items], dtype=torch.long, device=self.device)
                 R12, T12, R21, T21, info = interface_dense(
                     kz_air.index_select(0, idx).contiguous(), torch.ones(nm, dtype=c128, device=self.device),
                     wln.index_select(0, idx).contiguous(), J, Jd)
@@ -375,7 +380,9 @@ class ArrayBatcher(object):
             e.users += 1
         for key in missing:
             cache.put(key, used[key])
-        return per_pos, used
+        for e in used.values():
+            stream.wait_event(e.ready)
+        return key_at, used
 
     def _upload(self, ts):
         """Stack host (pinned) or device tensors of one shape on the device,
@@ -435,11 +442,9 @@ class ArrayBatcher(object):
                     np_sub = npj
                 if j == L - 1:
                     np_top = npj
-            per_pos, used = self._fill(reqs, arr_pos, kz_air, n_air, wln, stream)
-            for e in used.values():
-                stream.wait_event(e.ready)
+            key_at, used = self._fill(reqs, lambda b: arr_pos, lambda b: (kz_air, wln, b), stream)
             for j in arr_pos:
-                keys = per_pos[j]
+                keys = [key_at[(b, j)] for b in range(B)]
                 es = [used[k] for k in keys]
                 if all(k == keys[0] for k in keys):
                     e = es[0]
@@ -467,6 +472,15 @@ class ArrayBatcher(object):
             ev = torch.cuda.Event()
             ev.record(stream)
 
+        def result(h, b):
+            return {'R_net': h['R_net'][b], 'T_net': h['T_net'][b], 'a_list': h['a_list'][b],
+                    't_list': h['t_list'][b], 'r_list': float(h['r_list'][b]), 'flags': int(h['flags'][b])}
+
+        return ev, self._finisher(reqs, host, ukeys, used, key_at, result)
+
+    def _finisher(self, reqs, host, ukeys, used, key_at, result):
+        """finish(): releases the batch's cache entries (dropping singular
+        ones) and returns each request's result or exception."""
         cache = self.cache
 
         def finish():
@@ -482,12 +496,146 @@ class ArrayBatcher(object):
             cache.evict()
             res = []
             for b, r in enumerate(reqs):
-                if int(h['info'][b]) != 0 or any(per_pos[j][b] in bad for j in arr_pos):
+                if int(h['info'][b]) != 0 or any(k in bad for (bb, _), k in key_at.items() if bb == b):
                     res.append(np.linalg.LinAlgError('Singular matrix'))
-                    continue
-                res.append({'R_net': h['R_net'][b], 'T_net': h['T_net'][b], 'a_list': h['a_list'][b],
-                            't_list': h['t_list'][b], 'r_list': float(h['r_list'][b]),
-                            'flags': int(h['flags'][b])})
+                elif int(h['flags'][b]) & _lib.PT_BAD_POINT:
+                    res.append(_lib.EmuError(_lib.EMU_E_SHAPE, 'array request'))
+                else:
+                    res.append(result(h, b))
             return res
+
+        return finish
+
+    def launch_uneven(self, reqs, stream, slot_key, ws_budget_bytes):
+        """Queue array requests of ANY shapes as one uneven batch on
+        ``stream``: film modes and interfaces per order set, cached array
+        interfaces, then one emu_stack_var_batch launch for every cascade.
+        Returns (event, finish) as ``launch``."""
+        from .dense import StackVarSolver, VarStack
+        dev = self.device
+        sets = collections.OrderedDict()
+        for b, r in enumerate(reqs):
+            sets.setdefault((r.max_order, r.period, r.period_y, r.world_1d), []).append(b)
+        n = len(reqs)
+        air = [None] * n                 # (kz_air, wln, row) per request
+        film = {}                        # (b, j) -> (R, T, -R, kz2, row)
+        np_parts, spec_parts, order = [], [], []
+        keep = []
+        with torch.cuda.stream(stream):
+            for key, bs in sets.items():
+                r0 = reqs[bs[0]]
+                B = len(bs)
+                inst = [(b, j) for b in bs for j, ly in enumerate(reqs[b].layers)
+                        if not isinstance(ly, ArrayLayer)]
+                rows = {b: i for i, b in enumerate(bs)}
+                h = _pinned((4 * B + 4 * len(inst),), torch.float64)
+                hv = h.numpy()
+                hv[0:B] = [reqs[b].wl_nm for b in bs]
+                hv[B:3 * B] = np.stack([reqs[b].k_pll for b in bs]).reshape(-1)
+                hv[3 * B:4 * B] = [reqs[b].wl_norm() for b in bs]
+                o = 4 * B
+                hv[o:o + 2 * len(inst)].view(np.complex128)[:] = [reqs[b].layers[j] for b, j in inst]
+                hv[o + 2 * len(inst):o + 4 * len(inst)] = [rows[b] for b, _ in inst] + [0] * len(inst)
+                d = h.to(dev, non_blocking=True)
+                keep.append(h)
+                wl, kp, wln = d[0:B], d[B:3 * B].view(B, 2), d[3 * B:4 * B]
+                nf = d[o:o + 2 * len(inst)].view(c128)
+                irow = d[o + 2 * len(inst):o + 3 * len(inst)].to(torch.long)
+                px, py = self._order_tensors(r0)
+                n_air = torch.ones(B, dtype=c128, device=dev)
+                kz_air, sort_air, spec, np_air = self._modes(r0, px, py, wl, kp, n_air, None)
+                kz_i = kz_air.index_select(0, irow)
+                kz_f, _, _, np_f = self._modes(r0, px, py, wl.index_select(0, irow),
+                                               kp.index_select(0, irow).contiguous(), nf,
+                                               sort_air.index_select(0, irow).contiguous())
+                R, T = film_interface(kz_i, torch.ones(len(inst), dtype=c128, device=dev), kz_f, nf,
+                                      wln.index_select(0, irow))
+                mR = torch.neg(R)
+                kz2 = torch.cat([kz_f, kz_f], dim=1)
+                keep += [R, T, mR, kz2]
+                top = {}
+                sub = {}
+                for i, (b, j) in enumerate(inst):
+                    film[(b, j)] = i
+                    if j == 0:
+                        sub[b] = i
+                    if j == len(reqs[b].layers) - 1:
+                        top[b] = i
+                    air[b] = (kz_air, wln, rows[b])
+                for b in bs:
+                    air[b] = (kz_air, wln, rows[b])
+                film_rows = (R, T, mR, kz2)
+                for b in bs:
+                    film[('t', b)] = film_rows
+                ti = torch.tensor([top[b] for b in bs], dtype=torch.long, device=dev)
+                si = torch.tensor([sub[b] for b in bs], dtype=torch.long, device=dev)
+                np_parts.append(torch.stack([np_air, np_f.index_select(0, ti), np_f.index_select(0, si)], 1))
+                spec_parts.append(spec)
+                order += bs
+            key_at, used = self._fill(
+                reqs, lambda b: [j for j, ly in enumerate(reqs[b].layers) if isinstance(ly, ArrayLayer)],
+                lambda b: air[b], stream)
+            stacks = []
+            inc_keep = []
+            for b in order:
+                r = reqs[b]
+                P, L = 2 * r.npw, len(r.layers)
+                R, T, mR, kz2 = film[('t', b)]
+                lays = []
+                for j, ly in enumerate(r.layers):
+                    fin = 0 < j < L - 1
+                    hn = float(r.heights[j - 1]) / r.period if fin else 0.0
+                    if isinstance(ly, ArrayLayer):
+                        e = used[key_at[(b, j)]]
+                        lays.append((e.R12[0], e.T12[0], e.R21[0], e.T21[0], True, e.kz[0], hn))
+                    else:
+                        i = film[(b, j)]
+                        lays.append((R[i], T[i], mR[i], T[i], False, kz2[i] if fin else None, hn))
+                inc = None
+                if r.incoming is not None:
+                    hi = _pinned((P,), c128)
+                    hi.numpy()[:] = r.incoming
+                    inc = hi.to(dev, non_blocking=True)
+                    inc_keep.append(hi)
+                stacks.append(VarStack(lays, P, pol=r.pol if inc is None else 'TE', incoming=inc))
+            solver = self._solvers.get(('uneven', slot_key))   # one workspace per stream
+            if solver is None:
+                solver = self._solvers[('uneven', slot_key)] = StackVarSolver(dev)
+            out = solver.solve(stacks, spec=torch.cat(spec_parts), num_prop=torch.cat(np_parts),
+                               ws_budget_bytes=ws_budget_bytes)
+            ukeys = list(used)
+            host = {}
+            for k in ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags', 'info'):
+                t = _pinned(tuple(out[k].shape), out[k].dtype)
+                t.copy_(out[k], non_blocking=True)
+                host[k] = t
+            if ukeys:
+                infos = torch.cat([used[k].info for k in ukeys])
+                host['layer_info'] = _pinned(tuple(infos.shape), infos.dtype)
+                host['layer_info'].copy_(infos, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        # results come back in `order`; map them to the requests' positions
+        pos = {b: i for i, b in enumerate(order)}
+        ro, lo = out['rnet_off'], out['list_off']
+        ordered = [reqs[b] for b in order]
+        key_at_o = {(pos[b], j): k for (b, j), k in key_at.items()}
+
+        def result(h, i):
+            r = ordered[i]
+            P, L = 2 * r.npw, len(r.layers)
+            a, c = int(ro[i]), int(lo[i])
+            return {'R_net': h['R_net'][a:a + P * P].reshape(P, P), 'T_net': h['T_net'][a:a + P * P].reshape(P, P),
+                    'a_list': h['a_list'][c:c + L - 1], 't_list': h['t_list'][c:c + L - 1],
+                    'r_list': float(h['r_list'][i]), 'flags': int(h['flags'][i])}
+
+        fin_o = self._finisher(ordered, host, ukeys, used, key_at_o, result)
+        keep.append(out)
+
+        def finish():
+            res_o = fin_o()
+            keep.clear()
+            inc_keep.clear()
+            return [res_o[pos[b]] for b in range(n)]
 
         return ev, finish

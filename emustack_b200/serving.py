@@ -18,9 +18,13 @@ Film requests have two batching modes:
 * ``'grouped'``: requests are grouped by shape signature and each batch is
   one launch of the uniform film kernel (``emu_film_stack_batch``).
 
-Array requests are always grouped by shape signature (order set,
-polarisation, layer kinds and Bloch-mode counts): a batch is the chain of
-``ArrayBatcher.launch`` (film modes, missing interfaces, cascade + fluxes).
+Array requests whose matrices are small (D = max(P, M) <= uneven_max_dim)
+share one uneven batch whatever their shapes: film modes and missing
+interfaces per order set, then every cascade in ONE launch of the uneven
+dense kernel (``ArrayBatcher.launch_uneven``, one CTA per stack).  Larger
+ones are grouped by shape signature (order set, polarisation, layer kinds
+and Bloch-mode counts) and each group's cascade spreads over the GPU
+(``ArrayBatcher.launch``).
 
 Each batch is an async host-to-device copy of its packed inputs, one kernel,
 and an async device-to-host copy of its packed outputs on the slot's
@@ -142,23 +146,31 @@ class GsmServer(object):
     """Continuous batching of GSM solve requests on one GPU.
 
     hbm_budget_bytes bounds the device memory of the server: the layer
-    interface cache (smatrix_cache_bytes of it) plus the batches in flight;
+    interface cache (smatrix_cache_bytes of it; default an eighth, at most
+    16 GiB) plus the batches in flight; array requests with D = max(P, M) <=
+    uneven_max_dim share one-launch uneven batches whose workspace is at most
+    uneven_ws_bytes;
     n_streams batches may run at once; max_batch caps one launch;
     batching of film requests is 'mixed' (any shapes in one launch) or
     'grouped'.
     """
 
     def __init__(self, device=None, hbm_budget_bytes=150 << 30, max_batch=32768, n_streams=2,
-                 poll_s=2e-4, batching='mixed', smatrix_cache_bytes=16 << 30):
+                 poll_s=2e-4, batching='mixed', smatrix_cache_bytes=None, uneven_max_dim=256,
+                 uneven_ws_bytes=8 << 30):
         if batching not in ('mixed', 'grouped'):
             raise ValueError("batching must be 'mixed' or 'grouped'")
         self.device = (torch.device('cuda', torch.cuda.current_device()) if device is None
                        else torch.device(device))
         self.batching = batching
+        if smatrix_cache_bytes is None:
+            smatrix_cache_bytes = min(16 << 30, int(hbm_budget_bytes) // 8)
         if smatrix_cache_bytes >= hbm_budget_bytes:
             raise ValueError('the layer interface cache must leave room for batches in the budget')
         self.cache = SMatrixCache(smatrix_cache_bytes)
         self._arrays = None
+        self.uneven_max_dim = int(uneven_max_dim)
+        self.uneven_ws_bytes = int(uneven_ws_bytes)
         self.budget = int(hbm_budget_bytes) - int(smatrix_cache_bytes)
         self.max_batch = int(max_batch)
         self.poll_s = poll_s
@@ -234,9 +246,9 @@ class GsmServer(object):
 
     # ---------------------------------------------------------------- loop
     def _key(self, r):
-        if self.batching == 'mixed' and not isinstance(r, ArrayRequest):
-            return 'all'
-        return r.signature
+        if isinstance(r, ArrayRequest):
+            return 'array-uneven' if r.max_dim() <= self.uneven_max_dim else r.signature
+        return 'all' if self.batching == 'mixed' else r.signature
 
     def _take(self, block):
         if block and not self.q:
@@ -327,7 +339,9 @@ class GsmServer(object):
                 self.pending.move_to_end(key)
             if not reqs:
                 continue
-            if isinstance(reqs[0], ArrayRequest):
+            if key == 'array-uneven':
+                self._run_arrays(slot, reqs, nbytes, uneven=True)
+            elif isinstance(reqs[0], ArrayRequest):
                 self._run_arrays(slot, reqs, nbytes)
             elif self.batching == 'mixed':
                 self._run_mixed(slot, reqs, nbytes)
@@ -414,11 +428,14 @@ class GsmServer(object):
 
         self._submit(_Batch(reqs, slot, ev, nbytes, finish, (dwl, dkp, dn, dh)))
 
-    def _run_arrays(self, slot, reqs, nbytes):
+    def _run_arrays(self, slot, reqs, nbytes, uneven=False):
         if self._arrays is None:
             self._arrays = ArrayBatcher(self.device, self.cache)
         t1 = time.perf_counter()
-        ev, fin = self._arrays.launch(reqs, slot['stream'], id(slot))
+        if uneven:
+            ev, fin = self._arrays.launch_uneven(reqs, slot['stream'], id(slot), self.uneven_ws_bytes)
+        else:
+            ev, fin = self._arrays.launch(reqs, slot['stream'], id(slot))
         self.prof['launch_s'] += time.perf_counter() - t1
 
         def finish(b, t):
