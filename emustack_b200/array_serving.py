@@ -37,6 +37,7 @@ from __future__ import annotations
 import collections
 import ctypes as C
 import itertools
+import threading
 
 import numpy as np
 import torch
@@ -296,6 +297,9 @@ class ArrayBatcher(object):
     def __init__(self, device, cache):
         self.device = device
         self.cache = cache
+        # the cache and the entries' use counts are shared by batches launched
+        # from several threads
+        self.lock = threading.Lock()
         self._orders = {}
         self._solvers = {}
 
@@ -331,6 +335,10 @@ class ArrayBatcher(object):
         positions; air_of(b) = (kz_air, wln, row) locates its air reference
         in the device tensors of its order set.  Returns {(b, pos): cache
         key} and the distinct entries used {key: entry}."""
+        with self.lock:
+            return self._fill_locked(reqs, pos_of, air_of, stream)
+
+    def _fill_locked(self, reqs, pos_of, air_of, stream):
         cache = self.cache
         key_at = {}
         used = {}
@@ -483,17 +491,20 @@ class ArrayBatcher(object):
         ones) and returns each request's result or exception."""
         cache = self.cache
 
+        lock = self.lock
+
         def finish():
             h = {k: v.numpy() for k, v in host.items()}
             bad = set()
-            for i, k in enumerate(ukeys):
-                e = used[k]
-                e.users -= 1
-                if int(h['layer_info'][i]) != 0:
-                    e.bad = True
-                    bad.add(k)
-                    cache.drop(k)
-            cache.evict()
+            with lock:
+                for i, k in enumerate(ukeys):
+                    e = used[k]
+                    e.users -= 1
+                    if int(h['layer_info'][i]) != 0:
+                        e.bad = True
+                        bad.add(k)
+                        cache.drop(k)
+                cache.evict()
             res = []
             for b, r in enumerate(reqs):
                 if int(h['info'][b]) != 0 or any(k in bad for (bb, _), k in key_at.items() if bb == b):

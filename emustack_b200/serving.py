@@ -169,6 +169,8 @@ class GsmServer(object):
             raise ValueError('the layer interface cache must leave room for batches in the budget')
         self.cache = SMatrixCache(smatrix_cache_bytes)
         self._arrays = None
+        self._launcher = None
+        self.max_array_slots = max(1, n_streams - 1)
         self.uneven_max_dim = int(uneven_max_dim)
         self.uneven_ws_bytes = int(uneven_ws_bytes)
         self.budget = int(hbm_budget_bytes) - int(smatrix_cache_bytes)
@@ -218,6 +220,9 @@ class GsmServer(object):
         self._wake.set()
         if self._thread is not None:
             self._thread.join()
+        if self._launcher is not None:
+            self._launcher.shutdown(wait=True)
+            self._launcher = None
 
     def __enter__(self):
         return self.start()
@@ -307,6 +312,20 @@ class GsmServer(object):
         done_any = False
         keep = []
         for b in self.inflight:
+            if b.event is None:
+                # a shape group whose launches a worker thread is still issuing
+                if not b.keep.done():
+                    keep.append(b)
+                    continue
+                try:
+                    b.event, fin = b.keep.result()
+                except Exception as e:  # the launch failed: fail its requests only
+                    self._publish(b.reqs, exc=e)
+                    self.inflight_bytes -= b.nbytes
+                    b.slot['busy'] = False
+                    done_any = True
+                    continue
+                b.finish = self._array_finish(fin)
             if b.event.query():
                 t = time.perf_counter()
                 b.finish(b, t)
@@ -319,12 +338,25 @@ class GsmServer(object):
         self.inflight = keep
         return done_any
 
+    def _is_array_key(self, key):
+        return key == 'array-uneven' or (isinstance(key, tuple) and key[0] == 'array')
+
     def _launch(self):
         launched = False
         for slot in self.slots:
             if slot['busy'] or not self.pending:
                 continue
-            key = next(iter(self.pending))
+            # array batches may hold at most max_array_slots streams, so film
+            # requests always find a stream of their own
+            arrays_busy = sum(1 for sl in self.slots if sl['busy'] and sl.get('array'))
+            key = None
+            for k in self.pending:
+                if not self._is_array_key(k) or arrays_busy < self.max_array_slots:
+                    key = k
+                    break
+            if key is None:
+                continue
+            slot['array'] = self._is_array_key(key)
             dq = self.pending[key]
             reqs, nbytes = [], 0
             while dq and len(reqs) < self.max_batch:
@@ -434,10 +466,28 @@ class GsmServer(object):
         t1 = time.perf_counter()
         if uneven:
             ev, fin = self._arrays.launch_uneven(reqs, slot['stream'], id(slot), self.uneven_ws_bytes)
-        else:
-            ev, fin = self._arrays.launch(reqs, slot['stream'], id(slot))
-        self.prof['launch_s'] += time.perf_counter() - t1
+            self.prof['launch_s'] += time.perf_counter() - t1
+            self._submit(_Batch(reqs, slot, ev, nbytes, self._array_finish(fin), None))
+            return
+        # a shape group spreads each cascade step over the GPU: thousands of
+        # launches for large matrices.  A worker thread per stream issues them
+        # (the library releases the interpreter lock while it launches), so
+        # the scheduler keeps admitting and retiring other batches meanwhile.
+        if self._launcher is None:
+            import concurrent.futures as cf
+            self._launcher = cf.ThreadPoolExecutor(max_workers=len(self.slots),
+                                                   thread_name_prefix='gsm-array-launch')
+        dev, stream = self.device, slot['stream']
 
+        def work():
+            torch.cuda.set_device(dev)
+            return self._arrays.launch(reqs, stream, id(slot))
+
+        fut = self._launcher.submit(work)
+        self.prof['launch_s'] += time.perf_counter() - t1
+        self._submit(_Batch(reqs, slot, None, nbytes, None, fut))
+
+    def _array_finish(self, fin):
         def finish(b, t):
             t2 = time.perf_counter()
             vals = fin()
@@ -449,7 +499,7 @@ class GsmServer(object):
             self._record(b.reqs, t)
             self.prof['finish_s'] += time.perf_counter() - t2
 
-        self._submit(_Batch(reqs, slot, ev, nbytes, finish, None))
+        return finish
 
     def _submit(self, batch):
         batch.slot['busy'] = True
