@@ -16,29 +16,48 @@ constexpr int kDLThreads = 256;
 constexpr int kTM = 64, kTN = 64, kTK = 8;   // GEMM tile
 constexpr int kNB = 32;                      // LU / TRSM block
 
+// Shared tiles of cta_gemm_tile.  A: 64 rows x 8 complex columns stored as
+// (re, im) pairs; B: 8 complex rows x 64 complex columns stored as the real
+// 16 x 128 matrix [[Re, Im], [-Im, Re]] per element, so that the complex
+// product is one real product A_r (m x 2k) * B_r (2k x 2n) whose result,
+// read in (re, im) pairs, is the complex C.  Row paddings (+4 doubles) make
+// the tensor-core fragment reads free of bank conflicts.
+constexpr int kAS = 2 * kTK + 4, kBS = 2 * kTN + 4;
 struct GemmSmem {
-  cd As[kTK][kTM];
-  cd Bs[kTK][kTN];
+  double As[kTM][kAS];
+  double Bs[2 * kTK][kBS];
 };
 
 __device__ __forceinline__ cd ldc(const cd *p) { return *p; }
 
+// D = A B + D on the FP64 tensor cores: one 8 x 8 x 4 product per warp
+// (PTX mma.sync m8n8k4 f64; lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4) + {0,1}]).
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // One 64x64 tile of C = alpha * A(m x k) * B(k x n) + beta * C, tile origin
 // (r0, c0).  If dA / dB are non-null the rows of A / the rows of B are
-// first multiplied by dA[i] / dB[kk] (diagonal factors).  All threads of the
-// CTA must call it.  `conjA`: use conj(A).
+// first multiplied by dA[i] / dB[kk] (diagonal factors).  All kDLThreads
+// threads of the CTA must call it.  The product runs on the FP64 tensor
+// cores: 8 warps in a 2 x 4 grid, each owning a 32 x 32 block of the real
+// 64 x 128 result (4 x 4 fragments of 8 x 8).
 static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A, int lda, const cd *B,
                               int ldb, cd beta, cd *C, int ldc_, int r0, int c0, GemmSmem &sm,
                               const cd *dA_col = nullptr, const cd *dB_row = nullptr) {
-  const int tid = threadIdx.x;
-  const int ty = tid / 16, tx = tid % 16;
-  cd acc[4][4];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp >> 2, wn = warp & 3;
+  double acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = cd{0.0, 0.0};
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   for (int k0 = 0; k0 < k; k0 += kTK) {
-    // A tile: 64 x 8, two elements per thread
+    // A tile: 64 x 8 complex, two elements per thread, as (re, im) pairs
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int r = tid / 8 + 32 * h, c = tid % 8;
@@ -48,9 +67,10 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
         v = A[(size_t)gr * lda + gc];
         if (dA_col) v = cmul(v, dA_col[gc]);
       }
-      sm.As[c][r] = v;
+      sm.As[r][2 * c] = v.x;
+      sm.As[r][2 * c + 1] = v.y;
     }
-    // B tile: 8 x 64
+    // B tile: 8 x 64 complex, each element as the 2 x 2 block [[re, im], [-im, re]]
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int r = tid / 64 + 4 * h, c = tid % 64;
@@ -60,38 +80,36 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
         v = B[(size_t)gr * ldb + gc];
         if (dB_row) v = cmul(dB_row[gr], v);
       }
-      sm.Bs[r][c] = v;
+      sm.Bs[2 * r][2 * c] = v.x;
+      sm.Bs[2 * r][2 * c + 1] = v.y;
+      sm.Bs[2 * r + 1][2 * c] = -v.y;
+      sm.Bs[2 * r + 1][2 * c + 1] = v.x;
     }
     __syncthreads();
 #pragma unroll
-    for (int kk = 0; kk < kTK; ++kk) {
-      cd a[4], b[4];
+    for (int ks = 0; ks < 2 * kTK; ks += 4) {
+      double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sm.As[kk][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = sm.As[wm * 32 + i * 8 + g][ks + t];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = sm.Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) b[j] = sm.Bs[ks + t][wn * 32 + j * 8 + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
-          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
-          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
-          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
-        }
+        for (int j = 0; j < 4; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
     __syncthreads();
   }
   const bool zero_beta = beta.x == 0.0 && beta.y == 0.0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int gr = r0 + ty + 16 * i;
+    const int gr = r0 + wm * 32 + i * 8 + g;
     if (gr >= m) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int gc = c0 + tx + 16 * j;
+      const int gc = c0 + wn * 16 + j * 4 + t;
       if (gc >= n) continue;
-      cd v = cmul(alpha, acc[i][j]);
+      cd v = cmul(alpha, cd{acc[i][j][0], acc[i][j][1]});
       cd *pc = C + (size_t)gr * ldc_ + gc;
       if (!zero_beta) v = cadd(v, cmul(beta, *pc));
       *pc = v;

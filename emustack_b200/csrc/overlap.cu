@@ -372,8 +372,14 @@ struct OvGemm {
   int kchunk;
 };
 
+// Shared tiles of ov_gemm_kernel (complex, k-major).
+struct OvGemmSmem {
+  cd As[kTK][kTM];
+  cd Bs[kTK][kTN];
+};
+
 __global__ void __launch_bounds__(kDLThreads) ov_gemm_kernel(OvGemm g) {
-  __shared__ GemmSmem sm;
+  __shared__ OvGemmSmem sm;
   const int c = blockIdx.z;
   const int k0 = c * g.kchunk;
   const int kk = min(g.kchunk, g.k - k0);
