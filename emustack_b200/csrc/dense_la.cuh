@@ -56,10 +56,12 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  for (int k0 = 0; k0 < k; k0 += kTK) {
-    // A tile: 64 x 8 complex, two elements per thread, as (re, im) pairs
+  // the next k-tile's elements are fetched into registers while the
+  // tensor cores work on the current one
+  cd va[2], vb[2];
+  auto fetch = [&](int k0) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < 2; ++h) {  // A: 64 x 8 complex, two elements per thread
       const int r = tid / 8 + 32 * h, c = tid % 8;
       const int gr = r0 + r, gc = k0 + c;
       cd v = cd{0.0, 0.0};
@@ -67,12 +69,10 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
         v = A[(size_t)gr * lda + gc];
         if (dA_col) v = cmul(v, dA_col[gc]);
       }
-      sm.As[r][2 * c] = v.x;
-      sm.As[r][2 * c + 1] = v.y;
+      va[h] = v;
     }
-    // B tile: 8 x 64 complex, each element as the 2 x 2 block [[re, im], [-im, re]]
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < 2; ++h) {  // B: 8 x 64 complex
       const int r = tid / 64 + 4 * h, c = tid % 64;
       const int gr = k0 + r, gc = c0 + c;
       cd v = cd{0.0, 0.0};
@@ -80,12 +80,28 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
         v = B[(size_t)gr * ldb + gc];
         if (dB_row) v = cmul(dB_row[gr], v);
       }
-      sm.Bs[2 * r][2 * c] = v.x;
-      sm.Bs[2 * r][2 * c + 1] = v.y;
-      sm.Bs[2 * r + 1][2 * c] = -v.y;
-      sm.Bs[2 * r + 1][2 * c + 1] = v.x;
+      vb[h] = v;
+    }
+  };
+  if (k > 0) fetch(0);
+  for (int k0 = 0; k0 < k; k0 += kTK) {
+    // A as (re, im) pairs; B element as the 2 x 2 block [[re, im], [-im, re]]
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = tid / 8 + 32 * h, c = tid % 8;
+      sm.As[r][2 * c] = va[h].x;
+      sm.As[r][2 * c + 1] = va[h].y;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = tid / 64 + 4 * h, c = tid % 64;
+      sm.Bs[2 * r][2 * c] = vb[h].x;
+      sm.Bs[2 * r][2 * c + 1] = vb[h].y;
+      sm.Bs[2 * r + 1][2 * c] = -vb[h].y;
+      sm.Bs[2 * r + 1][2 * c + 1] = vb[h].x;
     }
     __syncthreads();
+    if (k0 + kTK < k) fetch(k0 + kTK);
 #pragma unroll
     for (int ks = 0; ks < 2 * kTK; ks += 4) {
       double a[4], b[4];

@@ -2,7 +2,8 @@
 on synthetic layers of a given shape.
 
     python -m emustack_b200.profile_dense [--npw-order O] [--period D] [--nval M]
-                                          [--layers K] [--batch B] [--steps S]
+                                          [--layers K] [--batch B] [--steps S] [--mode 0|1|2]
+    python -m emustack_b200.profile_dense --gemm [--batch B]   (the complex GEMM alone)
 
 Substrate n=1.46 and superstrate air are films; K nanostructured layers of M
 Bloch modes sit between them with random J (P x M) and J_dag (M x P), complex
@@ -36,6 +37,36 @@ def air_kz(px, py, wl, period, n=1.0):
     return kz
 
 
+def gemm_rate(args):
+    """TFLOP/s of the batched complex GEMM C[P x M] = A[P x P] B[P x M] over
+    the batch, 8 P^2 M real flop each."""
+    from emustack_b200.dense import zgemm_batched
+    from emustack_b200.films import grating_orders
+    from emustack_b200.probe import fp64_peak_tflops
+    dev = torch.device('cuda')
+    P = 2 * len(grating_orders(args.max_order, args.period, args.period)[0])
+    M, B = args.nval, args.batch
+    g = torch.Generator(device='cuda').manual_seed(0)
+    cr = lambda *sh: torch.complex(torch.randn(sh, dtype=torch.float64, device=dev, generator=g),
+                                   torch.randn(sh, dtype=torch.float64, device=dev, generator=g))
+    A, Bm = cr(B, P, P), cr(B, P, M)
+    C_ = torch.empty(B, P, M, dtype=torch.complex128, device=dev)
+    for _ in range(max(args.warmup, 1)):
+        zgemm_batched(A, Bm, C_)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(args.steps):
+        zgemm_batched(A, Bm, C_)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    tf = B * 8.0 * P * P * M / (ms / 1e3) / 1e12
+    peak = fp64_peak_tflops()
+    print(json.dumps({'gemm': [P, P, M], 'batch': B, 'ms': ms, 'tflops': tf, 'fp64_peak_tflops': peak,
+                      'frac': tf / peak}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--max-order', type=int, default=10)
@@ -46,7 +77,11 @@ def main():
     ap.add_argument('--steps', type=int, default=2)
     ap.add_argument('--warmup', type=int, default=1)
     ap.add_argument('--mode', type=int, default=0, help='cascade: 0 auto, 1 one CTA per solve, 2 multi-CTA')
+    ap.add_argument('--gemm', action='store_true',
+                    help='time only the batched complex GEMM (emu_zgemm_batched) at P x P x M')
     args = ap.parse_args()
+    if args.gemm:
+        return gemm_rate(args)
     from emustack_b200.dense import DenseLayer, DenseStackSolver, film_interface, interface_dense
     from emustack_b200.films import grating_orders
     from emustack_b200.probe import fp64_peak_tflops
