@@ -11,9 +11,11 @@ R/T/A spectral points per second.
 
 Arms
   ours       : device-resident inputs, one fused launch per step (`value`);
-               `e2e` repeats the step through the public solver with pinned
-               host inputs, host->device copies, the solve and the
-               device->host read of R_net/T_net diagonals and a/t/r lists.
+               `e2e` repeats the step through the public host-to-host API
+               (FilmHostPipeline) with pinned host inputs: host->device
+               copies, the solves and the device->host read of R_net/T_net
+               diagonals and a/t/r lists, in 8192-point pieces on two
+               streams so copies overlap solves.
   reference  : the reference's FP64 algorithm (the CPU oracle, a numpy
                restatement of backend/stack.py + backend/mode_calcs.py) on the
                host cores, a bounded sample per step.
@@ -38,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_WL, N_ANG, N_FILMS = 2048, 16, 10
+E2E_CHUNK = 8192   # points per piece of the host-to-host pipeline
 PERIOD, MAX_ORDER, POL = 500.0, 5, 'TE'
 METRIC = 'R/T/A spectral points/s (batched thin-film GSM, FP64)'
 L2_FLUSH_BYTES = 256 << 20
@@ -223,24 +226,23 @@ def run_ours(args, rank, world, local_rank):
     ms_per_step = total_ms / args.steps
     value = world * B * args.steps / (total_ms / 1e3)
 
-    # ---- e2e through the public solver with pinned host buffers
+    # ---- e2e through the public host-to-host API (FilmHostPipeline): pinned
+    # host inputs, the copies in, the solves and the copies out of R_net /
+    # T_net diagonals and a/t/r lists, in pieces whose copies overlap the
+    # solves of their neighbours
+    from emustack_b200.films import FilmHostPipeline
+    pipe = FilmHostPipeline(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev, chunk=E2E_CHUNK)
     h_wl = torch.from_numpy(w['wl']).pin_memory()
     h_kp = torch.from_numpy(w['k_pll']).pin_memory()
     h_n = torch.from_numpy(w['n']).pin_memory()
     h_h = torch.from_numpy(w['heights']).pin_memory()
-    outs_h = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory()
-              for k, v in solver.outputs(B).items()}
+    outs_h = pipe.outputs(B)
     h2d = sum(t.numel() * t.element_size() for t in (h_wl, h_kp, h_n, h_h))
+    h2d += (h_h.numel() * h_h.element_size()) * ((B + E2E_CHUNK - 1) // E2E_CHUNK - 1)
     d2h = sum(t.numel() * t.element_size() for t in outs_h.values())
 
     def e2e_step():
-        dw = h_wl.to(dev, non_blocking=True)
-        dk = h_kp.to(dev, non_blocking=True)
-        dn = h_n.to(dev, non_blocking=True)
-        dh = h_h.to(dev, non_blocking=True)
-        o = solver.solve(dw, dk, dn, dh, pol=POL)
-        for k, t in outs_h.items():
-            t.copy_(o[k], non_blocking=True)
+        pipe.solve(h_wl, h_kp, h_n, h_h, pol=POL)
 
     for _ in range(args.warmup):
         e2e_step()

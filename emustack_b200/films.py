@@ -198,6 +198,68 @@ class FilmStackSolver(object):
         return out
 
 
+class FilmHostPipeline(object):
+    """Host-to-host solves of batches of all-film stacks of one shape.
+
+    Inputs come from (pinned) host tensors and results land in pinned host
+    tensors.  The batch is cut into `chunk`-point pieces dealt round-robin to
+    `n_streams` streams, each with its own FilmStackSolver, so the
+    device-to-host copy of one piece's R_net / T_net / lists overlaps the
+    solve of the next and the host-to-device copy of the one after: the
+    host link and the SMs work at the same time.  Arguments as
+    FilmStackSolver; results as its `solve` (the same kernel per point).
+    """
+
+    OUT = ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags')
+
+    def __init__(self, n_layers, max_order, period, period_y=None, world_1d=False, device='cuda',
+                 chunk=8192, n_streams=2):
+        self.device = torch.device(device)
+        self.solvers = [FilmStackSolver(n_layers, max_order, period, period_y, world_1d, device=self.device)
+                        for _ in range(n_streams)]
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
+        self.chunk = int(chunk)
+        self._out = None
+
+    def outputs(self, B):
+        """Pinned host outputs for a batch of B points (reused across calls)."""
+        if self._out is None or self._out['r_list'].shape[0] != B:
+            dev = self.solvers[0].outputs(1)
+            self._out = {k: torch.empty((B,) + tuple(dev[k].shape[1:]), dtype=dev[k].dtype).pin_memory()
+                         for k in self.OUT}
+        return self._out
+
+    def solve(self, wl_nm, k_pll, n, heights_nm=None, pol='TE', variant=None):
+        """wl_nm float64 [B], k_pll float64 [B, 2], n complex128 [B, L],
+        heights_nm float64 [L-2] or [B, L-2]: host tensors (pinned for
+        asynchronous copies).  Returns the pinned host outputs; the current
+        stream waits for every piece, so they are complete once it has
+        reached this point (e.g. after torch.cuda.synchronize())."""
+        B = int(wl_nm.shape[0])
+        out = self.outputs(B)
+        cur = torch.cuda.current_stream(self.device)
+        for st in self.streams:
+            st.wait_stream(cur)
+        per_point_h = heights_nm is not None and heights_nm.dim() == 2
+        for c, b0 in enumerate(range(0, B, self.chunk)):
+            b1 = min(B, b0 + self.chunk)
+            i = c % len(self.streams)
+            st, sol = self.streams[i], self.solvers[i]
+            with torch.cuda.stream(st):
+                dw = wl_nm[b0:b1].to(self.device, non_blocking=True)
+                dk = k_pll[b0:b1].to(self.device, non_blocking=True)
+                dn = n[b0:b1].to(self.device, non_blocking=True)
+                dh = None
+                if heights_nm is not None:
+                    dh = (heights_nm[b0:b1] if per_point_h else heights_nm).to(self.device, non_blocking=True)
+                o = sol.solve(dw, dk, dn, dh, pol=pol, stream=st, variant=variant)
+                for k in self.OUT:
+                    out[k][b0:b1].copy_(o[k], non_blocking=True)
+        for st in self.streams:
+            cur.wait_stream(st)
+        return out
+
+
 # ---------------------------------------------------------------- uneven batches
 _POINT_DTYPE = np.dtype([
     ('n_layers', np.int32), ('n_pw', np.int32), ('world_1d', np.int32), ('pol', np.int32),

@@ -224,3 +224,25 @@ def test_launch_variants_agree(pol):
             else:
                 np.testing.assert_allclose(x, res[0][k], rtol=1e-12, atol=1e-14,
                                            err_msg='variant %d %s' % (v, k))
+
+
+@pytest.mark.parametrize('per_point_heights', [False, True])
+def test_host_pipeline_matches_device_solve(per_point_heights):
+    """FilmHostPipeline (host inputs, pieces on two streams, pinned host
+    outputs) gives the device solver's results bit for bit, also when the
+    batch is not a multiple of the piece size."""
+    from emustack_b200.films import FilmHostPipeline, FilmStackSolver
+    h, nl = _config2_stack(seed=2)
+    B = 1000
+    wl, kp = _points(B, seed=5)
+    n = np.tile(nl, (B, 1))
+    hs = np.tile(h, (B, 1)) * np.linspace(0.5, 1.5, B)[:, None] if per_point_heights else h
+    pipe = FilmHostPipeline(len(nl), 5, 500.0, chunk=300)
+    host = [torch.tensor(a).pin_memory() for a in (wl, kp, n, hs)]
+    out = pipe.solve(*host, pol='un')
+    torch.cuda.synchronize()
+    s = FilmStackSolver(len(nl), 5, 500.0)
+    dev = s.device
+    ref = s.solve(*[t.to(dev) for t in host], pol='un')
+    for k in FilmHostPipeline.OUT:
+        np.testing.assert_array_equal(out[k].numpy(), ref[k].cpu().numpy(), err_msg=k)
