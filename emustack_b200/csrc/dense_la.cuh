@@ -193,7 +193,7 @@ static __device__ int cta_getrf(int n, cd *A, int lda, int *ipiv, LuSmem &ls, Ge
             bv = ls.val[w];
             bx = ls.idx[w];
           }
-        ls.piv = bx;
+        ls.piv = bx < n ? bx : j;  // no comparable candidate (NaN column): keep the row
       }
       __syncthreads();
       const int p = ls.piv;

@@ -11,6 +11,8 @@
 // Batched matrices are (base pointer, batch stride in elements, leading
 // dimension); problem b is blockIdx.y (.z for the GEMM).
 #pragma once
+#include <algorithm>
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "dense_la.cuh"
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(cd *A_, long long 
           bv = ls.val[w];
           bx = ls.idx[w];
         }
-      ls.piv = bx;
+      ls.piv = bx < n ? bx : j;  // no comparable candidate (NaN column): keep the row
     }
     __syncthreads();
     const int p = ls.piv;
@@ -138,6 +140,212 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(cd *A_, long long 
     }
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------- cluster panel
+// The same panel factorisation by a thread-block cluster of cs <= 8 CTAs
+// per matrix: CTA q holds panel rows j0 + q, j0 + q + cs, ... (columns
+// j0 .. j0+jb-1) in shared memory.  Per column: each CTA finds its local
+// pivot candidate; after a cluster barrier every CTA reads all candidates
+// and the pivot row (and the owner of the pivot row reads row j) from the
+// other CTAs' shared memory; after a second barrier the rows are swapped
+// and every CTA scales and updates its own rows.  Same arithmetic and pivot
+// choice as cta_getrf.  The swaps of the columns outside the panel are left
+// to laswp_outside_kernel.  Waits are the hardware cluster barrier.
+constexpr int kPanelMaxCS = 8;
+constexpr int kPanelCTAThreads = 256;
+constexpr size_t kPanelMaxSmem = 200 * 1024;
+
+__global__ void __launch_bounds__(kPanelCTAThreads) panel_cluster_kernel(cd *A_, long long sA, int lda, int n,
+                                                                         int j0, int jb, int *ipiv_,
+                                                                         long long sip, int *info, int code) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char psm[];
+  __shared__ double cval[kPanelCTAThreads / 32];
+  __shared__ int cidx[kPanelCTAThreads / 32];
+  __shared__ double cand_v;  // this CTA's candidate, read by the others
+  __shared__ int cand_i;
+  __shared__ cd prow[kNB], jrow[kNB];
+  const int q = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+  const long long b = blockIdx.x / cs;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5;
+  cd *A = A_ + b * sA;
+  int *ipiv = ipiv_ + b * sip;
+  const int nr = n - j0;                                  // panel rows
+  const int my_rows = nr > q ? (nr - q + cs - 1) / cs : 0;
+  cd *Pm = reinterpret_cast<cd *>(psm);                  // [my_rows][kNB]
+  auto grow = [&](int l) { return j0 + q + cs * l; };   // local row l -> matrix row
+  for (int e = tid; e < my_rows * jb; e += nt) {
+    const int l = e / jb, c = e % jb;
+    Pm[l * kNB + c] = A[(size_t)grow(l) * lda + j0 + c];
+  }
+  __syncthreads();
+  int first_zero = 0;
+  for (int jj = 0; jj < jb; ++jj) {
+    const int j = j0 + jj;
+    // local pivot candidate among rows >= j (first maximum wins)
+    double best = -1.0;
+    int bi = n;
+    for (int l = tid; l < my_rows; l += nt) {
+      const int i = grow(l);
+      if (i < j) continue;
+      const double v = cabs1(Pm[l * kNB + jj]);
+      if (v > best || (v == best && i < bi)) {
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      cval[w] = best;
+      cidx[w] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bv = cval[0];
+      int bx = cidx[0];
+      for (int k = 1; k < nt / 32; ++k)
+        if (cval[k] > bv || (cval[k] == bv && cidx[k] < bx)) {
+          bv = cval[k];
+          bx = cidx[k];
+        }
+      cand_v = bv;
+      cand_i = bx;
+    }
+    cl.sync();  // candidates visible cluster-wide
+    // every CTA: the global pivot, then the rows it needs from their owners
+    double bv = -1.0;
+    int p = n;
+    for (int r = 0; r < cs; ++r) {
+      const double v = *cl.map_shared_rank(&cand_v, r);
+      const int i = *cl.map_shared_rank(&cand_i, r);
+      if (v > bv || (v == bv && i < p)) {
+        bv = v;
+        p = i;
+      }
+    }
+    if (p >= n) p = j;  // no comparable candidate (NaN column): keep the row
+    const int qp = (p - j0) % cs, lp = (p - j0) / cs;
+    const int qj = (j - j0) % cs, lj = (j - j0) / cs;
+    {
+      const cd *rp = cl.map_shared_rank(Pm, qp) + (size_t)lp * kNB;
+      for (int c = tid; c < jb; c += nt) prow[c] = rp[c];
+      if (q == qp && p != j) {
+        const cd *rj = cl.map_shared_rank(Pm, qj) + (size_t)lj * kNB;
+        for (int c = tid; c < jb; c += nt) jrow[c] = rj[c];
+      }
+    }
+    cl.sync();  // all remote reads done before any row changes
+    if (p != j) {
+      if (q == qj)
+        for (int c = tid; c < jb; c += nt) Pm[lj * kNB + c] = prow[c];
+      if (q == qp)
+        for (int c = tid; c < jb; c += nt) Pm[lp * kNB + c] = jrow[c];
+    }
+    if (q == 0 && tid == 0) ipiv[j] = p;
+    __syncthreads();
+    const cd ajj = prow[jj];
+    const bool zero = ajj.x == 0.0 && ajj.y == 0.0;
+    if (zero) {
+      if (!first_zero) first_zero = j + 1;
+    } else {
+      const cd r = crecip(ajj);
+      const int pc = jb - (jj + 1);
+      for (int l = tid; l < my_rows; l += nt) {
+        const int i = grow(l);
+        if (i <= j) continue;
+        const cd lv = cmul(Pm[l * kNB + jj], r);
+        Pm[l * kNB + jj] = lv;
+        for (int c = jj + 1; c < jj + 1 + pc; ++c) Pm[l * kNB + c] = csub(Pm[l * kNB + c], cmul(lv, prow[c]));
+      }
+    }
+    __syncthreads();
+  }
+  if (q == 0 && tid == 0 && first_zero && info && info[b] == 0) info[b] = code + first_zero;
+  for (int e = tid; e < my_rows * jb; e += nt) {
+    const int l = e / jb, c = e % jb;
+    A[(size_t)grow(l) * lda + j0 + c] = Pm[l * kNB + c];
+  }
+  cl.sync();  // no CTA leaves while others may still read its shared memory
+}
+
+// The panel's row interchanges ipiv[j0 .. j0+jb) applied in order to the
+// columns outside the panel, [0, j0) and [j0+jb, n).
+__global__ void laswp_outside_kernel(cd *A_, long long sA, int lda, int n, int j0, int jb, const int *ipiv_,
+                                     long long sip) {
+  const long long b = blockIdx.y;
+  cd *A = A_ + b * sA;
+  const int *ipiv = ipiv_ + b * sip;
+  const int ncols = n - jb;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncols; t += gridDim.x * blockDim.x) {
+    const int c = t < j0 ? t : t + jb;
+    for (int j = j0; j < j0 + jb; ++j) {
+      const int p = ipiv[j];
+      if (p != j) {
+        const cd v = A[(size_t)j * lda + c];
+        A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
+        A[(size_t)p * lda + c] = v;
+      }
+    }
+  }
+}
+
+// Launches the cluster panel; false if it would not beat panel_kernel or
+// cannot run (the caller then uses panel_kernel).  Cluster size: enough
+// CTAs for the panel to fit in shared memory, and as many more (up to 8) as
+// keep all clusters of the batch resident at once; a batch that already
+// fills the GPU with one wide CTA per matrix keeps panel_kernel.
+inline bool panel_cluster(cd *A, long long sA, int lda, int n, int j0, int jb, int *ipiv, long long sip,
+                          int *info, int code, int batch, cudaStream_t s) {
+  const size_t row_bytes = (size_t)kNB * sizeof(cd);
+  const long long nr = n - j0;
+  int cs = 0;
+  for (int c = kPanelMaxCS; c >= 1; --c) {
+    const size_t smem = (size_t)((nr + c - 1) / c) * row_bytes;
+    if (smem > kPanelMaxSmem) break;
+    const long long per_sm = std::min<long long>(2, (long long)(228 * 1024 / (smem + 2048)));
+    if ((long long)batch * c <= per_sm * sm_count()) {
+      cs = c;
+      break;
+    }
+  }
+  if (cs < 2) return false;
+  const size_t smem = (size_t)((nr + cs - 1) / cs) * row_bytes;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(batch * cs));
+  cfg.blockDim = dim3(kPanelCTAThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, panel_cluster_kernel, A, sA, lda, n, j0, jb, ipiv, sip, info, code) !=
+      cudaSuccess)
+    return false;
+  note_launch();
+  const int outside = n - jb;
+  if (outside > 0) {
+    laswp_outside_kernel<<<dim3((unsigned)((outside + 127) / 128), (unsigned)batch), 128, 0, s>>>(
+        A, sA, lda, n, j0, jb, ipiv, sip);
+    note_launch();
+  }
+  return true;
 }
 
 // X rows r0 .. r0+rb-1 := L11^{-1} X rows (unit lower L11 = L[r0.., r0..],
@@ -235,10 +443,14 @@ inline void getrf_multi(int n, cd *A, long long sA, int lda, int *ipiv, long lon
                         int batch, cudaStream_t s) {
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int jb = min(kNB, n - j0);
-    // a panel is a latency-bound chain of column steps: the widest CTA keeps
-    // each step short (the arithmetic does not depend on the width)
-    panel_kernel<<<batch, kPanelThreads, 0, s>>>(A, sA, lda, n, j0, jb, ipiv, sip, info, code);
-    note_launch();
+    // a panel is a latency-bound chain of column steps: a cluster of CTAs
+    // keeps the panel in shared memory (one wide CTA through L2 otherwise;
+    // the arithmetic is the same)
+    if (!panel_cluster(A, sA, lda, n, j0, jb, ipiv, sip, info, code, batch, s)) {
+      cudaGetLastError();
+      panel_kernel<<<batch, kPanelThreads, 0, s>>>(A, sA, lda, n, j0, jb, ipiv, sip, info, code);
+      note_launch();
+    }
     const int rest = n - (j0 + jb);
     if (rest > 0) {
       trsm_lower_kernel<<<col_grid(rest, batch), 128, 0, s>>>(A, sA, lda, j0, jb, A, sA, lda, j0 + jb, rest);
