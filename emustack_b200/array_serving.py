@@ -529,7 +529,8 @@ class ArrayBatcher(object):
             sets.setdefault((r.max_order, r.period, r.period_y, r.world_1d), []).append(b)
         n = len(reqs)
         air = [None] * n                 # (kz_air, wln, row) per request
-        film = {}                        # (b, j) -> (R, T, -R, kz2, row)
+        film_of = [None] * n             # (R, T, -R, kz2) of the request's order set
+        film = {}                        # (b, j) -> row of the film instance in those tensors
         np_parts, spec_parts, order = [], [], []
         keep = []
         with torch.cuda.stream(stream):
@@ -572,12 +573,9 @@ class ArrayBatcher(object):
                         sub[b] = i
                     if j == len(reqs[b].layers) - 1:
                         top[b] = i
-                    air[b] = (kz_air, wln, rows[b])
                 for b in bs:
                     air[b] = (kz_air, wln, rows[b])
-                film_rows = (R, T, mR, kz2)
-                for b in bs:
-                    film[('t', b)] = film_rows
+                    film_of[b] = (R, T, mR, kz2)
                 ti = torch.tensor([top[b] for b in bs], dtype=torch.long, device=dev)
                 si = torch.tensor([sub[b] for b in bs], dtype=torch.long, device=dev)
                 np_parts.append(torch.stack([np_air, np_f.index_select(0, ti), np_f.index_select(0, si)], 1))
@@ -591,7 +589,7 @@ class ArrayBatcher(object):
             for b in order:
                 r = reqs[b]
                 P, L = 2 * r.npw, len(r.layers)
-                R, T, mR, kz2 = film[('t', b)]
+                R, T, mR, kz2 = film_of[b]
                 lays = []
                 for j, ly in enumerate(r.layers):
                     fin = 0 < j < L - 1
