@@ -45,7 +45,7 @@ class EmuFilmStackBatch(C.Structure):
         ('variant', C.c_int),
     ]
 
-FILM_VARIANTS = (0, 1, 2, 3)
+FILM_VARIANTS = (0, 1, 2, 3, 4, 5)
 
 
 class EmuError(RuntimeError):

@@ -49,9 +49,9 @@ using namespace emu;
 // Launch variants (EmuFilmStackBatch.variant): threads per CTA and the
 // minimum resident CTAs per SM given to the compiler (which sets the
 // register cap: 65536 / (threads * min CTAs), at most 255).
-constexpr int kVariants = 4;
+constexpr int kVariants = 6;
 constexpr int kMaxCtaSmem = 200 * 1024;
-constexpr int kVarThreadsTab[kVariants] = {256, 128, 512, 256};
+constexpr int kVarThreadsTab[kVariants] = {256, 128, 512, 256, 256, 256};
 
 struct FilmArgs {
   EmuFilmStackBatch p;
@@ -144,9 +144,12 @@ struct Launch {
 
 using FilmKernel = void (*)(FilmArgs);
 // 0: 256 threads x 2 CTAs (128 registers), 1: 128 x 4 (128), 2: 512 x 1
-// (128), 3: 256 x 1 (255 registers, no spills, half the resident warps)
+// (128), 3: 256 x 1 (255 registers, no spills, half the resident warps),
+// 4: 256 x 3 (85 registers), 5: 256 x 4 (64): more warps to hide the FP64
+// latency chains, at the price of spills to L1
 const FilmKernel kVarKernels[kVariants] = {film_stack_kernel<256, 2>, film_stack_kernel<128, 4>,
-                                           film_stack_kernel<512, 1>, film_stack_kernel<256, 1>};
+                                           film_stack_kernel<512, 1>, film_stack_kernel<256, 1>,
+                                           film_stack_kernel<256, 3>, film_stack_kernel<256, 4>};
 
 Launch plan(const EmuFilmStackBatch *p) {
   Launch l;

@@ -180,7 +180,9 @@ typedef struct {
   int32_t *d_specular;   /* [B] specular order index                        */
   int32_t *d_num_prop;   /* [B][L+1] propagating orders per layer, air last */
   /* launch variant (threads per CTA x minimum CTAs per SM): 0 = 256 x 2
-   * (default), 1 = 128 x 4, 2 = 512 x 1, 3 = 256 x 1 (up to 255 registers);
+   * (default), 1 = 128 x 4, 2 = 512 x 1, 3 = 256 x 1 (up to 255 registers),
+   * 4 = 256 x 3, 5 = 256 x 4 (85 / 64 registers: more resident warps, some
+   * values spilled to L1);
    * results are identical, only speed differs (chosen by an autotuner) */
   int variant;
 } EmuFilmStackBatch;
