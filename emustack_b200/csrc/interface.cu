@@ -281,10 +281,11 @@ extern "C" int emu_interface_dense_batch(int batch, int P, int M, const emu_c128
   a.ws = (cd *)d_workspace;
   a.ipiv = (int *)((char *)d_workspace + align_up((size_t)batch * a.ws_stride * sizeof(cd), 16));
   int mode = emu::dense_mode();
-  // measured at P = 618, M = 400: one CTA per interface wins once the batch
-  // fills the GPU (2.0 vs 4.6 ms per interface at 148), the multi-CTA path
-  // below half of it (4.7 vs 15.9 ms at 16)
-  if (mode == 0) mode = (M >= 96 && 2 * batch <= emu::sm_count()) ? 2 : 1;
+  // measured at P = 618, M = 400 (per wavelength of 4 interfaces): with the
+  // tensor-core GEMM tile and the cluster LU panel the multi-CTA path wins up
+  // to a batch of one interface per SM (1.57 vs 1.79 ms at 148, 1.76 vs
+  // 3.61 ms at 64); one CTA per interface beyond that
+  if (mode == 0) mode = (M >= 96 && batch <= emu::sm_count()) ? 2 : 1;
   if (mode == 2) return interface_dense_multi(a, batch, (cudaStream_t)stream);
   interface_dense_kernel<<<batch, kDLThreads, 0, (cudaStream_t)stream>>>(a);
   emu::note_launch();
