@@ -180,7 +180,7 @@ class EmuOverlap(C.Structure):
         ('d_sol1', vp), ('d_sol2', vp), ('d_scale2', vp), ('d_perm2', vp),
         ('area_norm', C.c_double), ('d_J', vp), ('d_J_dag', vp), ('d_index_pw_inv', vp),
         ('elements_per_chunk', C.c_int), ('precision', C.c_int), ('d_error', vp),
-        ('tc_splits', C.c_int),
+        ('tc_splits', C.c_int), ('field_c64', C.c_int),
     ]
 
 

@@ -611,12 +611,20 @@ __global__ void diag_finish_kernel(const cd *part, int nchunks, int nval, int ba
 // (node 0-5, component 0-1) of each (element, mode) record are read with
 // consecutive lanes, staged in shared memory and written as rows of
 // 192 contiguous floats.
+// Field records may be complex128 (the reference's layout) or complex64 in
+// the same layout (half the bytes; the B operand is FP32 either way).
 constexpr int kBModes = 8, kBElems = 16;
+struct cf32 {
+  float x, y;
+};
+__device__ __forceinline__ cd to_cd(const cd &v) { return v; }
+__device__ __forceinline__ cd to_cd(const cf32 &v) { return cd{(double)v.x, (double)v.y}; }
 
-__global__ void __launch_bounds__(256) make_B_kernel(const cd *sol_, long long ssol, int nval, long e0, long ne,
+template <class Rec>
+__global__ void __launch_bounds__(256) make_B_kernel(const Rec *sol_, long long ssol, int nval, long e0, long ne,
                                                      int conj, int row0, float *B_, long long sB) {
   __shared__ cd v[kBModes][kBElems][12];
-  const cd *sol = sol_ + (size_t)blockIdx.z * ssol;  // problem blockIdx.z
+  const Rec *sol = sol_ + (size_t)blockIdx.z * ssol;  // problem blockIdx.z
   float *B = B_ + (size_t)blockIdx.z * sB;
   const long long K = 6LL * ne;
   const int m0 = blockIdx.x * kBModes;
@@ -631,7 +639,7 @@ __global__ void __launch_bounds__(256) make_B_kernel(const cd *sol_, long long s
     for (int e = eo; e < kBElems; e += 2) {
       const long el = el0 + e;
       cd x = cd{0.0, 0.0};
-      if (m < nval && el < ne) x = sol[((size_t)(e0 + el) * nval + m) * 39 + node * 3 + c];
+      if (m < nval && el < ne) x = to_cd(sol[((size_t)(e0 + el) * nval + m) * 39 + node * 3 + c]);
       v[w][e][j] = x;
     }
   }
@@ -908,8 +916,16 @@ static int overlap_tc(const EmuOverlap *p, void *ws, cudaStream_t s) {
       etable_kernel<true><<<dim3((unsigned)eg, (unsigned)ng), 32 * kEtWarps, et_smem32, s>>>(ea);
       const dim3 bg((M + kBModes - 1) / kBModes, (unsigned)((ne + kBElems - 1) / kBElems), (unsigned)ng);
       const long long sB = (long long)t.nb * K2;
-      if (sol1) make_B_kernel<<<bg, 256, 0, s>>>(sol1 + (size_t)g0 * ssol, ssol, M, e0, ne, 0, 0, B32, sB);
-      if (sol2) make_B_kernel<<<bg, 256, 0, s>>>(sol2 + (size_t)g0 * ssol, ssol, M, e0, ne, 1, t.off1, B32, sB);
+      if (p->field_c64) {
+        const cf32 *f1 = (const cf32 *)p->d_sol1, *f2 = (const cf32 *)p->d_sol2;
+        if (f1) make_B_kernel<cf32><<<bg, 256, 0, s>>>(f1 + (size_t)g0 * ssol, ssol, M, e0, ne, 0, 0, B32, sB);
+        if (f2)
+          make_B_kernel<cf32><<<bg, 256, 0, s>>>(f2 + (size_t)g0 * ssol, ssol, M, e0, ne, 1, t.off1, B32, sB);
+      } else {
+        if (sol1) make_B_kernel<cd><<<bg, 256, 0, s>>>(sol1 + (size_t)g0 * ssol, ssol, M, e0, ne, 0, 0, B32, sB);
+        if (sol2)
+          make_B_kernel<cd><<<bg, 256, 0, s>>>(sol2 + (size_t)g0 * ssol, ssol, M, e0, ne, 1, t.off1, B32, sB);
+      }
       emu::note_launch(1 + (sol1 ? 1 : 0) + (sol2 ? 1 : 0));
       int used = 0;
       const int tst = emu::tc_gemm_tf32x3_parts(A32, 2LL * npw * K2, B32, sB, 2 * npw, t.nb, (int)K2, ng, t.splits,
@@ -950,6 +966,8 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
   if (p->max_order < 0 || p->max_order > kMaxOrd) return EMU_E_UNSUPPORTED;
   if (p->precision != 0 && p->precision != 1) return EMU_E_ARG;
   if (p->tc_splits < 0) return EMU_E_ARG;
+  if (p->field_c64 != 0 && p->field_c64 != 1) return EMU_E_ARG;
+  if (p->field_c64 && p->precision != 1) return EMU_E_UNSUPPORTED;  // the FP64 path reads complex128
   if (p->batch == 0) return EMU_OK;
   if (!d_workspace || workspace_bytes < emu_overlap_workspace_size(p)) return EMU_E_WORKSPACE;
   int st = upload_tables();

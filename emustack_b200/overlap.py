@@ -39,11 +39,13 @@ def _dev_int32(a, dev):
     return torch.as_tensor(np.asarray(a, np.int32), device=dev)
 
 
-def _check_sol(sol, nel, name):
+def _check_sol(sol, nel, name, allow_c64=False):
     if sol is None:
         return
-    if sol.dtype != c128 or not sol.is_cuda or not sol.is_contiguous():
-        raise TypeError('%s must be a contiguous CUDA complex128 tensor' % name)
+    ok = (torch.complex128, torch.complex64) if allow_c64 else (c128,)
+    if sol.dtype not in ok or not sol.is_cuda or not sol.is_contiguous():
+        raise TypeError('%s must be a contiguous CUDA %s tensor' % (
+            name, 'complex128 or complex64' if allow_c64 else 'complex128'))
     if sol.dim() != 5 or tuple(sol.shape[1:2]) != (nel,) or tuple(sol.shape[3:]) != (13, 3):
         raise ValueError('%s must be [batch][nel][nval][13][3]' % name)
 
@@ -55,7 +57,9 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
 
     px, py     int32 [Npw] plane-wave orders (emustack_b200.films.grating_orders)
     bloch      float64 [B, 2] k_parallel * period;  k0 float64 [B] = 2 pi / wl_norm
-    sol1/sol2  complex128 [B, nel, M, 13, 3] prime / adjoint fields
+    sol1/sol2  complex128 [B, nel, M, 13, 3] prime / adjoint fields (complex64
+               accepted with precision='tf32x3': the operands are FP32 there,
+               and the fields are read at half the bytes)
     scale2     complex128 [B, M] adjoint normalisation factors (or None)
     precision  'fp64' (FP64 GEMM) or 'tf32x3' (tensor cores, split-TF32 products)
     elements_per_chunk, tc_splits: launch choices (0 = defaults); with
@@ -65,9 +69,12 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
                False inside CUDA-graph capture (the flag stays on the device)
     """
     dev = dmesh.x.device
-    _check_sol(sol1, dmesh.nel, 'sol1')
-    _check_sol(sol2, dmesh.nel, 'sol2')
+    _check_sol(sol1, dmesh.nel, 'sol1', allow_c64=precision == 'tf32x3')
+    _check_sol(sol2, dmesh.nel, 'sol2', allow_c64=precision == 'tf32x3')
     ref = sol1 if sol1 is not None else sol2
+    c64 = ref.dtype == torch.complex64
+    if sol1 is not None and sol2 is not None and sol1.dtype != sol2.dtype:
+        raise TypeError('sol1 and sol2 must have the same dtype')
     B, M = int(ref.shape[0]), int(ref.shape[2])
     npw = len(px)
     d_px, d_py = _dev_int32(px, dev), _dev_int32(py, dev)
@@ -95,6 +102,7 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     err = torch.zeros(1, dtype=torch.int32, device=dev)
     d.d_error = ptr(err)
     d.tc_splits = int(tc_splits)
+    d.field_c64 = int(c64)
     L = lib()
     cands = None
     if d.precision == 1 and tune and not elements_per_chunk and not tc_splits:
@@ -116,7 +124,7 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     if cands:
         from .autotune import default_tuner, size_bucket
         shape = dict(npw=npw, M=M, nel=size_bucket(dmesh.nel), B=B, J=sol1 is not None,
-                     Jd=sol2 is not None)
+                     Jd=sol2 is not None, c64=c64)
         choice = default_tuner().choose('overlap_tc', shape, cands, run, (0, 0))
     run(choice)
     if check_error and d.precision == 1 and int(err.item()) != 0:

@@ -386,6 +386,9 @@ typedef struct {
                               (tensor-core path), else left untouched; may be NULL */
   int tc_splits;           /* tensor-core path: K splits per GEMM (1-64), 0 = one
                               wave of CTAs; results differ only in FP32 rounding */
+  int field_c64;           /* tensor-core path only: 1 = d_sol1 / d_sol2 hold
+                              complex64 (float re, im) in the same layout (the
+                              operands are FP32 anyway; half the bytes read) */
 } EmuOverlap;
 
 size_t emu_overlap_workspace_size(const EmuOverlap *p);

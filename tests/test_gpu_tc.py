@@ -111,3 +111,32 @@ def test_overlap_tensor_cores_batched_problems():
         a, b = a.cpu().numpy(), b.cpu().numpy()
         for i in range(B):
             assert np.abs(a[i] - b[i]).max() <= 5e-6 * np.abs(b[i]).max()
+
+
+def test_overlap_tensor_cores_complex64_fields():
+    """Fields held as complex64 (the tensor-core operands are FP32 anyway):
+    the same J / J_dag bit for bit as complex128 fields holding the same
+    values, and the FP64 path's results to the tensor-core tolerance."""
+    from emustack_b200.films import grating_orders
+    from emustack_b200.overlap import DeviceMesh, overlap_batch
+    rng = np.random.default_rng(33)
+    mesh = square_cell(10, radius=0.3, jitter=0.2)
+    mo, nval, B = 3, 24, 2
+    px, py = grating_orders(mo, 600.0, 600.0)
+    s1 = torch.tensor(np.stack([_fields(rng, mesh.nel, nval) for _ in range(B)]), device='cuda')
+    s2 = torch.tensor(np.stack([_fields(rng, mesh.nel, nval) for _ in range(B)]), device='cuda')
+    s1_32, s2_32 = s1.to(torch.complex64), s2.to(torch.complex64)
+    s1_r, s2_r = s1_32.to(torch.complex128), s2_32.to(torch.complex128)   # same values, complex128
+    bloch = torch.tensor(rng.uniform(-0.4, 0.4, (B, 2)), device='cuda')
+    k0 = torch.tensor(2 * np.pi / rng.uniform(0.8, 1.6, B), device='cuda')
+    dm = DeviceMesh(mesh)
+    kw = dict(precision='tf32x3', elements_per_chunk=70, tc_splits=2)
+    J32, Jd32, _ = overlap_batch(dm, px, py, mo, bloch, k0, s1_32, s2_32, **kw)
+    Jr, Jdr, _ = overlap_batch(dm, px, py, mo, bloch, k0, s1_r, s2_r, **kw)
+    assert torch.equal(J32, Jr) and torch.equal(Jd32, Jdr)
+    J64, Jd64, _ = overlap_batch(dm, px, py, mo, bloch, k0, s1_r, s2_r, precision='fp64')
+    for a, b in ((J32, J64), (Jd32, Jd64)):
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.abs(a - b).max() <= 5e-6 * np.abs(b).max()
+    with pytest.raises(TypeError):
+        overlap_batch(dm, px, py, mo, bloch, k0, s1_32, s2_32, precision='fp64')
