@@ -227,7 +227,7 @@ class EmuFilmVarBatch(C.Structure):
         ('d_specular', vp), ('d_num_prop', vp),
         ('order_len', C.c_int64), ('n_len', C.c_int64), ('h_len', C.c_int64),
         ('inc_len', C.c_int64), ('rt_len', C.c_int64), ('list_len', C.c_int64),
-        ('np_len', C.c_int64), ('warps_per_cta', C.c_int),
+        ('np_len', C.c_int64), ('warps_per_cta', C.c_int), ('variant', C.c_int),
     ]
 
 

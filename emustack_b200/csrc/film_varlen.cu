@@ -114,7 +114,10 @@ __device__ __forceinline__ bool point_ok(const VarArgs &a, const EmuFilmPoint *d
   return true;
 }
 
-__global__ void __launch_bounds__(kVarThreads, 2) film_var_kernel(VarArgs a) {
+// kMinBlocks: CTAs per SM the register budget is cut for (2: 128 registers;
+// 3: 85, more resident warps, some values spilled to L1).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kVarThreads, kMinBlocks) film_var_kernel(VarArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp >= a.warps) return;  // whole warps leave; no CTA barrier follows
@@ -199,23 +202,25 @@ extern "C" int emu_film_var_batch(const EmuFilmVarBatch *p, void *d_workspace,
   a.ws_bytes = (int64_t)workspace_bytes;
   a.inv_sqrt2_ = 1.0 / sqrt(2.0);
   if (p->warps_per_cta < 0 || p->warps_per_cta > kVarThreads / 32) return EMU_E_ARG;
+  if (p->variant < 0 || p->variant > 1) return EMU_E_ARG;
+  const auto kern = p->variant ? film_var_kernel<3> : film_var_kernel<2>;
   a.warps = std::max(1, std::min(kVarThreads / 32, kMaxSlotBytes / stride));
   if (p->warps_per_cta > 0) a.warps = std::min(a.warps, p->warps_per_cta);
   const size_t smem = (size_t)stride * a.warps;
   if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(film_var_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
       return EMU_E_CUDA;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, film_var_kernel, 32 * a.warps, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * a.warps, smem) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const long long groups = ((long long)p->n_points + a.warps - 1) / a.warps;
   long long grid = (long long)emu::sm_count() * per_sm;
   if (grid > groups) grid = groups;
-  film_var_kernel<<<(int)grid, 32 * a.warps, smem, (cudaStream_t)stream>>>(a);
+  kern<<<(int)grid, 32 * a.warps, smem, (cudaStream_t)stream>>>(a);
   emu::note_launch();
   return emu::check_launch();
 }

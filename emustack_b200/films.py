@@ -445,12 +445,14 @@ class FilmVarSolver(object):
             pl.h_inc.numpy()[:inc_off] = np.concatenate(inc_parts)
         return pl
 
-    def solve(self, pl, stream=None, want_num_prop=False, warps=None):
+    def solve(self, pl, stream=None, want_num_prop=False, warps=None, variant=0):
         """Copy a plan to the device and solve it in one launch; returns
         device tensors R_net/T_net [rt_len], a_list/t_list [list_len],
         r_list/flags/specular [B] (and num_prop [np_len]), views of buffers
-        this solver reuses.  warps: points (warps) per CTA, 1-8; None takes
-        the autotuner's choice for batches of 1024 points or more, else 8."""
+        this solver reuses.  warps: points (warps) per CTA, 1-8, and variant:
+        register budget (EmuFilmVarBatch.variant); warps=None takes the
+        autotuner's choice of both for batches of 1024 points or more, else
+        8 warps, variant 0.  Results do not depend on them."""
         dev = self.device
         px, py = self._device_orders()
         s = stream if stream is not None else torch.cuda.current_stream(dev)
@@ -481,18 +483,18 @@ class FilmVarSolver(object):
             e.n_len, e.h_len, e.inc_len = pl.n_len, pl.h_len, pl.inc_len
             e.rt_len, e.list_len, e.np_len = pl.rt_len, pl.list_len, pl.np_len
 
-            def run(w):
-                e.warps_per_cta = int(w)
+            def run(c):
+                e.warps_per_cta, e.variant = int(c[0]), int(c[1])
                 check(lib().emu_film_var_batch(C.byref(e), ptr(ws), C.c_size_t(ws.numel()),
                                                stream_ptr(s)), 'emu_film_var_batch')
 
-            if warps is None:
-                warps = 0
-                if B >= 1024:
-                    from .autotune import default_tuner, size_bucket
-                    shape = dict(B=size_bucket(B), max_pw=size_bucket(pl.max_pw), max_L=pl.max_layers)
-                    warps = default_tuner().choose('film_var', shape, [2, 4, 8], run, 0, stream=s)
-            run(warps)
+            choice = (warps or 0, variant)
+            if warps is None and B >= 1024:
+                from .autotune import default_tuner, size_bucket
+                shape = dict(B=size_bucket(B), max_pw=size_bucket(pl.max_pw), max_L=pl.max_layers)
+                cands = [(w, v) for v in (0, 1) for w in (2, 4, 8)]
+                choice = default_tuner().choose('film_var2', shape, cands, run, (0, 0), stream=s)
+            run(choice)
         return out
 
     def fetch(self, out, stream=None):

@@ -512,6 +512,8 @@ typedef struct {
   int64_t order_len, n_len, h_len, inc_len, rt_len, list_len, np_len;
   int warps_per_cta;           /* 1-8 warps (points) per CTA, 0 = 8 (fewer if
                                   the shared-memory slots do not fit); speed only */
+  int variant;                 /* register budget: 0 = 2 CTAs per SM (128
+                                  registers), 1 = 3 (85); speed only */
 } EmuFilmVarBatch;
 
 /* Host-side plan over the host copy of the descriptors: fills rt_off,
