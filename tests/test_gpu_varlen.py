@@ -8,7 +8,9 @@ the CPU oracle and against the uniform film kernel point by point.
 Tolerance: FP64 throughout, rtol 1e-9 / atol 1e-10 against the oracle and
 the fixtures.  Against the uniform kernel, R_net / T_net come from the same
 per-order code and must agree bit for bit; the flux sums are accumulated
-with shared-memory atomics in team order, so a/t/r lists agree to 1e-13.
+with shared-memory atomics in no fixed order, so a/t/r lists agree to 1e-13
+(relative, and absolute for the near-zero absorptances that are differences
+of order-one fluxes).
 """
 import numpy as np
 import pytest
@@ -117,9 +119,9 @@ def test_random_mixed_batch_matches_uniform_kernel_and_oracle():
         msg = 'point %d' % i
         np.testing.assert_array_equal(r['R_net'], o['R_net'][0], err_msg=msg)
         np.testing.assert_array_equal(r['T_net'], o['T_net'][0], err_msg=msg)
-        np.testing.assert_allclose(r['a_list'], o['a_list'][0], rtol=1e-13, atol=1e-15, err_msg=msg)
-        np.testing.assert_allclose(r['t_list'], o['t_list'][0], rtol=1e-13, atol=1e-15, err_msg=msg)
-        np.testing.assert_allclose(r['r_list'], o['r_list'][0], rtol=1e-13, atol=1e-15, err_msg=msg)
+        np.testing.assert_allclose(r['a_list'], o['a_list'][0], rtol=1e-13, atol=1e-13, err_msg=msg)
+        np.testing.assert_allclose(r['t_list'], o['t_list'][0], rtol=1e-13, atol=1e-13, err_msg=msg)
+        np.testing.assert_allclose(r['r_list'], o['r_list'][0], rtol=1e-13, atol=1e-13, err_msg=msg)
         assert r['flags'] == o['flags'][0] and r['specular'] == o['specular'][0]
         if i % 10 == 0:
             ref = O.film_stack_point(list(p.n), list(p.heights), p.wl_nm, p.k_pll, p.period,
