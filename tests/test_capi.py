@@ -131,3 +131,44 @@ def test_film_var_plan_offsets_and_order():
     desc[2]['n_layers'] = 1
     assert _lib.lib().emu_film_var_plan(desc.ctypes.data_as(C.c_void_p), len(shapes), None,
                                         None, None, None, None, None, None) == 2
+
+
+def test_argument_checks_need_no_gpu():
+    """Descriptors the library must refuse are refused on the host, before
+    any device work: status codes as the header documents them."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    L = _lib.lib()
+    # uneven dense batch
+    assert L.emu_stack_var_batch(None, None, 0, None) == 1                 # EMU_E_ARG
+    d = _lib.EmuStackVarBatch()
+    d.n_stacks = 3
+    d.max_P, d.max_D, d.max_L = 26, 30, 4
+    assert L.emu_stack_var_workspace_size(C.byref(d)) == 0                 # no buffers: invalid
+    assert L.emu_stack_var_batch(C.byref(d), None, 0, None) == 1
+    for nm in ('d_points', 'd_layers', 'd_R_net', 'd_T_net', 'd_a_list', 'd_t_list', 'd_r_list', 'd_flags',
+               'd_info'):
+        setattr(d, nm, 256)
+    d.max_L = 65                                                           # above the 64-layer limit
+    assert L.emu_stack_var_batch(C.byref(d), None, 0, None) == 2           # EMU_E_SHAPE
+    d.max_L, d.max_D = 4, 20                                               # max_D below max_P
+    assert L.emu_stack_var_batch(C.byref(d), None, 0, None) == 2
+    d.max_D, d.n_slots = 30, 2
+    assert L.emu_stack_var_slots(C.byref(d)) == 2
+    assert L.emu_stack_var_batch(C.byref(d), None, 0, None) == 5           # EMU_E_WORKSPACE
+    d.n_stacks = 0
+    assert L.emu_stack_var_batch(C.byref(d), None, 0, None) == 0           # nothing to do
+    # overlap: complex64 fields only on the tensor-core path
+    o = _lib.EmuOverlap()
+    o.batch, o.nval, o.nel, o.npt, o.n_pw, o.max_order = 1, 4, 2, 4, 5, 1
+    for nm in ('d_px', 'd_py', 'd_x', 'd_table_nod', 'd_bloch', 'd_k0', 'd_sol1', 'd_J'):
+        setattr(o, nm, 256)
+    o.d, o.dy, o.area_norm = 1.0, 1.0, 1.0
+    o.field_c64, o.precision = 1, 0
+    assert L.emu_overlap_batch(C.byref(o), None, 0, None) == 8            # EMU_E_UNSUPPORTED
+    o.field_c64 = 2
+    assert L.emu_overlap_batch(C.byref(o), None, 0, None) == 1
+    # uneven film batch: register-budget variant out of range
+    f = _lib.EmuFilmVarBatch()
+    f.variant = 2
+    assert L.emu_film_var_batch(C.byref(f), None, 0, None) != 0
