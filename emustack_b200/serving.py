@@ -43,7 +43,8 @@ import time
 import numpy as np
 import torch
 
-from .array_serving import ArrayBatcher, ArrayLayer, ArrayRequest, SMatrixCache  # noqa: F401
+from .array_serving import (ArrayBatcher, ArrayLayer, ArrayRequest, SMatrixCache,  # noqa: F401
+                            dense_workspace_bytes)
 from .films import FilmPoint, FilmStackSolver, FilmVarSolver, grating_orders
 
 _NPW = {}
@@ -465,7 +466,12 @@ class GsmServer(object):
             self._arrays = ArrayBatcher(self.device, self.cache)
         t1 = time.perf_counter()
         if uneven:
-            ev, fin = self._arrays.launch_uneven(reqs, slot['stream'], id(slot), self.uneven_ws_bytes)
+            # the cascade workspace stays within what admission counted for
+            # these requests (each counts its own per-solve workspace)
+            counted = sum(dense_workspace_bytes(2 * r.npw, [ly.M if isinstance(ly, ArrayLayer) else 2 * r.npw
+                                                            for ly in r.layers]) for r in reqs)
+            ev, fin = self._arrays.launch_uneven(reqs, slot['stream'], id(slot),
+                                                 min(self.uneven_ws_bytes, counted))
             self.prof['launch_s'] += time.perf_counter() - t1
             self._submit(_Batch(reqs, slot, ev, nbytes, self._array_finish(fin), None))
             return
