@@ -291,7 +291,8 @@ static __device__ void cta_getrs(int n, int nrhs, const cd *LU, int lda, const i
         cd s = B[(size_t)(r0 + r) * ldb + c];
         for (int t = r + 1; t < rb; ++t)
           s = csub(s, cmul(LU[(size_t)(r0 + r) * lda + r0 + t], B[(size_t)(r0 + t) * ldb + c]));
-        B[(size_t)(r0 + r) * ldb + c] = cdiv(s, LU[(size_t)(r0 + r) * lda + r0 + r]);
+        // the diagonal's reciprocal does not depend on the solve: off the chain
+        B[(size_t)(r0 + r) * ldb + c] = cmul(s, crecip(LU[(size_t)(r0 + r) * lda + r0 + r]));
       }
     }
     __syncthreads();

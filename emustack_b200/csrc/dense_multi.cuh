@@ -388,6 +388,7 @@ __global__ void __launch_bounds__(128) trsm_lower_kernel(const cd *L_, long long
 __global__ void __launch_bounds__(128) trsm_upper_kernel(const cd *U_, long long sU, int ldu, int r0, int rb,
                                                          cd *X_, long long sX, int ldx, int ncols) {
   __shared__ cd Us[kNB][kNB];
+  __shared__ cd invd[kNB];
   const long long b = blockIdx.y;
   const cd *U = U_ + b * sU;
   cd *X = X_ + b * sX;
@@ -395,6 +396,7 @@ __global__ void __launch_bounds__(128) trsm_upper_kernel(const cd *U_, long long
     const int r = e / rb, t = e % rb;
     Us[r][t] = U[(size_t)(r0 + r) * ldu + r0 + t];
   }
+  if (threadIdx.x < rb) invd[threadIdx.x] = crecip(U[(size_t)(r0 + threadIdx.x) * ldu + r0 + threadIdx.x]);
   __syncthreads();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncols) return;
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(128) trsm_upper_kernel(const cd *U_, long long
 #pragma unroll
       for (int t = r + 1; t < kNB; ++t)
         if (t < rb) s = csub(s, cmul(Us[r][t], x[t]));
-      x[r] = cdiv(s, Us[r][r]);
+      x[r] = cmul(s, invd[r]);
     }
   }
 #pragma unroll
