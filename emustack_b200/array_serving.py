@@ -329,14 +329,24 @@ class ArrayBatcher(object):
         check(lib().emu_anallo_modes(C.byref(d), stream_ptr()), 'emu_anallo_modes')
         return kz, sort_out, spec, nprop
 
-    def _fill(self, reqs, pos_of, air_of, stream):
+    def _fill(self, reqs, pos_of, air_of, stream, pins=None):
         """Cache entries of the array layers of every request; computes and
         inserts the missing ones.  pos_of(b) lists request b's array
         positions; air_of(b) = (kz_air, wln, row) locates its air reference
         in the device tensors of its order set.  Returns {(b, pos): cache
         key} and the distinct entries used {key: entry}."""
         with self.lock:
-            return self._fill_locked(reqs, pos_of, air_of, stream)
+            key_at, used = self._fill_locked(reqs, pos_of, air_of, stream)
+            if pins is not None:
+                pins.extend(used.values())
+            return key_at, used
+
+    def _unpin(self, pins):
+        """Release the entries a batch pinned when its launch failed."""
+        with self.lock:
+            for e in pins:
+                e.users -= 1
+            self.cache.evict()
 
     def _fill_locked(self, reqs, pos_of, air_of, stream):
         cache = self.cache
@@ -401,8 +411,18 @@ class ArrayBatcher(object):
         return out
 
     def launch(self, reqs, stream, slot_key):
-        """Queue one batch on ``stream``; returns (event, finish) where
-        finish() -> list of per-request results (dicts) or exceptions."""
+        """Queue one batch of array requests of one signature on ``stream``;
+        returns (event, finish) where finish() -> list of per-request results
+        (dicts) or exceptions.  A launch that fails releases the cache
+        entries it pinned before raising."""
+        pins = []
+        try:
+            return self._launch_grouped(reqs, stream, slot_key, pins)
+        except Exception:
+            self._unpin(pins)
+            raise
+
+    def _launch_grouped(self, reqs, stream, slot_key, pins):
         r0 = reqs[0]
         B, npw = len(reqs), r0.npw
         P = 2 * npw
@@ -450,7 +470,7 @@ class ArrayBatcher(object):
                     np_sub = npj
                 if j == L - 1:
                     np_top = npj
-            key_at, used = self._fill(reqs, lambda b: arr_pos, lambda b: (kz_air, wln, b), stream)
+            key_at, used = self._fill(reqs, lambda b: arr_pos, lambda b: (kz_air, wln, b), stream, pins)
             for j in arr_pos:
                 keys = [key_at[(b, j)] for b in range(B)]
                 es = [used[k] for k in keys]
@@ -518,7 +538,17 @@ class ArrayBatcher(object):
         return finish
 
     def launch_uneven(self, reqs, stream, slot_key, ws_budget_bytes):
-        """Queue array requests of ANY shapes as one uneven batch on
+        """Array requests of any shapes as one uneven batch (see
+        _launch_uneven); releases its pinned cache entries if it fails."""
+        pins = []
+        try:
+            return self._launch_uneven(reqs, stream, slot_key, ws_budget_bytes, pins)
+        except Exception:
+            self._unpin(pins)
+            raise
+
+    def _launch_uneven(self, reqs, stream, slot_key, ws_budget_bytes, pins):
+        """Queues array requests of ANY shapes as one uneven batch on
         ``stream``: film modes and interfaces per order set, cached array
         interfaces, then one emu_stack_var_batch launch for every cascade.
         Returns (event, finish) as ``launch``."""
@@ -583,7 +613,7 @@ class ArrayBatcher(object):
                 order += bs
             key_at, used = self._fill(
                 reqs, lambda b: [j for j, ly in enumerate(reqs[b].layers) if isinstance(ly, ArrayLayer)],
-                lambda b: air[b], stream)
+                lambda b: air[b], stream, pins)
             stacks = []
             inc_keep = []
             for b in order:

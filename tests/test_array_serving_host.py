@@ -86,3 +86,18 @@ def test_array_request_validation_and_signature():
     inc[3] = 1
     r3 = ArrayRequest([1.46, ly, 1.0], [100.0], 600.0, [0, 0], 500.0, 2, incoming=inc)
     assert r3.pol == 'incoming' and r3.signature[5] == 'incoming'
+
+
+def test_failed_launch_releases_pinned_entries():
+    """A batch whose launch raises after pinning cache entries gives them back,
+    so the cache can evict them again."""
+    from emustack_b200.array_serving import ArrayBatcher, SMatrixCache
+    cache = SMatrixCache(100)
+    batcher = ArrayBatcher('cpu', cache)
+    a, b = _E(60), _E(60)
+    a.users = b.users = 1
+    cache.put('a', a)
+    cache.put('b', b)
+    assert cache.bytes == 120                       # both pinned: over capacity
+    batcher._unpin([a, b])
+    assert a.users == 0 and b.users == 0 and cache.bytes <= 100
