@@ -14,7 +14,7 @@ Arms
                `e2e` repeats the step through the public host-to-host API
                (FilmHostPipeline) with pinned host inputs: host->device
                copies, the solves and the device->host read of R_net/T_net
-               diagonals and a/t/r lists, in 8192-point pieces on two
+               diagonals and a/t/r lists, in 4096-point pieces on four
                streams so copies overlap solves.
   reference  : the reference's FP64 algorithm (the CPU oracle, a numpy
                restatement of backend/stack.py + backend/mode_calcs.py) on the
@@ -40,7 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_WL, N_ANG, N_FILMS = 2048, 16, 10
-E2E_CHUNK = 8192   # points per piece of the host-to-host pipeline
+E2E_CHUNK, E2E_STREAMS = 4096, 4   # pieces of the host-to-host pipeline and their streams
 PERIOD, MAX_ORDER, POL = 500.0, 5, 'TE'
 METRIC = 'R/T/A spectral points/s (batched thin-film GSM, FP64)'
 L2_FLUSH_BYTES = 256 << 20
@@ -231,7 +231,7 @@ def run_ours(args, rank, world, local_rank):
     # T_net diagonals and a/t/r lists, in pieces whose copies overlap the
     # solves of their neighbours
     from emustack_b200.films import FilmHostPipeline
-    pipe = FilmHostPipeline(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev, chunk=E2E_CHUNK)
+    pipe = FilmHostPipeline(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev, chunk=E2E_CHUNK, n_streams=E2E_STREAMS)
     h_wl = torch.from_numpy(w['wl']).pin_memory()
     h_kp = torch.from_numpy(w['k_pll']).pin_memory()
     h_n = torch.from_numpy(w['n']).pin_memory()
