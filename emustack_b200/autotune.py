@@ -27,8 +27,9 @@ class Autotuner(object):
     """time_fn(run, choice, stream) -> milliseconds per launch; the default
     times ``reps`` launches with CUDA events after ``warmup`` launches."""
 
-    def __init__(self, path=None, warmup=1, reps=3, time_fn=None):
+    def __init__(self, path=None, warmup=1, reps=3, time_fn=None, tie=0.02):
         self.path = path if path is not None else os.environ.get('EMUSTACK_AUTOTUNE_CACHE')
+        self.tie = float(tie)
         self.time_fn = time_fn or self._cuda_time
         self.enabled = os.environ.get('EMUSTACK_AUTOTUNE', '1') != '0'
         self.warmup, self.reps = warmup, reps
@@ -84,7 +85,10 @@ class Autotuner(object):
                 errors[json.dumps(c)] = e
         if not times:
             raise next(iter(errors.values()))
-        best = min(times, key=times.get)
+        # the first candidate (in the caller's order) within `tie` of the
+        # fastest: near-equal timings do not flip the choice from run to run
+        fastest = min(times.values())
+        best = next(k for k in times if times[k] <= fastest * (1.0 + self.tie))
         entry = {'choice': json.loads(best), 'ms': times}
         with self._lock:
             self.cache[key] = entry

@@ -56,3 +56,15 @@ def test_failing_candidate_is_skipped():
         return {0: 2.0, 1: 3.0}[c]
     at = Autotuner(path='', time_fn=t)
     assert at.choose('film_stack', {'L': 3}, [0, 1, 2], lambda c: None, 0) == 0
+
+
+def test_near_ties_keep_the_first_candidate():
+    """Candidates within 2 % of the fastest count as a tie, and the first of
+    them in the caller's order wins, so noise does not flip the choice."""
+    from emustack_b200.autotune import Autotuner
+    ms = {0: 2.50, 1: 3.90, 4: 2.44, 5: 2.40}
+    t = Autotuner(path='', time_fn=lambda run, c, s: ms[c])
+    assert t.choose('k', {'n': 1}, [0, 1, 4, 5], lambda c: None, 0) == 4   # 2.44 within 2 % of 2.40, 2.50 not
+    ms2 = {0: 2.44, 1: 3.90, 4: 2.46, 5: 2.40}
+    t2 = Autotuner(path='', time_fn=lambda run, c, s: ms2[c])
+    assert t2.choose('k', {'n': 1}, [0, 1, 4, 5], lambda c: None, 0) == 0
