@@ -25,6 +25,12 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
          '-Xcompiler', '-ffp-contract=off', '--expt-relaxed-constexpr',
          '-I' + os.path.join(ROOT, 'include')]
+# Sources whose floating-point operations keep the roundings written in the
+# source: with -fmad=false every multiply and add is emitted with an explicit
+# rounding mode, so the assembler fuses none of them and every launch variant
+# of a kernel (other register budgets, other schedules) returns the same bits.
+# The fused multiply-adds of these files are their explicit fma() calls.
+EXACT_ROUNDING = {'film_stack.cu', 'film_varlen.cu'}
 
 
 def nvcc():
@@ -55,7 +61,8 @@ def build_library(force=False, verbose=False):
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + '.o')
         if not force and not _newer([src] + headers, obj):
             return obj
-        cmd = [cc] + ARCH + FLAGS + ['-c', src, '-o', obj]
+        extra = ['-fmad=false'] if os.path.basename(src) in EXACT_ROUNDING else []
+        cmd = [cc] + ARCH + FLAGS + extra + ['-c', src, '-o', obj]
         if verbose:
             print(' '.join(cmd))
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -22,10 +22,20 @@ __host__ __device__ __forceinline__ cd csub(cd a, cd b) { return cd{a.x - b.x, a
 __host__ __device__ __forceinline__ cd cneg(cd a) { return cd{-a.x, -a.y}; }
 __host__ __device__ __forceinline__ cd cconj(cd a) { return cd{a.x, -a.y}; }
 __host__ __device__ __forceinline__ cd cscale(cd a, double s) { return cd{a.x * s, a.y * s}; }
-__host__ __device__ __forceinline__ cd cmul(cd a, cd b) {
-  return cd{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+// Products and squared magnitudes with their roundings written out (one
+// rounded product, one fused multiply-add), so that every kernel inlining
+// them rounds alike whatever contraction the compiler would choose.
+__host__ __device__ __forceinline__ double rmul(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
 }
-__host__ __device__ __forceinline__ double cabs2(cd a) { return a.x * a.x + a.y * a.y; }
+__host__ __device__ __forceinline__ cd cmul(cd a, cd b) {
+  return cd{fma(a.x, b.x, -rmul(a.y, b.y)), fma(a.x, b.y, rmul(a.y, b.x))};
+}
+__host__ __device__ __forceinline__ double cabs2(cd a) { return fma(a.x, a.x, rmul(a.y, a.y)); }
 __host__ __device__ __forceinline__ double cabsd(cd a) { return hypot(a.x, a.y); }
 __host__ __device__ __forceinline__ bool cis_zero(cd a) { return a.x == 0.0 && a.y == 0.0; }
 

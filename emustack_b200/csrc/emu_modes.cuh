@@ -62,7 +62,7 @@ __device__ __forceinline__ Fresnel fresnel(cd z1, cd z2) {
 }
 
 __device__ __forceinline__ cd shear_phase(double alpha, double beta, double c0, double c1, int ncoord) {
-  double th = (ncoord == 1) ? alpha * c0 : alpha * c0 + beta * c1;
+  double th = (ncoord == 1) ? __dmul_rn(alpha, c0) : __dadd_rn(__dmul_rn(alpha, c0), __dmul_rn(beta, c1));
   double s, c;
   sincos(th, &s, &c);
   return cd{c, s};

@@ -16,18 +16,23 @@ constexpr int kSave = 5;  // saved scalars per (layer, polarisation)
 
 struct LayerC {
   cd k, zcr, ik;  // wavenumber, 1/n, 1/k
+  cd zk, zka;     // k / n and k_air / n (k_air real)
 };
 
 // Shared-memory layout of one point's slot (byte offsets); a slot sized for
 // (npw, L) also holds any point with fewer orders and layers.
 struct SlotSmem {
-  int keys, rank, wood, nprop, acc, lay, h, misc, stride;
+  int keys, rank, wood, nprop, acc, lay, h, misc, ws, stride;
 };
 
-__host__ __device__ inline SlotSmem slot_layout(int npw, int L) {
+// with_ws: room for the flux-pass scalars of the one order that carries
+// light ([L][2][kSave]), for every polarisation but incoming amplitudes
+// (whose scalars, one set per order, stay in the global workspace).
+__host__ __device__ inline SlotSmem slot_layout(int npw, int L, bool with_ws = true) {
   SlotSmem s;
   int o = 0;
   s.lay = o; o += (int)sizeof(LayerC) * L;
+  s.ws = o; o += with_ws ? (int)sizeof(cd) * L * 2 * kSave : 0;
   s.acc = o; o += 16 * (L + 1);
   s.keys = o; o += 8 * npw;
   s.h = o; o += 8 * (L > 2 ? L - 2 : 1);
@@ -96,22 +101,63 @@ __device__ __forceinline__ cd flux_term(cd fm, cd fp, bool prop, bool tm) {
   return tm ? cneg(te) : te;
 }
 
+// Transmission coefficient T12 = T21 of the air / layer interface for
+// polarisation q (0 TE, 1 TM): 2 sqrt(z2) sqrt(z1) / (z2 + z1) with the
+// impedances z1 of air and z2 of the layer (backend/mode_calcs.py:199-218,
+// 451-477), principal square roots as numpy takes them.
+__device__ __forceinline__ cd t12_exact(const LayerC &c, cd kz, double kair, cd kz_air, int q) {
+  cd z1, z2;
+  if (q == 0) {
+    z1 = cscale(crcp_nr(kz_air), kair);
+    z2 = cmul(c.zcr, cmul(c.k, crcp_nr(kz)));
+  } else {
+    z1 = cscale(kz_air, 1.0 / kair);
+    z2 = cmul(c.zcr, cmul(kz, c.ik));
+  }
+  const cd is = crcp_nr(cadd(z2, z1));
+  return cmul(cscale(cmul(csqrt_nr(z2), csqrt_nr(z1)), 2.0), is);
+}
+
 // Cascade of one order (both polarisations) bottom to top, then, if the
 // order carries incident light, its flux pass top to bottom.
+//
+// The reference builds each interface from z1, z2 as R12 = (z2 - z1)/(z2 + z1)
+// and T12 = T21 = 2 sqrt(z2 z1)/(z2 + z1) and runs the recursion of
+// backend/stack.py:229-278 on them.  Here, for a layer between two air gaps:
+//  * z1 and z2 are scaled by k_z k_z,air (TE) or k k_air (TM), which leaves
+//    R12 unchanged and removes the quotient inside each impedance:
+//    R12 = (A - B)/(A + B) with A = k k_z,air / n, B = k_air k_z (TE) and
+//    A = k_air k_z / n, B = k k_z,air (TM);
+//  * T12 enters the reflection recursion only as T12 T21 = 4 A B/(A + B)^2,
+//    and the transmission and the downward gap fields of the flux pass only
+//    as the product over one layer x1 p x2 = T12 T21 p / (d1 d2), with
+//    d1 = 1 - R12 r (gap) and d2 = 1 + R12 p^2 r (film, p = exp(i k_z h)),
+//    so no square root is taken for them.
+// The outer layers (substrate, superstrate) and the optional per-layer
+// outputs (layer_rt, vec_coef) take T12 itself from t12_exact.  Every
+// result is the same whichever optional outputs are requested.
+// R12 and T12 T21 of the air / layer interface for polarisation q from the
+// scaled impedances A, B described above.
+__device__ __forceinline__ void iface_scaled(const LayerC &c, cd kz, double kair, cd kz_air, int q,
+                                             cd &R12, cd &TT) {
+  const cd A = q ? cmul(c.zka, kz) : cmul(c.zk, kz_air);
+  const cd Bz = q ? cmul(kz_air, c.k) : cscale(kz, kair);
+  const cd is = crcp_nr(cadd(A, Bz));
+  R12 = cmul(csub(A, Bz), is);
+  TT = cmul(cscale(cmul(A, Bz), 4.0), cmul(is, is));
+}
+
 template <class Pt>
 __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec, const LayerC *lay,
                             const double *hsm, const unsigned *wood, bool wood_air, double a0,
                             double b0, double sa0, double sb0, double wln, int np_air, int np_in,
-                            int np_out, cd *acc, int *nprop, bool count) {
+                            int np_out, cd *acc, int *nprop, bool count, cd *ws_smem) {
   const int L = p.L(), npw = p.npw(), P = 2 * npw;
   const int px = p.px()[u], py = p.py()[u];
   double al_air, be_air;
   order_ab(p.world_1d(), p.dy(), px, py, wood_air ? sa0 : a0, wood_air ? sb0 : b0, al_air, be_air);
-  const cd kair = wavenumber(cd{1.0, 0.0}, wln);
-  const cd kz_air = csqrt_p(kz_arg(kair, al_air, be_air));
-  // air impedances (1/n = 1): Z_TE = k/kz, Z_TM = kz/k
-  const cd z1[2] = {cmul(kair, crcp_nr(kz_air)), cmul(kz_air, crcp_nr(kair))};
-  const cd sz1[2] = {csqrt_nr(z1[0]), csqrt_nr(z1[1])};
+  const double kair = wavenumber(cd{1.0, 0.0}, wln).x;
+  const cd kz_air = csqrt_p(kz_arg(cd{kair, 0.0}, al_air, be_air));
   const double *sh = p.shears();
   double al_sh = 0.0, be_sh = 0.0;
   if (sh)
@@ -119,81 +165,120 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
              be_sh);
   const cd din[2] = {incidence(p, j, spec), incidence(p, j + npw, spec)};
   const bool active = !cis_zero(din[0]) || !cis_zero(din[1]);
-  const int aslot = p.slot_per_order() ? u : 0;
-  cd *wsv = p.ws() + ((size_t)aslot * L) * 2 * kSave;
-  cd tnet[2], rnet[2];
-  for (int l = 0; l < L; ++l) {
+  const bool want_vec = p.vcd() != nullptr;
+  const bool all_t = want_vec || p.layer_rt() != nullptr;
+  // flux-pass scalars: in the point's shared-memory slot when one order
+  // carries light, else per order in the global workspace
+  cd *wsv = p.slot_per_order() ? p.ws() + ((size_t)u * L) * 2 * kSave : ws_smem;
+  // k_z of the order in layer l (also stored when requested)
+  auto layer_kz = [&](int l) -> cd {
     const bool wl_l = (wood[l >> 5] >> (l & 31)) & 1u;
     double al, be;
     order_ab(p.world_1d(), p.dy(), px, py, wl_l ? sa0 : a0, wl_l ? sb0 : b0, al, be);
-    const LayerC c = lay[l];
-    const cd kz = csqrt_p(kz_arg(c.k, al, be));
-    const bool fin = (l >= 1 && l < L - 1);
-    if (count && fin && kz.y == 0.0) atomicAdd(&nprop[l], 1);
+    const cd kz = csqrt_p(kz_arg(lay[l].k, al, be));
     if (p.kz()) store_c(p.kz(), (size_t)l * npw + j, kz);
-    // Z_TE = (1/n) k / kz ; Z_TM = (1/n) kz / k
-    const cd z2[2] = {cmul(c.zcr, cmul(c.k, crcp_nr(kz))), cmul(c.zcr, cmul(kz, c.ik))};
-    const cd pr = fin ? cexp_ikh(kz, hsm[l - 1] / p.period()) : cd{1.0, 0.0};
-    cd Q = cd{1.0, 0.0}, Qi = cd{1.0, 0.0};
-    if (sh && l >= 1) {
-      double c0, c1;
-      if (l < L - 1) {
-        c0 = sh[2 * (l - 1)] - sh[2 * l];
-        c1 = sh[2 * (l - 1) + 1] - sh[2 * l + 1];
-      } else {
-        c0 = sh[2 * l];
-        c1 = sh[2 * l + 1];
-      }
-      Q = shear_phase(al_sh, be_sh, c0, c1, p.ncoord());
-      Qi = shear_phase(al_sh, be_sh, -1 * c0, -1 * c1, p.ncoord());
+    return kz;
+  };
+  // shear phase Q of the gap below layer l and its inverse (backend/stack.py:236-244, 267-275)
+  auto shear_q = [&](int l, cd &Q, cd &Qi) {
+    Q = cd{1.0, 0.0};
+    Qi = cd{1.0, 0.0};
+    if (!sh) return;
+    double c0, c1;
+    if (l < L - 1) {
+      c0 = sh[2 * (l - 1)] - sh[2 * l];
+      c1 = sh[2 * (l - 1) + 1] - sh[2 * l + 1];
+    } else {
+      c0 = sh[2 * l];
+      c1 = sh[2 * l + 1];
     }
+    Q = shear_phase(al_sh, be_sh, c0, c1, p.ncoord());
+    Qi = shear_phase(al_sh, be_sh, -1 * c0, -1 * c1, p.ncoord());
+  };
+  auto store_rt = [&](int l, int q, cd R12, cd T12) {
+    if (!p.layer_rt()) return;
+    const size_t o = (size_t)l * 2 * P;
+    store_c(p.layer_rt(), o + j + q * npw, R12);
+    store_c(p.layer_rt(), o + P + j + q * npw, T12);
+  };
+  cd tnet[2], rnet[2];
+  // substrate (l = 0)
+  {
+    const LayerC c = lay[0];
+    const cd kz = layer_kz(0);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      const cd is = crcp_nr(cadd(z2[q], z1[q]));
-      const cd R12 = cmul(csub(z2[q], z1[q]), is);
-      const cd T12 = cmul(cscale(cmul(csqrt_nr(z2[q]), sz1[q]), 2.0), is);
-      const cd R21 = cneg(R12), T21 = T12;
-      if (p.layer_rt()) {
-        const size_t o = (size_t)l * 2 * P;
-        store_c(p.layer_rt(), o + j + q * npw, R12);
-        store_c(p.layer_rt(), o + P + j + q * npw, T12);
-      }
-      cd *sv = wsv + ((size_t)l * 2 + q) * kSave;
-      if (l == 0) {
-        tnet[q] = T12;
-        rnet[q] = R12;
-        if (active) {
-          sv[0] = rnet[q];
-          sv[1] = tnet[q];
-        }
-        continue;
-      }
-      // air gap below layer l (backend/stack.py:229-247, 263-278)
-      cd x1;
-      if (sh) {
-        const cd rq = cmul(cmul(Qi, rnet[q]), Q);
-        x1 = cmul(T21, crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rq))));
-        tnet[q] = cmul(cmul(tnet[q], Q), x1);
-        rnet[q] = cadd(R21, cmul(cmul(T12, rq), x1));
-      } else {
-        x1 = cmul(T21, crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rnet[q]))));
-        tnet[q] = cmul(tnet[q], x1);
-        rnet[q] = cadd(R21, cmul(cmul(T12, rnet[q]), x1));
-      }
+      cd R12, TT;
+      iface_scaled(c, kz, kair, kz_air, q, R12, TT);
+      const cd T12 = t12_exact(c, kz, kair, kz_air, q);
+      store_rt(0, q, R12, T12);
+      tnet[q] = T12;
+      rnet[q] = R12;
       if (active) {
+        cd *sv = wsv + (size_t)q * kSave;
+        sv[0] = R12;
+        sv[1] = T12;
+      }
+    }
+  }
+  // films between air gaps (backend/stack.py:229-262)
+  for (int l = 1; l < L - 1; ++l) {
+    const LayerC c = lay[l];
+    const cd kz = layer_kz(l);
+    if (count && kz.y == 0.0) atomicAdd(&nprop[l], 1);
+    const cd pr = cexp_ikh(kz, hsm[l - 1] / p.period());
+    const cd pr2 = cmul(pr, pr);
+    cd Q, Qi;
+    shear_q(l, Q, Qi);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      cd R12, TT;
+      iface_scaled(c, kz, kair, kz_air, q, R12, TT);
+      const cd T12 = all_t ? t12_exact(c, kz, kair, kz_air, q) : cd{0.0, 0.0};
+      store_rt(l, q, R12, T12);
+      // air gap below layer l
+      const cd rq = sh ? cmul(cmul(Qi, rnet[q]), Q) : rnet[q];
+      const cd d1 = crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rq)));
+      const cd ug = cmul(TT, d1);
+      const cd rg = csub(cmul(ug, rq), R12);
+      // through layer l
+      const cd prr = cmul(pr2, rg);
+      const cd d2 = crcp_nr(cadd(cd{1.0, 0.0}, cmul(R12, prr)));
+      const cd g = cmul(ug, cmul(pr, d2));  // x1 p x2
+      tnet[q] = cmul(sh ? cmul(tnet[q], Q) : tnet[q], g);
+      rnet[q] = cadd(R12, cmul(cmul(TT, prr), d2));
+      if (active) {
+        cd *sv = wsv + ((size_t)l * 2 + q) * kSave;
+        sv[0] = g;
+        sv[1] = rg;
+        sv[2] = pr;
+        if (want_vec) sv[3] = cmul(T12, d2);
+        sv[4] = rnet[q];
+      }
+    }
+  }
+  // superstrate (l = L - 1): the air gap below it (backend/stack.py:263-278)
+  {
+    const int l = L - 1;
+    const LayerC c = lay[l];
+    const cd kz = layer_kz(l);
+    cd Q, Qi;
+    shear_q(l, Q, Qi);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      cd R12, TT;
+      iface_scaled(c, kz, kair, kz_air, q, R12, TT);
+      const cd T12 = t12_exact(c, kz, kair, kz_air, q);
+      store_rt(l, q, R12, T12);
+      const cd rq = sh ? cmul(cmul(Qi, rnet[q]), Q) : rnet[q];
+      const cd d1 = crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rq)));
+      const cd x1 = cmul(T12, d1);
+      tnet[q] = cmul(sh ? cmul(tnet[q], Q) : tnet[q], x1);
+      rnet[q] = csub(cmul(cmul(TT, d1), rq), R12);
+      if (active) {
+        cd *sv = wsv + ((size_t)l * 2 + q) * kSave;
         sv[0] = x1;
         sv[1] = rnet[q];
-      }
-      if (!fin) continue;
-      // through layer l (backend/stack.py:249-262)
-      const cd x2 = cmul(T12, crcp_nr(csub(cd{1.0, 0.0}, cmul(cmul(cmul(R21, pr), rnet[q]), pr))));
-      const cd px2 = cmul(pr, x2);
-      tnet[q] = cmul(tnet[q], px2);
-      rnet[q] = cadd(R12, cmul(cmul(cmul(T21, pr), rnet[q]), px2));
-      if (active) {
-        sv[2] = pr;
-        sv[3] = x2;
-        sv[4] = rnet[q];
       }
     }
   }
@@ -203,7 +288,6 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
   store_c(p.T_net(), j + npw, tnet[1]);
 
   // ---- flux pass (backend/stack.py:323-366)
-  const bool want_vec = p.vcd() != nullptr;
   if (!active) {
     if (want_vec) {
       for (int lv = 0; lv < L; ++lv)
@@ -235,13 +319,13 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
       const cd fl = flux_term(f1m, f1p, prop, q == 1);
       atomicAdd(&acc[1 + i].x, fl.x);
       atomicAdd(&acc[1 + i].y, fl.y);
-      const cd f2m = cmul(s[3], f1m);
-      const cd f2p = cmul(cmul(s[1], s[2]), f2m);
       if (want_vec) {
+        const cd f2m = cmul(s[3], f1m);
+        const cd f2p = cmul(cmul(s[1], s[2]), f2m);
         store_c(p.vcd(), (size_t)(1 + i) * P + pos, f2m);
         store_c(p.vcu(), (size_t)(1 + i) * P + pos, f2p);
       }
-      f1m = cmul(cmul(s[0], s[2]), f2m);
+      f1m = cmul(s[0], f1m);
     }
     const cd *s0 = wsv + ((size_t)0 * 2 + q) * kSave;
     const cd f2m = cmul(s0[1], f1m);
@@ -270,6 +354,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
   int *rank = (int *)(base + S.rank);
   int *nprop = (int *)(base + S.nprop);
   unsigned *wood = (unsigned *)(base + S.wood);
+  cd *ws_smem = (cd *)(base + S.ws);
   int *misc = (int *)(base + S.misc);
   const int lt = tm.lt, team = tm.size;
   const int L = valid ? p.L() : 2, npw = valid ? p.npw() : 1;
@@ -291,6 +376,8 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       c.k = wavenumber(n, wln);
       c.zcr = crecip(n);
       c.ik = crecip(c.k);
+      c.zk = cmul(c.zcr, c.k);
+      c.zka = cscale(c.zcr, wavenumber(cd{1.0, 0.0}, wln).x);
       lay[i] = c;
     }
     for (int i = lt; i < L - 2; i += team) hsm[i] = p.height(i);
@@ -372,7 +459,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
     const int np_air = nprop[L], np_in = nprop[L - 1], np_out = nprop[0];
     for (int u = lt; u < npw; u += team)
       solve_order(p, u, rank[u], spec, lay, hsm, wood, wood_air, a0, b0, sa0, sb0, wln, np_air,
-                  np_in, np_out, acc, nprop, count);
+                  np_in, np_out, acc, nprop, count, ws_smem);
   }
   // ---------------------------------------------------------- phase 5
   if (tm.any(layer_wood)) {
@@ -400,7 +487,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       const int np_air = nprop[L], np_in = nprop[L - 1], np_out = nprop[0];
       for (int u = lt; u < npw; u += team)
         solve_order(p, u, rank[u], spec, lay, hsm, wood, wood_air, a0, b0, sa0, sb0, wln, np_air,
-                    np_in, np_out, acc, nprop, count);
+                    np_in, np_out, acc, nprop, count, ws_smem);
     }
   }
   tm.sync();

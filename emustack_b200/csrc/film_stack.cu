@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) film_stack_kernel(FilmAr
   const int team = a.team, ppc = a.ppc;
   const int slot = threadIdx.x / team;
   const bool in_slot = slot < ppc;
-  const SlotSmem S = slot_layout(p.n_pw, p.n_layers);
+  const SlotSmem S = slot_layout(p.n_pw, p.n_layers, p.pol != EMU_POL_INCOMING);
   unsigned char *base = smem + (in_slot ? slot : 0) * S.stride;
   const CtaTeam tm{(int)(threadIdx.x % team), team};
   for (int bb = blockIdx.x * ppc; bb < B; bb += gridDim.x * ppc) {
@@ -157,10 +157,10 @@ Launch plan(const EmuFilmStackBatch *p) {
   l.team = p->n_pw <= threads ? p->n_pw : threads;
   l.ppc = threads / l.team;
   // at most kMaxCtaSmem of slots per CTA (small order sets, many points)
-  const int stride = slot_layout(p->n_pw, p->n_layers).stride;
+  const int stride = slot_layout(p->n_pw, p->n_layers, p->pol != EMU_POL_INCOMING).stride;
   if (l.ppc * stride > kMaxCtaSmem) l.ppc = kMaxCtaSmem / stride > 0 ? kMaxCtaSmem / stride : 1;
   l.n_act = (p->pol == EMU_POL_INCOMING) ? p->n_pw : 1;
-  l.smem = (size_t)slot_layout(p->n_pw, p->n_layers).stride * l.ppc;
+  l.smem = (size_t)stride * l.ppc;
   return l;
 }
 
@@ -178,7 +178,7 @@ int validate(const EmuFilmStackBatch *p) {
   if ((p->d_vec_coef_down == nullptr) != (p->d_vec_coef_up == nullptr)) return EMU_E_ARG;
   if (p->d_shears && p->shear_ncoord != 1 && p->shear_ncoord != 2) return EMU_E_ARG;
   if (p->variant < 0 || p->variant >= kVariants) return EMU_E_ARG;
-  if (slot_layout(p->n_pw, p->n_layers).stride > kMaxCtaSmem) return EMU_E_SHAPE;
+  if (slot_layout(p->n_pw, p->n_layers, p->pol != EMU_POL_INCOMING).stride > kMaxCtaSmem) return EMU_E_SHAPE;
   return EMU_OK;
 }
 
