@@ -39,7 +39,7 @@ __host__ __device__ inline SlotSmem slot_layout(int npw, int L, bool with_ws = t
   s.rank = o; o += 4 * npw;
   s.nprop = o; o += 4 * (L + 1);
   s.wood = o; o += 4 * ((L + 1 + 31) / 32);
-  s.misc = o; o += 16;  // [0] specular order, [1] layer-Wood flag
+  s.misc = o; o += 16;  // [0] specular order, [1] layer-Wood flag, [2] non-finite list entry
   s.stride = (o + 15) / 16 * 16;
   return s;
 }
@@ -337,6 +337,14 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
   atomicAdd(&acc[L - 1].x, out_sum);
 }
 
+// Sort key of -Re k_z + Im k_z as an unsigned integer with the order of the
+// doubles (sign bit flipped for positive values, all bits for negative
+// ones; -0 taken as +0, as the double comparison does).
+__device__ __forceinline__ unsigned long long sort_key(double k) {
+  const long long b = __double_as_longlong(k + 0.0);
+  return b < 0 ? ~(unsigned long long)b : (unsigned long long)b | 0x8000000000000000ull;
+}
+
 // One point, phases 0-6 (the film kernels' header comments describe them).
 // Every thread of the team calls this with the same `valid`, and with
 // `valid` false takes the same barriers without touching memory.  The point
@@ -349,7 +357,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
                                            unsigned char *base, const SlotSmem &S) {
   LayerC *lay = (LayerC *)(base + S.lay);
   cd *acc = (cd *)(base + S.acc);
-  double *keys = (double *)(base + S.keys);
+  unsigned long long *keys = (unsigned long long *)(base + S.keys);
   double *hsm = (double *)(base + S.h);
   int *rank = (int *)(base + S.rank);
   int *nprop = (int *)(base + S.nprop);
@@ -389,6 +397,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
     if (lt == 0) {
       misc[0] = -1;
       misc[1] = 0;
+      misc[2] = 0;
     }
   }
   tm.sync();
@@ -400,7 +409,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], a0, b0, al, be);
       const cd kz = csqrt_p(kz_arg(kair, al, be));
       if (cis_zero(kz)) atomicOr(&wood[L >> 5], 1u << (L & 31));
-      keys[u] = -1 * kz.x + kz.y;
+      keys[u] = sort_key(-1 * kz.x + kz.y);
       if (kz.y == 0.0) atomicAdd(&nprop[L], 1);
     }
   }
@@ -416,7 +425,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
         double al, be;
         order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], sa0, sb0, al, be);
         const cd kz = csqrt_p(kz_arg(kair, al, be));
-        keys[u] = -1 * kz.x + kz.y;
+        keys[u] = sort_key(-1 * kz.x + kz.y);
         if (kz.y == 0.0) atomicAdd(&nprop[L], 1);
       }
     }
@@ -426,11 +435,12 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
   if (valid) {
     int32_t *so = p.sort_order();
     for (int u = lt; u < npw; u += team) {
-      const double ku = keys[u];
+      const unsigned long long ku = keys[u];
       int r = 0;
+#pragma unroll 4
       for (int v = 0; v < npw; ++v) {
-        const double kv = keys[v];
-        r += (kv < ku) || (kv == ku && v < u);
+        const unsigned long long kv = keys[v];
+        r += (kv < ku) | ((kv == ku) & (v < u));
       }
       rank[u] = r;
       const int pxu = p.px()[u], pyu = p.py()[u];
@@ -492,15 +502,13 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
   }
   tm.sync();
   // ---------------------------------------------------------- phase 6
-  if (valid && lt == 0) {
-    uint32_t flags = 0;
-    if (wood_air) flags |= EMU_PT_WOOD_AIR;
-    if (layer_wood) flags |= EMU_PT_WOOD_LAYER;
+  // a_list / t_list / r_list (backend/stack.py:368-426), one entry per
+  // thread of the team; the flags word once every entry is checked
+  int nprop_in0 = 0, nprop_out0 = 0;
+  if (valid) {
     const int np_in = nprop[L - 1], np_out = nprop[0];
-    if (np_out == 0) flags |= EMU_PT_NO_PROP_SUB;
-    if (np_in == 0) flags |= EMU_PT_NO_PROP_SUP;
-    double *al = p.a_list();
-    double *tl = p.t_list();
+    nprop_in0 = np_in;
+    nprop_out0 = np_out;
     const double df0 = acc[0].x, up0 = acc[L].x, dsub = acc[L - 1].x;
     // |down_fluxes[i]| with down_fluxes = [df0, gap_1..gap_{L-2}, dsub]
     auto dfa = [&](int i) -> double {
@@ -508,35 +516,47 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       if (i == L - 1) return fabs(dsub);
       return hypot(acc[i].x, acc[i].y);
     };
-    double rr = 0.0;
-    if (np_out != 0) {
-      for (int i = 1; i <= L - 2; ++i) al[i - 1] = fabs(dfa(i) - dfa(i + 1));
-      al[L - 2] = fabs(df0 - dsub - up0);
-      for (int i = 0; i <= L - 3; ++i) tl[i] = fabs(dfa(i + 2) / dfa(i));
-      tl[L - 2] = fabs(dsub / df0);
-      rr = fabs(up0 / df0);
-    } else {
-      for (int i = 0; i < L - 1; ++i) {
-        al[i] = 0.0;
-        tl[i] = 0.0;
+    double *al = p.a_list();
+    double *tl = p.t_list();
+    bool fin = true;
+    for (int i = lt; i < L - 1; i += team) {
+      double a = 0.0, t = 0.0;
+      if (np_out != 0) {
+        a = (i < L - 2) ? fabs(dfa(i + 1) - dfa(i + 2)) : fabs(df0 - dsub - up0);
+        t = (i < L - 2) ? fabs(dfa(i + 2) / dfa(i)) : fabs(dsub / df0);
       }
+      al[i] = a;
+      tl[i] = t;
+      fin = fin && isfinite(a) && isfinite(t);
     }
-    *p.r_list() = rr;
-    bool fin = isfinite(rr);
-    for (int i = 0; i < L - 1; ++i) fin = fin && isfinite(al[i]) && isfinite(tl[i]);
-    if (!fin) flags |= EMU_PT_NONFINITE;
-    *p.flags() = flags;
-    if (p.specular()) *p.specular() = misc[0];
+    if (lt == 0) {
+      const double rr = (np_out != 0) ? fabs(up0 / df0) : 0.0;
+      *p.r_list() = rr;
+      fin = fin && isfinite(rr);
+      if (p.specular()) *p.specular() = misc[0];
+    }
+    if (!fin) atomicOr(&misc[2], 1);
     if (int32_t *np = p.num_prop())
-      for (int i = 0; i <= L; ++i) np[i] = nprop[i];
+      for (int i = lt; i <= L; i += team) np[i] = nprop[i];
     if (double *fo = p.fluxes()) {
-      for (int i = 0; i <= L; ++i) {
+      for (int i = lt; i <= L; i += team) {
         fo[2 * i] = acc[i].x;
         fo[2 * i + 1] = acc[i].y;
       }
     }
   }
   tm.sync();
+  // only misc[2] is read after the barrier, by the thread that resets it in
+  // phase 0 of the team's next point
+  if (valid && lt == 0) {
+    uint32_t flags = 0;
+    if (wood_air) flags |= EMU_PT_WOOD_AIR;
+    if (layer_wood) flags |= EMU_PT_WOOD_LAYER;
+    if (nprop_out0 == 0) flags |= EMU_PT_NO_PROP_SUB;
+    if (nprop_in0 == 0) flags |= EMU_PT_NO_PROP_SUP;
+    if (misc[2]) flags |= EMU_PT_NONFINITE;
+    *p.flags() = flags;
+  }
 }
 
 }  // namespace emu
