@@ -115,7 +115,7 @@ __device__ __forceinline__ cd t12_exact(const LayerC &c, cd kz, double kair, cd 
     z2 = cmul(c.zcr, cmul(kz, c.ik));
   }
   const cd is = crcp_nr(cadd(z2, z1));
-  return cmul(cscale(cmul(csqrt_nr(z2), csqrt_nr(z1)), 2.0), is);
+  return cmul(cscale(cmul(csqrt_k(z2), csqrt_k(z1)), 2.0), is);
 }
 
 // Cascade of one order (both polarisations) bottom to top, then, if the
@@ -157,7 +157,7 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
   double al_air, be_air;
   order_ab(p.world_1d(), p.dy(), px, py, wood_air ? sa0 : a0, wood_air ? sb0 : b0, al_air, be_air);
   const double kair = wavenumber(cd{1.0, 0.0}, wln).x;
-  const cd kz_air = csqrt_p(kz_arg(cd{kair, 0.0}, al_air, be_air));
+  const cd kz_air = csqrt_k(kz_arg(cd{kair, 0.0}, al_air, be_air));
   const double *sh = p.shears();
   double al_sh = 0.0, be_sh = 0.0;
   if (sh)
@@ -175,7 +175,7 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
     const bool wl_l = (wood[l >> 5] >> (l & 31)) & 1u;
     double al, be;
     order_ab(p.world_1d(), p.dy(), px, py, wl_l ? sa0 : a0, wl_l ? sb0 : b0, al, be);
-    const cd kz = csqrt_p(kz_arg(lay[l].k, al, be));
+    const cd kz = csqrt_k(kz_arg(lay[l].k, al, be));
     if (p.kz()) store_c(p.kz(), (size_t)l * npw + j, kz);
     return kz;
   };
@@ -449,8 +449,8 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       if (so) so[r] = u;
       double al, be;
       order_ab(p.world_1d(), p.dy(), pxu, pyu, a0, b0, al, be);
-      if (csqrt_p(kz_arg(lay[0].k, al, be)).y == 0.0) atomicAdd(&nprop[0], 1);
-      if (csqrt_p(kz_arg(lay[L - 1].k, al, be)).y == 0.0) atomicAdd(&nprop[L - 1], 1);
+      if (sqrt_is_real(kz_arg(lay[0].k, al, be))) atomicAdd(&nprop[0], 1);
+      if (sqrt_is_real(kz_arg(lay[L - 1].k, al, be))) atomicAdd(&nprop[L - 1], 1);
       // Wood check of every layer: k_z == 0 exactly iff its argument is 0
       for (int l = 0; l < L; ++l) {
         const cd arg = kz_arg(lay[l].k, al, be);
@@ -487,7 +487,7 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
           double al, be;
           order_ab(p.world_1d(), p.dy(), p.px()[u], p.py()[u], wl_l ? sa0 : a0, wl_l ? sb0 : b0,
                    al, be);
-          if (csqrt_p(kz_arg(lay[l].k, al, be)).y == 0.0) atomicAdd(&nprop[l], 1);
+          if (sqrt_is_real(kz_arg(lay[l].k, al, be))) atomicAdd(&nprop[l], 1);
         }
       }
     }

@@ -31,9 +31,11 @@
 //   5  (only if a layer hit a Wood anomaly) phase 4 again for those points
 //      with k_parallel scaled by 1 - 1e-9 in the marked layers
 //   6  a_list / t_list / r_list (backend/stack.py:368-426)
-// Divisions use the Newton reciprocal of emu_fastmath.cuh; k_z itself uses
-// IEEE square roots and quotients so that exact zeros (Wood anomalies) and
-// exactly real k_z (propagating orders) are decided as numpy decides them.
+// Divisions use the Newton reciprocal of emu_fastmath.cuh.  The decisions
+// taken on k_z (exact zeros at Wood anomalies, exactly real k_z of
+// propagating orders, the sort keys) use IEEE square roots and quotients;
+// the k_z entering the recursion comes from the Newton form, which is exactly
+// zero, real or imaginary for the same arguments.
 #include <cuda_runtime.h>
 
 #include "emu_cplx.cuh"
