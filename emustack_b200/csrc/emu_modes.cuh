@@ -17,6 +17,15 @@ __device__ __forceinline__ cd kz_arg(cd k, double alpha, double beta) {
   return cd{re, im};
 }
 
+// k^2 and the argument from it and alpha^2, beta^2: the same roundings as kz_arg.
+__device__ __forceinline__ cd k_squared(cd k) {
+  return cd{__dsub_rn(__dmul_rn(k.x, k.x), __dmul_rn(k.y, k.y)),
+            __dadd_rn(__dmul_rn(k.x, k.y), __dmul_rn(k.y, k.x))};
+}
+__device__ __forceinline__ cd kz_arg_sq(cd kk, double alpha2, double beta2) {
+  return cd{__dsub_rn(__dsub_rn(kk.x, alpha2), beta2), kk.y};
+}
+
 // alpha = alpha0 + (2 px) pi / 1 ;  beta = beta0 + (2 py) pi / dy
 __device__ __forceinline__ void order_ab(int world_1d, double dy, int px, int py, double a0,
                                          double b0, double &alpha, double &beta) {

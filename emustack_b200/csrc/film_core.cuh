@@ -17,6 +17,7 @@ constexpr int kSave = 5;  // saved scalars per (layer, polarisation)
 struct LayerC {
   cd k, zcr, ik;  // wavenumber, 1/n, 1/k
   cd zk, zka;     // k / n and k_air / n (k_air real)
+  cd kk;          // k^2, rounded as kz_arg rounds it
 };
 
 // Shared-memory layout of one point's slot (byte offsets); a slot sized for
@@ -154,10 +155,21 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
                             int np_out, cd *acc, int *nprop, bool count, cd *ws_smem) {
   const int L = p.L(), npw = p.npw(), P = 2 * npw;
   const int px = p.px()[u], py = p.py()[u];
-  double al_air, be_air;
-  order_ab(p.world_1d(), p.dy(), px, py, wood_air ? sa0 : a0, wood_air ? sb0 : b0, al_air, be_air);
+  // alpha^2 and beta^2 of the order, with k_parallel as given and scaled by
+  // 1 - 1e-9 (layers at a Wood anomaly)
+  double al2, be2, al2w, be2w;
+  {
+    double al, be;
+    order_ab(p.world_1d(), p.dy(), px, py, a0, b0, al, be);
+    al2 = __dmul_rn(al, al);
+    be2 = __dmul_rn(be, be);
+    order_ab(p.world_1d(), p.dy(), px, py, sa0, sb0, al, be);
+    al2w = __dmul_rn(al, al);
+    be2w = __dmul_rn(be, be);
+  }
   const double kair = wavenumber(cd{1.0, 0.0}, wln).x;
-  const cd kz_air = csqrt_k(kz_arg(cd{kair, 0.0}, al_air, be_air));
+  const cd kz_air = csqrt_k(kz_arg_sq(k_squared(cd{kair, 0.0}), wood_air ? al2w : al2,
+                                      wood_air ? be2w : be2));
   const double *sh = p.shears();
   double al_sh = 0.0, be_sh = 0.0;
   if (sh)
@@ -172,10 +184,8 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
   cd *wsv = p.slot_per_order() ? p.ws() + ((size_t)u * L) * 2 * kSave : ws_smem;
   // k_z of the order in layer l (also stored when requested)
   auto layer_kz = [&](int l) -> cd {
-    const bool wl_l = (wood[l >> 5] >> (l & 31)) & 1u;
-    double al, be;
-    order_ab(p.world_1d(), p.dy(), px, py, wl_l ? sa0 : a0, wl_l ? sb0 : b0, al, be);
-    const cd kz = csqrt_k(kz_arg(lay[l].k, al, be));
+    const int wl = (wood[l >> 5] >> (l & 31)) & 1u;
+    const cd kz = csqrt_k(kz_arg_sq(lay[l].kk, wl ? al2w : al2, wl ? be2w : be2));
     if (p.kz()) store_c(p.kz(), (size_t)l * npw + j, kz);
     return kz;
   };
@@ -226,7 +236,7 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
     const LayerC c = lay[l];
     const cd kz = layer_kz(l);
     if (count && kz.y == 0.0) atomicAdd(&nprop[l], 1);
-    const cd pr = cexp_ikh(kz, hsm[l - 1] / p.period());
+    const cd pr = cexp_ikh(kz, hsm[l - 1]);
     const cd pr2 = cmul(pr, pr);
     cd Q, Qi;
     shear_q(l, Q, Qi);
@@ -386,9 +396,10 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       c.ik = crecip(c.k);
       c.zk = cmul(c.zcr, c.k);
       c.zka = cscale(c.zcr, wavenumber(cd{1.0, 0.0}, wln).x);
+      c.kk = k_squared(c.k);
       lay[i] = c;
     }
-    for (int i = lt; i < L - 2; i += team) hsm[i] = p.height(i);
+    for (int i = lt; i < L - 2; i += team) hsm[i] = p.height(i) / p.period();
     for (int i = lt; i < L + 1; i += team) {
       acc[i] = cd{0.0, 0.0};
       nprop[i] = 0;
