@@ -119,6 +119,17 @@ __device__ __forceinline__ cd t12_exact(const LayerC &c, cd kz, double kair, cd 
   return cmul(cscale(cmul(csqrt_k(z2), csqrt_k(z1)), 2.0), is);
 }
 
+// R12 and T12 T21 of the air / layer interface for polarisation q from the
+// scaled impedances A, B (the scaling is described at solve_order).
+__device__ __forceinline__ void iface_scaled(const LayerC &c, cd kz, double kair, cd kz_air, int q,
+                                             cd &R12, cd &TT) {
+  const cd A = q ? cmul(c.zka, kz) : cmul(c.zk, kz_air);
+  const cd Bz = q ? cmul(kz_air, c.k) : cscale(kz, kair);
+  const cd is = crcp_nr(cadd(A, Bz));
+  R12 = cmul(csub(A, Bz), is);
+  TT = cmul(cscale(cmul(A, Bz), 4.0), cmul(is, is));
+}
+
 // Cascade of one order (both polarisations) bottom to top, then, if the
 // order carries incident light, its flux pass top to bottom.
 //
@@ -137,17 +148,6 @@ __device__ __forceinline__ cd t12_exact(const LayerC &c, cd kz, double kair, cd 
 // The outer layers (substrate, superstrate) and the optional per-layer
 // outputs (layer_rt, vec_coef) take T12 itself from t12_exact.  Every
 // result is the same whichever optional outputs are requested.
-// R12 and T12 T21 of the air / layer interface for polarisation q from the
-// scaled impedances A, B described above.
-__device__ __forceinline__ void iface_scaled(const LayerC &c, cd kz, double kair, cd kz_air, int q,
-                                             cd &R12, cd &TT) {
-  const cd A = q ? cmul(c.zka, kz) : cmul(c.zk, kz_air);
-  const cd Bz = q ? cmul(kz_air, c.k) : cscale(kz, kair);
-  const cd is = crcp_nr(cadd(A, Bz));
-  R12 = cmul(csub(A, Bz), is);
-  TT = cmul(cscale(cmul(A, Bz), 4.0), cmul(is, is));
-}
-
 template <class Pt>
 __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec, const LayerC *lay,
                             const double *hsm, const unsigned *wood, bool wood_air, double a0,
