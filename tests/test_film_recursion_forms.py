@@ -1,0 +1,137 @@
+"""The film kernels' rewritten recursion against the reference's, on the CPU.
+
+The film kernels (emustack_b200/csrc/film_core.cuh) do not evaluate the
+reference's interface and cascade formulas (backend/mode_calcs.py:451-477,
+backend/stack.py:229-278) literally: between two air gaps they use impedances
+scaled by k_z k_z,air (TE) or k k_air (TM), take T12 only through
+T12 T21 = 4AB/(A+B)^2, and fold the per-layer quotients into
+x1 p x2 = T12 T21 p / (d1 d2).  This file restates that form in numpy
+(vectorised over the orders of one point) and checks it against the oracle's
+literal restatement of the reference, so the algebra is pinned without a GPU.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from oracle import gsm_oracle as O  # noqa: E402
+
+
+def kernel_form(ns, heights_nm, wl_nm, k_pll, period, max_order):
+    """R_net, T_net diagonals (TE half then TM half) and the per-layer
+    products x1 p x2, in the kernels' form."""
+    air = O.make_air_ref(wl_nm, k_pll, period, None, max_order)
+    wln = O.wl_norm(wl_nm, period)
+    kair = 2 * np.pi / wln
+    npw = air.num_pw_per_pol
+    kz_air = air.k_z[:npw]
+    L = len(ns)
+    mods = [O.FilmModes(n, wl_nm, k_pll, period, None, max_order, air=air) for n in ns]
+    z_air = air.Z()
+
+    def scaled(l):
+        m = mods[l]
+        k, n, kz = m.k(), m.n_val, m.k_z[:npw]
+        A = np.concatenate((k / n * kz_air, kair / n * kz))
+        B = np.concatenate((kair * kz, k * kz_air))
+        R = (A - B) / (A + B)
+        TT = 4 * A * B / (A + B) ** 2
+        return R, TT
+
+    def t12(l):
+        z2 = mods[l].Z()
+        return 2 * np.sqrt(z2) * np.sqrt(z_air) / (z2 + z_air)
+
+    R0, _ = scaled(0)
+    rnet, tnet = R0, t12(0)
+    g_list = []
+    for l in range(1, L - 1):
+        R, TT = scaled(l)
+        kz = mods[l].k_z
+        p = np.exp(1j * kz * heights_nm[l - 1] / period)
+        d1 = 1 / (1 - R * rnet)
+        ug = TT * d1
+        rg = ug * rnet - R
+        prr = p * p * rg
+        d2 = 1 / (1 + R * prr)
+        g = ug * p * d2
+        g_list.append(g)
+        tnet = tnet * g
+        rnet = R + TT * prr * d2
+    R, TT = scaled(L - 1)
+    d1 = 1 / (1 - R * rnet)
+    tnet = tnet * t12(L - 1) * d1
+    rnet = TT * d1 * rnet - R
+    return rnet, tnet, g_list
+
+
+@pytest.mark.parametrize('seed', range(6))
+def test_kernel_form_equals_reference_recursion(seed):
+    rng = np.random.default_rng(seed)
+    L = int(rng.integers(2, 9))
+    ns = list(rng.uniform(1.2, 4.0, L) + 1j * rng.uniform(0.0, 0.4, L))
+    ns[-1] = 1.0 + 0j if seed % 2 else ns[-1]
+    heights = list(rng.uniform(20, 300, L - 2))
+    wl = float(rng.uniform(350, 1100))
+    th, ph = rng.uniform(0, 1.0), rng.uniform(0, 1.5)
+    kp = O.k_parallel_from_angles(wl, th, ph)
+    period, max_order = 500.0, 3
+    res = O.film_stack_point(ns, heights, wl, kp, period, max_order=max_order, pol='TE')
+    rnet, tnet, _ = kernel_form(ns, heights, wl, kp, period, max_order)
+    np.testing.assert_allclose(rnet, np.diag(res.R_net), rtol=1e-11, atol=1e-13)
+    np.testing.assert_allclose(tnet, np.diag(res.T_net), rtol=1e-11, atol=1e-13)
+
+
+def test_transmission_product_is_x1_p_x2():
+    """The per-layer product the kernels save for the flux pass equals the
+    reference's t21 (I - r12 r)^-1 p t12 (I + r12 p r_gap p)^-1 chain."""
+    rng = np.random.default_rng(11)
+    L = 6
+    ns = list(rng.uniform(1.3, 3.5, L) + 1j * rng.uniform(0.0, 0.3, L))
+    heights = list(rng.uniform(30, 250, L - 2))
+    wl, period, max_order = 633.0, 500.0, 2
+    kp = O.k_parallel_from_angles(wl, 0.3, 0.2)
+    _, _, g_list = kernel_form(ns, heights, wl, kp, period, max_order)
+    air = O.make_air_ref(wl, kp, period, None, max_order)
+    z_air = air.Z()
+    mods = [O.FilmModes(n, wl, kp, period, None, max_order, air=air) for n in ns]
+    # literal reference quantities, diagonal form
+    z0 = mods[0].Z()
+    r = (z0 - z_air) / (z0 + z_air)
+    for l in range(1, L - 1):
+        z2 = mods[l].Z()
+        R12 = (z2 - z_air) / (z2 + z_air)
+        T12 = 2 * np.sqrt(z2) * np.sqrt(z_air) / (z2 + z_air)
+        p = np.exp(1j * mods[l].k_z * heights[l - 1] / period)
+        x1 = T12 / (1 - R12 * r)
+        rg = -R12 + T12 * r * x1
+        x2 = T12 / (1 + R12 * p * rg * p)
+        np.testing.assert_allclose(g_list[l - 1], x1 * p * x2, rtol=1e-11, atol=1e-14)
+        r = R12 + T12 * p * rg * p * x2
+
+
+def _sort_key(k):
+    """numpy restatement of film_core.cuh sort_key: -0 taken as +0, then the
+    sign bit flipped for positive doubles and all bits for negative ones."""
+    b = (np.asarray(k, np.float64) + 0.0).view(np.int64)
+    u = b.view(np.uint64)
+    return np.where(b < 0, ~u, u | np.uint64(1 << 63))
+
+
+def test_integer_sort_keys_rank_as_the_doubles():
+    """The kernels rank orders by -Re k_z + Im k_z with integer keys; the
+    ranks (stable on ties) equal those of the double comparison, signed
+    zeros and exact ties included."""
+    rng = np.random.default_rng(3)
+    k = np.concatenate((rng.normal(size=200) * 10.0 ** rng.integers(-300, 300, 200),
+                        [0.0, -0.0, 1.0, 1.0, -1.0, -1.0, 5e-324, -5e-324, 1e308, -1e308]))
+    rng.shuffle(k)
+    keys = _sort_key(k)
+    r_int = np.array([np.sum((keys < keys[u]) | ((keys == keys[u]) & (np.arange(len(k)) < u)))
+                      for u in range(len(k))])
+    r_dbl = np.array([np.sum((k < k[u]) | ((k == k[u]) & (np.arange(len(k)) < u)))
+                      for u in range(len(k))])
+    np.testing.assert_array_equal(r_int, r_dbl)
+    np.testing.assert_array_equal(np.sort(r_int), np.arange(len(k)))
