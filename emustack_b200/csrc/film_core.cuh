@@ -392,8 +392,8 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       const cd n = cd{v.re, v.im};
       LayerC c;
       c.k = wavenumber(n, wln);
-      c.zcr = crecip(n);
-      c.ik = crecip(c.k);
+      c.zcr = crcp_nr(n);
+      c.ik = crcp_nr(c.k);
       c.zk = cmul(c.zcr, c.k);
       c.zka = cscale(c.zcr, wavenumber(cd{1.0, 0.0}, wln).x);
       c.kk = k_squared(c.k);
@@ -460,11 +460,12 @@ __device__ __forceinline__ void film_point(const Team &tm, const Pt &p, bool val
       if (so) so[r] = u;
       double al, be;
       order_ab(p.world_1d(), p.dy(), pxu, pyu, a0, b0, al, be);
-      if (sqrt_is_real(kz_arg(lay[0].k, al, be))) atomicAdd(&nprop[0], 1);
-      if (sqrt_is_real(kz_arg(lay[L - 1].k, al, be))) atomicAdd(&nprop[L - 1], 1);
+      const double al2 = __dmul_rn(al, al), be2 = __dmul_rn(be, be);
+      if (sqrt_is_real(kz_arg_sq(lay[0].kk, al2, be2))) atomicAdd(&nprop[0], 1);
+      if (sqrt_is_real(kz_arg_sq(lay[L - 1].kk, al2, be2))) atomicAdd(&nprop[L - 1], 1);
       // Wood check of every layer: k_z == 0 exactly iff its argument is 0
       for (int l = 0; l < L; ++l) {
-        const cd arg = kz_arg(lay[l].k, al, be);
+        const cd arg = kz_arg_sq(lay[l].kk, al2, be2);
         if (arg.x == 0.0 && arg.y == 0.0) {
           atomicOr(&wood[l >> 5], 1u << (l & 31));
           misc[1] = 1;
