@@ -135,3 +135,38 @@ def test_integer_sort_keys_rank_as_the_doubles():
                       for u in range(len(k))])
     np.testing.assert_array_equal(r_int, r_dbl)
     np.testing.assert_array_equal(np.sort(r_int), np.arange(len(k)))
+
+
+def test_layer_recursion_as_moebius_product():
+    """The per-layer step r -> r' of the film recursion is a Moebius map whose
+    2 x 2 matrix, with T12 T21 + R12^2 = 1, is [[p^2 - R^2, R(1 - p^2)],
+    [R(p^2 - 1), 1 - R^2 p^2]]; the superstrate's gap is [[1, -R], [-R, 1]].
+    The product of the matrices applied to (R_substrate, 1) gives R_net, and
+    T_net = T12(substrate) prod(T12 T21 p) T12(top) / (second component):
+    the form a layer-parallel reduction would evaluate."""
+    rng = np.random.default_rng(5)
+    for trial in range(4):
+        L = int(rng.integers(3, 10))
+        ns = list(rng.uniform(1.2, 4.0, L) + 1j * rng.uniform(0.0, 0.4, L))
+        heights = list(rng.uniform(20, 300, L - 2))
+        wl = float(rng.uniform(400, 1000))
+        kp = O.k_parallel_from_angles(wl, rng.uniform(0, 1.0), rng.uniform(0, 1.5))
+        period, max_order = 500.0, 2
+        res = O.film_stack_point(ns, heights, wl, kp, period, max_order=max_order, pol='TE')
+        air = O.make_air_ref(wl, kp, period, None, max_order)
+        z_air = air.Z()
+        mods = [O.FilmModes(n, wl, kp, period, None, max_order, air=air) for n in ns]
+        R = [(m.Z() - z_air) / (m.Z() + z_air) for m in mods]
+        T12 = [2 * np.sqrt(m.Z()) * np.sqrt(z_air) / (m.Z() + z_air) for m in mods]
+        N, D = R[0].copy(), np.ones_like(R[0])
+        tprod = T12[0].copy()
+        for l in range(1, L - 1):
+            p = np.exp(1j * mods[l].k_z * heights[l - 1] / period)
+            u, r = p * p, R[l]
+            m00, m01, m10, m11 = u - r * r, r * (1 - u), r * (u - 1), 1 - r * r * u
+            N, D = m00 * N + m01 * D, m10 * N + m11 * D
+            tprod = tprod * T12[l] * T12[l] * p
+        r = R[L - 1]
+        N, D = N - r * D, -r * N + D
+        np.testing.assert_allclose(N / D, np.diag(res.R_net), rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(tprod * T12[L - 1] / D, np.diag(res.T_net), rtol=1e-10, atol=1e-12)
