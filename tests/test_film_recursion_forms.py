@@ -170,3 +170,34 @@ def test_layer_recursion_as_moebius_product():
         N, D = N - r * D, -r * N + D
         np.testing.assert_allclose(N / D, np.diag(res.R_net), rtol=1e-10, atol=1e-12)
         np.testing.assert_allclose(tprod * T12[L - 1] / D, np.diag(res.T_net), rtol=1e-10, atol=1e-12)
+
+
+def _seed(x, bits=16):
+    """A seed with only `bits` correct bits: the exact value with its
+    mantissa cut to that width and perturbed by up to 2^-bits relative."""
+    x = np.asarray(x, np.float64)
+    m, e = np.frexp(x)
+    m = np.round(m * 2.0 ** bits) / 2.0 ** bits
+    rng = np.random.default_rng(1)
+    return np.ldexp(m, e) * (1 + rng.uniform(-1, 1, x.shape) * 2.0 ** -bits)
+
+
+def test_newton_steps_reach_double_precision_from_a_16_bit_seed():
+    """emu_fastmath.cuh takes two Newton steps from the hardware's approximate
+    reciprocal and reciprocal square root.  From any seed with 16 correct
+    bits, two steps land within a few ulps over the range the kernels use
+    (numpy rounds the products that the kernels fuse into multiply-adds, so
+    the kernels' steps are at least as accurate as these)."""
+    rng = np.random.default_rng(0)
+    a = 10.0 ** rng.uniform(-290, 290, 20000) * rng.choice([-1.0, 1.0], 20000)
+    x = _seed(1.0 / a)
+    for _ in range(2):
+        e = np.float64(1.0) - a * x          # fma(-a, x, 1) up to the last bit
+        x = x + x * e
+    assert np.max(np.abs(x * a - 1.0)) < 8 * np.finfo(np.float64).eps
+    q = np.abs(a)[np.abs(np.log10(np.abs(a))) < 280]
+    y = _seed(1.0 / np.sqrt(q))
+    for _ in range(2):
+        e = 0.5 - (0.5 * q * y) * y
+        y = y + y * e
+    assert np.max(np.abs(y * np.sqrt(q) - 1.0)) < 8 * np.finfo(np.float64).eps
