@@ -172,3 +172,10 @@ def test_argument_checks_need_no_gpu():
     f = _lib.EmuFilmVarBatch()
     f.variant = 2
     assert L.emu_film_var_batch(C.byref(f), None, 0, None) != 0
+
+
+def test_film_sources_build_with_exact_rounding():
+    """The film kernels' launch shapes return the same bits only when their
+    sources are compiled without compiler-chosen multiply-add contraction."""
+    from emustack_b200 import build
+    assert {'film_stack.cu', 'film_varlen.cu'} <= build.EXACT_ROUNDING
