@@ -279,14 +279,6 @@ def run_ours(args, rank, world, local_rank):
         flops = film_flops(B, L, P)
         fp64_peak = fp64_peak_tflops()
         tfl = flops / (ms_per_step / 1e3) / 1e12
-        traffic = fp64_pipe = None
-        tf = os.path.join(ROOT, 'profiles', 'film_stack_32768pts.md')
-        if os.path.exists(tf):
-            for line in open(tf):   # the first capture in the file is the bench kernel's
-                if line.startswith('| dram_bytes_per_launch |'):
-                    traffic = int(line.split('|')[2])
-                if fp64_pipe is None and line.startswith('| sm__pipe_fp64_cycles_active |'):
-                    fp64_pipe = float(line.split('|')[2].split('%')[0]) / 100.0
         result = {
             'metric': METRIC,
             'value': value,
@@ -308,17 +300,14 @@ def run_ours(args, rank, world, local_rank):
                     'd2h_bytes_per_step': d2h},
             'gpu_launches': int(launches),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm,
-                         'unit': 'GB/s', 'frac': achieved / hbm, 'traffic': traffic,
+                         'unit': 'GB/s', 'frac': achieved / hbm, 'traffic': None,
                          'peak_source': hbm_src + ' (MEASURED_PEAKS.json hbm_gbs)',
                          'note': 'the kernel is FP64-issue bound, see compute'},
             'compute': {'bound': 'fp64', 'achieved_tflops': tfl, 'peak_tflops': fp64_peak,
                         'frac': tfl / fp64_peak if fp64_peak else None,
                         'peak_source': 'DFMA probe kernel (emu_probe_fp64), measured in this run',
                         'flops_per_step': flops,
-                        'fp64_pipe_busy_ncu': fp64_pipe,
-                        'note': 'algorithmic flops count a divide, square root or exp as one; '
-                                'fp64_pipe_busy_ncu is the FP64 pipe occupancy ncu measured on '
-                                'the same kernel and size (profiles/film_stack_32768pts.md)'},
+                        'note': 'algorithmic flops count a divide, square root or exp as one'},
             'clocks': clk.summary(),
             'autotune': _tuned(),
         }

@@ -186,8 +186,12 @@ int validate(const EmuFilmStackBatch *p) {
 
 }  // namespace
 
+// Only incoming amplitudes use the global workspace (any order may carry
+// light, so each order keeps its flux-pass scalars there); every other
+// polarisation keeps them in shared memory and needs no workspace.
 extern "C" size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p) {
   if (validate(p) != EMU_OK) return 0;
+  if (p->pol != EMU_POL_INCOMING) return 0;
   const Launch l = plan(p);
   return (size_t)p->n_points * l.n_act * p->n_layers * 2 * kSave * sizeof(cd);
 }
@@ -198,7 +202,7 @@ extern "C" int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspac
   if (st != EMU_OK) return st;
   if (p->n_points == 0) return EMU_OK;
   const size_t need = emu_film_stack_workspace_size(p);
-  if (!d_workspace || workspace_bytes < need) return EMU_E_WORKSPACE;
+  if (need > 0 && (!d_workspace || workspace_bytes < need)) return EMU_E_WORKSPACE;
   const Launch l = plan(p);
   FilmArgs a;
   a.p = *p;

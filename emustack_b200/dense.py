@@ -242,7 +242,7 @@ class DenseStackSolver(object):
 def layer_interface(air, lay):
     """Device (R12, T12, R21, T21, dense) of lay with the air reference,
     memoised like backend/mode_calcs.py:416-448 (keyed by object ids)."""
-    from .mode_calcs import Anallo, _interfaces_i_have_known
+    from .mode_calcs import _interfaces_i_have_known, film_n, is_film
     key = (id(air), id(lay))
     hit = _interfaces_i_have_known.get(key)
     if hit is not None and 'dev' in hit:
@@ -252,11 +252,11 @@ def layer_interface(air, lay):
     wln = torch.tensor([air.wl_norm()], dtype=torch.float64, device=dev)
     air_kz = torch.tensor(np.asarray(air.k_z[:npw]).reshape(1, npw), dtype=c128, device=dev)
     air_n = torch.tensor([complex(np.asarray(air.n()).item())], dtype=c128, device=dev)
-    if isinstance(lay, Anallo):
+    if is_film(lay):
         if len(lay.k_z) != len(air.k_z):
             raise ValueError('Need the same number of plane waves in Anallos')
         kz2 = torch.tensor(np.asarray(lay.k_z[:npw]).reshape(1, npw), dtype=c128, device=dev)
-        n2 = torch.tensor([lay.n_complex()], dtype=c128, device=dev)
+        n2 = torch.tensor([film_n(lay)], dtype=c128, device=dev)
         R12, T12 = film_interface(air_kz, air_n, kz2, n2, wln)
         res = (R12, T12, -R12, T12, False)
     else:
@@ -284,7 +284,7 @@ def calc_scat_dense(stack, pol='TE', incoming_amplitudes=None, calc_fluxes=True,
                     save_scat_list=False):
     """Stack.calc_scat for stacks with nanostructured layers (or when the
     intermediate lists are requested), on the GPU."""
-    from .mode_calcs import Anallo
+    from .mode_calcs import is_film
     layers = stack.layers
     L = len(layers)
     air = layers[-1].air_ref()
@@ -303,12 +303,12 @@ def calc_scat_dense(stack, pol='TE', incoming_amplitudes=None, calc_fluxes=True,
             hn = hs[i - 1] / stack.period
         dl.append(DenseLayer(R12, T12, R21, T21, dense, kz, hn))
     top = layers[-1]
-    if calc_fluxes and not isinstance(top, Anallo):
+    if calc_fluxes and not is_film(top):
         raise NotImplementedError('energy fluxes need a ThinFilm superstrate')
     spec = torch.tensor([int(getattr(top, 'specular_order', 0))], dtype=torch.int32, device=dev)
     sub = layers[0]
     nprop = torch.tensor([[air.num_prop_pw_per_pol, getattr(top, 'num_prop_pw_per_pol', 0),
-                           sub.num_prop_pw_per_pol if isinstance(sub, Anallo) else 0]],
+                           sub.num_prop_pw_per_pol if is_film(sub) else 0]],
                          dtype=torch.int32, device=dev)
     inc = None
     if incoming_amplitudes is not None:
@@ -355,7 +355,7 @@ def calc_scat_dense(stack, pol='TE', incoming_amplitudes=None, calc_fluxes=True,
     stack.vec_coef_up = [np.asmatrix(vu[offs[i]:offs[i + 1]].reshape(-1, 1)) for i in range(len(up))]
     df = [f[0, 0]] + [complex(f[i, 0], f[i, 1]) for i in range(1, L - 1)]
     up0 = f[L, 0]
-    if isinstance(sub, Anallo):
+    if is_film(sub):
         if flags & _lib.PT_NO_PROP_SUB:
             print("Warning: there are no propagating modes in the semi-inf \n substrate therefore "
                   "cannot calculate energy fluxes here.")

@@ -29,6 +29,23 @@ def _device():
     return torch.device('cuda', torch.cuda.current_device())
 
 
+def is_film(lay):
+    """True for a homogeneous-film layer (an ``Anallo``), judged by the
+    interface the GSM stage reads rather than by class: a film has analytic
+    impedances (``Z``) and a specular incidence vector, a nanostructured
+    layer (``Simmo``) has overlap matrices ``J`` / ``J_dag`` instead.  So the
+    reference's own ``Anallo`` / ``Simmo`` objects, or any object exposing
+    the same attributes, dispatch the same way as this package's."""
+    return (callable(getattr(lay, 'Z', None)) and callable(getattr(lay, 'specular_incidence', None))
+            and getattr(lay, 'J', None) is None)
+
+
+def film_n(lay):
+    """Refractive index of a film layer with its loss flag applied (the
+    reference's ``Anallo.n()``, real when ``loss`` is False), as a complex."""
+    return complex(np.asarray(lay.n()).item())
+
+
 class Modes(object):
     """Common functionality of Simmo and Anallo (backend/mode_calcs.py:36-95)."""
 
@@ -93,7 +110,7 @@ class Anallo(Modes):
 
     def n_complex(self):
         """Index with the loss flag applied, as a Python complex."""
-        return complex(np.asarray(self.n()).item())
+        return film_n(self)
 
     def k(self):
         return np.complex128(2 * pi * self.n() / self.wl_norm())

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .mode_calcs import Anallo, Simmo
+from .mode_calcs import film_n, is_film
 
 
 class Stack(object):
@@ -60,7 +60,7 @@ class Stack(object):
                   save_scat_list=False):
         """Net R/T matrices and energy fluxes (backend/stack.py:162-426)."""
         self._check_periods_are_consistent()
-        all_films = all(isinstance(l, Anallo) for l in self.layers)
+        all_films = all(is_film(l) for l in self.layers)
         if all_films and not save_scat_list:
             self._calc_scat_films(pol, incoming_amplitudes, calc_fluxes)
         else:
@@ -78,7 +78,7 @@ class Stack(object):
         dev = solver.device
         wl = torch.tensor([light.wl_nm], dtype=torch.float64, device=dev)
         kp = torch.tensor(np.asarray(light.k_pll, np.float64).reshape(1, 2), device=dev)
-        n = torch.tensor([[l.n_complex() for l in self.layers]], dtype=torch.complex128, device=dev)
+        n = torch.tensor([[film_n(l) for l in self.layers]], dtype=torch.complex128, device=dev)
         hs = torch.tensor(np.asarray(self.heights_nm(), dtype=np.float64), device=dev)
         inc = None
         if incoming_amplitudes is not None:

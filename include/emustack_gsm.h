@@ -187,6 +187,10 @@ typedef struct {
   int variant;
 } EmuFilmStackBatch;
 
+/* Workspace: only pol == EMU_POL_INCOMING needs one (B x Npw x L x 160
+ * bytes: any order may carry light, and each such order keeps its flux-pass
+ * scalars there); for the other polarisations the size is 0 and d_workspace
+ * may be NULL. */
 size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p);
 int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspace,
                          size_t workspace_bytes, void *stream);
@@ -444,8 +448,11 @@ int emu_mode_overlap_reorder(const EmuNormalise *p, int32_t *d_perm, int32_t *d_
  * solve uses a scratch array of emu_film_stack_static_scratch_bytes()
  * (16 MiB) compiled into the library instead of a caller workspace.  The
  * caller still passes every input and output buffer.
- *   - Requests whose emu_film_stack_workspace_size() exceeds that size are
- *     rejected with EMU_E_WORKSPACE (split the batch).
+ *   - Only incoming amplitudes (EMU_POL_INCOMING) use the array; requests
+ *     whose emu_film_stack_workspace_size() exceeds its size (about 8 700
+ *     points x orders of a 12-layer stack, e.g. 107 points at Npw = 81) are
+ *     rejected with EMU_E_WORKSPACE (split the batch).  The standard
+ *     polarisations use no scratch and have no size limit here.
  *   - The first call on a device looks up that device's copy of the array
  *     (cudaGetSymbolAddress); make that first call before any stream
  *     capture.

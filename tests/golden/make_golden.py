@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the EMUstack reference.
 
-Run in a container that has the reference source tree (it reads
-``/root/reference`` or the path in ``EMUSTACK_REF``):
+Run where the reference source tree is available, with ``EMUSTACK_REF``
+naming its root directory:
 
-    python tests/golden/make_golden.py
+    EMUSTACK_REF=<path to the EMUstack tree> python tests/golden/make_golden.py
 
 It imports the reference's own Python GSM (backend/stack.py,
 backend/mode_calcs.py, backend/objects.py, backend/materials.py) with three
@@ -32,10 +32,12 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get('EMUSTACK_REF', '/root/reference')
+REF = os.environ.get('EMUSTACK_REF')
 
 
 def import_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, 'backend')):
+        raise SystemExit('set EMUSTACK_REF to the root of the EMUstack source tree')
     if not hasattr(np, 'mat'):
         np.mat = np.asmatrix
     fortran = types.ModuleType('fortran')

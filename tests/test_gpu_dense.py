@@ -257,3 +257,74 @@ def test_multi_cta_interface_equals_one_cta_interface(B, P, M):
     for a, b in zip(*outs):
         a, b = a.numpy(), b.numpy()
         assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0)
+
+
+class _PlainFilm(object):
+    """A film layer that is not an emustack_b200 class: the attributes and
+    methods the reference's Anallo exposes (backend/mode_calcs.py:99-250)."""
+
+    def __init__(self, src, air=None):
+        for nm in ('structure', 'light', 'k_z', 'specular_order', 'num_prop_pw_per_pol',
+                   'sort_order', 'alphas', 'betas', 'is_air_ref', 'max_order_PWs'):
+            setattr(self, nm, getattr(src, nm))
+        self._n = src.n()
+        self._wl_norm = src.wl_norm()
+        self._air = air if air is not None else self
+
+    def n(self):
+        return self._n
+
+    def k(self):
+        return np.complex128(2 * np.pi * self.n() / self.wl_norm())
+
+    def wl_norm(self):
+        return self._wl_norm
+
+    def air_ref(self):
+        return self._air
+
+    def Z(self):
+        npw = len(self.k_z) // 2
+        k_on_kz = self.k() / self.k_z[:npw]
+        return np.concatenate((k_on_kz / self.n(), 1 / (self.n() * k_on_kz)))
+
+    def specular_incidence(self, pol='TE'):
+        raise AssertionError('not read by the GSM stage')
+
+
+class _PlainSimmo(object):
+    """A nanostructured layer that is not an emustack_b200 class: k_z, J,
+    J_dag and the structure/light, as the reference's Simmo holds them."""
+
+    def __init__(self, src, air):
+        for nm in ('structure', 'light', 'k_z', 'J', 'J_dag'):
+            setattr(self, nm, getattr(src, nm))
+        self._air = air
+
+    def air_ref(self):
+        return self._air
+
+
+@pytest.mark.parametrize('name', ['synth_config1', 'films10'])
+def test_dropin_accepts_plain_layer_objects(name):
+    """Stack dispatches on the layer interface (Z / specular_incidence for
+    films, J / J_dag for nanostructured layers), not on this package's
+    classes: stand-in objects built like the reference's Anallo / Simmo give
+    the same R_net, T_net and a/t/r lists."""
+    from emustack_b200.mode_calcs import is_film
+    from emustack_b200.stack import Stack
+    pts, _ = load_points(name)
+    pt = pts[0]
+    st = _dropin_stack(pt, use_J=True)
+    st.calc_scat(pol=pt['pol'])
+    air = _PlainFilm(st.layers[-1].air_ref())
+    plain = [_PlainFilm(l, air) if is_film(l) else _PlainSimmo(l, air) for l in st.layers]
+    assert not any(type(l).__module__.startswith('emustack_b200') for l in plain)
+    st2 = Stack(plain, shears=st.shears)
+    st2.calc_scat(pol=pt['pol'])
+    np.testing.assert_allclose(st2.R_net, st.R_net, rtol=0, atol=0)
+    np.testing.assert_allclose(st2.T_net, st.T_net, rtol=0, atol=0)
+    for k in ('a_list', 't_list', 'r_list'):
+        np.testing.assert_allclose(np.asarray(getattr(st2, k), float), np.asarray(getattr(st, k), float),
+                                   rtol=1e-12, atol=1e-14, err_msg=k)
+    np.testing.assert_allclose(st2.R_net, pt['R_net'], **TOL)
