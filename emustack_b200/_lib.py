@@ -275,3 +275,31 @@ EXTRA_SIGNATURES.extend([
     ('emu_stack_var_workspace_size', C.c_size_t, [C.POINTER(EmuStackVarBatch)]),
     ('emu_stack_var_batch', C.c_int, [C.POINTER(EmuStackVarBatch), vp, C.c_size_t, vp]),
 ])
+
+
+class EmuOverlap1D(C.Structure):
+    _fields_ = [
+        ('batch', C.c_int), ('nval', C.c_int), ('nel', C.c_int), ('npt', C.c_int),
+        ('max_order', C.c_int), ('d_x', vp), ('d_table_nod', vp), ('period_x', C.c_double),
+        ('d_bloch', vp), ('d_index_pw_inv', vp), ('d_sol1', vp), ('d_sol2', vp),
+        ('d_scale', vp), ('d_perm2', vp), ('d_J', vp), ('d_J_dag', vp),
+        ('npw_2d', C.c_int), ('d_row_2d', vp), ('d_J_2d', vp), ('d_J_dag_2d', vp), ('d_error', vp),
+    ]
+
+
+class EmuNormalise1D(C.Structure):
+    _fields_ = [
+        ('batch', C.c_int), ('nval', C.c_int), ('nel', C.c_int), ('npt', C.c_int),
+        ('n_types', C.c_int), ('d_x', vp), ('d_table_nod', vp), ('d_type_el', vp), ('d_pp', vp),
+        ('d_k0', vp), ('d_bloch', vp), ('d_beta1', vp), ('d_sol1', vp), ('d_sol2', vp),
+        ('d_perm2', vp), ('d_out', vp), ('d_scale', vp), ('d_n_small', vp), ('d_error', vp),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_pw_order_1d', C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, vp]),
+    ('emu_pw_embed_1d_to_2d', C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, vp,
+                                        C.c_int, C.POINTER(C.c_int)]),
+    ('emu_overlap1d_batch', C.c_int, [C.POINTER(EmuOverlap1D), vp]),
+    ('emu_mode_overlap_1d', C.c_int, [C.POINTER(EmuNormalise1D), C.c_int, vp]),
+])

@@ -231,7 +231,16 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
       }
     }
   }
-  // films between air gaps (backend/stack.py:229-262)
+  // films between air gaps (backend/stack.py:229-262).  With s = A + B and
+  // d = A - B the interface is R12 = d/s, T12 T21 = 4AB/s^2, and
+  // T12 T21 + R12^2 = 1, so the gap and layer steps of the reference,
+  //   rg = T12 (1 - R12 rq)^-1 T21 rq - R12,   (air gap, rq = rnet below)
+  //   rnet' = R12 + T12 p rg p (1 + R12 p rg p)^-1 T21,
+  // are Moebius maps: rg = v/u and rnet' = N/D with
+  //   u = s - d rq,  v = s rq - d,  D = s u + d p^2 v,  N = d u + s p^2 v,
+  // and the transmission through gap and layer, x1 p x2 = 4AB p / D, shares
+  // the one quotient 1/D (x1 = T12 (1 - R12 rq)^-1, x2 the layer's
+  // (1 + R12 p rg p)^-1 T21 = s u / D with T21 folded in).
   for (int l = 1; l < L - 1; ++l) {
     const LayerC c = lay[l];
     const cd kz = layer_kz(l);
@@ -242,27 +251,31 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
     shear_q(l, Q, Qi);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      cd R12, TT;
-      iface_scaled(c, kz, kair, kz_air, q, R12, TT);
-      const cd T12 = all_t ? t12_exact(c, kz, kair, kz_air, q) : cd{0.0, 0.0};
-      store_rt(l, q, R12, T12);
-      // air gap below layer l
+      const cd A = q ? cmul(c.zka, kz) : cmul(c.zk, kz_air);
+      const cd Bz = q ? cmul(kz_air, c.k) : cscale(kz, kair);
+      const cd s = cadd(A, Bz), d = csub(A, Bz);
+      cd T12 = cd{0.0, 0.0};
+      if (all_t) {
+        T12 = t12_exact(c, kz, kair, kz_air, q);
+        store_rt(l, q, cmul(d, crcp_nr(s)), T12);
+      }
       const cd rq = sh ? cmul(cmul(Qi, rnet[q]), Q) : rnet[q];
-      const cd d1 = crcp_nr(csub(cd{1.0, 0.0}, cmul(R12, rq)));
-      const cd ug = cmul(TT, d1);
-      const cd rg = csub(cmul(ug, rq), R12);
-      // through layer l
-      const cd prr = cmul(pr2, rg);
-      const cd d2 = crcp_nr(cadd(cd{1.0, 0.0}, cmul(R12, prr)));
-      const cd g = cmul(ug, cmul(pr, d2));  // x1 p x2
+      const cd u = csub(s, cmul(d, rq));
+      const cd v = csub(cmul(s, rq), d);
+      const cd Dn = cadd(cmul(s, u), cmul(cmul(d, pr2), v));
+      const cd Nn = cadd(cmul(d, u), cmul(cmul(s, pr2), v));
+      const cd iD = crcp_nr(Dn);
+      const cd g = cmul(cscale(cmul(cmul(A, Bz), pr), 4.0), iD);  // x1 p x2
       tnet[q] = cmul(sh ? cmul(tnet[q], Q) : tnet[q], g);
-      rnet[q] = cadd(R12, cmul(cmul(TT, prr), d2));
+      rnet[q] = cmul(Nn, iD);
       if (active) {
         cd *sv = wsv + ((size_t)l * 2 + q) * kSave;
         sv[0] = g;
-        sv[1] = rg;
         sv[2] = pr;
-        if (want_vec) sv[3] = cmul(T12, d2);
+        if (want_vec) {
+          sv[1] = cmul(v, crcp_nr(u));               // rg
+          sv[3] = cmul(cmul(T12, cmul(s, u)), iD);  // T12 x2 / T21 = T12 (1 + R12 p rg p)^-1
+        }
         sv[4] = rnet[q];
       }
     }

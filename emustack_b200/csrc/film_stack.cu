@@ -66,7 +66,11 @@ struct FilmArgs {
 };
 
 // Point accessor over the uniform batch: every field is derived from the
-// kernel parameters and the point index when used.
+// kernel parameters and the point index when used.  kPlain: the request asks
+// for no optional output, has no shears and a standard polarisation, so
+// those accessors are compile-time NULL and the recursion carries none of
+// their checks or live values.
+template <bool kPlain>
 struct UniformPoint {
   const FilmArgs &a;
   int b;
@@ -76,28 +80,29 @@ struct UniformPoint {
   __device__ int world_1d() const { return a.p.world_1d; }
   __device__ int pol() const { return a.p.pol; }
   __device__ int ncoord() const { return a.p.shear_ncoord; }
-  __device__ bool slot_per_order() const { return a.p.pol == EMU_POL_INCOMING; }
+  __device__ bool slot_per_order() const { return !kPlain && a.p.pol == EMU_POL_INCOMING; }
   __device__ double dy() const { return a.dy; }
   __device__ double period() const { return a.p.period; }
   __device__ double inv_sqrt2() const { return a.inv_sqrt2; }
   __device__ const int32_t *px() const { return a.p.d_px; }
   __device__ const int32_t *py() const { return a.p.d_py; }
   __device__ const emu_c128 *incoming() const { return a.p.d_incoming + (size_t)b * P(); }
-  __device__ const double *shears() const { return a.p.d_shears; }
+  __device__ const double *shears() const { return kPlain ? nullptr : a.p.d_shears; }
   __device__ cd *ws() const { return a.ws + (size_t)b * a.n_act * L() * 2 * kSave; }
   __device__ emu_c128 *R_net() const { return a.p.d_R_net + (size_t)b * P(); }
   __device__ emu_c128 *T_net() const { return a.p.d_T_net + (size_t)b * P(); }
   __device__ emu_c128 *kz() const {
-    return a.p.d_kz ? a.p.d_kz + (size_t)b * L() * npw() : nullptr;
+    return (!kPlain && a.p.d_kz) ? a.p.d_kz + (size_t)b * L() * npw() : nullptr;
   }
   __device__ emu_c128 *layer_rt() const {
-    return a.p.d_layer_rt ? a.p.d_layer_rt + (size_t)b * L() * 2 * P() : nullptr;
+    return (!kPlain && a.p.d_layer_rt) ? a.p.d_layer_rt + (size_t)b * L() * 2 * P() : nullptr;
   }
   __device__ emu_c128 *vcd() const {
-    return a.p.d_vec_coef_down ? a.p.d_vec_coef_down + (size_t)b * L() * P() : nullptr;
+    return (!kPlain && a.p.d_vec_coef_down) ? a.p.d_vec_coef_down + (size_t)b * L() * P() : nullptr;
   }
   __device__ emu_c128 *vcu() const {
-    return a.p.d_vec_coef_up ? a.p.d_vec_coef_up + (size_t)b * (L() - 1) * P() : nullptr;
+    return (!kPlain && a.p.d_vec_coef_up) ? a.p.d_vec_coef_up + (size_t)b * (L() - 1) * P()
+                                           : nullptr;
   }
   __device__ double wl_nm() const { return a.p.d_wl_nm[b]; }
   __device__ double kx() const { return a.p.d_k_pll[2 * (size_t)b]; }
@@ -107,14 +112,16 @@ struct UniformPoint {
     return a.p.d_heights_nm[(a.p.heights_per_point ? (size_t)b * (L() - 2) : 0) + i];
   }
   __device__ int32_t *sort_order() const {
-    return a.p.d_sort_order ? a.p.d_sort_order + (size_t)b * npw() : nullptr;
+    return (!kPlain && a.p.d_sort_order) ? a.p.d_sort_order + (size_t)b * npw() : nullptr;
   }
-  __device__ int32_t *specular() const { return a.p.d_specular ? a.p.d_specular + b : nullptr; }
+  __device__ int32_t *specular() const {
+    return (!kPlain && a.p.d_specular) ? a.p.d_specular + b : nullptr;
+  }
   __device__ int32_t *num_prop() const {
-    return a.p.d_num_prop ? a.p.d_num_prop + (size_t)b * (L() + 1) : nullptr;
+    return (!kPlain && a.p.d_num_prop) ? a.p.d_num_prop + (size_t)b * (L() + 1) : nullptr;
   }
   __device__ double *fluxes() const {
-    return a.p.d_fluxes ? a.p.d_fluxes + (size_t)b * (L() + 1) * 2 : nullptr;
+    return (!kPlain && a.p.d_fluxes) ? a.p.d_fluxes + (size_t)b * (L() + 1) * 2 : nullptr;
   }
   __device__ double *a_list() const { return a.p.d_a_list + (size_t)b * (L() - 1); }
   __device__ double *t_list() const { return a.p.d_t_list + (size_t)b * (L() - 1); }
@@ -122,7 +129,7 @@ struct UniformPoint {
   __device__ uint32_t *flags() const { return a.p.d_flags + b; }
 };
 
-template <int kThreads, int kMinBlocks>
+template <int kThreads, int kMinBlocks, bool kPlain>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) film_stack_kernel(FilmArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const EmuFilmStackBatch &p = a.p;
@@ -135,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) film_stack_kernel(FilmAr
   const CtaTeam tm{(int)(threadIdx.x % team), team};
   for (int bb = blockIdx.x * ppc; bb < B; bb += gridDim.x * ppc) {
     const int b = bb + slot;
-    film_point(tm, UniformPoint{a, b}, in_slot && b < B, base, S);
+    film_point(tm, UniformPoint<kPlain>{a, b}, in_slot && b < B, base, S);
   }
 }
 
@@ -148,10 +155,22 @@ using FilmKernel = void (*)(FilmArgs);
 // 0: 256 threads x 2 CTAs (128 registers), 1: 128 x 4 (128), 2: 512 x 1
 // (128), 3: 256 x 1 (255 registers, no spills, half the resident warps),
 // 4: 256 x 3 (85 registers), 5: 256 x 4 (64): more warps to hide the FP64
-// latency chains, at the price of spills to L1
-const FilmKernel kVarKernels[kVariants] = {film_stack_kernel<256, 2>, film_stack_kernel<128, 4>,
-                                           film_stack_kernel<512, 1>, film_stack_kernel<256, 1>,
-                                           film_stack_kernel<256, 3>, film_stack_kernel<256, 4>};
+// latency chains, at the price of spills to L1.  Row 1: the plain
+// specialisation (see UniformPoint), same arithmetic, same results.
+const FilmKernel kVarKernels[2][kVariants] = {
+    {film_stack_kernel<256, 2, false>, film_stack_kernel<128, 4, false>,
+     film_stack_kernel<512, 1, false>, film_stack_kernel<256, 1, false>,
+     film_stack_kernel<256, 3, false>, film_stack_kernel<256, 4, false>},
+    {film_stack_kernel<256, 2, true>, film_stack_kernel<128, 4, true>,
+     film_stack_kernel<512, 1, true>, film_stack_kernel<256, 1, true>,
+     film_stack_kernel<256, 3, true>, film_stack_kernel<256, 4, true>}};
+
+// True when the request needs none of what the plain specialisation drops.
+bool is_plain(const EmuFilmStackBatch *p) {
+  return p->pol != EMU_POL_INCOMING && !p->d_shears && !p->d_kz && !p->d_layer_rt &&
+         !p->d_vec_coef_down && !p->d_vec_coef_up && !p->d_fluxes && !p->d_sort_order &&
+         !p->d_specular && !p->d_num_prop;
+}
 
 Launch plan(const EmuFilmStackBatch *p) {
   Launch l;
@@ -212,7 +231,7 @@ extern "C" int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspac
   a.ws = (cd *)d_workspace;
   a.dy = p->period_y / p->period;
   a.inv_sqrt2 = 1.0 / sqrt(2.0);
-  const FilmKernel kern = kVarKernels[p->variant];
+  const FilmKernel kern = kVarKernels[is_plain(p) ? 1 : 0][p->variant];
   const int threads = kVarThreadsTab[p->variant];
   if (l.smem > 48 * 1024) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem) !=

@@ -91,3 +91,49 @@ def square_cell(n, dy=1.0, radius=None, center=(0.5, 0.5), jitter=0.0, seed=0):
         r = np.hypot(cen[:, 0] - center[0], cen[:, 1] - center[1])
         typ[r <= radius] = 2
     return Mesh(x, table + 1, typ)
+
+
+class Mesh1D(object):
+    """P2 mesh of a 1D grating's period (backend/fortran/py_calc_modes_1d.f
+    conventions): node coordinates ``x`` (the unit the periodic span is
+    measured in, the period itself for the drop-in objects), ``table_nod``
+    [nel][3] with 1-based node numbers (element ends, then midpoint) and
+    1-based material types ``type_el``."""
+
+    def __init__(self, x, table_nod, type_el=None):
+        self.x = np.ascontiguousarray(x, np.float64).ravel()
+        self.table_nod = np.ascontiguousarray(table_nod, np.int64)
+        if self.table_nod.ndim != 2 or self.table_nod.shape[1] != 3:
+            raise ValueError('table_nod must be [nel][3]')
+        if self.table_nod.min() < 1 or self.table_nod.max() > len(self.x):
+            raise ValueError('table_nod must hold 1-based node numbers')
+        n = len(self.table_nod)
+        self.type_el = np.ones(n, np.int64) if type_el is None else np.ascontiguousarray(type_el, np.int64)
+
+    @property
+    def npt(self):
+        return len(self.x)
+
+    @property
+    def nel(self):
+        return len(self.table_nod)
+
+    @property
+    def period_x(self):
+        """Span of the periodic cell (periodic_cond_1d.f:120-135 takes the
+        distance between the two periodic end nodes)."""
+        return float(self.x.max() - self.x.min())
+
+    @classmethod
+    def uniform(cls, n_el, x0=0.0, x1=1.0, jitter=0.0, seed=0, types=None):
+        """n_el elements over [x0, x1] (interior end nodes moved by up to
+        ``jitter`` of the spacing); end nodes first, then the midpoints."""
+        e = np.linspace(x0, x1, n_el + 1)
+        if jitter:
+            rng = np.random.default_rng(seed)
+            e[1:-1] += jitter * (x1 - x0) / n_el * rng.uniform(-0.5, 0.5, n_el - 1)
+        mid = 0.5 * (e[:-1] + e[1:])
+        x = np.concatenate([e, mid])
+        tab = np.stack([np.arange(1, n_el + 1), np.arange(2, n_el + 2),
+                        n_el + 2 + np.arange(n_el)], axis=1)
+        return cls(x, tab, types)

@@ -254,3 +254,209 @@ def overlap_from_fields(simmo, fields):
                                precision=fields.get('precision', 'fp64'))
     simmo.overlap_diag = diag[0].cpu().numpy()
     return np.asmatrix(J[0].cpu().numpy()), np.asmatrix(Jd[0].cpu().numpy())
+
+
+# ---------------------------------------------------------------------------
+# 1D gratings (periodicity '1D_array')
+# ---------------------------------------------------------------------------
+
+class DeviceMesh1D(object):
+    """A Mesh1D (emustack_b200.mesh) resident on the GPU."""
+
+    def __init__(self, mesh, device='cuda'):
+        self.mesh = mesh
+        self.x = torch.tensor(mesh.x, device=device)
+        self.table_nod = torch.tensor(mesh.table_nod, device=device)
+        self.type_el = torch.tensor(mesh.type_el, device=device)
+        self.nel, self.npt = mesh.nel, mesh.npt
+        self.period_x = mesh.period_x
+
+
+def pw_order_1d(max_order, period_x, bloch_x, bloch_y, k0):
+    """0-based sorted position of each 1D order px = -max_order..max_order
+    (emu_pw_order_1d: the reference's pw_ordering_1d ranking)."""
+    out = np.empty(2 * max_order + 1, np.int32)
+    check(lib().emu_pw_order_1d(int(max_order), float(period_x), float(bloch_x), float(bloch_y),
+                                float(k0), out.ctypes.data_as(C.c_void_p)), 'emu_pw_order_1d')
+    return out
+
+
+def pw_rows_2d(max_order, period_x, bloch_x, bloch_y, k0):
+    """(row of each 1D order in the sorted 2D order set, size of that set)
+    (emu_pw_embed_1d_to_2d: the placement of pw_matrix_1d_to_2d)."""
+    n = C.c_int(0)
+    rows = np.empty(2 * max_order + 1, np.int32)
+    check(lib().emu_pw_embed_1d_to_2d(int(max_order), float(period_x), float(bloch_x), float(bloch_y),
+                                      float(k0), rows.ctypes.data_as(C.c_void_p), len(rows),
+                                      C.byref(n)), 'emu_pw_embed_1d_to_2d')
+    return rows, int(n.value)
+
+
+def _check_sol1d(sol, nel, name):
+    if sol is None:
+        return
+    if sol.dtype != c128 or not sol.is_cuda or not sol.is_contiguous():
+        raise TypeError('%s must be a contiguous CUDA complex128 tensor' % name)
+    if sol.dim() != 4 or sol.shape[1] != nel or sol.shape[3] != 11:
+        raise ValueError('%s must be [batch][nel][nval][11]' % name)
+
+
+def mode_overlap_1d(dmesh, pp, k0, bloch, beta1, sol1, sol2, perm2=None, full=False):
+    """Orthogonality of adjoint and prime 1D modes (emu_mode_overlap_1d).
+    full=False: (diag [B, M], scale [B, M], n_small [B]); full=True: the
+    matrix [B, M, M]."""
+    _check_sol1d(sol1, dmesh.nel, 'sol1')
+    _check_sol1d(sol2, dmesh.nel, 'sol2')
+    B, _, M, _ = sol1.shape
+    dev = sol1.device
+    pp_t = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
+    d = _lib.EmuNormalise1D()
+    d.batch, d.nval, d.nel, d.npt = B, M, dmesh.nel, dmesh.npt
+    d.n_types = int(pp_t.numel())
+    d.d_x, d.d_table_nod, d.d_type_el = ptr(dmesh.x), ptr(dmesh.table_nod), ptr(dmesh.type_el)
+    d.d_pp, d.d_k0, d.d_bloch, d.d_beta1 = ptr(pp_t), ptr(k0), ptr(bloch), ptr(beta1)
+    d.d_sol1, d.d_sol2 = ptr(sol1), ptr(sol2)
+    d.d_perm2 = ptr(perm2)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    d.d_error = ptr(err)
+    if full:
+        out = torch.empty((B, M, M), dtype=c128, device=dev)
+        d.d_out = ptr(out)
+        check(lib().emu_mode_overlap_1d(C.byref(d), 1, stream_ptr()), 'emu_mode_overlap_1d')
+        res = out
+    else:
+        diag = torch.empty((B, M), dtype=c128, device=dev)
+        scale = torch.empty((B, M), dtype=c128, device=dev)
+        nsmall = torch.zeros(B, dtype=torch.int32, device=dev)
+        d.d_out, d.d_scale, d.d_n_small = ptr(diag), ptr(scale), ptr(nsmall)
+        check(lib().emu_mode_overlap_1d(C.byref(d), 0, stream_ptr()), 'emu_mode_overlap_1d')
+        res = (diag, scale, nsmall)
+    if int(err.item()) != 0:
+        raise ValueError('1D mesh: element nodes or material types out of range')
+    return res
+
+
+def reorder_pairs_1d(ovl):
+    """Conjugate-pair swaps of the adjoint modes over the orthogonality
+    matrix ``ovl`` [M, M] (rows adjoint, columns prime), as the loop of
+    orthogonal_1d.f:160-215 performs them: a mode whose <j|j> vanishes
+    (<= 1e-7) swaps its adjoint with every later adjoint j2 with
+    |<j2|j>| > 1e-7, and the mode after it is left alone.  Returns the
+    permutation (adjoint mode taken for each position) and the count of
+    unpaired last modes (the reference's pair_warning)."""
+    ovl = np.asarray(ovl)
+    M = ovl.shape[0]
+    perm = np.arange(M)
+    warn = 0
+    j, skip = 0, 0
+    while j < M:
+        if abs(ovl[j, j]) > 1e-7:
+            j += 1
+        elif skip == 0:
+            if j == M - 1:
+                warn += 1
+            for j2 in range(j + 1, M):
+                if abs(ovl[j2, j]) > 1e-7:
+                    perm[j], perm[j2] = perm[j2], perm[j]
+            skip = 1
+            j += 1
+        else:
+            skip = 0
+            j += 1
+    return perm.astype(np.int32), warn
+
+
+def overlap_1d_batch(dmesh, max_order, bloch, k0, sol1=None, sol2=None, scale=None, perm2=None,
+                     embed_2d=False, period_x=None):
+    """J [B, 2 Npw, M] and J_dag [B, M, 2 Npw] of 1D Bloch-mode fields
+    (emu_overlap1d_batch), rows at the reference's sorted positions; with
+    embed_2d also J_2d, J_dag_2d in the 2D order set.  bloch float64
+    [B, 2] (k_parallel * period), k0 [B] (2 pi / wl_norm) as host arrays.
+    Returns (J, J_dag, J_2d, J_dag_2d, index_pw_inv, rows_2d)."""
+    _check_sol1d(sol1, dmesh.nel, 'sol1')
+    _check_sol1d(sol2, dmesh.nel, 'sol2')
+    ref = sol1 if sol1 is not None else sol2
+    B, _, M, _ = ref.shape
+    dev = ref.device
+    px_ = float(dmesh.period_x if period_x is None else period_x)
+    bloch = np.asarray(bloch, np.float64).reshape(B, 2)
+    k0 = np.asarray(k0, np.float64).reshape(B)
+    npw = 2 * max_order + 1
+    inv = np.stack([pw_order_1d(max_order, px_, bloch[b, 0], bloch[b, 1], k0[b]) for b in range(B)])
+    rows = npw2 = None
+    if embed_2d:
+        r = [pw_rows_2d(max_order, px_, bloch[b, 0], bloch[b, 1], k0[b]) for b in range(B)]
+        rows = np.stack([x[0] for x in r])
+        npw2 = r[0][1]
+    d = _lib.EmuOverlap1D()
+    d.batch, d.nval, d.nel, d.npt, d.max_order = B, M, dmesh.nel, dmesh.npt, int(max_order)
+    d.d_x, d.d_table_nod, d.period_x = ptr(dmesh.x), ptr(dmesh.table_nod), px_
+    d_bloch = torch.tensor(bloch, device=dev)
+    d_inv = torch.tensor(inv, dtype=torch.int32, device=dev)
+    d.d_bloch, d.d_index_pw_inv = ptr(d_bloch), ptr(d_inv)
+    d.d_sol1, d.d_sol2, d.d_scale, d.d_perm2 = ptr(sol1), ptr(sol2), ptr(scale), ptr(perm2)
+    J = torch.empty((B, 2 * npw, M), dtype=c128, device=dev) if sol1 is not None else None
+    Jd = torch.empty((B, M, 2 * npw), dtype=c128, device=dev) if sol2 is not None else None
+    d.d_J, d.d_J_dag = ptr(J), ptr(Jd)
+    J2 = Jd2 = d_rows = None
+    if embed_2d:
+        d.npw_2d = npw2
+        d_rows = torch.tensor(rows, dtype=torch.int32, device=dev)
+        d.d_row_2d = ptr(d_rows)
+        if sol1 is not None:
+            J2 = torch.empty((B, 2 * npw2, M), dtype=c128, device=dev)
+        if sol2 is not None:
+            Jd2 = torch.empty((B, M, 2 * npw2), dtype=c128, device=dev)
+        d.d_J_2d, d.d_J_dag_2d = ptr(J2), ptr(Jd2)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    d.d_error = ptr(err)
+    check(lib().emu_overlap1d_batch(C.byref(d), stream_ptr()), 'emu_overlap1d_batch')
+    if int(err.item()) != 0:
+        raise ValueError('1D mesh: element nodes out of range')
+    return J, Jd, J2, Jd2, inv, rows
+
+
+def overlap_from_fields_1d(simmo, fields):
+    """J and J_dag of a 1D-grating Simmo from its mode fields, as
+    backend/fortran/py_calc_modes_1d.f:525-620 and backend/mode_calcs.py:
+    323-355 produce them: orthogonality of adjoint and prime modes, the
+    conjugate-pair swaps, normalisation of both by 1/sqrt(<m|m>), then J,
+    J_dag (in the 1D order set for world_1d layers, embedded in the 2D set
+    otherwise; no area division for 1D layers).
+
+    fields: 'sol1', 'sol2' ([nel][M][11], the reference layout of
+    sol(11, M, nel)), 'beta1' (default simmo.k_z), 'pp' (per material type,
+    default 1) and optionally 'mesh' (a Mesh1D, else simmo.structure.mesh).
+    """
+    st = simmo.structure
+    mesh = fields.get('mesh', getattr(st, 'mesh', None))
+    if mesh is None:
+        raise ValueError('overlap integrals need the mesh of the mode fields')
+    dev = torch.device('cuda', torch.cuda.current_device())
+    dm = DeviceMesh1D(mesh, dev)
+    sol1 = torch.as_tensor(np.ascontiguousarray(fields['sol1'], np.complex128), device=dev).unsqueeze(0)
+    sol2 = torch.as_tensor(np.ascontiguousarray(fields['sol2'], np.complex128), device=dev).unsqueeze(0)
+    M = sol1.shape[2]
+    beta1 = torch.as_tensor(np.asarray(fields.get('beta1', simmo.k_z), np.complex128).reshape(1, M),
+                            device=dev)
+    pp = fields.get('pp', np.ones(int(mesh.type_el.max()), np.complex128))
+    k0v = 2 * np.pi / simmo.wl_norm()
+    bl = np.asarray(simmo.k_pll_norm(), np.float64).reshape(1, 2)
+    k0 = torch.tensor([k0v], dtype=torch.float64, device=dev)
+    bloch = torch.tensor(bl, device=dev)
+    diag, scale, nsmall = mode_overlap_1d(dm, pp, k0, bloch, beta1, sol1, sol2)
+    perm = None
+    if int(nsmall[0].item()) != 0:
+        full = mode_overlap_1d(dm, pp, k0, bloch, beta1, sol1, sol2, full=True)[0].cpu().numpy()
+        p, warn = reorder_pairs_1d(full)
+        if warn and M <= 20:
+            print('Warning found 1 BM of cmplx conj pair, increase num_BMs to include the other.')
+        perm = torch.tensor(p.reshape(1, M), device=dev)
+        diag, scale, _ = mode_overlap_1d(dm, pp, k0, bloch, beta1, sol1, sol2, perm2=perm)
+    w1d = bool(st.world_1d)
+    J, Jd, J2, Jd2, _, _ = overlap_1d_batch(dm, simmo.max_order_PWs, bl, [k0v], sol1, sol2, scale=scale,
+                                            perm2=perm, embed_2d=not w1d)
+    simmo.overlap_diag = diag[0].cpu().numpy()
+    if w1d:
+        return np.asmatrix(J[0].cpu().numpy()), np.asmatrix(Jd[0].cpu().numpy())
+    return np.asmatrix(J2[0].cpu().numpy()), np.asmatrix(Jd2[0].cpu().numpy())

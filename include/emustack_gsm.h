@@ -439,6 +439,103 @@ size_t emu_mode_overlap_reorder_workspace_size(const EmuNormalise *p);
 int emu_mode_overlap_reorder(const EmuNormalise *p, int32_t *d_perm, int32_t *d_warn,
                              void *d_workspace, size_t workspace_bytes, void *stream);
 
+/* ----------------------------- a11, a12 for 1D gratings ('1D_array')
+ * Plane-wave order of the 1D set px = -max_order..max_order: the rank of
+ * each order (generation index s = px + max_order) when the keys
+ * -Re(kz^2), kz = sqrt(k0^2 - alpha^2 - beta^2), alpha = bloch_x +
+ * 2 pi px / period_x, beta = bloch_y, are sorted by the reference's
+ * quicksort (ties ranked as it ranks them).  Replaces pw_ordering_1d
+ * (backend/fortran/pw_ordering_1d.f:1-80 with z_indexx.f).  Host only.
+ * h_index_pw_inv: [2 max_order + 1], 0-based. */
+int emu_pw_order_1d(int max_order, double period_x, double bloch_x, double bloch_y, double k0,
+                    int32_t *h_index_pw_inv);
+
+/* Row of each 1D order (generation index) in the 2D order set of the same
+ * max_order built with period_x in both directions, sorted the same way:
+ * the placement of pw_matrix_1d_to_2d (backend/fortran/pw_matrix_1d_to_2d.f:
+ * 60-120).  Host only.  h_row_2d may be NULL to query *h_npw_2d (the 2D
+ * set's size); capacity >= 2 max_order + 1 otherwise. */
+int emu_pw_embed_1d_to_2d(int max_order, double period_x, double bloch_x, double bloch_y,
+                          double k0, int32_t *h_row_2d, int capacity, int *h_npw_2d);
+
+/* J (2 Npw x nval: E rows then K rows) and J_dag (nval x 2 Npw) of 1D
+ * Bloch-mode fields with the plane waves exp(-i alpha x) and exp(+i alpha x)
+ * (Npw = 2 max_order + 1), rows at the sorted positions of
+ * emu_pw_order_1d; with d_row_2d also both matrices embedded in the 2D
+ * order set (zero outside the (px, 0) rows).  Replaces J_overlap_1d
+ * (backend/fortran/J_overlap_1d.f:8-225), J_dagger_overlap_1d
+ * (backend/fortran/J_dagger_overlap_1d.f:1-225) and pw_matrix_1d_to_2d,
+ * called from backend/fortran/py_calc_modes_1d.f:583-620 and returned by
+ * backend/mode_calcs.py:323-355 (J, J_dag when world_1d, else J_2d,
+ * J_dag_2d; no area division for 1D layers).
+ * Fields use the reference layout sol(11, nval, nel) (Fortran order), i.e.
+ * [nel][nval][11] complex: Ex at the P2 nodes (x_min, x_max, midpoint), Ey
+ * at the P3 nodes (x_min, x_max, x_min + h/3, x_min + 2h/3), Ez (unused);
+ * table_nod is [nel][3], 1-based, its first two entries the element's end
+ * nodes.  An element whose end nodes fall outside [1, npt] is skipped and
+ * *d_error set to 1. */
+typedef struct {
+  int batch;               /* problems (wavelengths / k_parallel) on one mesh */
+  int nval;                /* Bloch modes                                   */
+  int nel, npt;            /* elements, P2 nodes                            */
+  int max_order;           /* 1D orders px = -max_order..max_order          */
+  const double *d_x;       /* [npt] node coordinates                        */
+  const int64_t *d_table_nod; /* [nel][3], 1-based                          */
+  double period_x;         /* period in the units of d_x (the reference's
+                              period_x: the span of the periodic nodes)     */
+  const double *d_bloch;   /* [batch][2] bloch_vec_x, bloch_vec_y           */
+  const int32_t *d_index_pw_inv; /* [batch][Npw] from emu_pw_order_1d       */
+  const emu_c128 *d_sol1;  /* [batch][nel][nval][11] or NULL                */
+  const emu_c128 *d_sol2;  /* adjoint fields, same layout, or NULL          */
+  const emu_c128 *d_scale; /* [batch][nval] normalisation of prime and adjoint
+                              mode n (emu_mode_overlap_1d), or NULL         */
+  const int32_t *d_perm2;  /* [batch][nval] adjoint mode taken for mode n
+                              after conjugate-pair swaps, or NULL           */
+  emu_c128 *d_J;           /* [batch][2 Npw][nval] (with d_sol1)            */
+  emu_c128 *d_J_dag;       /* [batch][nval][2 Npw] (with d_sol2)            */
+  int npw_2d;              /* 2D embedding: the 2D set's size, or 0         */
+  const int32_t *d_row_2d; /* [batch][Npw] from emu_pw_embed_1d_to_2d, or NULL */
+  emu_c128 *d_J_2d;        /* [batch][2 npw_2d][nval]                       */
+  emu_c128 *d_J_dag_2d;    /* [batch][nval][2 npw_2d]                       */
+  int32_t *d_error;        /* [1] or NULL                                   */
+} EmuOverlap1D;
+
+int emu_overlap1d_batch(const EmuOverlap1D *p, void *stream);
+
+/* Orthogonality of the adjoint and prime 1D Bloch modes,
+ *   <i|j> = beta1(j) / k0 sum_el pp(type) (u_x Mxx v_x + u_y Myy v_y
+ *           - u_x Kxy v_z - i bloch_y u_y Myy v_z),
+ * u the adjoint mode perm2[i] and v the prime mode j on each element
+ * (Mxx, Myy the P2 and P3 mass matrices, Kxy = int phi_P2 dpsi_P3/dx).
+ * full = 0: the diagonal into d_out [batch][nval], the normalisation
+ * factors 1/sqrt(<m|m>) (1 where |sqrt| <= 1e-8) into d_scale (optional)
+ * and the count of |<m|m>| <= 1e-7 into d_n_small (optional); full = 1: the
+ * whole matrix into d_out [batch][nval][nval].  Replaces orthogonal_1d
+ * (backend/fortran/orthogonal_1d.f:1-158; its conjugate-pair swap loop,
+ * :160-215, runs on the host over the full matrix) and normalisation_1d
+ * (backend/fortran/normalisation_1d.f:1-34), called from
+ * backend/fortran/py_calc_modes_1d.f:531-547. */
+typedef struct {
+  int batch, nval, nel, npt;
+  int n_types;               /* material types (1-based in d_type_el)       */
+  const double *d_x;         /* [npt]                                       */
+  const int64_t *d_table_nod;/* [nel][3], 1-based                           */
+  const int64_t *d_type_el;  /* [nel], 1-based                              */
+  const emu_c128 *d_pp;      /* [n_types]                                   */
+  const double *d_k0;        /* [batch] 2 pi / wl_norm                      */
+  const double *d_bloch;     /* [batch][2]                                  */
+  const emu_c128 *d_beta1;   /* [batch][nval] prime propagation constants   */
+  const emu_c128 *d_sol1;    /* [batch][nel][nval][11]                      */
+  const emu_c128 *d_sol2;    /* [batch][nel][nval][11]                      */
+  const int32_t *d_perm2;    /* [batch][nval] or NULL                       */
+  emu_c128 *d_out;
+  emu_c128 *d_scale;         /* [batch][nval] or NULL                       */
+  int32_t *d_n_small;        /* [batch] or NULL                             */
+  int32_t *d_error;          /* [1] or NULL                                 */
+} EmuNormalise1D;
+
+int emu_mode_overlap_1d(const EmuNormalise1D *p, int full, void *stream);
+
 /* Allocation-free variant of emu_film_stack_batch (no counterpart in the
  * reference, which has no GPU path).  For callers that cannot allocate
  * device memory where they solve -- a thread in a latency-critical loop

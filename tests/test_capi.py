@@ -68,7 +68,7 @@ def test_grating_orders_1d_and_errors():
 
 STRUCTS = ('EmuFilmStackBatch', 'EmuAnalloModes', 'EmuLayer', 'EmuStackDense', 'EmuOverlap',
            'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch', 'EmuVarLayer', 'EmuStackPoint',
-           'EmuStackVarBatch')
+           'EmuStackVarBatch', 'EmuOverlap1D', 'EmuNormalise1D')
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -179,3 +179,48 @@ def test_film_sources_build_with_exact_rounding():
     sources are compiled without compiler-chosen multiply-add contraction."""
     from emustack_b200 import build
     assert {'film_stack.cu', 'film_varlen.cu'} <= build.EXACT_ROUNDING
+
+
+@pytest.mark.parametrize('max_order', [0, 1, 3, 4, 6, 9, 15, 20])
+def test_pw_order_1d_matches_the_oracle(max_order):
+    """emu_pw_order_1d ranks the 1D plane waves as the oracle's restatement
+    of pw_ordering_1d / z_indexx does, tied keys included (zero Bloch
+    vector: +-px tie)."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    from oracle import overlap1d_oracle as O
+    L = _lib.lib()
+    rng = np.random.default_rng(max_order)
+    cases = [(0.0, 0.0, 2 * np.pi / 1.3), (0.0, 0.0, 2 * np.pi / 0.61)] + \
+        [(rng.uniform(-1, 1), rng.uniform(-1, 1), 2 * np.pi / rng.uniform(0.5, 2.5)) for _ in range(4)]
+    for period_x in (1.0, 0.83):
+        for bx, by, k0 in cases:
+            out = np.empty(2 * max_order + 1, np.int32)
+            assert L.emu_pw_order_1d(max_order, period_x, bx, by, k0, out.ctypes.data_as(C.c_void_p)) == 0
+            _, inv = O.pw_order_1d(max_order, period_x, bx, by, k0)
+            np.testing.assert_array_equal(out, inv)
+
+
+@pytest.mark.parametrize('max_order', [1, 3, 4, 6, 10])
+def test_pw_embed_1d_to_2d_matches_the_oracle(max_order):
+    """emu_pw_embed_1d_to_2d places each 1D order where the oracle's
+    restatement of pw_matrix_1d_to_2d puts its J row."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    from oracle import overlap1d_oracle as O
+    L = _lib.lib()
+    for period_x, bx, by, k0 in ((1.0, 0.0, 0.0, 2 * np.pi / 1.1), (1.0, 0.31, -0.2, 7.3),
+                                 (0.7, 0.0, 0.0, 4.0)):
+        n2 = C.c_int(0)
+        assert L.emu_pw_embed_1d_to_2d(max_order, period_x, bx, by, k0, None, 0, C.byref(n2)) == 0
+        rows = np.empty(2 * max_order + 1, np.int32)
+        assert L.emu_pw_embed_1d_to_2d(max_order, period_x, bx, by, k0, rows.ctypes.data_as(C.c_void_p),
+                                       len(rows), C.byref(n2)) == 0
+        _, inv = O.pw_order_1d(max_order, period_x, bx, by, k0)
+        npw1 = 2 * max_order + 1
+        J = np.zeros((2 * npw1, 1), complex)
+        J[:npw1, 0] = 1 + np.arange(npw1)          # label each sorted 1D row
+        J2, _, (p2, _) = O.pw_matrix_1d_to_2d(J, J.T.copy(), period_x, bx, by, max_order, k0, inv)
+        assert n2.value == len(p2)
+        for o in range(npw1):
+            assert J2[rows[o], 0] == 1 + inv[o]

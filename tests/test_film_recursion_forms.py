@@ -3,9 +3,10 @@
 The film kernels (emustack_b200/csrc/film_core.cuh) do not evaluate the
 reference's interface and cascade formulas (backend/mode_calcs.py:451-477,
 backend/stack.py:229-278) literally: between two air gaps they use impedances
-scaled by k_z k_z,air (TE) or k k_air (TM), take T12 only through
-T12 T21 = 4AB/(A+B)^2, and fold the per-layer quotients into
-x1 p x2 = T12 T21 p / (d1 d2).  This file restates that form in numpy
+scaled by k_z k_z,air (TE) or k k_air (TM), use T12 T21 + R12^2 = 1 to
+write each gap-and-layer step as a Moebius map with one quotient, and fold
+the per-layer transmission into x1 p x2 = 4AB p / D over the same
+denominator.  This file restates that form in numpy
 (vectorised over the orders of one point) and checks it against the oracle's
 literal restatement of the reference, so the algebra is pinned without a GPU.
 """
@@ -31,11 +32,15 @@ def kernel_form(ns, heights_nm, wl_nm, k_pll, period, max_order):
     mods = [O.FilmModes(n, wl_nm, k_pll, period, None, max_order, air=air) for n in ns]
     z_air = air.Z()
 
-    def scaled(l):
+    def scaled_ab(l):
         m = mods[l]
         k, n, kz = m.k(), m.n_val, m.k_z[:npw]
         A = np.concatenate((k / n * kz_air, kair / n * kz))
         B = np.concatenate((kair * kz, k * kz_air))
+        return A, B
+
+    def scaled(l):
+        A, B = scaled_ab(l)
         R = (A - B) / (A + B)
         TT = 4 * A * B / (A + B) ** 2
         return R, TT
@@ -48,18 +53,20 @@ def kernel_form(ns, heights_nm, wl_nm, k_pll, period, max_order):
     rnet, tnet = R0, t12(0)
     g_list = []
     for l in range(1, L - 1):
-        R, TT = scaled(l)
+        # Moebius form: s = A + B, d = A - B, u = s - d r, v = s r - d,
+        # D = s u + d p^2 v, N = d u + s p^2 v; r' = N / D, x1 p x2 = 4 A B p / D
+        A, B = scaled_ab(l)
+        s_, d_ = A + B, A - B
         kz = mods[l].k_z
         p = np.exp(1j * kz * heights_nm[l - 1] / period)
-        d1 = 1 / (1 - R * rnet)
-        ug = TT * d1
-        rg = ug * rnet - R
-        prr = p * p * rg
-        d2 = 1 / (1 + R * prr)
-        g = ug * p * d2
+        u = s_ - d_ * rnet
+        v = s_ * rnet - d_
+        D = s_ * u + d_ * p * p * v
+        N = d_ * u + s_ * p * p * v
+        g = 4 * A * B * p / D
         g_list.append(g)
         tnet = tnet * g
-        rnet = R + TT * prr * d2
+        rnet = N / D
     R, TT = scaled(L - 1)
     d1 = 1 / (1 - R * rnet)
     tnet = tnet * t12(L - 1) * d1

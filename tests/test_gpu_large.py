@@ -13,10 +13,13 @@ backend/stack.py:196-426 for the cascade and the fluxes).
 
 Layers get seeded synthetic Bloch modes (complex normal J, J_dag of scale
 0.25 / sqrt(P), k_z with Re U(0, 2 k0), Im U(0, 0.1 k0)).  With these inputs a
-relative perturbation of the J entries is amplified about 3e3-fold into
-R_net, so FP64 results computed in different orders agree to about 1e-12;
-the tests hold every entry to rtol 1e-9 with an absolute floor of
-1e-10 x max(1, max |entry|).
+relative perturbation of the J entries is amplified 2e3- to 6e3-fold into
+R_net and T_net (measured on the oracle), and the rounding of LU
+factorisations of order 600 amounts to a relative perturbation of about
+1e-13, so FP64 results computed in different orders differ by up to about
+1e-10 of the largest entry.  The tests hold every entry to rtol 1e-9 with an
+absolute floor of 1e-9 x max(1, max |entry|) (a normwise relative bar of
+1e-9; the product bar is 1e-6 absolute).
 """
 import numpy as np
 import pytest
@@ -27,7 +30,7 @@ pytestmark = pytest.mark.gpu
 
 def _close(got, ref, msg):
     got, ref = np.asarray(got), np.asarray(ref)
-    atol = 1e-10 * max(1.0, float(np.abs(ref).max()) if ref.size else 1.0)
+    atol = 1e-9 * max(1.0, float(np.abs(ref).max()) if ref.size else 1.0)
     np.testing.assert_allclose(got, ref, rtol=1e-9, atol=atol, err_msg=msg)
 
 

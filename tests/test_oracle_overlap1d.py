@@ -178,3 +178,71 @@ def test_embedding_in_the_2d_order_set():
         np.testing.assert_array_equal(Jd2[:, s + npw2], Jd[:, inv[o] + npw1])
     rest = np.setdiff1d(np.arange(2 * npw2), used)
     assert not J2[rest].any() and not Jd2[:, rest].any()
+
+
+def test_z_indexx_hand_traced_ties():
+    """The reference ranks plane waves with Numerical Recipes' indexx
+    (z_indexx.f).  For px = -4..4 at zero Bloch vector the keys are
+    alpha^2 - k0^2 with alpha = 2 pi px, tied in pairs +-px.  Traced by hand
+    through its steps (n = 9 > 7: one partition about the median of
+    keys(1), keys(5), keys(9), which leaves positions 1-7 to straight
+    insertion and 8-9 in place) the order is px = 0, -1, 1, -2, 2, 3, -3,
+    -4, 4: ties are NOT broken by generation index for px = +-3."""
+    px, inv = O.pw_order_1d(4, 1.0, 0.0, 0.0, 2 * np.pi / 1.3)
+    order = np.empty_like(inv)
+    order[inv] = np.arange(len(inv))
+    np.testing.assert_array_equal(px[order], [0, -1, 1, -2, 2, 3, -3, -4, 4])
+
+
+def test_z_indexx_sorts_and_is_stable_below_seven():
+    rng = np.random.default_rng(3)
+    for t in range(400):
+        n = int(rng.integers(1, 70))
+        keys = rng.integers(0, 6, n).astype(float) if t % 2 else rng.standard_normal(n)
+        idx = O.z_indexx(keys)
+        assert sorted(idx.tolist()) == list(range(n))
+        assert np.all(np.diff(keys[idx]) >= 0)
+        if n < 7:   # straight insertion only: ties keep their input order
+            np.testing.assert_array_equal(idx, np.argsort(keys, kind='stable'))
+
+
+def test_element_matrices_are_the_lagrange_integrals():
+    """The GPU kernel forms the element matrices of the 1D orthogonality
+    integral from the Lagrange coefficients of the P2 / P3 bases on [0, 1]
+    (overlap1d.cu kP2c / kP3c); they equal the reference's rational tables
+    (matrix_mxx_1d.f, matrix_myy_1d.f, matrix_kxy_1d.f)."""
+    P2 = np.array([[1, -3, 2], [0, -1, 2], [0, 4, -4]], float)
+    P3 = np.array([[1, -5.5, 9, -4.5], [0, 1, -4.5, 4.5], [0, 9, -22.5, 13.5], [0, -4.5, 18, -13.5]])
+    for node, coef, pts in ((O.p2_nodes, P2, 3), (O.p3_nodes, P3, 4)):
+        t = node(0.0, 1.0)
+        V = np.vander(t, pts, increasing=True)
+        np.testing.assert_allclose(coef @ V.T, np.eye(pts), atol=1e-14)   # l_i(t_j) = delta_ij
+    mxx = np.array([[sum(P2[i, p] * P2[j, q] / (p + q + 1) for p in range(3) for q in range(3))
+                     for j in range(3)] for i in range(3)])
+    myy = np.array([[sum(P3[i, p] * P3[j, q] / (p + q + 1) for p in range(4) for q in range(4))
+                     for j in range(4)] for i in range(4)])
+    kxy = np.array([[sum(P2[i, p] * q * P3[j, q] / (p + q) for p in range(3) for q in range(1, 4))
+                     for j in range(4)] for i in range(3)])
+    h = 0.37
+    rm, ry, rk = O.element_matrices_1d(0.2, 0.2 + h)
+    np.testing.assert_allclose(h * mxx, rm, atol=1e-15)
+    np.testing.assert_allclose(h * myy, ry, atol=1e-14)
+    np.testing.assert_allclose(kxy, rk, atol=1e-14)
+
+
+def test_host_pair_swap_matches_the_oracle():
+    """The drop-in's host port of the conjugate-pair swap loop
+    (emustack_b200.overlap.reorder_pairs_1d) gives the same permutation as
+    the oracle's literal restatement, on matrices with vanishing diagonals."""
+    from emustack_b200.overlap import reorder_pairs_1d
+    rng = np.random.default_rng(8)
+    for t in range(60):
+        M = int(rng.integers(2, 12))
+        ovl = rng.standard_normal((M, M)) + 1j * rng.standard_normal((M, M))
+        ovl[rng.random((M, M)) < 0.4] *= 1e-9
+        small = rng.random(M) < 0.5
+        ovl[np.arange(M)[small], np.arange(M)[small]] = 1e-9
+        perm, warn = reorder_pairs_1d(ovl)
+        lab, w = O.pair_swap_order_1d(ovl)
+        np.testing.assert_array_equal(perm, lab)
+        assert warn == w
