@@ -1,13 +1,14 @@
-"""Benchmark of the B200 GSM stage on the batched thin-film workload.
+"""Benchmark of the B200 GSM stage.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config 1|2|3|4|5] [--no-extras]
 
-Workload (one "step" = one batch): 10 films per stack (heights U(20,300) nm,
-n U(1.3,4.0) + i U(0,0.5)) on an n=1.46 substrate under n=1.0, period
-500 nm, max_order_PWs 5 (81 orders per polarisation, P = 162), evaluated at
-2048 wavelengths U(350,1100) nm x 16 angles theta U(0,60), phi U(0,90)
-(32768 spectral points), TE incidence, seeded synthetic data.  The metric is
-R/T/A spectral points per second.
+Headline workload (config 2, the default; one "step" = one batch): 10 films
+per stack (heights U(20,300) nm, n U(1.3,4.0) + i U(0,0.5)) on an n=1.46
+substrate under n=1.0, period 500 nm, max_order_PWs 5 (81 orders per
+polarisation, P = 162), evaluated at 2048 wavelengths U(350,1100) nm x 16
+angles theta U(0,60), phi U(0,90) (32768 spectral points), TE incidence,
+seeded synthetic data.  The metric is R/T/A spectral points per second.
 
 Arms
   ours       : device-resident inputs, one fused launch per step (`value`);
@@ -15,10 +16,19 @@ Arms
                (FilmHostPipeline) with pinned host inputs: host->device
                copies, the solves and the device->host read of R_net/T_net
                diagonals and a/t/r lists, in 4096-point pieces on four
-               streams so copies overlap solves.
+               streams so copies overlap solves.  Unless --no-extras, the
+               same JSON line carries `north_star`: the batched GSM against
+               the plain FP64 GPU GSM (this library called once per solve,
+               the way the reference calls its GSM) on config 2, on the
+               config-1 chain (tensor-core J) and on a config-4 mix of
+               uneven film and array solves, and a short Poisson-arrival
+               serving run (config 5) with request p50 / p99 latency.
   reference  : the reference's FP64 algorithm (the CPU oracle, a numpy
                restatement of backend/stack.py + backend/mode_calcs.py) on the
                host cores, a bounded sample per step.
+
+--config 1|3|4|5 prints one JSON line of that workload alone, in more depth
+(the commands under profiles/ use them); --config 2 is the contract line.
 
 Multi-GPU (torchrun): replicas; every rank solves its own full batch, no
 collective on the data path (weak scaling); the step time is the max over
@@ -27,11 +37,14 @@ ranks.
 from __future__ import annotations
 
 import argparse
+import collections
+import gc
 import json
 import multiprocessing as mp
 import os
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -166,12 +179,51 @@ class ClockSampler(object):
                 'samples': len(sm)}
 
 
-# ---------------------------------------------------------------- GPU arm
+def _events(n):
+    import torch
+    return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+
+
+def _timed(fn, steps, warmup=2, flush=None):
+    """Median ms of `steps` calls of fn (CUDA events on the current stream,
+    after `warmup` untimed calls; L2 flushed before each timed call when a
+    flush buffer is given)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for i in range(steps):
+        if flush is not None:
+            flush.fill_(i & 0xff)
+        a, b = _events(2)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+# ---------------------------------------------------------------- config 2
 def algorithmic_counts(B, L, P):
     """Algorithmic bytes of one batch: inputs read once (wl, k_pll, n) and the
     outputs written once (R_net, T_net diagonals, a/t lists, r, flags)."""
     by = B * (8 + 16 + 16 * L + 2 * 16 * P + 2 * 8 * (L - 1) + 8 + 4)
     return by
+
+
+def film_flops(B, L, P):
+    """Algorithmic FP64 operations of one batch of all-film stacks (each of
+    + - * / sqrt counted as one), counted on the reference's recursion for
+    diagonal matrices: per (point, order, layer) the k_z square root
+    argument and root (12), k and impedances (24), per polarisation the
+    Fresnel pair (2 roots, 2 quotients: 40) and one cascade step (2 complex
+    quotients, 6 complex products, 3 complex sums: 64).  The kernel's
+    one-quotient form does less arithmetic than this count."""
+    npw = P // 2
+    per_order_layer = 12 + 24 + 2 * (40 + 64)
+    return float(B) * npw * L * per_order_layer
 
 
 def run_ours(args, rank, world, local_rank):
@@ -205,8 +257,8 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = _events(args.steps)
+    ends = _events(args.steps)
     launches0 = lib.emu_launch_count()
     with ClockSampler(local_rank) as clk:
         for i in range(args.steps):
@@ -249,8 +301,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_s = _events(args.steps)
+    e_e = _events(args.steps)
     for i in range(args.steps):
         flush.fill_(i & 0xff)
         e_s[i].record(stream)
@@ -311,6 +363,8 @@ def run_ours(args, rank, world, local_rank):
             'clocks': clk.summary(),
             'autotune': _tuned(),
         }
+        if not args.no_extras:
+            result['north_star'] = north_star_extras(dev, w, solver, value)
     return result
 
 
@@ -323,15 +377,377 @@ def _tuned():
             for k, e in default_tuner().log]
 
 
-def film_flops(B, L, P):
-    """Algorithmic FP64 operations of one batch of all-film stacks (each of
-    + - * / sqrt counted as one): per (point, order, layer) the k_z square
-    root argument and root (12), k and impedances (24), per polarisation the
-    Fresnel pair (2 roots, 2 quotients: 40) and one cascade step (2 complex
-    quotients, 6 complex products, 3 complex sums: 64)."""
-    npw = P // 2
-    per_order_layer = 12 + 24 + 2 * (40 + 64)
-    return float(B) * npw * L * per_order_layer
+# ---------------------------------------------------------------- extras
+def plain_config2(dev, w, n_points=1024):
+    """The plain FP64 GPU GSM on the config-2 points: one spectral point per
+    call of the public solver (emu_film_stack_batch with B = 1), inputs
+    already on the device, as the reference calls its GSM once per
+    Stack.calc_scat.  Returns points/s."""
+    import torch
+    from emustack_b200.films import FilmStackSolver
+    s = FilmStackSolver(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev)
+    idx = np.random.default_rng(5).choice(len(w['wl']), n_points, replace=False)
+    pts = [(torch.tensor(w['wl'][i:i + 1], device=dev), torch.tensor(w['k_pll'][i:i + 1], device=dev),
+            torch.tensor(w['n'][i:i + 1], device=dev)) for i in idx]
+    h = torch.tensor(w['heights'], device=dev)
+
+    def run():
+        for wl, kp, n in pts:
+            s.solve(wl, kp, n, h, pol=POL)
+
+    ms = _timed(run, 3, warmup=1)
+    return n_points / (ms / 1e3)
+
+
+def order_table(period, max_mo=16):
+    from emustack_b200.films import grating_orders
+    return np.array([len(grating_orders(m, period, period)[0]) for m in range(max_mo + 1)])
+
+
+def film_requests(n, seed=0, period=500.0):
+    """Uneven all-film solves of the uneven-batch distribution: P = 2 Npw
+    log-uniform in [50, 900] (the order set of the max order whose Npw is
+    nearest), 2-12 finite layers, n U(1.3, 4.0) + i U(0, 0.5) on n = 1.46
+    under air, heights U(20, 300) nm, wavelength U(350, 1100) nm, theta
+    U(0, 60), phi U(0, 90) degrees, polarisations TE / TM / un / R Circ."""
+    from emustack_b200.serving import FilmRequest
+    rng = np.random.default_rng(seed)
+    tab = order_table(period)
+    pols = ('TE', 'TM', 'un', 'R Circ')
+    reqs = []
+    P = np.exp(rng.uniform(np.log(50), np.log(900), n))
+    for i in range(n):
+        mo = int(np.argmin(np.abs(tab - P[i] / 2)))
+        L = int(rng.integers(2, 13)) + 2
+        nn = np.concatenate([[1.46 + 0j], rng.uniform(1.3, 4.0, L - 2) + 1j * rng.uniform(0, 0.5, L - 2),
+                             [1.0 + 0j]])
+        wl = rng.uniform(350, 1100)
+        th, ph = np.radians(rng.uniform(0, 60)), np.radians(rng.uniform(0, 90))
+        k = 2 * np.pi / wl
+        kp = np.array([k * np.sin(th) * np.cos(ph), k * np.sin(th) * np.sin(ph)])
+        reqs.append(FilmRequest(nn, rng.uniform(20, 300, L - 2), wl, kp, period, mo, pol=pols[i % 4]))
+    return reqs
+
+
+def time_film_mix(dev, reqs, per_solve=256):
+    """Uneven film solves: one emu_film_var_batch launch for all of them
+    against one emu_film_stack_batch launch per solve (a sample,
+    extrapolated).  Returns (batched ms, per-solve ms) for the whole set."""
+    import torch
+    from emustack_b200.films import FilmStackSolver, FilmVarSolver
+    vs = FilmVarSolver(dev)
+    pl = vs.plan(reqs)
+    ms_var = _timed(lambda: vs.solve(pl), 5, warmup=2)
+    single = []
+    for r in reqs[:per_solve]:
+        L = len(r.n)
+        s = FilmStackSolver(L, r.max_order, 500.0, device=dev)
+        single.append((s, torch.tensor([r.wl_nm], dtype=torch.float64, device=dev),
+                       torch.tensor(r.k_pll.reshape(1, 2), dtype=torch.float64, device=dev),
+                       torch.tensor(r.n.reshape(1, L), dtype=torch.complex128, device=dev),
+                       torch.tensor(r.heights, dtype=torch.float64, device=dev), r.pol))
+
+    def run():
+        for s, wl, kp, n, h, pol in single:
+            s.solve(wl, kp, n, h, pol=pol)
+
+    ms_one = _timed(run, 2, warmup=1) / len(single) * len(reqs)
+    return ms_var, ms_one
+
+
+def array_stack_specs(n, seed=0, period=500.0):
+    """Nanostructured-array stacks of the uneven distribution: P = 2 Npw
+    log-uniform in [50, 900] (nearest order set), M = P + 20 Bloch modes per
+    array layer (the reference's default num_BMs), 2-12 array layers between
+    a film substrate (n = 1.46) and air, heights U(50, 200) nm, wavelength
+    U(350, 1100) nm, normal incidence, TE.  The layers' J (P x M) and J_dag
+    (M x P) are complex N(0,1)/sqrt(P), Bloch k_z Re U(0, 2 k0),
+    Im U(0, 0.1 k0)."""
+    rng = np.random.default_rng(seed)
+    tab = order_table(period)
+    P = np.exp(rng.uniform(np.log(50), np.log(900), n))
+    out = []
+    for i in range(n):
+        mo = int(np.argmin(np.abs(tab - P[i] / 2)))
+        out.append(dict(mo=mo, npw=int(tab[mo]), K=int(rng.integers(2, 13)), wl=float(rng.uniform(350, 1100)),
+                        seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def _air_kz(px, py, wl, period, n=1.0):
+    k = 2 * np.pi * n / (wl / period)
+    al = 2 * np.pi * px + 2 * np.pi * 1e-12
+    be = 2 * np.pi * py
+    return np.sqrt((k * k - al * al - be * be).astype(np.complex128))
+
+
+def prepare_array_groups(stacks, period=500.0, group=True):
+    """Device inputs of the array stacks grouped by shape (order set,
+    number of layers), or one group per stack."""
+    import torch
+    from emustack_b200.films import grating_orders
+    dev = torch.device('cuda')
+    keyf = (lambda s: (s['mo'], s['K'])) if group else (lambda s: id(s))
+    groups = collections.defaultdict(list)
+    for s in stacks:
+        groups[keyf(s)].append(s)
+    prepared = []
+    for _, ss in groups.items():
+        mo, K = ss[0]['mo'], ss[0]['K']
+        px, py = grating_orders(mo, period, period)
+        npw = len(px)
+        P, M, B = 2 * npw, 2 * npw + 20, len(ss)
+        wl = np.array([s['wl'] for s in ss])
+        wln = wl / period
+        kza = np.stack([_air_kz(px, py, x, period) for x in wl])
+        order = np.argsort(-kza.real + kza.imag, axis=1, kind='stable')
+        kza = np.take_along_axis(kza, order, 1)
+        kzs = np.take_along_axis(np.stack([_air_kz(px, py, x, period, 1.46) for x in wl]), order, 1)
+        g = torch.Generator(device='cuda').manual_seed(ss[0]['seed'])
+        cr = lambda *sh: torch.complex(torch.randn(sh, dtype=torch.float64, device=dev, generator=g),
+                                       torch.randn(sh, dtype=torch.float64, device=dev, generator=g))
+        k0 = torch.tensor(2 * np.pi / wln, device=dev)
+        prepared.append(dict(
+            B=B, P=P, M=M, K=K, kza=torch.tensor(kza, device=dev), kzs=torch.tensor(kzs, device=dev),
+            wln=torch.tensor(wln, device=dev),
+            J=[cr(B, P, M) / np.sqrt(P) for _ in range(K)], Jd=[cr(B, M, P) / np.sqrt(P) for _ in range(K)],
+            kz=[torch.complex(2 * torch.rand(B, M, dtype=torch.float64, device=dev, generator=g),
+                              0.1 * torch.rand(B, M, dtype=torch.float64, device=dev, generator=g))
+                * k0[:, None] for _ in range(K)],
+            h=[float(x) for x in np.random.default_rng(ss[0]['seed']).uniform(50, 200, K) / period],
+            spec=torch.zeros(B, dtype=torch.int32, device=dev),
+            nprop=torch.tensor([[int((kza[b].imag == 0).sum())] * 2 + [int((kzs[b].imag == 0).sum())]
+                                for b in range(B)], dtype=torch.int32, device=dev)))
+    return prepared
+
+
+def _group_layers(lay):
+    """Interfaces of one group (film substrate, K array layers, air)."""
+    import torch
+    from emustack_b200.dense import DenseLayer, film_interface, interface_dense
+    B = lay['B']
+    dev = lay['kza'].device
+    na = torch.ones(B, dtype=torch.complex128, device=dev)
+    ns = torch.full((B,), 1.46 + 0j, dtype=torch.complex128, device=dev)
+    Rs, Ts = film_interface(lay['kza'], na, lay['kzs'], ns, lay['wln'])
+    Ra, Ta = film_interface(lay['kza'], na, lay['kza'], na, lay['wln'])
+    layers = [DenseLayer(Rs, Ts, -Rs, Ts, False)]
+    for k in range(lay['K']):
+        R12, T12, R21, T21, _ = interface_dense(lay['kza'], na, lay['wln'], lay['J'][k], lay['Jd'][k])
+        layers.append(DenseLayer(R12, T12, R21, T21, True, lay['kz'][k], lay['h'][k]))
+    layers.append(DenseLayer(Ra, Ta, -Ra, Ta, False))
+    return layers
+
+
+def time_array_stacks(stacks, group=True, n_streams=4):
+    """Array stacks, interfaces included: grouped by shape into batched
+    calls dealt round-robin to n_streams streams, or one call per stack.
+    Returns ms for the set."""
+    import torch
+    from emustack_b200.dense import DenseStackSolver
+    dev = torch.device('cuda')
+    prepared = prepare_array_groups(stacks, group=group)
+    streams = [torch.cuda.Stream(dev) for _ in range(n_streams)]
+    solvers = [DenseStackSolver(dev) for _ in range(n_streams)]
+
+    def one(lay, solver):
+        solver.solve(_group_layers(lay), lay['P'], pol='TE', specular=lay['spec'], num_prop=lay['nprop'])
+
+    def run():
+        main = torch.cuda.current_stream(dev)
+        for st in streams:
+            st.wait_stream(main)
+        for i, lay in enumerate(prepared):
+            with torch.cuda.stream(streams[i % n_streams]):
+                one(lay, solvers[i % n_streams])
+        for st in streams:
+            main.wait_stream(st)
+
+    return _timed(run, 1, warmup=1)
+
+
+def config1_chain(dev, batch=50, steps=10):
+    """Config-1 chain (film k_z, adjoint normalisation, J / J_dag,
+    interfaces, cascade, fluxes) of one 2D array (period 600 nm, 2048-
+    triangle P2 mesh, 60 Bloch modes, max order 3) at `batch` wavelengths
+    400-900 nm: plain = one wavelength per call, FP64 J, eager; batched =
+    all wavelengths in one CUDA graph with the tensor-core (split-TF32 x3) J.
+    Returns wavelengths/s of both and the largest |delta| of the a/t/r lists
+    of the batched tensor-core chain against the batched FP64 chain."""
+    import torch
+    from emustack_b200.mesh import square_cell
+    from emustack_b200.pipeline import NanoStackPipeline
+    period, M = 600.0, 60
+    mesh = square_cell(32, radius=120.0 / period)
+    wl = np.linspace(400.0, 900.0, batch)
+    th = np.radians(1e-5)
+    k = 2 * np.pi / wl
+    kp = np.stack([k * np.sin(th) * np.cos(th), k * np.sin(th) * np.sin(th)], axis=1)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    shape = (batch, mesh.nel, M, 13, 3)
+    cr = lambda: 0.02 * torch.complex(torch.randn(shape, dtype=torch.float64, device=dev, generator=g),
+                                      torch.randn(shape, dtype=torch.float64, device=dev, generator=g))
+    s1, s2 = cr(), cr()
+    k0 = 2 * np.pi / (wl / period)
+    rng = np.random.default_rng(0)
+    beta = rng.uniform(0, 2, (batch, M)) * k0[:, None] + 1j * rng.uniform(0, 0.1, (batch, M)) * k0[:, None]
+    beta = torch.tensor(beta, device=dev)
+    res = {}
+    lists = {}
+    for prec in ('fp64', 'tf32x3'):
+        pl = NanoStackPipeline(mesh, period, 3, M, batch, 100.0, precision=prec)
+        pl.load(wl, kp, s1, s2, beta)
+        out = pl.capture()
+        ms = _timed(pl.replay, steps, warmup=2)
+        res[prec] = batch / (ms / 1e3)
+        lists[prec] = np.concatenate([out[k].cpu().numpy().reshape(batch, -1)
+                                      for k in ('a_list', 't_list', 'r_list')], axis=1)
+        del pl
+    # plain: one wavelength per call, FP64, eager
+    pl1 = NanoStackPipeline(mesh, period, 3, M, 1, 100.0, precision='fp64')
+    n_plain = 10
+    loads = [(wl[i:i + 1], kp[i:i + 1], s1[i:i + 1].clone(), s2[i:i + 1].clone(), beta[i:i + 1].clone())
+             for i in range(n_plain)]
+
+    def plain():
+        for a in loads:
+            pl1.load(*a)
+            pl1.forward()
+
+    ms1 = _timed(plain, 3, warmup=1)
+    plain_wl = n_plain / (ms1 / 1e3)
+    return {'batched_wl_per_s': res['tf32x3'], 'batched_fp64_wl_per_s': res['fp64'],
+            'plain_wl_per_s': plain_wl, 'ratio': res['tf32x3'] / plain_wl,
+            'max_abs_delta_RTA_vs_fp64': float(np.abs(lists['tf32x3'] - lists['fp64']).max()),
+            'workload': 'config 1: 1 array (period 600 nm, 2048 triangles, 60 modes, P = 58), '
+                        '%d wavelengths 400-900 nm; batched = one CUDA graph, split-TF32 x3 J, FP64 '
+                        'interfaces/cascade; plain = one wavelength per call, FP64, eager' % batch}
+
+
+def serving_run(rate, seconds=1.0, seed=0):
+    """Open-loop Poisson arrivals of uneven film requests at `rate` per
+    second through the continuous-batching server (GsmServer); latency from
+    each request's scheduled arrival to its result on the host."""
+    from emustack_b200.serving import GsmServer
+    n = max(int(rate * seconds), 200)
+    reqs = film_requests(n, seed)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, n)
+    srv = GsmServer(max_batch=32768, batching='mixed', n_streams=2).start()
+    warm = film_requests(max(64, min(32768, int(rate * 0.2))), seed + 2)
+    for _ in range(2):
+        for f in [srv.submit(r) for r in warm]:
+            f.result(timeout=300)
+    srv.latencies.clear()
+    srv.batch_sizes.clear()
+    srv.n_batches = 0
+    srv.t_first = srv.t_last = None
+    t0 = time.perf_counter() + 0.05
+    arrivals = t0 + np.cumsum(gaps)
+    futs = []
+
+    def submitter():
+        i = 0
+        while i < n:
+            now = time.perf_counter()
+            while i < n and arrivals[i] <= now:
+                reqs[i].t_arrival = float(arrivals[i])
+                futs.append(srv.submit(reqs[i]))
+                i += 1
+            if i < n:
+                time.sleep(max(2e-4, arrivals[i] - time.perf_counter()))
+
+    gc.collect()
+    gc.disable()
+    try:
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for f in futs:
+            f.result(timeout=300)
+    finally:
+        gc.enable()
+    srv.stop()
+    st = srv.stats()
+    return {'offered_per_s': rate, 'requests': n, 'achieved_per_s': st['throughput_per_s'],
+            'p50_ms': st['p50_ms'], 'p99_ms': st['p99_ms'], 'batches': st['batches'],
+            'mean_batch': st['mean_batch'],
+            'workload': 'config 5: Poisson arrivals of uneven all-film solves (P log-uniform 50-900, '
+                        '2-12 layers, mixed polarisations) through GsmServer (host scheduling thread, '
+                        'continuous batching on 2 streams); latency from scheduled arrival to host result'}
+
+
+def north_star_extras(dev, w, solver, value):
+    """The batched / mixed-precision GSM against the plain FP64 GPU GSM, and a
+    short serving run (bounded work: about half a minute)."""
+    import torch
+    out = {'note': 'plain FP64 GPU GSM = this library called once per solve from Python (about '
+                   '35 us of host work per call), as the reference calls its GSM once per '
+                   'Stack.calc_scat'}
+    t0 = time.perf_counter()
+    plain2 = plain_config2(dev, w)
+    out['config2'] = {'plain_points_per_s': plain2, 'batched_points_per_s': value, 'ratio': value / plain2}
+    try:
+        out['config1'] = config1_chain(dev)
+    except Exception as e:   # report, do not lose the headline line
+        out['config1'] = {'error': repr(e)}
+    torch.cuda.empty_cache()
+    reqs = film_requests(4096, seed=0)
+    ms_var, ms_one = time_film_mix(dev, reqs)
+    specs = array_stack_specs(96, seed=1)
+    ms_ag = time_array_stacks(specs, group=True)
+    ms_a1 = time_array_stacks(specs[:12], group=False, n_streams=1) / 12 * len(specs)
+    torch.cuda.empty_cache()
+    nf, na = len(reqs), len(specs)
+    out['config4_mix'] = {
+        'films': {'solves': nf, 'batched_per_s': nf / (ms_var / 1e3), 'plain_per_s': nf / (ms_one / 1e3),
+                  'ratio': ms_one / ms_var},
+        'arrays': {'solves': na, 'batched_per_s': na / (ms_ag / 1e3), 'plain_per_s': na / (ms_a1 / 1e3),
+                   'ratio': ms_a1 / ms_ag},
+        'mix_50_50': {'ratio': (ms_one / nf + ms_a1 / na) / (ms_var / nf + ms_ag / na)},
+        'workload': 'config 4: uneven film solves in one emu_film_var_batch launch vs one launch per '
+                    'solve; array stacks (P 50-900, M = P + 20, 2-12 arrays, interfaces included) '
+                    'grouped by shape on 4 streams vs one call per stack (samples of 256 and 12, '
+                    'extrapolated); mix_50_50 = equal numbers of both'}
+    try:
+        out['serving'] = serving_run(20000.0, 1.0)
+    except Exception as e:
+        out['serving'] = {'error': repr(e)}
+    out['seconds'] = time.perf_counter() - t0
+    return out
+
+
+# ---------------------------------------------------------------- --config N
+def config3_line(steps):
+    """Config 3 per wavelength: 4 arrays, period 700 nm, max order 10
+    (P = 618), M = 400, J + J_dag on the tensor cores from complex64 fields on
+    a 20 000-triangle mesh, interfaces and cascade (FP64) for 148
+    wavelengths at once."""
+    import torch
+    from emustack_b200.dense import DenseStackSolver
+    from emustack_b200.films import grating_orders
+    from emustack_b200.mesh import square_cell
+    from emustack_b200.overlap import DeviceMesh, overlap_batch
+    dev = torch.device('cuda')
+    period, mo, M = 700.0, 10, 400
+    mesh = square_cell(100, radius=0.3)
+    px, py = grating_orders(mo, period, period)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    shape = (1, mesh.nel, M, 13, 3)
+    cr = lambda: torch.complex(torch.randn(shape, dtype=torch.float32, device=dev, generator=g),
+                               torch.randn(shape, dtype=torch.float32, device=dev, generator=g))
+    s1, s2 = cr(), cr()
+    dm = DeviceMesh(mesh)
+    bloch = torch.tensor([[1e-6, 1e-13]], dtype=torch.float64, device=dev)
+    k0 = torch.tensor([2 * np.pi / (650.0 / period)], dtype=torch.float64, device=dev)
+    ms_j = _timed(lambda: overlap_batch(dm, px, py, mo, bloch, k0, s1, s2, precision='tf32x3'), steps)
+    del s1, s2
+    torch.cuda.empty_cache()
+    specs = [dict(mo=mo, npw=len(px), K=4, wl=float(w), seed=i)
+             for i, w in enumerate(np.linspace(400, 900, 148))]
+    ms_gsm = time_array_stacks(specs, group=True, n_streams=1)
+    return {'config': 3, 'P': 2 * len(px), 'M': M, 'nel': mesh.nel,
+            'J_pair_ms_per_layer': ms_j, 'interfaces_cascade_ms_per_wavelength': ms_gsm / 148,
+            'ms_per_wavelength': 4 * ms_j + ms_gsm / 148}
 
 
 def main():
@@ -340,6 +756,8 @@ def main():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument('--no-extras', action='store_true', help='skip the north_star comparison keys')
     ap.add_argument('--cpu-sample', type=int, default=0,
                     help='points in the CPU sample (default: 8 per host core, >= 64)')
     args = ap.parse_args()
@@ -372,6 +790,27 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.config != 2:
+        import torch
+        dev = torch.device('cuda')
+        if args.config == 1:
+            print(json.dumps(dict(config1_chain(dev, steps=args.steps), config=1)))
+        elif args.config == 3:
+            print(json.dumps(config3_line(args.steps)))
+        elif args.config == 4:
+            reqs = film_requests(4096, seed=0)
+            ms_var, ms_one = time_film_mix(dev, reqs, per_solve=512)
+            specs = array_stack_specs(512, seed=1)
+            ms_ag = time_array_stacks(specs, group=True)
+            ms_a1 = time_array_stacks(specs[:32], group=False, n_streams=1) / 32 * len(specs)
+            print(json.dumps({'config': 4, 'film_solves': len(reqs), 'film_batched_ms': ms_var,
+                              'film_per_solve_ms': ms_one, 'array_stacks': len(specs),
+                              'array_grouped_ms': ms_ag, 'array_per_call_ms': ms_a1}))
+        else:
+            for r in (1000.0, 10000.0, 100000.0):
+                print(json.dumps(dict(serving_run(r, 2.0), config=5)), flush=True)
+        return
+
     # CPU baseline first, in spawned workers, before any GPU work
     cpu = None
     if rank == 0 and world == 1:
@@ -385,6 +824,7 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+        args.no_extras = True
     res = run_ours(args, rank, world, local_rank)
     if rank == 0:
         res['cpu_baseline'] = cpu

@@ -309,6 +309,12 @@ def mode_overlap_1d(dmesh, pp, k0, bloch, beta1, sol1, sol2, perm2=None, full=Fa
     _check_sol1d(sol2, dmesh.nel, 'sol2')
     B, _, M, _ = sol1.shape
     dev = sol1.device
+    for t, nm, dt, shape in ((k0, 'k0', torch.float64, (B,)), (bloch, 'bloch', torch.float64, (B, 2)),
+                             (beta1, 'beta1', c128, (B, M))):
+        if t.dtype != dt or not t.is_cuda or not t.is_contiguous() or tuple(t.shape) != shape:
+            raise TypeError('%s must be a contiguous CUDA %s tensor of shape %s' % (nm, dt, shape))
+    if perm2 is not None and (perm2.dtype != torch.int32 or tuple(perm2.shape) != (B, M)):
+        raise TypeError('perm2 must be an int32 CUDA tensor [B, M]')
     pp_t = torch.as_tensor(np.asarray(pp, np.complex128), device=dev)
     d = _lib.EmuNormalise1D()
     d.batch, d.nval, d.nel, d.npt = B, M, dmesh.nel, dmesh.npt

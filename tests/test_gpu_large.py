@@ -136,3 +136,60 @@ def test_uneven_batch_with_P882_stack_matches_oracle():
         _close(h['a_list'][lo:lo + L - 1], np.asarray(ref.a_list, float), 'stack %d a_list' % i)
         _close(h['t_list'][lo:lo + L - 1], np.asarray(ref.t_list, float), 'stack %d t_list' % i)
         _close(h['r_list'][i], float(ref.r_list[0]), 'stack %d r_list' % i)
+
+
+def test_tensor_core_J_at_config3_size_within_product_bar():
+    """The split-TF32 x3 tensor-core J / J_dag at full config-3 size (20 000
+    P2 triangles, M = 400 Bloch modes, period 700 nm, max order 10:
+    K = 12 nel = 240 000 per GEMM) against the FP64 path on the same fields,
+    and R / T / A of a four-array stack built from each: within the product
+    bar of 1e-6 absolute."""
+    from emustack_b200 import materials, objects
+    from emustack_b200.films import grating_orders
+    from emustack_b200.mesh import square_cell
+    from emustack_b200.overlap import DeviceMesh, overlap_batch
+    from emustack_b200.stack import Stack
+    period, mo, M, wl = 700.0, 10, 400, 650.0
+    mesh = square_cell(100, radius=0.3)
+    assert mesh.nel == 20000
+    dev = torch.device('cuda')
+    g = torch.Generator(device='cuda').manual_seed(3)
+    shape = (1, mesh.nel, M, 13, 3)
+    cr = lambda: torch.complex(torch.randn(shape, dtype=torch.float32, device=dev, generator=g),
+                               torch.randn(shape, dtype=torch.float32, device=dev, generator=g))
+    s1_32, s2_32 = cr(), cr()                       # config 3: complex64 fields
+    px, py = grating_orders(mo, period, period)
+    light = objects.Light(wl, max_order_PWs=mo, theta=0.0, phi=0.0)
+    bloch = torch.tensor(np.asarray(light.k_pll * period).reshape(1, 2), device=dev)
+    k0 = torch.tensor([2 * np.pi / (wl / period)], dtype=torch.float64, device=dev)
+    dm = DeviceMesh(mesh)
+    Jt, Jdt, _ = overlap_batch(dm, px, py, mo, bloch, k0, s1_32, s2_32, precision='tf32x3')
+    Jt, Jdt = Jt[0].cpu().numpy(), Jdt[0].cpu().numpy()
+    s1, s2 = s1_32.to(torch.complex128), s2_32.to(torch.complex128)
+    del s1_32, s2_32
+    J6, Jd6, _ = overlap_batch(dm, px, py, mo, bloch, k0, s1, s2, precision='fp64')
+    J6, Jd6 = J6[0].cpu().numpy(), Jd6[0].cpu().numpy()
+    del s1, s2
+    torch.cuda.empty_cache()
+    for a, b in ((Jt, J6), (Jdt, Jd6)):
+        assert np.abs(a - b).max() <= 5e-6 * np.abs(b).max()
+    # stacks from each J: scaled so that the interfaces are well conditioned
+    sc = 0.25 / np.sqrt(2 * len(px)) / np.abs(J6).std()
+    rng = np.random.default_rng(5)
+    k0v = 2 * np.pi / (wl / period)
+    kzs = [rng.uniform(0, 2 * k0v, M) + 1j * rng.uniform(0, 0.1 * k0v, M) for _ in range(4)]
+    hs = rng.uniform(50, 200, 4)
+    out = {}
+    for nm, (J, Jd) in (('tf32x3', (Jt, Jdt)), ('fp64', (J6, Jd6))):
+        sub = objects.ThinFilm(period, height_nm='semi_inf', material=materials.Material(1.46 + 0j), loss=False)
+        sup = objects.ThinFilm(period, height_nm='semi_inf', material=materials.Air, loss=False)
+        lays = [sub.calc_modes(light)]
+        for kz, h in zip(kzs, hs):
+            ns = objects.NanoStruct('2D_array', period, 250, height_nm=float(h))
+            lays.append(ns.calc_modes(light, k_z=kz, J=sc * J, J_dag=sc * Jd))
+        lays.append(sup.calc_modes(light))
+        st = Stack(lays)
+        st.calc_scat(pol='TE')
+        out[nm] = np.concatenate([np.asarray(st.a_list, float), np.asarray(st.t_list, float),
+                                  np.asarray(st.r_list, float)])
+    np.testing.assert_allclose(out['tf32x3'], out['fp64'], rtol=0, atol=1e-6)

@@ -140,3 +140,65 @@ def test_pair_reordering_on_gpu_matches_oracle():
     oinv, _, _ = OV.pw_ordering(mo, 1.0, 1.0, bl, k0)
     Jdo = OV.J_dagger_overlap(mesh.x, mesh.table_nod, s2n, 1.0, 1.0, bl, oinv, mo)
     np.testing.assert_allclose(Jd[0].cpu().numpy(), Jdo, rtol=1e-9, atol=1e-11)
+
+
+@pytest.mark.parametrize('name', ['4testing-600_120.mail', '4testing-940_266_sq.mail'])
+def test_reference_meshes_match_oracle(name):
+    """J, J_dag and the adjoint normalisation on the reference's own test
+    meshes (read with Mesh.from_mail: 518 and 2 528 P2 triangles, two
+    material types), FP64 path against the C restatement."""
+    from fixtures import reference_mesh
+    from emustack_b200.films import grating_orders
+    from emustack_b200.overlap import DeviceMesh, mode_normalisation, overlap_batch
+    mesh = reference_mesh(name)
+    rng = np.random.default_rng(mesh.nel)
+    nval, mo = 12, 3
+    s1, s2 = _fields(rng, mesh.nel, nval), _fields(rng, mesh.nel, nval)
+    bloch, k0 = np.array([0.013, -0.021]), 2 * np.pi / 1.3
+    px, py = grating_orders(mo, 600.0, 600.0)
+    dm = DeviceMesh(mesh)
+    J, Jd, inv = overlap_batch(dm, px, py, mo, torch.tensor(bloch[None], device='cuda'),
+                               torch.tensor([k0], dtype=torch.float64, device='cuda'),
+                               torch.tensor(s1[None], device='cuda'),
+                               torch.tensor(s2[None], device='cuda'))
+    oinv, _, _ = OV.pw_ordering(mo, 1.0, 1.0, bloch, k0)
+    np.testing.assert_array_equal(inv[0].cpu().numpy(), oinv)
+    Jo = OV.J_overlap(mesh.x, mesh.table_nod, s1, 1.0, 1.0, bloch, oinv, mo)
+    Jdo = OV.J_dagger_overlap(mesh.x, mesh.table_nod, s2, 1.0, 1.0, bloch, oinv, mo)
+    np.testing.assert_allclose(J[0].cpu().numpy(), Jo, **TOL)
+    np.testing.assert_allclose(Jd[0].cpu().numpy(), Jdo, **TOL)
+    b1 = rng.uniform(1, 3, nval) + 1j * rng.uniform(0, 0.1, nval)
+    pp = np.array([1.0 + 0j, 3.5 ** 2 + 0.07j])
+    ovl, perm, scale, warn, s2n, b2 = OV.orthogonal_normalise(mesh.x, mesh.table_nod, mesh.type_el, pp, b1,
+                                                              b1, s1, s2, k0)
+    diag, sc, ns = mode_normalisation(dm, pp, torch.tensor([k0], dtype=torch.float64, device='cuda'),
+                                      torch.tensor(b1[None], device='cuda'), torch.tensor(s1[None], device='cuda'),
+                                      torch.tensor(s2[None], device='cuda'))
+    np.testing.assert_allclose(diag[0].cpu().numpy(), np.diag(ovl), rtol=1e-10)
+    np.testing.assert_allclose(sc[0].cpu().numpy(), scale, rtol=1e-10)
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'tf32x3'])
+def test_quadratic_fields_known_answer_gpu(precision):
+    """Fields quadratic over the cell on the reference's 518-triangle mesh:
+    J against the exact cell integrals (the quadrature error bound of the
+    16-point rule per max order; the tensor-core path adds its split-TF32
+    error, <= 5e-6 of max |J|)."""
+    from fixtures import QUAD_BOUND, exact_J, quadratic_fields, reference_mesh
+    from emustack_b200.films import grating_orders
+    from emustack_b200.overlap import DeviceMesh, overlap_batch
+    mesh = reference_mesh('4testing-600_120.mail')
+    rng = np.random.default_rng(4)
+    sol, Cf = quadratic_fields(mesh, 5, rng)
+    bloch, k0 = np.array([0.31, -0.17]), 2 * np.pi / 1.1
+    dm = DeviceMesh(mesh)
+    for mo, bound in QUAD_BOUND.items():
+        px, py = grating_orders(mo, 600.0, 600.0)
+        J, _, inv = overlap_batch(dm, px, py, mo, torch.tensor(bloch[None], device='cuda'),
+                                  torch.tensor([k0], dtype=torch.float64, device='cuda'),
+                                  torch.tensor(sol[None], device='cuda'),
+                                  torch.tensor(sol[None], device='cuda'), precision=precision)
+        Je = exact_J(Cf, px, py, bloch, 1.0, 1.0, (0.0, 1.0, -1.0, 0.0), inv[0].cpu().numpy())
+        tol = bound + (5e-6 if precision == 'tf32x3' else 0.0)
+        err = np.abs(J[0].cpu().numpy() - Je).max() / np.abs(Je).max()
+        assert err <= tol, (mo, err)

@@ -75,7 +75,8 @@ def test_orthogonality_matrix_and_normalisation_match_the_oracle():
     k0, by = 2 * np.pi / 1.2, 0.43
     dev = torch.device('cuda')
     dm = DeviceMesh1D(mesh, dev)
-    args = (dm, pp, torch.tensor([k0], device=dev), torch.tensor([[0.1, by]], device=dev),
+    args = (dm, pp, torch.tensor([k0], dtype=torch.float64, device=dev),
+            torch.tensor([[0.1, by]], dtype=torch.float64, device=dev),
             torch.tensor(beta.reshape(1, M), device=dev), torch.tensor(s1[None], device=dev),
             torch.tensor(s2[None], device=dev))
     full = mode_overlap_1d(*args, full=True)[0].cpu().numpy()

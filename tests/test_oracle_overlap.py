@@ -112,3 +112,22 @@ def test_pair_reordering_swaps_adjoint_modes():
     # mode 0 is swapped with 1 then with 2 (both overlap prime mode 0)
     assert list(perm) == [2, 0, 1]
     np.testing.assert_allclose(b2, [3, 1, 2])
+
+
+@pytest.mark.parametrize('name', ['4testing-600_120.mail', '4testing-940_266_sq.mail'])
+def test_quadratic_fields_known_answer_on_reference_meshes(name):
+    """Fields that are quadratic polynomials over the cell, on the
+    reference's own test meshes (read by Mesh.from_mail): the oracle's J
+    (16-point rule, degree 8, on each element) against the exact cell
+    integrals of polynomial x plane wave; the difference is the quadrature
+    error, bounded per max order."""
+    from fixtures import QUAD_BOUND, exact_J, quadratic_fields, reference_mesh
+    mesh = reference_mesh(name)
+    rng = np.random.default_rng(len(name))
+    sol, Cf = quadratic_fields(mesh, 3, rng)
+    bloch, k0 = np.array([0.31, -0.17]), 2 * np.pi / 1.1
+    for mo, bound in QUAD_BOUND.items():
+        inv, px, py = OV.pw_ordering(mo, 1.0, 1.0, bloch, k0)
+        Jo = OV.J_overlap(mesh.x, mesh.table_nod, sol, 1.0, 1.0, bloch, inv, mo)
+        Je = exact_J(Cf, px, py, bloch, 1.0, 1.0, (0.0, 1.0, -1.0, 0.0), inv)
+        assert np.abs(Jo - Je).max() <= bound * np.abs(Je).max(), (mo, np.abs(Jo - Je).max())
