@@ -57,6 +57,12 @@ E2E_CHUNK, E2E_STREAMS = 4096, 4   # pieces of the host-to-host pipeline and the
 PERIOD, MAX_ORDER, POL = 500.0, 5, 'TE'
 METRIC = 'R/T/A spectral points/s (batched thin-film GSM, FP64)'
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes of one 32768-point launch of the bench kernel, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum); reported only when
+# the autotuner picks the captured launch variant
+NCU_TRAFFIC = {'bytes': 171111424, 'variant': 4, 'kernel': 'film_stack_kernel<256, 3, true>',
+               'kernel_ms_under_ncu': 1.138,
+               'source': 'ncu --set full capture, profiles/film_stack_32768pts.md'}
 
 
 def workload(seed=0):
@@ -330,6 +336,10 @@ def run_ours(args, rank, world, local_rank):
         achieved = by / (ms_per_step / 1e3) / 1e9
         flops = film_flops(B, L, P)
         fp64_peak = fp64_peak_tflops()
+        tuned = _tuned()
+        variant = next((t['choice'] for t in tuned if t['kernel'] == 'film_stack' and
+                        t['shape'].get('B') == _bucket(B) and not t['shape'].get('inc')), None)
+        traffic = NCU_TRAFFIC['bytes'] if variant == NCU_TRAFFIC['variant'] else None
         tfl = flops / (ms_per_step / 1e3) / 1e12
         result = {
             'metric': METRIC,
@@ -352,7 +362,8 @@ def run_ours(args, rank, world, local_rank):
                     'd2h_bytes_per_step': d2h},
             'gpu_launches': int(launches),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm,
-                         'unit': 'GB/s', 'frac': achieved / hbm, 'traffic': None,
+                         'unit': 'GB/s', 'frac': achieved / hbm, 'traffic': traffic,
+                         'traffic_source': dict(NCU_TRAFFIC, launch_variant_now=variant),
                          'peak_source': hbm_src + ' (MEASURED_PEAKS.json hbm_gbs)',
                          'note': 'the kernel is FP64-issue bound, see compute'},
             'compute': {'bound': 'fp64', 'achieved_tflops': tfl, 'peak_tflops': fp64_peak,
@@ -361,11 +372,16 @@ def run_ours(args, rank, world, local_rank):
                         'flops_per_step': flops,
                         'note': 'algorithmic flops count a divide, square root or exp as one'},
             'clocks': clk.summary(),
-            'autotune': _tuned(),
+            'autotune': tuned,
         }
         if not args.no_extras:
             result['north_star'] = north_star_extras(dev, w, solver, value)
     return result
+
+
+def _bucket(n):
+    from emustack_b200.autotune import size_bucket
+    return size_bucket(n)
 
 
 def _tuned():
@@ -676,6 +692,53 @@ def serving_run(rate, seconds=1.0, seed=0):
                         'continuous batching on 2 streams); latency from scheduled arrival to host result'}
 
 
+def ring_serving_run(rate, seconds=1.0, seed=0):
+    """Open-loop Poisson arrivals of uneven film requests at `rate` per
+    second through the device-resident request loop (DeviceFilmServer: a
+    persistent kernel picks requests up from a pinned host ring, no launch
+    per request); latency from each request's scheduled arrival to the host
+    seeing its completion word."""
+    from emustack_b200.serving import DeviceFilmServer
+    n = max(int(rate * seconds), 200)
+    reqs = [r for r in film_requests(n, seed) if len(r.n) <= 16 and r.npw <= 512]
+    n = len(reqs)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, n)
+    srv = DeviceFilmServer(capacity=8192, idle_seconds=1.0)
+    try:
+        for r in film_requests(256, seed + 2):       # warm the loop
+            srv.take(srv.submit(r))
+        pending, lat = collections.OrderedDict(), []
+        t0 = time.perf_counter() + 0.02
+        arrivals = t0 + np.cumsum(gaps)
+        gc.collect()
+        gc.disable()
+        try:
+            i = 0
+            while i < n or pending:
+                now = time.perf_counter()
+                while i < n and arrivals[i] <= now:
+                    pending[srv.submit(reqs[i])] = arrivals[i]
+                    i += 1
+                for t in list(pending)[:64]:
+                    if srv.poll(t) is not None:
+                        lat.append(time.perf_counter() - pending.pop(t))
+                if i < n and not pending:
+                    time.sleep(max(0.0, min(1e-4, arrivals[i] - time.perf_counter())))
+        finally:
+            gc.enable()
+        t_end = time.perf_counter()
+        srv.stop()
+    finally:
+        srv.close()
+    lat = np.array(lat) * 1e3
+    return {'offered_per_s': rate, 'requests': n, 'achieved_per_s': n / (t_end - t0),
+            'p50_ms': float(np.percentile(lat, 50)), 'p99_ms': float(np.percentile(lat, 99)),
+            'workload': 'config 5: Poisson arrivals of uneven all-film solves (P log-uniform 50-900, '
+                        '2-12 layers, mixed polarisations) through the device-resident request loop '
+                        '(one persistent kernel, pinned host ring, one warp per request); latency from '
+                        'scheduled arrival to the host seeing the result'}
+
+
 def north_star_extras(dev, w, solver, value):
     """The batched / mixed-precision GSM against the plain FP64 GPU GSM, and a
     short serving run (bounded work: about half a minute)."""
@@ -712,6 +775,10 @@ def north_star_extras(dev, w, solver, value):
         out['serving'] = serving_run(20000.0, 1.0)
     except Exception as e:
         out['serving'] = {'error': repr(e)}
+    try:
+        out['serving_device_loop'] = ring_serving_run(20000.0, 1.0)
+    except Exception as e:
+        out['serving_device_loop'] = {'error': repr(e)}
     out['seconds'] = time.perf_counter() - t0
     return out
 
@@ -809,6 +876,8 @@ def main():
         else:
             for r in (1000.0, 10000.0, 100000.0):
                 print(json.dumps(dict(serving_run(r, 2.0), config=5)), flush=True)
+            for r in (1000.0, 10000.0, 50000.0, 100000.0):
+                print(json.dumps(dict(ring_serving_run(r, 2.0), config=5)), flush=True)
         return
 
     # CPU baseline first, in spawned workers, before any GPU work

@@ -303,3 +303,44 @@ EXTRA_SIGNATURES.extend([
     ('emu_overlap1d_batch', C.c_int, [C.POINTER(EmuOverlap1D), vp]),
     ('emu_mode_overlap_1d', C.c_int, [C.POINTER(EmuNormalise1D), C.c_int, vp]),
 ])
+
+
+MAT_CONSTANT, MAT_TABLE, MAT_DRUDE = 0, 1, 2
+
+
+class EmuMaterial(C.Structure):
+    _fields_ = [
+        ('kind', C.c_int), ('n_rows', C.c_int), ('d_wl', vp), ('d_n', vp), ('n_const', EmuC128),
+        ('drude', C.c_double * 3), ('loss', C.c_int),
+    ]
+
+
+EXTRA_SIGNATURES.append(('emu_material_n_batch', C.c_int, [C.POINTER(EmuMaterial), C.c_int, C.c_int, vp, vp,
+                                                           vp, vp]))
+
+
+class EmuFilmRingRequest(C.Structure):
+    _fields_ = [
+        ('n_layers', C.c_int), ('n_pw', C.c_int), ('world_1d', C.c_int), ('pol', C.c_int),
+        ('period', C.c_double), ('period_y', C.c_double), ('wl_nm', C.c_double), ('k_pll', C.c_double * 2),
+        ('h_px', vp), ('h_py', vp), ('h_n', vp), ('h_heights_nm', vp),
+    ]
+
+
+class EmuFilmRingResult(C.Structure):
+    _fields_ = [('h_R_net', vp), ('h_T_net', vp), ('h_a_list', vp), ('h_t_list', vp), ('h_r_list', vp),
+                ('h_flags', vp)]
+
+
+RING_MAX_PW, RING_MAX_LAYERS = 512, 16
+
+EXTRA_SIGNATURES.extend([
+    ('emu_film_ring_slot_bytes', C.c_size_t, []),
+    ('emu_film_ring_create', C.c_int, [C.c_int, C.c_double, C.POINTER(vp)]),
+    ('emu_film_ring_submit', C.c_int, [vp, C.POINTER(EmuFilmRingRequest), C.POINTER(C.c_longlong)]),
+    ('emu_film_ring_poll', C.c_int, [vp, C.c_longlong, C.POINTER(EmuFilmRingResult)]),
+    ('emu_film_ring_wait', C.c_int, [vp, C.c_longlong, C.c_double, C.POINTER(EmuFilmRingResult)]),
+    ('emu_film_ring_running', C.c_int, [vp]),
+    ('emu_film_ring_stop', C.c_int, [vp]),
+    ('emu_film_ring_destroy', C.c_int, [vp]),
+])

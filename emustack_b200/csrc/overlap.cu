@@ -785,6 +785,14 @@ struct TcPlan {
 };
 
 constexpr size_t kTcGroupBytes = (size_t)4 << 30;  // scratch budget of one group
+// Longest K range one tensor-core accumulation covers.  The tensor cores
+// accumulate in FP32 and the sum drifts toward zero by about 7e-9 x K
+// relative (measured: 1.9e-6 rms at K = 256, 7.3e-6 at 1024, 1.8e-3 at
+// 262144, for random operands); the K splits are summed in FP64.
+constexpr long long kTcMaxKSplit = 256;
+constexpr int kTcMaxSplits = 256;
+// element chunk whose K range (12 values per element) fits kTcMaxSplits splits
+constexpr long kTcMaxChunk = kTcMaxSplits * kTcMaxKSplit / 12;
 
 static size_t tc_problem_bytes(const EmuOverlap *p, const TcPlan &t) {
   const size_t npw = p->n_pw, M = p->nval;
@@ -795,7 +803,8 @@ static size_t tc_problem_bytes(const EmuOverlap *p, const TcPlan &t) {
 
 static TcPlan tc_plan(const EmuOverlap *p) {
   TcPlan t;
-  const long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
+  long chunk = p->elements_per_chunk > 0 ? p->elements_per_chunk : 4096;
+  if (chunk > kTcMaxChunk) chunk = kTcMaxChunk;
   t.nec = chunk < p->nel ? chunk : p->nel;
   t.K2 = 12 * (long long)t.nec;
   t.nb = (p->d_sol1 ? 2 * p->nval : 0) + (p->d_sol2 ? 2 * p->nval : 0);
@@ -815,7 +824,11 @@ static TcPlan tc_plan(const EmuOverlap *p) {
   const int maxsp = (int)(t.K2 / 256 > 0 ? t.K2 / 256 : 1);
   if (sp > maxsp) sp = maxsp;
   if (p->tc_splits > 0) sp = p->tc_splits;
-  if (sp > 64) sp = 64;
+  // accuracy floor, also under an explicit choice: no split longer than
+  // kTcMaxKSplit
+  const int need = (int)((t.K2 + kTcMaxKSplit - 1) / kTcMaxKSplit);
+  if (sp < need) sp = need;
+  if (sp > kTcMaxSplits) sp = kTcMaxSplits;
   if (sp * t.group > 65535) sp = 65535 / t.group;
   t.splits = sp < 1 ? 1 : sp;
   return t;

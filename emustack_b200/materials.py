@@ -50,3 +50,53 @@ class Material(object):
 
 
 Air = Material(1.00 + 0.0j)
+
+
+def n_batch(materials, wl_nm, losses=None):
+    """Refractive indices of the layers of a stack at a batch of wavelengths,
+    on the device (emu_material_n_batch): complex128 [B, L] for
+    ``materials`` (L Material objects, bottom to top) at ``wl_nm`` (a CUDA
+    float64 tensor [B]), each layer's imaginary part dropped where its
+    ``losses`` flag is False (ThinFilm(loss=False)).  The result is the ``n``
+    argument of films.FilmStackSolver.solve.  Raises ValueError for
+    wavelengths outside a table, as the reference's interpolation does."""
+    import ctypes as C
+    import torch
+    from . import _lib
+    if not (torch.is_tensor(wl_nm) and wl_nm.is_cuda and wl_nm.dtype == torch.float64
+            and wl_nm.dim() == 1 and wl_nm.is_contiguous()):
+        raise TypeError('wl_nm must be a contiguous CUDA float64 tensor [B]')
+    L = len(materials)
+    losses = [True] * L if losses is None else list(losses)
+    dev = wl_nm.device
+    arr = (_lib.EmuMaterial * L)()
+    keep = []
+    for l, (m, loss) in enumerate(zip(materials, losses)):
+        e = arr[l]
+        e.loss = int(bool(loss))
+        if m.data_wls is None:
+            e.kind = _lib.MAT_CONSTANT
+            v = complex(np.asarray(m.data_ns).item())
+            e.n_const = _lib.EmuC128(v.real, v.imag)
+        elif isinstance(m.data_wls, str):
+            e.kind = _lib.MAT_DRUDE
+            for i in range(3):
+                e.drude[i] = float(m.data_ns[i])
+        else:
+            cache = getattr(m, '_device_table', None)
+            if cache is None or cache[0].device != dev:
+                cache = (torch.tensor(np.asarray(m.data_wls, np.float64), device=dev),
+                         torch.tensor(np.asarray(m.data_ns, np.complex128), device=dev))
+                m._device_table = cache
+            e.kind = _lib.MAT_TABLE
+            e.n_rows = int(cache[0].numel())
+            e.d_wl, e.d_n = _lib.ptr(cache[0]), _lib.ptr(cache[1])
+            keep.append(cache)
+    B = int(wl_nm.shape[0])
+    out = torch.empty((B, L), dtype=torch.complex128, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.lib().emu_material_n_batch(arr, L, B, _lib.ptr(wl_nm), _lib.ptr(out), _lib.ptr(err),
+                                               _lib.stream_ptr()), 'emu_material_n_batch')
+    if int(err.item()) != 0:
+        raise ValueError('wavelength outside the tabulated range')
+    return out

@@ -37,6 +37,7 @@ operations per point.
 from __future__ import annotations
 
 import collections
+import ctypes as C
 import threading
 import time
 
@@ -45,6 +46,8 @@ import torch
 
 from .array_serving import (ArrayBatcher, ArrayLayer, ArrayRequest, SMatrixCache,  # noqa: F401
                             dense_workspace_bytes)
+from . import _lib
+from ._lib import check
 from .films import FilmPoint, FilmStackSolver, FilmVarSolver, grating_orders
 
 _NPW = {}
@@ -513,3 +516,122 @@ class GsmServer(object):
         self.inflight_bytes += batch.nbytes
         self.n_batches += 1
         self.batch_sizes.append(len(batch.reqs))
+
+
+class DeviceFilmServer(object):
+    """All-film solves served by a device-resident request loop
+    (emu_film_ring_*): a persistent kernel picks requests up from a ring in
+    pinned host memory as they are submitted, one warp per request, and
+    writes each result back into its slot.  No kernel launch or host
+    scheduling thread per request; the loop ends by itself idle_seconds after
+    the last request and restarts on the next submit.
+
+    submit(req) takes a FilmRequest (standard polarisation, at most
+    EMU_RING_MAX_LAYERS layers and EMU_RING_MAX_PW orders per polarisation)
+    and returns a ticket; poll(ticket) returns the result dict once done
+    (R_net, T_net diagonals, a_list, t_list, r_list, flags) or None;
+    wait(ticket) blocks (outside the interpreter lock) until done.  While the
+    loop runs it holds every SM of the device."""
+
+    def __init__(self, capacity=4096, idle_seconds=1.0):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        check(self._L.emu_film_ring_create(int(capacity), float(idle_seconds), C.byref(h)),
+              'emu_film_ring_create')
+        self._h = h
+        self._pending = {}
+        self._orders = {}
+
+    def _order_arrays(self, r):
+        key = (r.max_order, r.period, r.period_y, r.world_1d)
+        o = self._orders.get(key)
+        if o is None:
+            from .films import grating_orders
+            px, py = grating_orders(r.max_order, r.period, r.period_y, r.world_1d)
+            o = self._orders[key] = (np.ascontiguousarray(px, np.int32), np.ascontiguousarray(py, np.int32))
+        return o
+
+    def submit(self, r):
+        if r.incoming is not None:
+            raise ValueError('the device request loop takes standard polarisations only')
+        px, py = self._order_arrays(r)
+        n = np.ascontiguousarray(r.n, np.complex128)
+        h = np.ascontiguousarray(r.heights, np.float64)
+        q = _lib.EmuFilmRingRequest()
+        q.n_layers, q.n_pw, q.world_1d, q.pol = len(n), len(px), int(bool(r.world_1d)), _lib.POL[r.pol]
+        q.period, q.period_y, q.wl_nm = r.period, r.period_y, r.wl_nm
+        q.k_pll[0], q.k_pll[1] = float(r.k_pll[0]), float(r.k_pll[1])
+        q.h_px, q.h_py = px.ctypes.data_as(C.c_void_p), py.ctypes.data_as(C.c_void_p)
+        q.h_n, q.h_heights_nm = n.ctypes.data_as(C.c_void_p), h.ctypes.data_as(C.c_void_p)
+        t = C.c_longlong()
+        while True:
+            st = self._L.emu_film_ring_submit(self._h, C.byref(q), C.byref(t))
+            if st != 5:      # EMU_E_WORKSPACE: the ring is full until results are read
+                break
+            self._drain_one()
+        check(st, 'emu_film_ring_submit')
+        self._pending[t.value] = (len(n), len(px))
+        return t.value
+
+    def _result(self, ticket):
+        L, npw = self._pending[ticket]
+        res = {'R_net': np.empty(2 * npw, np.complex128), 'T_net': np.empty(2 * npw, np.complex128),
+               'a_list': np.empty(L - 1), 't_list': np.empty(L - 1), 'r_list': np.empty(1),
+               'flags': np.empty(1, np.uint32)}
+        o = _lib.EmuFilmRingResult()
+        o.h_R_net, o.h_T_net = (res[k].ctypes.data_as(C.c_void_p) for k in ('R_net', 'T_net'))
+        o.h_a_list, o.h_t_list = (res[k].ctypes.data_as(C.c_void_p) for k in ('a_list', 't_list'))
+        o.h_r_list, o.h_flags = res['r_list'].ctypes.data_as(C.c_void_p), res['flags'].ctypes.data_as(C.c_void_p)
+        return res, o
+
+    def poll(self, ticket):
+        res, o = self._result(ticket)
+        st = self._L.emu_film_ring_poll(self._h, int(ticket), C.byref(o))
+        if st == 0:
+            return None
+        if st < 0 or st > 1:
+            raise _lib.EmuError(abs(st), 'emu_film_ring_poll')
+        del self._pending[ticket]
+        res['flags'] = int(res['flags'][0])
+        return res
+
+    def wait(self, ticket, timeout_s=60.0):
+        res, o = self._result(ticket)
+        st = self._L.emu_film_ring_wait(self._h, int(ticket), float(timeout_s), C.byref(o))
+        if st != 1:
+            raise _lib.EmuError(abs(st), 'emu_film_ring_wait')
+        del self._pending[ticket]
+        res['flags'] = int(res['flags'][0])
+        return res
+
+    def _drain_one(self):
+        """Read the oldest pending result (it frees its slot)."""
+        t = min(self._pending)
+        self._done_early = getattr(self, '_done_early', {})
+        self._done_early[t] = self.wait(t)
+
+    def take(self, ticket):
+        """Result of a ticket whether it was read early (to free its slot) or not."""
+        early = getattr(self, '_done_early', {})
+        if ticket in early:
+            return early.pop(ticket)
+        return self.wait(ticket)
+
+    def running(self):
+        return bool(self._L.emu_film_ring_running(self._h))
+
+    def stop(self):
+        """End the loop; returns the status (EMU_OK, or EMU_E_TIMEOUT if a
+        device wait gave up)."""
+        return self._L.emu_film_ring_stop(self._h)
+
+    def close(self):
+        if self._h is not None:
+            self._L.emu_film_ring_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -195,6 +195,82 @@ size_t emu_film_stack_workspace_size(const EmuFilmStackBatch *p);
 int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspace,
                          size_t workspace_bytes, void *stream);
 
+/* ---------------------------------------- materials: n(lambda) per layer
+ * Refractive index of every layer of a stack at a batch of wavelengths,
+ * into the [B][L] array the film kernels take: constant, tabulated (linear
+ * interpolation with scipy.interpolate.interp1d's arithmetic, the reference's
+ * choice) or Drude materials, each with its loss flag applied (imaginary
+ * part dropped when loss == 0).  Replaces Material.n
+ * (backend/materials.py:31-186) and Anallo.n (backend/mode_calcs.py:186-192)
+ * for a sweep.  Wavelengths outside a table set *d_error = 1 and give NaN
+ * (the reference raises ValueError there).  At most 32 layers per call. */
+#define EMU_MAT_CONSTANT 0
+#define EMU_MAT_TABLE 1
+#define EMU_MAT_DRUDE 2
+typedef struct {
+  int kind;              /* EMU_MAT_*                                        */
+  int n_rows;            /* table rows (>= 2)                                */
+  const double *d_wl;    /* [n_rows] ascending wavelengths (nm), device      */
+  const emu_c128 *d_n;   /* [n_rows] refractive indices, device              */
+  emu_c128 n_const;      /* EMU_MAT_CONSTANT                                 */
+  double drude[3];       /* omega_plasma, omega_gamma, eps_inf (EMU_MAT_DRUDE) */
+  int loss;              /* 0: imaginary part dropped                        */
+} EmuMaterial;
+
+int emu_material_n_batch(const EmuMaterial *h_materials, int n_layers, int n_points,
+                         const double *d_wl_nm, emu_c128 *d_n, int32_t *d_error, void *stream);
+
+/* ------------------------------ serving: device-resident request loop
+ * A persistent kernel that solves all-film spectral points as the host
+ * writes them into a ring of slots in pinned, device-mapped host memory:
+ * no kernel launch per request or batch.  Each request is one
+ * Stack(layers).calc_scat(pol) of an all-film stack (backend/stack.py:
+ * 162-426; in the reference, one Python call per point) of any shape up to
+ * EMU_RING_MAX_LAYERS layers and EMU_RING_MAX_PW orders per polarisation,
+ * with a standard polarisation; results are those of emu_film_var_batch
+ * for the same point (one warp per request, the same recursion).
+ *   create  : allocates the ring (capacity slots of emu_film_ring_slot_bytes()
+ *             pinned host bytes) and the device state; the loop ends by itself
+ *             idle_seconds after the last request (every device wait is
+ *             bounded) and restarts on the next submit.
+ *   submit  : copies a request into its slot and wakes the loop; returns a
+ *             ticket, or EMU_E_WORKSPACE while the ring is full (poll the
+ *             oldest results first).  Thread-safe.
+ *   poll    : 1 and the outputs copied out when the ticket is done, 0 while
+ *             pending (each result can be read once); wait: poll until done
+ *             or timeout (-EMU_E_TIMEOUT).
+ *   stop    : ends the loop and waits for it; returns EMU_E_TIMEOUT if a
+ *             device wait gave up, else EMU_OK.
+ * While the loop runs it holds every SM; other kernels on the device wait
+ * for it to end (stop, or idle_seconds without requests). */
+#define EMU_RING_MAX_PW 512
+#define EMU_RING_MAX_LAYERS 16
+typedef struct EmuFilmRing EmuFilmRing;
+typedef struct {
+  int n_layers, n_pw, world_1d, pol;  /* pol: EMU_POL_TE .. EMU_POL_LCIRC    */
+  double period, period_y;            /* nm                                  */
+  double wl_nm;
+  double k_pll[2];                    /* nm^-1                               */
+  const int32_t *h_px, *h_py;         /* [n_pw] orders (emu_grating_orders)  */
+  const emu_c128 *h_n;                /* [n_layers] indices, loss applied    */
+  const double *h_heights_nm;         /* [n_layers - 2]                      */
+} EmuFilmRingRequest;
+typedef struct {
+  emu_c128 *h_R_net, *h_T_net;        /* [2 n_pw] each, or NULL              */
+  double *h_a_list, *h_t_list;        /* [n_layers - 1] each, or NULL        */
+  double *h_r_list;                   /* [1] or NULL                         */
+  uint32_t *h_flags;                  /* [1] EMU_PT_* or NULL                */
+} EmuFilmRingResult;
+
+size_t emu_film_ring_slot_bytes(void);
+int emu_film_ring_create(int capacity, double idle_seconds, EmuFilmRing **out);
+int emu_film_ring_submit(EmuFilmRing *ring, const EmuFilmRingRequest *req, long long *ticket);
+int emu_film_ring_poll(EmuFilmRing *ring, long long ticket, EmuFilmRingResult *out);
+int emu_film_ring_wait(EmuFilmRing *ring, long long ticket, double timeout_s, EmuFilmRingResult *out);
+int emu_film_ring_running(EmuFilmRing *ring);
+int emu_film_ring_stop(EmuFilmRing *ring);
+int emu_film_ring_destroy(EmuFilmRing *ring);
+
 /* ------------------------------------------ dense linear algebra
  * Batched complex128 GEMM, C_b = alpha A_b B_b + beta C_b (row-major; A_b is
  * m x k, B_b k x n), and batched LU solve A_b X_b = B_b with partial pivoting
@@ -388,8 +464,11 @@ typedef struct {
                               FP64 sum of the splits                          */
   int32_t *d_error;        /* [1] set to 1 if a bounded device wait gave up
                               (tensor-core path), else left untouched; may be NULL */
-  int tc_splits;           /* tensor-core path: K splits per GEMM (1-64), 0 = one
-                              wave of CTAs; results differ only in FP32 rounding */
+  int tc_splits;           /* tensor-core path: K splits per GEMM (1-256), 0 = one
+                              wave of CTAs; never fewer than keep each split's K
+                              range within 256 values (the tensor cores'
+                              FP32 accumulation drifts by ~7e-9 x K relative);
+                              results differ by that accumulation error */
   int field_c64;           /* tensor-core path only: 1 = d_sol1 / d_sol2 hold
                               complex64 (float re, im) in the same layout (the
                               operands are FP32 anyway; half the bytes read) */

@@ -507,3 +507,29 @@ def film_stack_point(ns, heights_nm, wl_nm, k_pll, period, period_y=None,
     res.layers = layers
     res.air = air
     return res
+
+
+# ---------------------------------------------------------------------------
+# Materials
+# ---------------------------------------------------------------------------
+
+def material_n(spec, wl_nm, loss=True):
+    """Refractive index of a material at wl_nm as backend/materials.py:
+    131-161 evaluates it (Material.n) with Anallo.n's loss flag
+    (backend/mode_calcs.py:186-192): ``spec`` is a scalar index, a table
+    [(wl, n)] or [(wl, Re n, Im n)] interpolated by
+    scipy.interpolate.interp1d (linear, the reference's call), or the
+    three Drude parameters (omega_plasma, omega_gamma, eps_inf)."""
+    from scipy.interpolate import interp1d
+    spec = np.asarray(spec)
+    if spec.shape == ():
+        n = spec.item()
+    elif spec.shape == (3,):
+        wp, wg, eps_inf = spec
+        c = 299792458
+        w = (2 * np.pi * c) / (wl_nm * 1e-9)
+        n = np.sqrt(eps_inf - wp ** 2 / (w ** 2 + 1j * wg * w))
+    else:
+        ns = spec[:, 1] if spec.shape[1] == 2 else spec[:, 1] + 1j * spec[:, 2]
+        n = interp1d(spec[:, 0], ns)(wl_nm)
+    return n if loss else np.real(n)

@@ -108,8 +108,18 @@ def _stack_1d(seed, world_1d, swap=False):
                            loss=False)
     lays = [sub.calc_modes(light)]
     olays = [G.film_layer(1.46 + 0j, wl, kp, period, air, None, period, mo, world_1d, False)]
-    hs = [150.0, 900.0]
-    for h in hs:
+    # two gratings with a film between them: in the 2D order set the orders
+    # with py != 0 do not couple to a 1D grating (R12 = -1 for them), so two
+    # gratings with only an air gap between them make those orders an
+    # exactly singular cavity -- in the reference as here
+    hs = [150.0, 80.0, 900.0]
+    for li, h in enumerate(hs):
+        if li == 1:
+            nf = 2.1 + 0.05j
+            f = objects.ThinFilm(period, height_nm=h, world_1d=world_1d, material=materials.Material(nf))
+            lays.append(f.calc_modes(light))
+            olays.append(G.film_layer(nf, wl, kp, period, air, h, period, mo, world_1d, True))
+            continue
         mesh = _mesh(60, seed=int(h))
         M = 46
         kz = rng.uniform(0, 2 * k0, M) + 1j * rng.uniform(0, 0.1 * k0, M)
@@ -141,7 +151,7 @@ def test_stack_of_1d_gratings_from_fields_matches_the_oracle(world_1d, swap):
     NanoStruct('1D_array').calc_modes(fields=...) and Stack.calc_scat."""
     from emustack_b200.stack import Stack
     lays, olays, air, hs, period = _stack_1d(5, world_1d, swap)
-    for i in (1, 2):
+    for i in (1, 3):
         Jo = olays[i].J
         _close(lays[i].J, Jo, rel=1e-11, msg='layer %d J' % i)
         _close(lays[i].J_dag, olays[i].J_dag, rel=1e-11, msg='layer %d J_dag' % i)
