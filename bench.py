@@ -14,9 +14,11 @@ Arms
   ours       : device-resident inputs, one fused launch per step (`value`);
                `e2e` repeats the step through the public host-to-host API
                (FilmHostPipeline) with pinned host inputs: host->device
-               copies, the solves and the device->host read of R_net/T_net
-               diagonals and a/t/r lists, in 4096-point pieces on four
-               streams so copies overlap solves.  Unless --no-extras, the
+               copies, the solves and the device->host read of every
+               point's R/T/A (a/t/r lists and flags), in 4096-point pieces
+               on four streams so copies overlap solves;
+               `e2e_with_R_T_net` also reads the R_net / T_net diagonals
+               back (176 MB per step: the host link bounds it).  Unless --no-extras, the
                same JSON line carries `north_star`: the batched GSM against
                the plain FP64 GPU GSM (this library called once per solve,
                the way the reference calls its GSM) on config 2, on the
@@ -289,39 +291,44 @@ def run_ours(args, rank, world, local_rank):
     # T_net diagonals and a/t/r lists, in pieces whose copies overlap the
     # solves of their neighbours
     from emustack_b200.films import FilmHostPipeline
-    pipe = FilmHostPipeline(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev, chunk=E2E_CHUNK, n_streams=E2E_STREAMS)
     h_wl = torch.from_numpy(w['wl']).pin_memory()
     h_kp = torch.from_numpy(w['k_pll']).pin_memory()
     h_n = torch.from_numpy(w['n']).pin_memory()
     h_h = torch.from_numpy(w['heights']).pin_memory()
-    outs_h = pipe.outputs(B)
-    h2d = sum(t.numel() * t.element_size() for t in (h_wl, h_kp, h_n, h_h))
-    h2d += (h_h.numel() * h_h.element_size()) * ((B + E2E_CHUNK - 1) // E2E_CHUNK - 1)
-    d2h = sum(t.numel() * t.element_size() for t in outs_h.values())
 
-    def e2e_step():
-        pipe.solve(h_wl, h_kp, h_n, h_h, pol=POL)
+    def e2e_run(outputs):
+        """points/s through FilmHostPipeline bringing `outputs` back to the
+        host, and the bytes copied each way per step"""
+        pipe = FilmHostPipeline(N_FILMS + 2, MAX_ORDER, PERIOD, device=dev, chunk=E2E_CHUNK,
+                                n_streams=E2E_STREAMS, outputs=outputs)
+        outs_h = pipe.outputs(B)
+        h2d = sum(t.numel() * t.element_size() for t in (h_wl, h_kp, h_n, h_h))
+        h2d += (h_h.numel() * h_h.element_size()) * ((B + E2E_CHUNK - 1) // E2E_CHUNK - 1)
+        d2h = sum(t.numel() * t.element_size() for t in outs_h.values())
+        for _ in range(args.warmup):
+            pipe.solve(h_wl, h_kp, h_n, h_h, pol=POL)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e_s, e_e = _events(args.steps), _events(args.steps)
+        for i in range(args.steps):
+            flush.fill_(i & 0xff)
+            e_s[i].record(stream)
+            pipe.solve(h_wl, h_kp, h_n, h_h, pol=POL)
+            e_e[i].record(stream)
+        torch.cuda.synchronize()
+        e_ms = np.array([s.elapsed_time(e) for s, e in zip(e_s, e_e)])
+        etot = torch.tensor([e_ms.sum()], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(etot, op=dist.ReduceOp.MAX)
+        # sanity: the copied results are the device results' lists
+        assert np.isfinite(outs_h['a_list'].numpy()).all()
+        return world * B * args.steps / (float(etot.item()) / 1e3), h2d, d2h
 
-    for _ in range(args.warmup):
-        e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    e_s = _events(args.steps)
-    e_e = _events(args.steps)
-    for i in range(args.steps):
-        flush.fill_(i & 0xff)
-        e_s[i].record(stream)
-        e2e_step()
-        e_e[i].record(stream)
-    torch.cuda.synchronize()
-    e_ms = np.array([s.elapsed_time(e) for s, e in zip(e_s, e_e)])
-    etot = torch.tensor([e_ms.sum()], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(etot, op=dist.ReduceOp.MAX)
-    e2e_value = world * B * args.steps / (float(etot.item()) / 1e3)
-    # sanity: the copied results are the device results
-    assert np.isfinite(outs_h['a_list'].numpy()).all()
+    # the metric's result per point is its R/T/A: the a/t/r lists come back;
+    # the same with the R_net / T_net diagonals as well is reported beside it
+    e2e_value, h2d, d2h = e2e_run(FilmHostPipeline.SPECTRA)
+    e2e_full, h2d_f, d2h_f = e2e_run(FilmHostPipeline.OUT)
 
     result = None
     if rank == 0:
@@ -359,7 +366,11 @@ def run_ours(args, rank, world, local_rank):
                            'p99': float(np.percentile(step_ms, 99)),
                            'unit': 'one 32768-point batch'},
             'e2e': {'value': e2e_value, 'unit': 'points/s', 'h2d_bytes_per_step': h2d,
-                    'd2h_bytes_per_step': d2h},
+                    'd2h_bytes_per_step': d2h,
+                    'result': 'a_list, t_list, r_list and flags of every point (the R/T/A spectra)'},
+            'e2e_with_R_T_net': {'value': e2e_full, 'unit': 'points/s', 'h2d_bytes_per_step': h2d_f,
+                                 'd2h_bytes_per_step': d2h_f,
+                                 'result': 'the R/T/A spectra and the R_net / T_net diagonals'},
             'gpu_launches': int(launches),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm,
                          'unit': 'GB/s', 'frac': achieved / hbm, 'traffic': traffic,

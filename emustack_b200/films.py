@@ -211,9 +211,17 @@ class FilmHostPipeline(object):
     """
 
     OUT = ('R_net', 'T_net', 'a_list', 't_list', 'r_list', 'flags')
+    SPECTRA = ('a_list', 't_list', 'r_list', 'flags')
 
     def __init__(self, n_layers, max_order, period, period_y=None, world_1d=False, device='cuda',
-                 chunk=8192, n_streams=2):
+                 chunk=8192, n_streams=2, outputs=OUT):
+        """outputs: the results copied back to the host, a subset of OUT
+        (SPECTRA: the absorptance / transmittance / reflectance lists and
+        flags only, the R/T/A spectra of a sweep; R_net and T_net are
+        computed on the device either way)."""
+        if not outputs or any(k not in self.OUT for k in outputs):
+            raise ValueError('outputs must be a non-empty subset of %s' % (self.OUT,))
+        self.keys = tuple(outputs)
         self.device = torch.device(device)
         self.solvers = [FilmStackSolver(n_layers, max_order, period, period_y, world_1d, device=self.device)
                         for _ in range(n_streams)]
@@ -223,10 +231,10 @@ class FilmHostPipeline(object):
 
     def outputs(self, B):
         """Pinned host outputs for a batch of B points (reused across calls)."""
-        if self._out is None or self._out['r_list'].shape[0] != B:
+        if self._out is None or next(iter(self._out.values())).shape[0] != B:
             dev = self.solvers[0].outputs(1)
             self._out = {k: torch.empty((B,) + tuple(dev[k].shape[1:]), dtype=dev[k].dtype).pin_memory()
-                         for k in self.OUT}
+                         for k in self.keys}
         return self._out
 
     def solve(self, wl_nm, k_pll, n, heights_nm=None, pol='TE', variant=None):
@@ -253,7 +261,7 @@ class FilmHostPipeline(object):
                 if heights_nm is not None:
                     dh = (heights_nm[b0:b1] if per_point_h else heights_nm).to(self.device, non_blocking=True)
                 o = sol.solve(dw, dk, dn, dh, pol=pol, stream=st, variant=variant)
-                for k in self.OUT:
+                for k in self.keys:
                     out[k][b0:b1].copy_(o[k], non_blocking=True)
         for st in self.streams:
             cur.wait_stream(st)

@@ -103,8 +103,9 @@ int emu_grating_orders(int max_order, double period, double period_y, int world_
  * k_parallel * (1 - 1e-9) (backend/mode_calcs.py:147-162), the specular
  * order and the number of propagating orders (k_z.imag == 0).
  * Replaces Anallo.calc_kz (backend/mode_calcs.py:116-186).  Ties in the air
- * sort keys are ranked by order index (numpy's argsort leaves their order
- * unspecified; tied orders have identical k_z). */
+ * sort keys (only when a k_parallel component is exactly zero) are ranked by
+ * order index, as numpy's argsort ranks them for up to 16 orders; tied
+ * orders have identical k_z. */
 typedef struct {
   int n_points;            /* B films (each with its own wavelength)        */
   int n_pw;                /* Npw                                           */

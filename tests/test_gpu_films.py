@@ -246,3 +246,24 @@ def test_host_pipeline_matches_device_solve(per_point_heights):
     ref = s.solve(*[t.to(dev) for t in host], pol='un')
     for k in FilmHostPipeline.OUT:
         np.testing.assert_array_equal(out[k].numpy(), ref[k].cpu().numpy(), err_msg=k)
+
+
+def test_host_pipeline_spectra_only():
+    """FilmHostPipeline(outputs=SPECTRA) brings back only the a/t/r lists and
+    flags, equal to the full device solve's."""
+    from emustack_b200.films import FilmHostPipeline, FilmStackSolver
+    h, nl = _config2_stack(seed=3)
+    B = 700
+    wl, kp = _points(B, seed=6)
+    n = np.tile(nl, (B, 1))
+    pipe = FilmHostPipeline(len(nl), 5, 500.0, chunk=256, outputs=FilmHostPipeline.SPECTRA)
+    host = [torch.tensor(a).pin_memory() for a in (wl, kp, n, h)]
+    out = pipe.solve(*host, pol='TM')
+    torch.cuda.synchronize()
+    assert set(out) == set(FilmHostPipeline.SPECTRA)
+    s = FilmStackSolver(len(nl), 5, 500.0)
+    ref = s.solve(*[t.to(s.device) for t in host], pol='TM')
+    for k in FilmHostPipeline.SPECTRA:
+        np.testing.assert_array_equal(out[k].numpy(), ref[k].cpu().numpy(), err_msg=k)
+    with pytest.raises(ValueError):
+        FilmHostPipeline(len(nl), 5, 500.0, outputs=('R_net', 'nonsense'))
