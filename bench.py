@@ -192,6 +192,16 @@ def _events(n):
     return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
 
 
+def hbm_peak():
+    """HBM copy bandwidth (GB/s) measured on this pool's B200s, else the
+    earlier measurement used as the fallback."""
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
 def _timed(fn, steps, warmup=2, flush=None):
     """Median ms of `steps` calls of fn (CUDA events on the current stream,
     after `warmup` untimed calls; L2 flushed before each timed call when a
@@ -332,13 +342,7 @@ def run_ours(args, rank, world, local_rank):
 
     result = None
     if rank == 0:
-        hbm = None
-        try:
-            with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
-                peaks = json.load(f)
-            hbm, hbm_src = float(peaks['hbm_gbs']), 'measured'
-        except Exception:
-            hbm, hbm_src = 6650.0, 'fallback'
+        hbm, hbm_src = hbm_peak()
         by = algorithmic_counts(B, L, P)
         achieved = by / (ms_per_step / 1e3) / 1e9
         flops = film_flops(B, L, P)
@@ -828,6 +832,97 @@ def config3_line(steps):
             'ms_per_wavelength': 4 * ms_j + ms_gsm / 148}
 
 
+# ----------------------------------------------------------------- --fields
+def fields_line(steps):
+    """Field reconstruction from the GSM amplitudes.
+
+    Plane-wave fields (emu_pw_fields): one film layer (the 6th of 12) of 256
+    points of the thin-film workload (81 orders per polarisation), on a
+    51 x 51 x 4 grid per point (fields_in_plane's grid), against the numpy
+    restatement of the reference's loop on a sample.  Bloch-mode node fields
+    (emu_bloch_fields_plane): one 2D layer of 20 000 elements and 400 modes
+    (the config-3 layer size), against the numpy restatement of
+    field_value_plane on 2 000 elements."""
+    import torch
+    from emustack_b200.fields import bloch_fields_plane, film_batch_fields, pw_fields
+    from emustack_b200.films import FilmStackSolver
+    from emustack_b200.probe import fp64_peak_tflops
+    from oracle import fields_oracle as F
+    dev = torch.device('cuda')
+    w = workload(seed=0)
+    B, L, layer = 256, N_FILMS + 2, 6
+    solver = FilmStackSolver(L, MAX_ORDER, PERIOD)
+    S = solver.npw
+    wl = torch.tensor(w['wl'][:B], device=dev)
+    kp = torch.tensor(w['k_pll'][:B], device=dev)
+    n = torch.tensor(w['n'][:B], device=dev)
+    hs = torch.tensor(w['heights'], device=dev)
+    out = solver.solve(wl, kp, n, hs, pol=POL, want=('kz', 'vec_coef', 'sort_order'))
+    h_norm = float(w['heights'][layer - 1]) / PERIOD
+    r = np.linspace(0.0, 1.0, 51)
+    zs = np.linspace(0.0, h_norm, 4)
+    # inputs of the kernel, formed once (film_batch_fields forms them per call)
+    film_batch_fields(solver, out, kp, n, layer, r, r, zs, heights_nm=hs, grid=True)
+    two_pi = 2 * np.pi
+    kpn = kp * PERIOD
+    alphas = (kpn[:, 0:1] + solver.d_px.to(torch.float64)[None] * two_pi).contiguous()
+    betas = (kpn[:, 1:2] + solver.d_py.to(torch.float64)[None] * two_pi).contiguous()
+    row = L - 1 - layer
+    args = dict(alphas=alphas, betas=betas, sort_order=out['sort_order'].clone(),
+                kz=out['kz'][:, layer].contiguous(), n=n[:, layer].contiguous(),
+                vec_coef_down=out['vec_coef_down'][:, row].contiguous(),
+                vec_coef_up=out['vec_coef_up'][:, row].contiguous(),
+                x=torch.tensor(r, device=dev), y=torch.tensor(r, device=dev), z=torch.tensor(zs, device=dev),
+                height_norm=torch.full((B,), h_norm, dtype=torch.float64, device=dev), grid=True)
+    Q = 51 * 51 * 4
+    ms = _timed(lambda: pw_fields(**args), steps, warmup=3)
+    terms = B * Q * S
+    # CPU: the restatement of the reference's per-point loop on 2 points x 11 x 11 x 4
+    a = {k: (v.cpu().numpy() if hasattr(v, 'cpu') else v) for k, v in args.items()}
+    rs = np.linspace(0.0, 1.0, 11)
+    t0 = time.perf_counter()
+    for b in range(2):
+        F.pw_field_grid(a['alphas'][b], a['betas'][b], a['sort_order'][b], a['kz'][b], a['n'][b],
+                        a['vec_coef_down'][b], a['vec_coef_up'][b], rs, rs, zs, height_norm=h_norm)
+    cpu_s = time.perf_counter() - t0
+    cpu_pts = 2 * 11 * 11 * 4 / cpu_s
+    # FP64 operations per (point, order): 2 phase products and 1 add, 2 multiply-adds for the
+    # arguments, 2 sincos, 2 exp, 4 products for the magnitudes, 6 complex multiply-adds (8 each)
+    flops_per_term = 3 + 4 + 2 + 2 + 4 + 48
+    pw = {'stacks': B, 'points_per_stack': Q, 'orders': S, 'ms': ms,
+          'field_points_per_s': B * Q / (ms / 1e3), 'order_terms_per_s': terms / (ms / 1e3),
+          'cpu_field_points_per_s': cpu_pts, 'cpu_sample': '2 stacks x 11 x 11 x 4 points, numpy, 1 core',
+          'fp64_peak_tflops': fp64_peak_tflops(),
+          'note': 'FP64-issue bound: each term takes two sincos and two exp (counted as one operation each)'}
+    pw['fp64_tflops'] = terms * flops_per_term / (ms / 1e3) / 1e12
+    pw['frac'] = pw['fp64_tflops'] / pw['fp64_peak_tflops']
+    del out, args
+    torch.cuda.empty_cache()
+    # Bloch-mode node fields at the config-3 layer size
+    nel, M = 20000, 400
+    g = torch.Generator(device='cuda').manual_seed(0)
+    sol = torch.complex(torch.randn((1, nel, M, 13, 3), dtype=torch.float64, device=dev, generator=g),
+                        torch.randn((1, nel, M, 13, 3), dtype=torch.float64, device=dev, generator=g))
+    kz = torch.complex(torch.rand((1, M), dtype=torch.float64, device=dev, generator=g) * 3 + 0.5,
+                       torch.rand((1, M), dtype=torch.float64, device=dev, generator=g) * 0.5)
+    vc = torch.complex(torch.randn((1, 2 * M), dtype=torch.float64, device=dev, generator=g),
+                       torch.randn((1, 2 * M), dtype=torch.float64, device=dev, generator=g))
+    msb = _timed(lambda: bloch_fields_plane(sol, kz, vc, 0.5, 0.2), steps, warmup=3)
+    bytes_alg = nel * M * 18 * 16 + 2 * M * 16 + M * 16 + nel * 18 * 16
+    hbm, hbm_src = hbm_peak()
+    ns = 2000
+    sol_s = sol[0, :ns].cpu().numpy()
+    kz_h, vc_h = kz[0].cpu().numpy(), vc[0].cpu().numpy()
+    t0 = time.perf_counter()
+    F.bloch_field_plane(sol_s, kz_h, vc_h, 0.5, 0.2)
+    cpu_b = time.perf_counter() - t0
+    bl = {'elements': nel, 'modes': M, 'ms': msb, 'elements_per_s': nel / (msb / 1e3),
+          'achieved_gbs': bytes_alg / (msb / 1e3) / 1e9, 'peak_gbs': hbm, 'peak_source': hbm_src,
+          'frac': bytes_alg / (msb / 1e3) / 1e9 / hbm, 'algorithmic_bytes': bytes_alg,
+          'cpu_elements_per_s': ns / cpu_b, 'cpu_sample': '2000 elements, numpy, 1 core'}
+    return {'workload': 'fields', 'pw_fields': pw, 'bloch_fields_plane': bl}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -836,6 +931,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument('--no-extras', action='store_true', help='skip the north_star comparison keys')
+    ap.add_argument('--fields', action='store_true',
+                    help='time the field reconstruction kernels instead of the GSM')
     ap.add_argument('--cpu-sample', type=int, default=0,
                     help='points in the CPU sample (default: 8 per host core, >= 64)')
     args = ap.parse_args()
@@ -866,6 +963,10 @@ def main():
                     'd2h_bytes_per_step': 0},
         }
         print(json.dumps(line))
+        return
+
+    if args.fields:
+        print(json.dumps(fields_line(max(args.steps, 5))))
         return
 
     if args.config != 2:

@@ -12,7 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libemustack_gsm.so')
 
 EMU_OK = 0
+EMU_E_ARG = 1
 EMU_E_SHAPE = 2
+EMU_E_WORKSPACE = 5
 STATUS_NAMES = {
     0: 'EMU_OK', 1: 'EMU_E_ARG', 2: 'EMU_E_SHAPE', 3: 'EMU_E_SINGULAR',
     4: 'EMU_E_NONFINITE', 5: 'EMU_E_WORKSPACE', 6: 'EMU_E_TIMEOUT',
@@ -340,7 +342,34 @@ EXTRA_SIGNATURES.extend([
     ('emu_film_ring_submit', C.c_int, [vp, C.POINTER(EmuFilmRingRequest), C.POINTER(C.c_longlong)]),
     ('emu_film_ring_poll', C.c_int, [vp, C.c_longlong, C.POINTER(EmuFilmRingResult)]),
     ('emu_film_ring_wait', C.c_int, [vp, C.c_longlong, C.c_double, C.POINTER(EmuFilmRingResult)]),
+    ('emu_film_ring_ready', C.c_int, [vp, C.c_longlong]),
     ('emu_film_ring_running', C.c_int, [vp]),
     ('emu_film_ring_stop', C.c_int, [vp]),
     ('emu_film_ring_destroy', C.c_int, [vp]),
+])
+
+
+class EmuPwFields(C.Structure):
+    _fields_ = [
+        ('n_stacks', C.c_int), ('n_pw', C.c_int), ('substrate', C.c_int), ('grid', C.c_int),
+        ('nx', C.c_int), ('ny', C.c_int), ('nz', C.c_int),
+        ('d_alphas', vp), ('d_betas', vp), ('d_sort', vp), ('d_kz', vp), ('d_n', vp), ('d_height', vp),
+        ('d_vec_coef_down', vp), ('d_vec_coef_up', vp), ('vcd_stride', C.c_longlong),
+        ('vcu_stride', C.c_longlong), ('d_x', vp), ('d_y', vp), ('d_z', vp), ('d_E', vp), ('d_E_abs', vp),
+    ]
+
+
+class EmuBlochFieldsPlane(C.Structure):
+    _fields_ = [
+        ('n_stacks', C.c_int), ('n_modes', C.c_int), ('n_elements', C.c_int), ('d_sol', vp),
+        ('sol_stride', C.c_longlong), ('d_k_z', vp), ('d_vec_coef', vp), ('h', C.c_double),
+        ('hz', C.c_double), ('d_E', vp),
+    ]
+
+
+PW_FIELDS_MAX_ORDERS = 1536
+
+EXTRA_SIGNATURES.extend([
+    ('emu_pw_fields', C.c_int, [C.POINTER(EmuPwFields), vp]),
+    ('emu_bloch_fields_plane', C.c_int, [C.POINTER(EmuBlochFieldsPlane), vp]),
 ])

@@ -464,13 +464,14 @@ extern "C" int emu_film_ring_submit(EmuFilmRing *r, const EmuFilmRingRequest *q,
   return ring_ensure_running(r);
 }
 
-extern "C" int emu_film_ring_poll(EmuFilmRing *r, long long ticket, EmuFilmRingResult *out) {
-  if (!r || ticket < 0) return EMU_E_ARG;
-  std::lock_guard<std::mutex> lock(r->mu);
-  if (ticket >= r->next || ticket < r->next - r->cap) return EMU_E_ARG;
-  unsigned char *s = r->slot(ticket);
-  if (r->consumed[(size_t)(ticket % r->cap)] >= ticket) return EMU_E_ARG;  // already read
-  const long long done = *(volatile long long *)(s + kOffDone);
+namespace {
+// 1 when the ticket's result is in its slot, 0 when not yet (restarting the
+// loop if a request raced its idle end), negative on a bad ticket or error.
+// Caller holds r->mu.
+int ring_ready(EmuFilmRing *r, long long ticket) {
+  if (ticket < 0 || ticket >= r->next || ticket < r->next - r->cap) return -EMU_E_ARG;
+  if (r->consumed[(size_t)(ticket % r->cap)] >= ticket) return -EMU_E_ARG;  // already read
+  const long long done = *(volatile long long *)(r->slot(ticket) + kOffDone);
   if (done != ticket + 1) {
     if (*(volatile int32_t *)&r->ctl()->exited && cudaStreamQuery(r->stream) != cudaErrorNotReady) {
       const int st = ring_ensure_running(r);  // a request raced the idle end
@@ -478,6 +479,23 @@ extern "C" int emu_film_ring_poll(EmuFilmRing *r, long long ticket, EmuFilmRingR
     }
     return 0;
   }
+  return 1;
+}
+}  // namespace
+
+extern "C" int emu_film_ring_ready(EmuFilmRing *r, long long ticket) {
+  if (!r) return -EMU_E_ARG;
+  std::lock_guard<std::mutex> lock(r->mu);
+  return ring_ready(r, ticket);
+}
+
+extern "C" int emu_film_ring_poll(EmuFilmRing *r, long long ticket, EmuFilmRingResult *out) {
+  if (!r || ticket < 0) return EMU_E_ARG;
+  std::lock_guard<std::mutex> lock(r->mu);
+  const int ready = ring_ready(r, ticket);
+  if (ready == -EMU_E_ARG) return EMU_E_ARG;
+  if (ready != 1) return ready;
+  unsigned char *s = r->slot(ticket);
   std::atomic_thread_fence(std::memory_order_acquire);
   const SlotHdr *h = (const SlotHdr *)(s + kOffHdr);
   if (out) {

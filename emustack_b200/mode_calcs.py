@@ -225,6 +225,7 @@ class Simmo(Modes):
             self.J = np.asmatrix(np.asarray(J, dtype=np.complex128))
             self.J_dag = np.asmatrix(np.asarray(J_dag, dtype=np.complex128))
         elif fields is not None:
+            self.sol1 = fields['sol1']        # prime-mode fields, for field reconstruction
             if getattr(self.structure, 'periodicity', '2D_array') == '1D_array':
                 from .overlap import overlap_from_fields_1d
                 self.J, self.J_dag = overlap_from_fields_1d(self, fields)

@@ -540,6 +540,7 @@ class DeviceFilmServer(object):
               'emu_film_ring_create')
         self._h = h
         self._pending = {}
+        self._early = {}
         self._orders = {}
 
     def _order_arrays(self, r):
@@ -566,7 +567,7 @@ class DeviceFilmServer(object):
         t = C.c_longlong()
         while True:
             st = self._L.emu_film_ring_submit(self._h, C.byref(q), C.byref(t))
-            if st != 5:      # EMU_E_WORKSPACE: the ring is full until results are read
+            if st != _lib.EMU_E_WORKSPACE:   # the ring is full until results are read
                 break
             self._drain_one()
         check(st, 'emu_film_ring_submit')
@@ -585,17 +586,25 @@ class DeviceFilmServer(object):
         return res, o
 
     def poll(self, ticket):
-        res, o = self._result(ticket)
-        st = self._L.emu_film_ring_poll(self._h, int(ticket), C.byref(o))
+        if ticket in self._early:
+            return self._early.pop(ticket)
+        if ticket not in self._pending:
+            raise _lib.EmuError(_lib.EMU_E_ARG, 'emu_film_ring_poll: unknown or already read ticket')
+        st = self._L.emu_film_ring_ready(self._h, int(ticket))
         if st == 0:
             return None
-        if st < 0 or st > 1:
-            raise _lib.EmuError(abs(st), 'emu_film_ring_poll')
-        del self._pending[ticket]
-        res['flags'] = int(res['flags'][0])
-        return res
+        if st != 1:
+            raise _lib.EmuError(abs(st), 'emu_film_ring_ready')
+        return self._read(ticket, 0.0)
 
     def wait(self, ticket, timeout_s=60.0):
+        if ticket in self._early:
+            return self._early.pop(ticket)
+        if ticket not in self._pending:
+            raise _lib.EmuError(_lib.EMU_E_ARG, 'emu_film_ring_wait: unknown or already read ticket')
+        return self._read(ticket, timeout_s)
+
+    def _read(self, ticket, timeout_s):
         res, o = self._result(ticket)
         st = self._L.emu_film_ring_wait(self._h, int(ticket), float(timeout_s), C.byref(o))
         if st != 1:
@@ -605,16 +614,14 @@ class DeviceFilmServer(object):
         return res
 
     def _drain_one(self):
-        """Read the oldest pending result (it frees its slot)."""
+        """Read the oldest pending result (it frees its slot); poll, wait
+        and take return it later."""
         t = min(self._pending)
-        self._done_early = getattr(self, '_done_early', {})
-        self._done_early[t] = self.wait(t)
+        self._early[t] = self._read(t, 60.0)
 
     def take(self, ticket):
-        """Result of a ticket whether it was read early (to free its slot) or not."""
-        early = getattr(self, '_done_early', {})
-        if ticket in early:
-            return early.pop(ticket)
+        """Result of a ticket, waiting for it if needed (also when it was
+        read early to free its slot)."""
         return self.wait(ticket)
 
     def running(self):

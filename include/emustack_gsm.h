@@ -221,6 +221,58 @@ typedef struct {
 int emu_material_n_batch(const EmuMaterial *h_materials, int n_layers, int n_points,
                          const double *d_wl_nm, emu_c128 *d_n, int32_t *d_error, void *stream);
 
+/* ------------------------------------------ fields from the amplitudes
+ * emu_pw_fields: E = (E_x, E_y, E_z) inside one homogeneous layer of B
+ * solved stacks, from the layer's plane-wave amplitudes, at the points
+ * (x, y, z) in units of the period -- the ThinFilm branch of fields_in_plane
+ * (backend/plotting.py:1759-1833) and field_values (plotting.py:2857-2996).
+ * z is the distance from the bottom of the layer (from the top of the
+ * substrate, into it, for layer 0); a finite layer's height enters the
+ * down-going term as exp(-i gamma (z - h)), a semi-infinite layer's as
+ * h = 0.  E[b] holds E_x, E_y, E_z, each over the Q points (grid: Q =
+ * nx ny nz in [x][y][z] order, the reference's E_x_array[x, y, z]).
+ * At most 1536 orders per polarisation. */
+typedef struct {
+  int n_stacks;            /* B                                               */
+  int n_pw;                /* Npw orders per polarisation                     */
+  int substrate;           /* 1: layer 0 (z -> -z, no upward amplitudes)      */
+  int grid;                /* 1: grid x[nx] x y[ny] x z[nz]; 0: nx points     */
+  int nx, ny, nz;
+  const double *d_alphas;  /* [B][Npw] unsorted (Anallo.alphas)               */
+  const double *d_betas;   /* [B][Npw] unsorted (world_1d: beta0 everywhere)  */
+  const int32_t *d_sort;   /* [B][Npw] the air reference's sort order         */
+  const emu_c128 *d_kz;    /* [B][Npw] sorted k_z (Anallo.calc_kz())          */
+  const emu_c128 *d_n;     /* [B] layer index, loss flag applied              */
+  const double *d_height;  /* [B] height / period, 0 if semi-infinite; or NULL */
+  const emu_c128 *d_vec_coef_down; /* row b at b * vcd_stride: TE then TM     */
+  const emu_c128 *d_vec_coef_up;   /* same, or NULL (zero)                    */
+  long long vcd_stride, vcu_stride;
+  const double *d_x, *d_y, *d_z;   /* units of the period                     */
+  emu_c128 *d_E;           /* [B][3][Q]                                       */
+  double *d_E_abs;         /* [B][Q] |E|, or NULL                             */
+} EmuPwFields;
+int emu_pw_fields(const EmuPwFields *p, void *stream);
+
+/* emu_bloch_fields_plane: E at the six P2 nodes of every element of a 2D
+ * nanostructured layer at the plane hz (distance from the top of the layer,
+ * in units of the period, 0 <= hz <= h; EMU_E_ARG otherwise), from the
+ * layer's Bloch-mode amplitudes -- field_value_plane
+ * (backend/fortran/field_value_plane.f:6-132), used by fields_in_plane and
+ * fields_interpolator_in_plane (backend/plotting.py:1700-1737, 1943-1990).
+ * d_E[b][el][node][component] is the routine's m_E(el, node, component). */
+typedef struct {
+  int n_stacks;            /* B                                               */
+  int n_modes;             /* M Bloch modes                                   */
+  int n_elements;          /* nel                                             */
+  const emu_c128 *d_sol;   /* [B][nel][M][13][3], Fortran sol(3, 13, M, nel)  */
+  long long sol_stride;    /* complex values between stacks                   */
+  const emu_c128 *d_k_z;   /* [B][M] propagation constants                    */
+  const emu_c128 *d_vec_coef; /* [B][2M] vec_coef_down then vec_coef_up       */
+  double h, hz;            /* layer height / period; plane                    */
+  emu_c128 *d_E;           /* [B][nel][6][3]                                  */
+} EmuBlochFieldsPlane;
+int emu_bloch_fields_plane(const EmuBlochFieldsPlane *p, void *stream);
+
 /* ------------------------------ serving: device-resident request loop
  * A persistent kernel that solves all-film spectral points as the host
  * writes them into a ring of slots in pinned, device-mapped host memory:
@@ -239,7 +291,8 @@ int emu_material_n_batch(const EmuMaterial *h_materials, int n_layers, int n_poi
  *             oldest results first).  Thread-safe.
  *   poll    : 1 and the outputs copied out when the ticket is done, 0 while
  *             pending (each result can be read once); wait: poll until done
- *             or timeout (-EMU_E_TIMEOUT).
+ *             or timeout (-EMU_E_TIMEOUT); ready: 1 when done, 0 while
+ *             pending, without reading (or consuming) the result.
  *   stop    : ends the loop and waits for it; returns EMU_E_TIMEOUT if a
  *             device wait gave up, else EMU_OK.
  * While the loop runs it holds every SM; other kernels on the device wait
@@ -268,6 +321,7 @@ int emu_film_ring_create(int capacity, double idle_seconds, EmuFilmRing **out);
 int emu_film_ring_submit(EmuFilmRing *ring, const EmuFilmRingRequest *req, long long *ticket);
 int emu_film_ring_poll(EmuFilmRing *ring, long long ticket, EmuFilmRingResult *out);
 int emu_film_ring_wait(EmuFilmRing *ring, long long ticket, double timeout_s, EmuFilmRingResult *out);
+int emu_film_ring_ready(EmuFilmRing *ring, long long ticket);
 int emu_film_ring_running(EmuFilmRing *ring);
 int emu_film_ring_stop(EmuFilmRing *ring);
 int emu_film_ring_destroy(EmuFilmRing *ring);

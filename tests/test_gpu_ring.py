@@ -106,3 +106,32 @@ def test_ring_refuses_requests_it_cannot_hold():
         assert srv.stop() == 0
     finally:
         srv.close()
+
+
+def test_poll_returns_results_read_early_to_free_slots():
+    """More submissions than slots with nothing read: submit frees slots by
+    reading the oldest results itself; poll / wait must still return every
+    ticket's result exactly once, and ready() never consumes one."""
+    from emustack_b200 import _lib
+    from emustack_b200.serving import DeviceFilmServer
+    reqs = _requests(60, seed=5, max_mo=4)
+    srv = DeviceFilmServer(capacity=16, idle_seconds=0.5)
+    try:
+        tickets = [srv.submit(r) for r in reqs]
+        got = {}
+        deadline = time.time() + 30.0
+        while len(got) < len(tickets) and time.time() < deadline:
+            for t in tickets:
+                if t not in got:
+                    res = srv.poll(t)
+                    if res is not None:
+                        got[t] = res
+        assert len(got) == len(tickets)
+        with pytest.raises(_lib.EmuError):
+            srv.poll(tickets[-1])                   # read once only
+        assert srv.stop() == 0
+    finally:
+        srv.close()
+    ref = _var_results(reqs)
+    for t, v in zip(tickets, ref):
+        np.testing.assert_array_equal(got[t]['R_net'], np.asarray(v['R_net']))
