@@ -75,7 +75,8 @@ __global__ void __launch_bounds__(kPwThreads) pw_fields_kernel(PwArgs a) {
   const double h = a.height ? a.height[b] : 0.0;
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
     const int j = a.sort[(size_t)b * S + s];
-    const double al = a.alphas[(size_t)b * S + j], be = a.betas[(size_t)b * S + j];
+    const bool ok = j >= 0 && j < S;  // a sort order that is not a permutation gives NaN fields
+    const double al = ok ? a.alphas[(size_t)b * S + j] : nan(""), be = ok ? a.betas[(size_t)b * S + j] : nan("");
     const cd g = a.kz[(size_t)b * S + s];
     const double ab2 = al * al + be * be;
     const double norm = sqrt(ab2);
