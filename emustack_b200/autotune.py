@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import json
 import os
+import warnings
 import threading
 
 import torch
@@ -28,7 +29,9 @@ class Autotuner(object):
     times ``reps`` launches with CUDA events after ``warmup`` launches."""
 
     def __init__(self, path=None, warmup=1, reps=3, time_fn=None, tie=0.02):
-        self.path = path if path is not None else os.environ.get('EMUSTACK_AUTOTUNE_CACHE')
+        self.path = path if path is not None else _ENV_PATH
+        if self.path:
+            self.path = os.path.abspath(self.path)
         self.tie = float(tie)
         self.time_fn = time_fn or self._cuda_time
         self.enabled = os.environ.get('EMUSTACK_AUTOTUNE', '1') != '0'
@@ -95,9 +98,12 @@ class Autotuner(object):
             self.log.append((key, entry))
             if self.path:
                 tmp = self.path + '.tmp'
-                with open(tmp, 'w') as f:
-                    json.dump(self.cache, f, indent=1, sort_keys=True)
-                os.replace(tmp, self.path)
+                try:
+                    with open(tmp, 'w') as f:
+                        json.dump(self.cache, f, indent=1, sort_keys=True)
+                    os.replace(tmp, self.path)
+                except OSError as e:   # the choice stands; only its record is lost
+                    warnings.warn('autotune cache %s not written: %s' % (self.path, e))
         return _as_choice(entry['choice'])
 
 
@@ -106,6 +112,11 @@ def _as_choice(c):
 
 
 _default = None
+# the cache file named by the environment, resolved against the working
+# directory at import, so that later directory changes keep the same file
+_ENV_PATH = os.environ.get('EMUSTACK_AUTOTUNE_CACHE')
+if _ENV_PATH:
+    _ENV_PATH = os.path.abspath(_ENV_PATH)
 
 
 def default_tuner():
