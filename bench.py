@@ -519,7 +519,7 @@ def prepare_array_groups(stacks, period=500.0, group=True):
     import torch
     from emustack_b200.films import grating_orders
     dev = torch.device('cuda')
-    keyf = (lambda s: (s['mo'], s['K'])) if group else (lambda s: id(s))
+    keyf = (lambda s: (s['mo'], s['K'], s.get('M'))) if group else (lambda s: id(s))
     groups = collections.defaultdict(list)
     for s in stacks:
         groups[keyf(s)].append(s)
@@ -528,7 +528,8 @@ def prepare_array_groups(stacks, period=500.0, group=True):
         mo, K = ss[0]['mo'], ss[0]['K']
         px, py = grating_orders(mo, period, period)
         npw = len(px)
-        P, M, B = 2 * npw, 2 * npw + 20, len(ss)
+        P, B = 2 * npw, len(ss)
+        M = ss[0].get('M') or P + 20    # Bloch modes per array layer (default: the reference's num_BMs)
         wl = np.array([s['wl'] for s in ss])
         wln = wl / period
         kza = np.stack([_air_kz(px, py, x, period) for x in wl])
@@ -827,7 +828,7 @@ def config3_line(steps):
     ms_j = _timed(lambda: overlap_batch(dm, px, py, mo, bloch, k0, s1, s2, precision='tf32x3'), steps)
     del s1, s2
     torch.cuda.empty_cache()
-    specs = [dict(mo=mo, npw=len(px), K=4, wl=float(w), seed=i)
+    specs = [dict(mo=mo, npw=len(px), K=4, M=M, wl=float(w), seed=i)
              for i, w in enumerate(np.linspace(400, 900, 148))]
     ms_gsm = time_array_stacks(specs, group=True, n_streams=1)
     return {'config': 3, 'P': 2 * len(px), 'M': M, 'nel': mesh.nel,
@@ -889,14 +890,15 @@ def fields_line(steps, nel=20000):
                         a['vec_coef_down'][b], a['vec_coef_up'][b], rs, rs, zs, height_norm=h_norm)
     cpu_s = time.perf_counter() - t0
     cpu_pts = 2 * 11 * 11 * 4 / cpu_s
-    # FP64 operations per (point, order): 2 phase products and 1 add, 2 multiply-adds for the
-    # arguments, 2 sincos, 2 exp, 4 products for the magnitudes, 6 complex multiply-adds (8 each)
-    flops_per_term = 3 + 4 + 2 + 2 + 4 + 48
+    # the grid path: per (x, y) point and order one complex product X Y (6 FP64 operations),
+    # per z value three complex multiply-adds (8 each); the per-axis tables are not counted
+    flops_per_term = 24 + 6.0 / len(zs)
     pw = {'stacks': B, 'points_per_stack': Q, 'orders': S, 'ms': ms,
           'field_points_per_s': B * Q / (ms / 1e3), 'order_terms_per_s': terms / (ms / 1e3),
           'cpu_field_points_per_s': cpu_pts, 'cpu_sample': '2 stacks x 11 x 11 x 4 points, numpy, 1 core',
           'fp64_peak_tflops': fp64_peak_tflops(),
-          'note': 'FP64-issue bound: each term takes two sincos and two exp (counted as one operation each)'}
+          'path': 'grid: per-axis exponential tables (emu_pw_fields workspace), then a contraction over orders',
+          'note': 'fp64_tflops counts the contraction (24 + 6 / nz FP64 operations per term)'}
     pw['fp64_tflops'] = terms * flops_per_term / (ms / 1e3) / 1e12
     pw['frac'] = pw['fp64_tflops'] / pw['fp64_peak_tflops']
     del out, args

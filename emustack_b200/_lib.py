@@ -356,6 +356,7 @@ class EmuPwFields(C.Structure):
         ('d_alphas', vp), ('d_betas', vp), ('d_sort', vp), ('d_kz', vp), ('d_n', vp), ('d_height', vp),
         ('d_vec_coef_down', vp), ('d_vec_coef_up', vp), ('vcd_stride', C.c_longlong),
         ('vcu_stride', C.c_longlong), ('d_x', vp), ('d_y', vp), ('d_z', vp), ('d_E', vp), ('d_E_abs', vp),
+        ('d_workspace', vp), ('workspace_bytes', C.c_size_t),
     ]
 
 
@@ -370,6 +371,7 @@ class EmuBlochFieldsPlane(C.Structure):
 PW_FIELDS_MAX_ORDERS = 1536
 
 EXTRA_SIGNATURES.extend([
+    ('emu_pw_fields_workspace_size', C.c_size_t, [C.POINTER(EmuPwFields)]),
     ('emu_pw_fields', C.c_int, [C.POINTER(EmuPwFields), vp]),
     ('emu_bloch_fields_plane', C.c_int, [C.POINTER(EmuBlochFieldsPlane), vp]),
 ])

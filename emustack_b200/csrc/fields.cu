@@ -66,6 +66,38 @@ __device__ __forceinline__ void pw_coefs(cd c_te, cd c_tm, const double ete[3], 
   }
 }
 
+// Order s of stack b: sorted alpha, beta, k_z and the TE + TM coefficients
+// of the down and up amplitudes (backend/plotting.py:2896-2941).
+__device__ __forceinline__ PwOrder pw_order(const PwArgs &a, int b, int s, cd n) {
+  const int S = a.S;
+  const int j = a.sort[(size_t)b * S + s];
+  const bool ok = j >= 0 && j < S;  // a sort order that is not a permutation gives NaN fields
+  const double al = ok ? a.alphas[(size_t)b * S + j] : nan(""), be = ok ? a.betas[(size_t)b * S + j] : nan("");
+  const cd g = a.kz[(size_t)b * S + s];
+  const double ab2 = al * al + be * be;
+  const double norm = sqrt(ab2);
+  const cd k = csqrt_p(cd{ab2 + (g.x * g.x - g.y * g.y), 2.0 * g.x * g.y});
+  const cd chi_te = csqrt_p(cdiv(cmul(n, g), k));
+  const cd chi_tm = csqrt_p(cdiv(cmul(n, k), g));
+  const double ete[3] = {be / norm, -al / norm, 0.0};
+  const cd etm[3] = {cd{al / norm, 0.0}, cd{be / norm, 0.0}, cdiv(cd{-norm, 0.0}, g)};
+  PwOrder o;
+  o.a = al;
+  o.b = be;
+  o.gr = g.x;
+  o.gi = g.y;
+  const cd *vd = a.vcd + (size_t)b * a.vcd_stride;
+  pw_coefs(vd[s], vd[S + s], ete, etm, chi_te, chi_tm, o.d);
+  if (a.has_up) {
+    const cd *vu = a.vcu + (size_t)b * a.vcu_stride;
+    pw_coefs(vu[s], vu[S + s], ete, etm, chi_te, chi_tm, o.u);
+  } else {
+    for (int c = 0; c < 3; ++c) o.u[c] = cd{0.0, 0.0};
+  }
+  return o;
+}
+
+// Points (x[q], y[q], z[q]): every term evaluated directly.
 __global__ void __launch_bounds__(kPwThreads) pw_fields_kernel(PwArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PwOrder *ord = (PwOrder *)smem_raw;
@@ -73,33 +105,7 @@ __global__ void __launch_bounds__(kPwThreads) pw_fields_kernel(PwArgs a) {
   const int S = a.S;
   const cd n = a.n[b];
   const double h = a.height ? a.height[b] : 0.0;
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const int j = a.sort[(size_t)b * S + s];
-    const bool ok = j >= 0 && j < S;  // a sort order that is not a permutation gives NaN fields
-    const double al = ok ? a.alphas[(size_t)b * S + j] : nan(""), be = ok ? a.betas[(size_t)b * S + j] : nan("");
-    const cd g = a.kz[(size_t)b * S + s];
-    const double ab2 = al * al + be * be;
-    const double norm = sqrt(ab2);
-    const cd k = csqrt_p(cd{ab2 + (g.x * g.x - g.y * g.y), 2.0 * g.x * g.y});
-    const cd chi_te = csqrt_p(cdiv(cmul(n, g), k));
-    const cd chi_tm = csqrt_p(cdiv(cmul(n, k), g));
-    const double ete[3] = {be / norm, -al / norm, 0.0};
-    const cd etm[3] = {cd{al / norm, 0.0}, cd{be / norm, 0.0}, cdiv(cd{-norm, 0.0}, g)};
-    PwOrder o;
-    o.a = al;
-    o.b = be;
-    o.gr = g.x;
-    o.gi = g.y;
-    const cd *vd = a.vcd + (size_t)b * a.vcd_stride;
-    pw_coefs(vd[s], vd[S + s], ete, etm, chi_te, chi_tm, o.d);
-    if (a.has_up) {
-      const cd *vu = a.vcu + (size_t)b * a.vcu_stride;
-      pw_coefs(vu[s], vu[S + s], ete, etm, chi_te, chi_tm, o.u);
-    } else {
-      for (int c = 0; c < 3; ++c) o.u[c] = cd{0.0, 0.0};
-    }
-    ord[s] = o;
-  }
+  for (int s = threadIdx.x; s < S; s += blockDim.x) ord[s] = pw_order(a, b, s, n);
   __syncthreads();
 
   cd *E = a.E + (size_t)b * 3 * a.Q;
@@ -139,6 +145,118 @@ __global__ void __launch_bounds__(kPwThreads) pw_fields_kernel(PwArgs a) {
     }
     for (int c = 0; c < 3; ++c) E[(size_t)c * a.Q + q] = e[c];
     if (a.E_abs) a.E_abs[(size_t)b * a.Q + q] = sqrt(cabs2(e[0]) + cabs2(e[1]) + cabs2(e[2]));
+  }
+}
+
+// Grid x[nx] x y[ny] x z[nz]: the exponential of every term factors as
+// exp(i alpha x) exp(i beta y) times a z factor, so per stack three tables
+// are formed once,
+//   X[ix][s] = exp(i alpha_s x_ix),  Y[iy][s] = exp(i beta_s y_iy),
+//   Z[iz][s][c] = eta_down,c exp(-i gamma_s (z1 - h)) + eta_up,c exp(i gamma_s z1),
+// and E_c(ix, iy, iz) = sum_s X Y Z is a contraction with no transcendental
+// function per term.
+constexpr int kZc = 4;   // z values per pass (accumulators in registers)
+__device__ __forceinline__ cd ldg_c(const cd *p) {
+  const double2 v = __ldg((const double2 *)p);
+  return cd{v.x, v.y};
+}
+constexpr int kSc = 64;  // orders per shared-memory stage of Z
+
+__global__ void __launch_bounds__(kPwThreads) pw_tables_kernel(PwArgs a, cd *ws, long long ws_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PwOrder *ord = (PwOrder *)smem_raw;
+  const int b = blockIdx.x;
+  const int S = a.S;
+  const cd n = a.n[b];
+  const double h = a.height ? a.height[b] : 0.0;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) ord[s] = pw_order(a, b, s, n);
+  __syncthreads();
+  cd *X = ws + (size_t)b * ws_stride;
+  cd *Y = X + (size_t)a.nx * S;
+  cd *Z = Y + (size_t)a.ny * S;
+  for (int i = threadIdx.x; i < a.nx * S; i += blockDim.x) {
+    double sn, cs;
+    sincos(ord[i % S].a * a.x[i / S], &sn, &cs);
+    X[i] = cd{cs, sn};
+  }
+  for (int i = threadIdx.x; i < a.ny * S; i += blockDim.x) {
+    double sn, cs;
+    sincos(ord[i % S].b * a.y[i / S], &sn, &cs);
+    Y[i] = cd{cs, sn};
+  }
+  for (int i = threadIdx.x; i < a.nz * S; i += blockDim.x) {
+    const PwOrder &o = ord[i % S];
+    const double z = a.z[i / S];
+    const double z1 = a.substrate ? -z : fabs(z);
+    const double dzd = z1 - h;
+    double sd, cdn;
+    sincos(-o.gr * dzd, &sd, &cdn);
+    const double md = exp(o.gi * dzd);
+    const cd ed{md * cdn, md * sd};
+    cd zc[3];
+    for (int c = 0; c < 3; ++c) zc[c] = cmul(o.d[c], ed);
+    if (a.has_up) {
+      double su, cu;
+      sincos(o.gr * z1, &su, &cu);
+      const double mu = exp(-o.gi * z1);
+      const cd eu{mu * cu, mu * su};
+      for (int c = 0; c < 3; ++c) zc[c] = cadd(zc[c], cmul(o.u[c], eu));
+    }
+    for (int c = 0; c < 3; ++c) Z[(size_t)i * 3 + c] = zc[c];
+  }
+}
+
+__global__ void __launch_bounds__(kPwThreads) pw_grid_kernel(PwArgs a, const cd *ws, long long ws_stride) {
+  __shared__ cd zs[kZc][kSc][3];
+  const int b = blockIdx.y;
+  const int S = a.S, nxy = a.nx * a.ny;
+  const cd *X = ws + (size_t)b * ws_stride;
+  const cd *Y = X + (size_t)a.nx * S;
+  const cd *Z = Y + (size_t)a.ny * S;
+  cd *E = a.E + (size_t)b * 3 * a.Q;
+  for (int t0 = blockIdx.x * blockDim.x; t0 < nxy; t0 += gridDim.x * blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const bool live = t < nxy;
+    const int ix = live ? t / a.ny : 0, iy = live ? t % a.ny : 0;
+    const cd *xr = X + (size_t)ix * S, *yr = Y + (size_t)iy * S;
+    for (int z0 = 0; z0 < a.nz; z0 += kZc) {
+      const int zc = min(kZc, a.nz - z0);
+      cd acc[kZc][3];
+#pragma unroll
+      for (int k = 0; k < kZc; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[k][c] = cd{0.0, 0.0};
+      for (int s0 = 0; s0 < S; s0 += kSc) {
+        const int sc = min(kSc, S - s0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < zc * sc * 3; i += blockDim.x) {
+          const int k = i / (sc * 3), r = i % (sc * 3);
+          zs[k][r / 3][r % 3] = Z[((size_t)(z0 + k) * S + s0 + r / 3) * 3 + r % 3];
+        }
+        __syncthreads();
+        if (live) {
+          for (int s = 0; s < sc; ++s) {
+            const cd xy = cmul(ldg_c(xr + s0 + s), ldg_c(yr + s0 + s));
+#pragma unroll
+            for (int k = 0; k < kZc; ++k)
+              if (k < zc)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc[k][c] = cadd(acc[k][c], cmul(xy, zs[k][s][c]));
+          }
+        }
+      }
+      if (live) {
+#pragma unroll
+        for (int k = 0; k < kZc; ++k) {
+          if (k < zc) {
+            const size_t q = (size_t)t * a.nz + z0 + k;
+            for (int c = 0; c < 3; ++c) E[(size_t)c * a.Q + q] = acc[k][c];
+            if (a.E_abs)
+              a.E_abs[(size_t)b * a.Q + q] = sqrt(cabs2(acc[k][0]) + cabs2(acc[k][1]) + cabs2(acc[k][2]));
+          }
+        }
+      }
+    }
   }
 }
 
@@ -194,6 +312,17 @@ __global__ void __launch_bounds__(kBlochThreads) bloch_plane_kernel(BlochArgs a)
 
 }  // namespace
 
+namespace {
+long long pw_ws_stride(const EmuPwFields *p) {
+  return ((long long)p->nx + p->ny + 3LL * p->nz) * p->n_pw;  // complex values per stack
+}
+}  // namespace
+
+extern "C" size_t emu_pw_fields_workspace_size(const EmuPwFields *p) {
+  if (!p || !p->grid || p->n_stacks <= 0 || p->n_pw < 1 || p->nx < 0 || p->ny < 0 || p->nz < 0) return 0;
+  return (size_t)p->n_stacks * (size_t)pw_ws_stride(p) * sizeof(cd);
+}
+
 extern "C" int emu_pw_fields(const EmuPwFields *p, void *stream) {
   if (!p || p->n_stacks < 0 || p->n_pw < 1 || p->n_pw > kPwMaxOrders) return EMU_E_ARG;
   if (p->nx < 0 || (p->grid && (p->ny < 0 || p->nz < 0))) return EMU_E_ARG;
@@ -231,6 +360,26 @@ extern "C" int emu_pw_fields(const EmuPwFields *p, void *stream) {
   a.E = (cd *)p->d_E;
   a.E_abs = p->d_E_abs;
   const size_t smem = sizeof(PwOrder) * (size_t)p->n_pw;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->grid) {
+    const size_t need = emu_pw_fields_workspace_size(p);
+    if (!p->d_workspace || p->workspace_bytes < need) return EMU_E_WORKSPACE;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(pw_tables_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+      return EMU_E_CUDA;
+    cd *ws = (cd *)p->d_workspace;
+    const long long stride = pw_ws_stride(p);
+    pw_tables_kernel<<<(unsigned)p->n_stacks, kPwThreads, smem, st>>>(a, ws, stride);
+    emu::note_launch();
+    long long tiles = ((long long)p->nx * p->ny + kPwThreads - 1) / kPwThreads;
+    long long want = (8LL * emu::sm_count() + p->n_stacks - 1) / p->n_stacks;
+    if (want < 1) want = 1;
+    if (tiles > want) tiles = want;
+    pw_grid_kernel<<<dim3((unsigned)tiles, (unsigned)p->n_stacks), kPwThreads, 0, st>>>(a, ws, stride);
+    emu::note_launch();
+    return emu::check_launch();
+  }
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(pw_fields_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess)
@@ -241,7 +390,7 @@ extern "C" int emu_pw_fields(const EmuPwFields *p, void *stream) {
   long long want = (4LL * emu::sm_count() + p->n_stacks - 1) / p->n_stacks;
   if (want < 1) want = 1;
   if (tiles > want) tiles = want;
-  pw_fields_kernel<<<dim3((unsigned)tiles, (unsigned)p->n_stacks), kPwThreads, smem, (cudaStream_t)stream>>>(a);
+  pw_fields_kernel<<<dim3((unsigned)tiles, (unsigned)p->n_stacks), kPwThreads, smem, st>>>(a);
   emu::note_launch();
   return emu::check_launch();
 }

@@ -93,6 +93,11 @@ def pw_fields(alphas, betas, sort_order, kz, n, vec_coef_down, vec_coef_up, x, y
     d.d_vec_coef_up, d.vcu_stride = ptr(vcu), 2 * S
     d.d_x, d.d_y, d.d_z = ptr(x), ptr(y), ptr(z)
     d.d_E, d.d_E_abs = ptr(E), ptr(Eabs)
+    ws = None
+    nbytes = lib().emu_pw_fields_workspace_size(C.byref(d))
+    if nbytes:
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        d.d_workspace, d.workspace_bytes = ptr(ws), nbytes
     check(lib().emu_pw_fields(C.byref(d), stream_ptr(stream)), 'emu_pw_fields')
     return E, Eabs
 

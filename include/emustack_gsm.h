@@ -231,6 +231,10 @@ int emu_material_n_batch(const EmuMaterial *h_materials, int n_layers, int n_poi
  * down-going term as exp(-i gamma (z - h)), a semi-infinite layer's as
  * h = 0.  E[b] holds E_x, E_y, E_z, each over the Q points (grid: Q =
  * nx ny nz in [x][y][z] order, the reference's E_x_array[x, y, z]).
+ * On a grid the exponentials factor into per-axis tables (x, y and z
+ * factors of every order, in the workspace: B (nx + ny + 3 nz) Npw complex
+ * values; EMU_E_WORKSPACE when it is missing or short) and the sum over
+ * orders is a contraction; points are evaluated term by term.
  * At most 1536 orders per polarisation. */
 typedef struct {
   int n_stacks;            /* B                                               */
@@ -250,7 +254,10 @@ typedef struct {
   const double *d_x, *d_y, *d_z;   /* units of the period                     */
   emu_c128 *d_E;           /* [B][3][Q]                                       */
   double *d_E_abs;         /* [B][Q] |E|, or NULL                             */
+  void *d_workspace;       /* grid: emu_pw_fields_workspace_size bytes        */
+  size_t workspace_bytes;
 } EmuPwFields;
+size_t emu_pw_fields_workspace_size(const EmuPwFields *p);
 int emu_pw_fields(const EmuPwFields *p, void *stream);
 
 /* emu_bloch_fields_plane: E at the six P2 nodes of every element of a 2D

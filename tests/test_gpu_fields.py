@@ -214,3 +214,39 @@ def test_bloch_plane_refuses_a_plane_outside_the_layer():
     d = _lib.EmuBlochFieldsPlane()
     d.n_stacks, d.n_modes, d.n_elements, d.h, d.hz = 1, 3, 4, 0.5, -0.1
     assert _lib.lib().emu_bloch_fields_plane(C.byref(d), None) == 1   # EMU_E_ARG before any launch
+
+
+@pytest.mark.parametrize('nz,substrate', [(1, False), (5, False), (9, True)])
+def test_grid_tables_match_the_term_by_term_points(nz, substrate):
+    """The grid path (per-axis exponential tables and a contraction over
+    orders, z in passes of 4, orders in stages of 64) equals the term-by-term
+    point evaluation of the same grid."""
+    from emustack_b200.fields import pw_fields
+    from emustack_b200.films import grating_orders
+    rng = np.random.default_rng(nz)
+    B, mo = 3, 6
+    px, py = grating_orders(mo, 500.0, 500.0, False)
+    S = len(px)
+    assert S > 64
+    k0 = 2 * np.pi / rng.uniform(0.8, 2.0, B)
+    alphas = rng.uniform(-0.3, 0.3, (B, 1)) + 2 * np.pi * px[None]
+    betas = rng.uniform(-0.3, 0.3, (B, 1)) + 2 * np.pi * py[None]
+    n = rng.uniform(1.2, 3.0, B) + 1j * rng.uniform(0, 0.2, B)
+    kz = np.sqrt(((n * k0)[:, None] ** 2 - alphas ** 2 - betas ** 2).astype(complex))
+    sort = np.argsort(-kz.real + kz.imag, axis=1, kind='stable').astype(np.int32)
+    kz = np.take_along_axis(kz, sort, 1)
+    vcd = rng.normal(size=(B, 2 * S)) + 1j * rng.normal(size=(B, 2 * S))
+    vcu = rng.normal(size=(B, 2 * S)) + 1j * rng.normal(size=(B, 2 * S))
+    h = rng.uniform(0.1, 0.4, B)
+    xs, ys = np.linspace(0, 1, 7), np.linspace(0, 1, 6)
+    zs = np.linspace(0, 0.1, nz)
+    args = dict(alphas=alphas, betas=betas, sort_order=sort, kz=kz, n=n, vec_coef_down=vcd,
+                vec_coef_up=vcu, height_norm=None if substrate else h, substrate=substrate)
+    G, Gabs = pw_fields(x=xs, y=ys, z=zs, grid=True, **args)
+    pts = np.array([(x, y, z) for x in xs for y in ys for z in zs])
+    P, Pabs = pw_fields(x=pts[:, 0], y=pts[:, 1], z=pts[:, 2], grid=False, **args)
+    G, P = G.cpu().numpy(), P.cpu().numpy()
+    for b in range(B):
+        scale = np.abs(P[b]).max()
+        np.testing.assert_allclose(G[b], P[b], rtol=0, atol=1e-13 * scale)
+    np.testing.assert_allclose(Gabs.cpu().numpy(), Pabs.cpu().numpy(), rtol=1e-12, atol=1e-13 * np.abs(P).max())
