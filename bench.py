@@ -657,20 +657,73 @@ def config1_chain(dev, batch=50, steps=10):
                         'interfaces/cascade; plain = one wavelength per call, FP64, eager' % batch}
 
 
-def serving_run(rate, seconds=1.0, seed=0):
-    """Open-loop Poisson arrivals of uneven film requests at `rate` per
-    second through the continuous-batching server (GsmServer); latency from
-    each request's scheduled arrival to its result on the host."""
+def array_pool(n_points, seed=0, period=500.0):
+    """Spectral points with two synthetic nanostructured-array layers each
+    (ArrayLayer: Bloch k_z and J / J_dag made on the device): P = 2 Npw
+    log-uniform in [50, 900] (nearest order set), M = P + 20, wavelength
+    U(350, 1100) nm, theta U(0, 60), phi U(0, 90) degrees."""
+    import torch
+    from emustack_b200.array_serving import ArrayLayer
+    rng = np.random.default_rng(seed)
+    tab = order_table(period)
+    g = torch.Generator(device='cuda').manual_seed(seed)
+    pool = []
+    for _ in range(n_points):
+        mo = int(np.argmin(np.abs(tab - float(np.exp(rng.uniform(np.log(50), np.log(900)))) / 2)))
+        P = 2 * int(tab[mo])
+        M = P + 20
+        wl = float(rng.uniform(350, 1100))
+        th, ph = np.radians(rng.uniform(0, 60)), np.radians(rng.uniform(0, 90))
+        k = 2 * np.pi / wl
+        kp = np.array([k * np.sin(th) * np.cos(ph), k * np.sin(th) * np.sin(ph)])
+        k0 = 2 * np.pi / (wl / period)
+        cr = lambda *sh: torch.complex(torch.randn(sh, dtype=torch.float64, device='cuda', generator=g),
+                                       torch.randn(sh, dtype=torch.float64, device='cuda', generator=g))
+        lays = [ArrayLayer(rng.uniform(0, 2, M) * k0 + 1j * rng.uniform(0, 0.1, M) * k0,
+                           J=cr(P, M) / np.sqrt(P), J_dag=cr(M, P) / np.sqrt(P)) for _ in range(2)]
+        pool.append((mo, wl, kp, lays))
+    return pool
+
+
+def mixed_requests(n, seed, array_frac=0.0, pool=None, period=500.0):
+    """n requests in random order: film requests (film_requests) and a
+    fraction array_frac of array stacks (film substrate, 2-12 finite layers
+    each a film or one of the two array layers of a pool point, air), so
+    that requests share layers and the server's interface cache is used."""
+    from emustack_b200.array_serving import ArrayRequest
+    na = int(round(n * array_frac)) if pool else 0
+    reqs = film_requests(n - na, seed, period)
+    rng = np.random.default_rng(seed + 7)
+    pols = ('TE', 'TM', 'un', 'R Circ')
+    for i in range(na):
+        mo, wl, kp, lays = pool[int(rng.integers(len(pool)))]
+        K = int(rng.integers(2, 13))
+        mid = [lays[int(rng.integers(2))] if rng.random() < 0.5
+               else complex(rng.uniform(1.3, 4.0), rng.uniform(0, 0.5)) for _ in range(K)]
+        reqs.append(ArrayRequest([1.46 + 0j] + mid + [1.0 + 0j], rng.uniform(20, 300, K), wl, kp, period, mo,
+                                 pol=pols[i % 4]))
+    order = np.random.default_rng(seed + 3).permutation(len(reqs))
+    return [reqs[i] for i in order]
+
+
+def serving_run(rate, seconds=1.0, seed=0, array_frac=0.0, pool=None, n_streams=2):
+    """Open-loop Poisson arrivals of uneven requests at `rate` per second
+    through the continuous-batching server (GsmServer); latency from each
+    request's scheduled arrival to its result on the host.  array_frac > 0
+    mixes in array-stack requests built on the layers of `pool`."""
     from emustack_b200.serving import GsmServer
     n = max(int(rate * seconds), 200)
-    reqs = film_requests(n, seed)
+    reqs = mixed_requests(n, seed, array_frac, pool)
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, n)
-    srv = GsmServer(max_batch=32768, batching='mixed', n_streams=2).start()
-    warm = film_requests(max(64, min(32768, int(rate * 0.2))), seed + 2)
+    srv = GsmServer(max_batch=32768, batching='mixed', n_streams=n_streams).start()
+    warm = mixed_requests(max(64, min(32768, int(rate * 0.2))), seed + 2, array_frac, pool)
     for _ in range(2):
         for f in [srv.submit(r) for r in warm]:
             f.result(timeout=300)
     srv.latencies.clear()
+    srv.array_latencies.clear()
+    c = srv.cache
+    c.hits = c.misses = c.evictions = 0
     srv.batch_sizes.clear()
     srv.n_batches = 0
     srv.t_first = srv.t_last = None
@@ -701,12 +754,20 @@ def serving_run(rate, seconds=1.0, seed=0):
         gc.enable()
     srv.stop()
     st = srv.stats()
-    return {'offered_per_s': rate, 'requests': n, 'achieved_per_s': st['throughput_per_s'],
-            'p50_ms': st['p50_ms'], 'p99_ms': st['p99_ms'], 'batches': st['batches'],
-            'mean_batch': st['mean_batch'],
-            'workload': 'config 5: Poisson arrivals of uneven all-film solves (P log-uniform 50-900, '
-                        '2-12 layers, mixed polarisations) through GsmServer (host scheduling thread, '
-                        'continuous batching on 2 streams); latency from scheduled arrival to host result'}
+    out = {'offered_per_s': rate, 'requests': n, 'achieved_per_s': st['throughput_per_s'],
+           'p50_ms': st['p50_ms'], 'p99_ms': st['p99_ms'], 'batches': st['batches'],
+           'mean_batch': st['mean_batch'], 'streams': n_streams,
+           'workload': 'config 5: Poisson arrivals of uneven all-film solves (P log-uniform 50-900, '
+                       '2-12 layers, mixed polarisations) through GsmServer (host scheduling thread, '
+                       'continuous batching); latency from scheduled arrival to host result'}
+    if array_frac:
+        cs = st['smatrix_cache']
+        out.update(array_frac=array_frac, array_requests=st['array_requests'],
+                   array_p50_ms=st['array_p50_ms'], array_p99_ms=st['array_p99_ms'],
+                   cache_hits=cs['hits'], cache_misses=cs['misses'],
+                   workload=out['workload'] + '; a fraction array_frac are array stacks (P 50-900, M = P + 20, '
+                   'layers shared across requests through the device interface cache)')
+    return out
 
 
 def ring_serving_run(rate, seconds=1.0, seed=0):
@@ -997,6 +1058,10 @@ def main():
                 print(json.dumps(dict(serving_run(r, 2.0), config=5)), flush=True)
             for r in (1000.0, 10000.0, 50000.0, 100000.0):
                 print(json.dumps(dict(ring_serving_run(r, 2.0), config=5)), flush=True)
+            pool = array_pool(32, seed=11)
+            for r, frac in ((10000.0, 0.01), (150.0, 0.5)):
+                print(json.dumps(dict(serving_run(r, 2.0, array_frac=frac, pool=pool, n_streams=4), config=5)),
+                      flush=True)
         return
 
     # CPU baseline first, in spawned workers, before any GPU work

@@ -539,7 +539,7 @@ class DeviceFilmServer(object):
         check(self._L.emu_film_ring_create(int(capacity), float(idle_seconds), C.byref(h)),
               'emu_film_ring_create')
         self._h = h
-        self._pending = {}
+        self._pending = collections.OrderedDict()   # ticket -> shape, oldest first
         self._early = {}
         self._orders = {}
 
@@ -616,7 +616,7 @@ class DeviceFilmServer(object):
     def _drain_one(self):
         """Read the oldest pending result (it frees its slot); poll, wait
         and take return it later."""
-        t = min(self._pending)
+        t = next(iter(self._pending))               # tickets increase: the oldest, O(1)
         self._early[t] = self._read(t, 60.0)
 
     def take(self, ticket):
