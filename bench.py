@@ -819,6 +819,36 @@ def ring_serving_run(rate, seconds=1.0, seed=0):
                         'scheduled arrival to the host seeing the result'}
 
 
+def ring_capacity(n=8000, seed=0):
+    """The device-resident loop apart from the client's pace: n requests
+    submitted back to back, then the time until the last is solved (read
+    without reading the others) and the host cost per submit and per read."""
+    from emustack_b200 import _lib
+    from emustack_b200.serving import DeviceFilmServer
+    reqs = [r for r in film_requests(n, seed) if len(r.n) <= _lib.RING_MAX_LAYERS and r.npw <= _lib.RING_MAX_PW]
+    srv = DeviceFilmServer(capacity=max(8192, len(reqs) + 1), idle_seconds=2.0)
+    try:
+        for r in film_requests(256, seed + 2):
+            srv.take(srv.submit(r))
+        L = _lib.lib()
+        t0 = time.perf_counter()
+        tickets = [srv.submit(r) for r in reqs]
+        t1 = time.perf_counter()
+        while L.emu_film_ring_ready(srv._h, tickets[-1]) != 1:
+            pass
+        t2 = time.perf_counter()
+        for t in tickets:
+            srv.take(t)
+        t3 = time.perf_counter()
+        srv.stop()
+    finally:
+        srv.close()
+    m = len(reqs)
+    return {'requests': m, 'submit_us': (t1 - t0) / m * 1e6, 'read_us': (t3 - t2) / m * 1e6,
+            'solved_after_last_submit_ms': (t2 - t1) * 1e3, 'device_rate_at_least_per_s': m / (t2 - t0),
+            'workload': 'config 5 requests submitted back to back to the device-resident loop'}
+
+
 def north_star_extras(dev, w, solver, value):
     """The batched / mixed-precision GSM against the plain FP64 GPU GSM, and a
     short serving run (bounded work: about half a minute)."""
@@ -1058,6 +1088,7 @@ def main():
                 print(json.dumps(dict(serving_run(r, 2.0), config=5)), flush=True)
             for r in (1000.0, 10000.0, 50000.0, 100000.0):
                 print(json.dumps(dict(ring_serving_run(r, 2.0), config=5)), flush=True)
+            print(json.dumps(dict(ring_capacity(), config=5)), flush=True)
             pool = array_pool(32, seed=11)
             for r, frac in ((10000.0, 0.01), (150.0, 0.5)):
                 print(json.dumps(dict(serving_run(r, 2.0, array_frac=frac, pool=pool, n_streams=4), config=5)),

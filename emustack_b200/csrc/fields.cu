@@ -235,7 +235,6 @@ __global__ void __launch_bounds__(kPwThreads) pw_grid_kernel(PwArgs a, const cd 
         }
         __syncthreads();
         if (live) {
-#pragma unroll 4
           for (int s = 0; s < sc; ++s) {
             const cd xy = cmul(ldg_c(xr + s0 + s), ldg_c(yr + s0 + s));
 #pragma unroll
