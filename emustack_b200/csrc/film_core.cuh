@@ -262,8 +262,9 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
       const cd rq = sh ? cmul(cmul(Qi, rnet[q]), Q) : rnet[q];
       const cd u = csub(s, cmul(d, rq));
       const cd v = csub(cmul(s, rq), d);
-      const cd Dn = cadd(cmul(s, u), cmul(cmul(d, pr2), v));
-      const cd Nn = cadd(cmul(d, u), cmul(cmul(s, pr2), v));
+      const cd w = cmul(pr2, v);
+      const cd Dn = cadd(cmul(s, u), cmul(d, w));
+      const cd Nn = cadd(cmul(d, u), cmul(s, w));
       const cd iD = crcp_nr(Dn);
       const cd g = cmul(cscale(cmul(cmul(A, Bz), pr), 4.0), iD);  // x1 p x2
       tnet[q] = cmul(sh ? cmul(tnet[q], Q) : tnet[q], g);
@@ -323,6 +324,18 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
   const bool prop = j < np_air;
   double in_sum = 0.0, up_sum = 0.0, out_sum = 0.0;
   for (int q = 0; q < 2; ++q) {
+    // a polarisation without incident light (TE or TM incidence) carries
+    // zero amplitudes through every layer and adds nothing to the fluxes,
+    // unless its saved scalars are not finite (0 times them is NaN, as in
+    // the reference's dense products): then it runs like the other
+    if (!want_vec && cis_zero(din[q])) {
+      double chk = 0.0;
+      for (int k = 0; k < L; ++k) {
+        const cd *sk = wsv + ((size_t)k * 2 + q) * kSave;
+        chk += sk[0].x + sk[0].y + sk[1].x + sk[1].y + sk[4].x + sk[4].y;
+      }
+      if (isfinite(chk)) continue;
+    }
     const int pos = j + q * npw;
     const cd *top = wsv + ((size_t)(L - 1) * 2 + q) * kSave;
     const cd dp = cmul(top[1], din[q]);  // d_plus = r_top d

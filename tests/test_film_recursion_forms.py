@@ -61,8 +61,9 @@ def kernel_form(ns, heights_nm, wl_nm, k_pll, period, max_order):
         p = np.exp(1j * kz * heights_nm[l - 1] / period)
         u = s_ - d_ * rnet
         v = s_ * rnet - d_
-        D = s_ * u + d_ * p * p * v
-        N = d_ * u + s_ * p * p * v
+        w = p * p * v
+        D = s_ * u + d_ * w
+        N = d_ * u + s_ * w
         g = 4 * A * B * p / D
         g_list.append(g)
         tnet = tnet * g
