@@ -353,8 +353,13 @@ __device__ __forceinline__ void solve_order(const Pt &p, int u, int j, int spec,
       const cd *s = wsv + ((size_t)k * 2 + q) * kSave;
       const cd f1p = cmul(s[4], f1m);
       const cd fl = flux_term(f1m, f1p, prop, q == 1);
-      atomicAdd(&acc[1 + i].x, fl.x);
-      atomicAdd(&acc[1 + i].y, fl.y);
+      if (p.slot_per_order()) {  // several orders carry light: they add concurrently
+        atomicAdd(&acc[1 + i].x, fl.x);
+        atomicAdd(&acc[1 + i].y, fl.y);
+      } else {                   // the one order that carries light adds alone
+        acc[1 + i].x += fl.x;
+        acc[1 + i].y += fl.y;
+      }
       if (want_vec) {
         const cd f2m = cmul(s[3], f1m);
         const cd f2p = cmul(cmul(s[1], s[2]), f2m);
