@@ -32,6 +32,9 @@ class Light(object):
             raise ValueError("Specify incident angle either by \n k_parallel OR by theta, phi and n_inc.")
         if theta is None:
             self.k_pll = np.array(k_parallel, dtype='float64')
+            if np.abs(self.k_pll[0]) == 0 or np.abs(self.k_pll[1]) == 0:
+                print("Warning: a component of k_parallel is exactly zero, \n"
+                      "this can lead to degeneracies and errors.")
         else:
             if k_parallel is not None or phi is None:
                 raise ValueError("Specify incident angle either by \n k_parallel OR by theta, phi and n_inc.")
