@@ -235,8 +235,14 @@ __global__ void __launch_bounds__(kPwThreads) pw_grid_kernel(PwArgs a, const cd 
         }
         __syncthreads();
         if (live) {
+          // the next order's table entries are loaded while this one is summed
+          cd xn = ldg_c(xr + s0), yn = ldg_c(yr + s0);
           for (int s = 0; s < sc; ++s) {
-            const cd xy = cmul(ldg_c(xr + s0 + s), ldg_c(yr + s0 + s));
+            const cd xy = cmul(xn, yn);
+            if (s + 1 < sc) {
+              xn = ldg_c(xr + s0 + s + 1);
+              yn = ldg_c(yr + s0 + s + 1);
+            }
 #pragma unroll
             for (int k = 0; k < kZc; ++k)
               if (k < zc)
