@@ -928,13 +928,17 @@ def config3_line(steps):
     bloch = torch.tensor([[1e-6, 1e-13]], dtype=torch.float64, device=dev)
     k0 = torch.tensor([2 * np.pi / (650.0 / period)], dtype=torch.float64, device=dev)
     ms_j = _timed(lambda: overlap_batch(dm, px, py, mo, bloch, k0, s1, s2, precision='tf32x3'), steps)
+    s1, s2 = s1.to(torch.complex128), s2.to(torch.complex128)
+    ms_j64 = _timed(lambda: overlap_batch(dm, px, py, mo, bloch, k0, s1, s2, precision='fp64'), max(1, steps // 2),
+                    warmup=1)
     del s1, s2
     torch.cuda.empty_cache()
     specs = [dict(mo=mo, npw=len(px), K=4, M=M, wl=float(w), seed=i)
              for i, w in enumerate(np.linspace(400, 900, 148))]
     ms_gsm = time_array_stacks(specs, group=True, n_streams=1)
     return {'config': 3, 'P': 2 * len(px), 'M': M, 'nel': mesh.nel,
-            'J_pair_ms_per_layer': ms_j, 'interfaces_cascade_ms_per_wavelength': ms_gsm / 148,
+            'J_pair_ms_per_layer': ms_j, 'J_pair_fp64_ms_per_layer': ms_j64,
+            'interfaces_cascade_ms_per_wavelength': ms_gsm / 148,
             'ms_per_wavelength': 4 * ms_j + ms_gsm / 148}
 
 

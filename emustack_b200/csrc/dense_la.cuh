@@ -41,13 +41,14 @@ __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, doubl
 
 // One 64x64 tile of C = alpha * A(m x k) * B(k x n) + beta * C, tile origin
 // (r0, c0).  If dA / dB are non-null the rows of A / the rows of B are
-// first multiplied by dA[i] / dB[kk] (diagonal factors).  All kDLThreads
+// first multiplied by dA[i] / dB[kk] (diagonal factors); conjA conjugates A's
+// elements as they are read.  All kDLThreads
 // threads of the CTA must call it.  The product runs on the FP64 tensor
 // cores: 8 warps in a 2 x 4 grid, each owning a 32 x 32 block of the real
 // 64 x 128 result (4 x 4 fragments of 8 x 8).
 static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A, int lda, const cd *B,
                               int ldb, cd beta, cd *C, int ldc_, int r0, int c0, GemmSmem &sm,
-                              const cd *dA_col = nullptr, const cd *dB_row = nullptr) {
+                              const cd *dA_col = nullptr, const cd *dB_row = nullptr, bool conjA = false) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
@@ -67,6 +68,7 @@ static __device__ void cta_gemm_tile(int m, int n, int k, cd alpha, const cd *A,
       cd v = cd{0.0, 0.0};
       if (gr < m && gc < k) {
         v = A[(size_t)gr * lda + gc];
+        if (conjA) v.y = -v.y;
         if (dA_col) v = cmul(v, dA_col[gc]);
       }
       va[h] = v;

@@ -372,76 +372,17 @@ struct OvGemm {
   int kchunk;
 };
 
-// Shared tiles of ov_gemm_kernel (complex, k-major).
-struct OvGemmSmem {
-  cd As[kTK][kTM];
-  cd Bs[kTK][kTN];
-};
-
-__global__ void __launch_bounds__(kDLThreads) ov_gemm_kernel(OvGemm g) {
-  __shared__ OvGemmSmem sm;
+// The contraction on the FP64 tensor cores: one 64 x 64 complex tile of
+// G_part[c] per CTA through cta_gemm_tile (mma.sync m8n8k4 f64).
+__global__ void __launch_bounds__(kDLThreads) ov_gemm_tc_kernel(OvGemm g) {
+  __shared__ GemmSmem sm;
   const int c = blockIdx.z;
   const int k0 = c * g.kchunk;
   const int kk = min(g.kchunk, g.k - k0);
   if (kk <= 0) return;
-  const int r0 = blockIdx.y * kTM, c0 = blockIdx.x * kTN;
-  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-  cd acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = cd{0.0, 0.0};
-  const cd *A = g.E + k0;
-  const cd *B = g.S + (size_t)k0 * g.n;
-  for (int kb = 0; kb < kk; kb += kTK) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = tid / 8 + 32 * h, cc = tid % 8;
-      const int gr = r0 + r, gc = kb + cc;
-      cd v = cd{0.0, 0.0};
-      if (gr < g.m && gc < kk) {
-        v = A[(size_t)gr * g.ldE + gc];
-        if (g.conjA) v.y = -v.y;
-      }
-      sm.As[cc][r] = v;
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = tid / 64 + 4 * h, cc = tid % 64;
-      const int gr = kb + r, gc = c0 + cc;
-      sm.Bs[r][cc] = (gr < kk && gc < g.n) ? B[(size_t)gr * g.n + gc] : cd{0.0, 0.0};
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kTK; ++q) {
-      cd a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sm.As[q][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = sm.Bs[q][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
-          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
-          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
-          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
-        }
-    }
-    __syncthreads();
-  }
-  cd *G = g.G + (size_t)c * g.sG;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int gr = r0 + ty + 16 * i;
-    if (gr >= g.m) continue;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int gc = c0 + tx + 16 * j;
-      if (gc < g.n) G[(size_t)gr * g.n + gc] = acc[i][j];
-    }
-  }
+  cta_gemm_tile(g.m, g.n, kk, cd{1.0, 0.0}, g.E + k0, (int)g.ldE, g.S + (size_t)k0 * g.n, g.n, cd{0.0, 0.0},
+                g.G + (size_t)c * g.sG, g.n, blockIdx.y * kTM, blockIdx.x * kTN, sm, nullptr, nullptr,
+                g.conjA != 0);
 }
 
 // Sum the chunk partials into the accumulator (fixed order: deterministic).
@@ -1071,7 +1012,7 @@ extern "C" int emu_overlap_batch(const EmuOverlap *p, void *d_workspace, size_t 
         g.kchunk = (int)(((6 * ne + nparts - 1) / nparts + kTK - 1) / kTK * kTK);
         const int used = (g.k + g.kchunk - 1) / g.kchunk;
         dim3 grid((2 * M + kTN - 1) / kTN, (npw + kTM - 1) / kTM, used);
-        ov_gemm_kernel<<<grid, kDLThreads, 0, s>>>(g);
+        ov_gemm_tc_kernel<<<grid, kDLThreads, 0, s>>>(g);
         const long long rgs = (gsz + 255) / 256;
         reduce_parts_kernel<<<(int)(rgs < 8 * sms ? rgs : 8 * sms), 256, 0, s>>>(parts, used, gsz, acc, gsz,
                                                                                   first);
