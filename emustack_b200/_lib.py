@@ -341,6 +341,8 @@ EXTRA_SIGNATURES.extend([
     ('emu_film_ring_create', C.c_int, [C.c_int, C.c_double, C.POINTER(vp)]),
     ('emu_film_ring_submit', C.c_int, [vp, C.POINTER(EmuFilmRingRequest), C.POINTER(C.c_longlong)]),
     ('emu_film_ring_poll', C.c_int, [vp, C.c_longlong, C.POINTER(EmuFilmRingResult)]),
+    ('emu_film_ring_submit_many', C.c_int, [vp, vp, C.c_int, vp, C.POINTER(C.c_int)]),
+    ('emu_film_ring_poll_many', C.c_int, [vp, vp, C.c_int, vp, vp]),
     ('emu_film_ring_wait', C.c_int, [vp, C.c_longlong, C.c_double, C.POINTER(EmuFilmRingResult)]),
     ('emu_film_ring_ready', C.c_int, [vp, C.c_longlong]),
     ('emu_film_ring_running', C.c_int, [vp]),

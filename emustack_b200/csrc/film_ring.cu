@@ -432,15 +432,20 @@ extern "C" int emu_film_ring_running(EmuFilmRing *r) {
   return (r->launched && cudaStreamQuery(r->stream) == cudaErrorNotReady) ? 1 : 0;
 }
 
-extern "C" int emu_film_ring_submit(EmuFilmRing *r, const EmuFilmRingRequest *q, long long *ticket) {
-  if (!r || !q || !ticket) return EMU_E_ARG;
+namespace {
+int request_check(const EmuFilmRingRequest *q) {
   if (q->n_layers < 2 || q->n_layers > kRingL || q->n_pw < 1 || q->n_pw > kRingNpw) return EMU_E_SHAPE;
   if (q->pol < EMU_POL_TE || q->pol > EMU_POL_LCIRC || !(q->period > 0) || !(q->period_y > 0) ||
       !(q->wl_nm > 0) || !q->h_px || !q->h_py || !q->h_n || (q->n_layers > 2 && !q->h_heights_nm))
     return EMU_E_ARG;
-  std::lock_guard<std::mutex> lock(r->mu);
+  return EMU_OK;
+}
+
+// Write request q into the next ticket's slot; false when the ring is full.
+// Caller holds r->mu and publishes the tail afterwards.
+bool slot_write(EmuFilmRing *r, const EmuFilmRingRequest *q, long long *ticket) {
   const long long t = r->next;
-  if (r->consumed[(size_t)(t % r->cap)] != t - r->cap) return EMU_E_WORKSPACE;  // ring full
+  if (r->consumed[(size_t)(t % r->cap)] != t - r->cap) return false;
   unsigned char *s = r->slot(t);
   SlotHdr h{};
   h.n_layers = q->n_layers;
@@ -457,10 +462,42 @@ extern "C" int emu_film_ring_submit(EmuFilmRing *r, const EmuFilmRingRequest *q,
   std::memcpy(s + kOffPy, q->h_py, 4 * (size_t)q->n_pw);
   std::memcpy(s + kOffN, q->h_n, 16 * (size_t)q->n_layers);
   if (q->n_layers > 2) std::memcpy(s + kOffH, q->h_heights_nm, 8 * (size_t)(q->n_layers - 2));
-  std::atomic_thread_fence(std::memory_order_release);
-  *(volatile int64_t *)&r->ctl()->tail = t + 1;
   r->next = t + 1;
   *ticket = t;
+  return true;
+}
+
+void publish_tail(EmuFilmRing *r) {
+  std::atomic_thread_fence(std::memory_order_release);
+  *(volatile int64_t *)&r->ctl()->tail = r->next;
+}
+}  // namespace
+
+extern "C" int emu_film_ring_submit(EmuFilmRing *r, const EmuFilmRingRequest *q, long long *ticket) {
+  if (!r || !q || !ticket) return EMU_E_ARG;
+  const int st = request_check(q);
+  if (st != EMU_OK) return st;
+  std::lock_guard<std::mutex> lock(r->mu);
+  if (!slot_write(r, q, ticket)) return EMU_E_WORKSPACE;  // ring full
+  publish_tail(r);
+  return ring_ensure_running(r);
+}
+
+extern "C" int emu_film_ring_submit_many(EmuFilmRing *r, const EmuFilmRingRequest *q, int n, long long *tickets,
+                                         int *n_submitted) {
+  if (!r || n < 0 || (n > 0 && (!q || !tickets)) || !n_submitted) return EMU_E_ARG;
+  *n_submitted = 0;
+  for (int i = 0; i < n; ++i) {
+    const int st = request_check(q + i);
+    if (st != EMU_OK) return st;
+  }
+  if (n == 0) return EMU_OK;
+  std::lock_guard<std::mutex> lock(r->mu);
+  int k = 0;
+  while (k < n && slot_write(r, q + k, tickets + k)) ++k;
+  *n_submitted = k;
+  if (k == 0) return EMU_E_WORKSPACE;  // ring full
+  publish_tail(r);
   return ring_ensure_running(r);
 }
 
@@ -490,10 +527,9 @@ extern "C" int emu_film_ring_ready(EmuFilmRing *r, long long ticket) {
 }
 
 extern "C" int emu_film_ring_poll(EmuFilmRing *r, long long ticket, EmuFilmRingResult *out) {
-  if (!r || ticket < 0) return EMU_E_ARG;
+  if (!r || ticket < 0) return -EMU_E_ARG;
   std::lock_guard<std::mutex> lock(r->mu);
   const int ready = ring_ready(r, ticket);
-  if (ready == -EMU_E_ARG) return EMU_E_ARG;
   if (ready != 1) return ready;
   unsigned char *s = r->slot(ticket);
   std::atomic_thread_fence(std::memory_order_acquire);
@@ -509,6 +545,19 @@ extern "C" int emu_film_ring_poll(EmuFilmRing *r, long long ticket, EmuFilmRingR
   }
   r->consumed[(size_t)(ticket % r->cap)] = ticket;
   return 1;
+}
+
+extern "C" int emu_film_ring_poll_many(EmuFilmRing *r, const long long *tickets, int n,
+                                       const EmuFilmRingResult *outs, int32_t *done) {
+  if (!r || n < 0 || (n > 0 && (!tickets || !outs || !done))) return -EMU_E_ARG;
+  int count = 0;
+  for (int i = 0; i < n; ++i) {
+    const int st = emu_film_ring_poll(r, tickets[i], const_cast<EmuFilmRingResult *>(outs + i));
+    if (st < 0) return st;
+    done[i] = st == 1 ? 1 : 0;
+    count += done[i];
+  }
+  return count;
 }
 
 extern "C" int emu_film_ring_wait(EmuFilmRing *r, long long ticket, double timeout_s, EmuFilmRingResult *out) {

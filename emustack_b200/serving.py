@@ -519,6 +519,7 @@ class GsmServer(object):
 
 
 class DeviceFilmServer(object):
+
     """All-film solves served by a device-resident request loop
     (emu_film_ring_*): a persistent kernel picks requests up from a ring in
     pinned host memory as they are submitted, one warp per request, and
@@ -533,13 +534,16 @@ class DeviceFilmServer(object):
     wait(ticket) blocks (outside the interpreter lock) until done.  While the
     loop runs it holds every SM of the device."""
 
+    _REQ = None   # numpy layouts of EmuFilmRingRequest / EmuFilmRingResult
+    _RES = None
+
     def __init__(self, capacity=4096, idle_seconds=1.0):
         self._L = _lib.lib()
         h = C.c_void_p()
         check(self._L.emu_film_ring_create(int(capacity), float(idle_seconds), C.byref(h)),
               'emu_film_ring_create')
         self._h = h
-        self._pending = collections.OrderedDict()   # ticket -> shape, oldest first
+        self._pending = collections.OrderedDict()   # ticket -> (layers, orders), oldest first
         self._early = {}
         self._orders = {}
 
@@ -573,6 +577,111 @@ class DeviceFilmServer(object):
         check(st, 'emu_film_ring_submit')
         self._pending[t.value] = (len(n), len(px))
         return t.value
+
+    @staticmethod
+    def _dtype(cs):
+        """numpy layout of a ctypes descriptor (the C struct's offsets)."""
+        names, formats, offsets = [], [], []
+        for f, t in cs._fields_:
+            names.append(f)
+            offsets.append(getattr(cs, f).offset)
+            if t is C.c_int:
+                formats.append(np.int32)
+            elif t is C.c_double:
+                formats.append(np.float64)
+            elif t is C.c_void_p:
+                formats.append(np.uintp)
+            else:   # c_double * k
+                formats.append((np.float64, (t._length_,)))
+        return np.dtype({'names': names, 'formats': formats, 'offsets': offsets, 'itemsize': C.sizeof(cs)})
+
+    def submit_many(self, reqs):
+        """Submit requests in order with one call into the library per batch
+        of free slots; returns their tickets.  When the ring is full the
+        oldest results are read first (poll, poll_many, wait and take still
+        return them)."""
+        reqs = list(reqs)
+        if any(r.incoming is not None for r in reqs):
+            raise ValueError('the device request loop takes standard polarisations only')
+        n = len(reqs)
+        if n == 0:
+            return []
+        if self._REQ is None:
+            type(self)._REQ = self._dtype(_lib.EmuFilmRingRequest)
+        orders = [self._order_arrays(r) for r in reqs]
+        ns = [np.ascontiguousarray(r.n, np.complex128) for r in reqs]
+        hs = [np.ascontiguousarray(r.heights, np.float64) for r in reqs]
+        a = np.zeros(n, self._REQ)
+        a['n_layers'] = [len(x) for x in ns]
+        a['n_pw'] = [len(o[0]) for o in orders]
+        a['world_1d'] = [int(bool(r.world_1d)) for r in reqs]
+        a['pol'] = [_lib.POL[r.pol] for r in reqs]
+        a['period'] = [r.period for r in reqs]
+        a['period_y'] = [r.period_y for r in reqs]
+        a['wl_nm'] = [r.wl_nm for r in reqs]
+        a['k_pll'] = [r.k_pll for r in reqs]
+        a['h_px'] = [o[0].ctypes.data for o in orders]
+        a['h_py'] = [o[1].ctypes.data for o in orders]
+        a['h_n'] = [x.ctypes.data for x in ns]
+        a['h_heights_nm'] = [x.ctypes.data for x in hs]
+        tickets = np.empty(n, np.int64)
+        done = 0
+        k = C.c_int()
+        while done < n:
+            st = self._L.emu_film_ring_submit_many(self._h, C.c_void_p(a[done:].ctypes.data), n - done,
+                                                   C.c_void_p(tickets[done:].ctypes.data), C.byref(k))
+            if st not in (0, _lib.EMU_E_WORKSPACE):
+                check(st, 'emu_film_ring_submit_many')
+            for i in range(done, done + k.value):
+                self._pending[int(tickets[i])] = (int(a['n_layers'][i]), int(a['n_pw'][i]))
+            done += k.value
+            if done < n:
+                self._drain_one()   # the ring is full until results are read
+        return tickets.tolist()
+
+    def poll_many(self, tickets):
+        """{ticket: result} for the given tickets that are done (the others
+        stay pending), with one call into the library."""
+        out, rest = {}, []
+        for t in tickets:
+            if t in self._early:
+                out[t] = self._early.pop(t)
+            elif t in self._pending:
+                rest.append(t)
+            else:
+                raise _lib.EmuError(_lib.EMU_E_ARG, 'poll_many: unknown or already read ticket')
+        if not rest:
+            return out
+        if self._RES is None:
+            type(self)._RES = self._dtype(_lib.EmuFilmRingResult)
+        n = len(rest)
+        shp = np.array([self._pending[t] for t in rest], np.int64)
+        P, Lm = 2 * shp[:, 1], shp[:, 0] - 1
+        ro, lo = np.cumsum(P) - P, np.cumsum(Lm) - Lm
+        R, T = np.empty(int(P.sum()), np.complex128), np.empty(int(P.sum()), np.complex128)
+        A, Tl = np.empty(int(Lm.sum())), np.empty(int(Lm.sum()))
+        Rl, F = np.empty(n), np.empty(n, np.uint32)
+        res = np.zeros(n, self._RES)
+        idx = np.arange(n)
+        res['h_R_net'] = R.ctypes.data + 16 * ro
+        res['h_T_net'] = T.ctypes.data + 16 * ro
+        res['h_a_list'] = A.ctypes.data + 8 * lo
+        res['h_t_list'] = Tl.ctypes.data + 8 * lo
+        res['h_r_list'] = Rl.ctypes.data + 8 * idx
+        res['h_flags'] = F.ctypes.data + 4 * idx
+        done = np.zeros(n, np.int32)
+        tk = np.array(rest, np.int64)
+        st = self._L.emu_film_ring_poll_many(self._h, C.c_void_p(tk.ctypes.data), n, C.c_void_p(res.ctypes.data),
+                                             C.c_void_p(done.ctypes.data))
+        if st < 0:
+            raise _lib.EmuError(-st, 'emu_film_ring_poll_many')
+        for i in np.nonzero(done)[0]:
+            t = rest[i]
+            del self._pending[t]
+            a, b, c, d = ro[i], ro[i] + P[i], lo[i], lo[i] + Lm[i]
+            out[t] = {'R_net': R[a:b], 'T_net': T[a:b], 'a_list': A[c:d], 't_list': Tl[c:d],
+                      'r_list': Rl[i:i + 1], 'flags': int(F[i])}
+        return out
 
     def _result(self, ticket):
         L, npw = self._pending[ticket]

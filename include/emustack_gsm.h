@@ -295,11 +295,15 @@ int emu_bloch_fields_plane(const EmuBlochFieldsPlane *p, void *stream);
  *             bounded) and restarts on the next submit.
  *   submit  : copies a request into its slot and wakes the loop; returns a
  *             ticket, or EMU_E_WORKSPACE while the ring is full (poll the
- *             oldest results first).  Thread-safe.
+ *             oldest results first).  Thread-safe.  submit_many: the same
+ *             for n requests in order, as many as there are free slots
+ *             (*n_submitted; EMU_E_WORKSPACE when none).
  *   poll    : 1 and the outputs copied out when the ticket is done, 0 while
- *             pending (each result can be read once); wait: poll until done
- *             or timeout (-EMU_E_TIMEOUT); ready: 1 when done, 0 while
- *             pending, without reading (or consuming) the result.
+ *             pending, a negative status for an unknown or already read
+ *             ticket (each result can be read once); poll_many: the same for
+ *             n tickets (done[i]), returns how many were read; wait: poll
+ *             until done or timeout (-EMU_E_TIMEOUT); ready: 1 when done, 0
+ *             while pending, without reading (or consuming) the result.
  *   stop    : ends the loop and waits for it; returns EMU_E_TIMEOUT if a
  *             device wait gave up, else EMU_OK.
  * While the loop runs it holds every SM; other kernels on the device wait
@@ -326,7 +330,11 @@ typedef struct {
 size_t emu_film_ring_slot_bytes(void);
 int emu_film_ring_create(int capacity, double idle_seconds, EmuFilmRing **out);
 int emu_film_ring_submit(EmuFilmRing *ring, const EmuFilmRingRequest *req, long long *ticket);
+int emu_film_ring_submit_many(EmuFilmRing *ring, const EmuFilmRingRequest *reqs, int n, long long *tickets,
+                              int *n_submitted);
 int emu_film_ring_poll(EmuFilmRing *ring, long long ticket, EmuFilmRingResult *out);
+int emu_film_ring_poll_many(EmuFilmRing *ring, const long long *tickets, int n, const EmuFilmRingResult *outs,
+                            int32_t *done);
 int emu_film_ring_wait(EmuFilmRing *ring, long long ticket, double timeout_s, EmuFilmRingResult *out);
 int emu_film_ring_ready(EmuFilmRing *ring, long long ticket);
 int emu_film_ring_running(EmuFilmRing *ring);

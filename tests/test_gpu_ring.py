@@ -135,3 +135,30 @@ def test_poll_returns_results_read_early_to_free_slots():
     ref = _var_results(reqs)
     for t, v in zip(tickets, ref):
         np.testing.assert_array_equal(got[t]['R_net'], np.asarray(v['R_net']))
+
+
+def test_batched_submit_and_poll_match_the_single_calls():
+    """submit_many / poll_many (one library call per batch) return what the
+    one-request calls return, bit for bit, also when a batch is larger than
+    the free slots (the oldest results are then read to make room)."""
+    from emustack_b200.serving import DeviceFilmServer
+    reqs = _requests(90, seed=6, max_mo=6)
+    srv = DeviceFilmServer(capacity=32, idle_seconds=0.5)
+    try:
+        tickets = srv.submit_many(reqs[:70])          # more than the 32 slots
+        tickets += srv.submit_many(reqs[70:])
+        assert len(tickets) == len(reqs) and len(set(tickets)) == len(reqs)
+        got = {}
+        deadline = time.time() + 30.0
+        while len(got) < len(tickets) and time.time() < deadline:
+            got.update(srv.poll_many([t for t in tickets if t not in got][:40]))
+        assert len(got) == len(tickets)
+        assert srv.stop() == 0
+    finally:
+        srv.close()
+    ref = _var_results(reqs)
+    for t, v in zip(tickets, ref):
+        np.testing.assert_array_equal(got[t]['R_net'], np.asarray(v['R_net']))
+        np.testing.assert_array_equal(got[t]['T_net'], np.asarray(v['T_net']))
+        np.testing.assert_array_equal(got[t]['a_list'], np.asarray(v['a_list']))
+        assert got[t]['flags'] == int(v['flags'])
