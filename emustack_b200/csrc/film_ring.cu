@@ -487,18 +487,20 @@ extern "C" int emu_film_ring_submit_many(EmuFilmRing *r, const EmuFilmRingReques
                                          int *n_submitted) {
   if (!r || n < 0 || (n > 0 && (!q || !tickets)) || !n_submitted) return EMU_E_ARG;
   *n_submitted = 0;
-  for (int i = 0; i < n; ++i) {
-    const int st = request_check(q + i);
-    if (st != EMU_OK) return st;
-  }
   if (n == 0) return EMU_OK;
   std::lock_guard<std::mutex> lock(r->mu);
-  int k = 0;
-  while (k < n && slot_write(r, q + k, tickets + k)) ++k;
+  // each request is checked as it is written: the ones before a bad
+  // request are submitted, and its status is returned
+  int k = 0, st = EMU_OK;
+  for (; k < n; ++k) {
+    st = request_check(q + k);
+    if (st != EMU_OK || !slot_write(r, q + k, tickets + k)) break;
+  }
   *n_submitted = k;
-  if (k == 0) return EMU_E_WORKSPACE;  // ring full
+  if (k == 0) return st != EMU_OK ? st : EMU_E_WORKSPACE;  // bad first request, or the ring is full
   publish_tail(r);
-  return ring_ensure_running(r);
+  const int run = ring_ensure_running(r);
+  return run != EMU_OK ? run : st;
 }
 
 namespace {

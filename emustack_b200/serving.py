@@ -38,6 +38,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import itertools
 import threading
 import time
 
@@ -630,14 +631,25 @@ class DeviceFilmServer(object):
         while done < n:
             st = self._L.emu_film_ring_submit_many(self._h, C.c_void_p(a[done:].ctypes.data), n - done,
                                                    C.c_void_p(tickets[done:].ctypes.data), C.byref(k))
-            if st not in (0, _lib.EMU_E_WORKSPACE):
-                check(st, 'emu_film_ring_submit_many')
             for i in range(done, done + k.value):
                 self._pending[int(tickets[i])] = (int(a['n_layers'][i]), int(a['n_pw'][i]))
             done += k.value
+            if st not in (0, _lib.EMU_E_WORKSPACE):
+                check(st, 'emu_film_ring_submit_many')
             if done < n:
-                self._drain_one()   # the ring is full until results are read
+                self._drain_some()   # the ring is full until results are read
         return tickets.tolist()
+
+    def _drain_some(self, upto=1024):
+        """Read the oldest results that are done (at least the oldest one,
+        waiting for it); they free their slots, and poll, poll_many, wait and
+        take return them later."""
+        oldest = list(itertools.islice(self._pending, upto))
+        early = self.poll_many(oldest)
+        if not early:
+            t = oldest[0]
+            early = {t: self._read(t, 60.0)}
+        self._early.update(early)
 
     def poll_many(self, tickets):
         """{ticket: result} for the given tickets that are done (the others
