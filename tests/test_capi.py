@@ -225,3 +225,46 @@ def test_pw_embed_1d_to_2d_matches_the_oracle(max_order):
         assert n2.value == len(p2)
         for o in range(npw1):
             assert J2[rows[o], 0] == 1 + inv[o]
+
+
+def test_field_entry_points_check_their_arguments_on_the_host():
+    """emu_pw_fields and emu_bloch_fields_plane refuse bad descriptors before
+    touching the device: order counts out of range, a grid without its
+    workspace, a plane outside the layer; emu_pw_fields_workspace_size is
+    the tables' size for grids and 0 for points."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    L = _lib.lib()
+    d = _lib.EmuPwFields()
+    d.n_stacks, d.n_pw, d.grid, d.nx, d.ny, d.nz = 2, 81, 1, 51, 51, 4
+    assert L.emu_pw_fields_workspace_size(C.byref(d)) == 2 * (51 + 51 + 3 * 4) * 81 * 16
+    d.grid = 0
+    assert L.emu_pw_fields_workspace_size(C.byref(d)) == 0
+    d.n_pw = 0
+    assert L.emu_pw_fields(C.byref(d), None) == _lib.EMU_E_ARG
+    d.n_pw = _lib.PW_FIELDS_MAX_ORDERS + 1
+    assert L.emu_pw_fields(C.byref(d), None) == _lib.EMU_E_ARG
+    # a grid with every input present but no workspace
+    d.n_pw, d.grid = 81, 1
+    for f in ('d_alphas', 'd_betas', 'd_sort', 'd_kz', 'd_n', 'd_vec_coef_down', 'd_x', 'd_y', 'd_z', 'd_E'):
+        setattr(d, f, 256)
+    d.vcd_stride = 162
+    assert L.emu_pw_fields(C.byref(d), None) == _lib.EMU_E_WORKSPACE
+    b = _lib.EmuBlochFieldsPlane()
+    b.n_stacks, b.n_modes, b.n_elements, b.h, b.hz = 1, 10, 5, 0.3, 0.31
+    assert L.emu_bloch_fields_plane(C.byref(b), None) == _lib.EMU_E_ARG
+    b.hz = -0.01
+    assert L.emu_bloch_fields_plane(C.byref(b), None) == _lib.EMU_E_ARG
+
+
+def test_ring_entry_points_check_their_arguments_on_the_host():
+    """The request-loop calls refuse a null ring and bad arguments with
+    negative (poll) or positive (submit) statuses before any device work."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    L = _lib.lib()
+    k = C.c_int(7)
+    assert L.emu_film_ring_submit_many(None, None, 0, None, C.byref(k)) == _lib.EMU_E_ARG
+    assert L.emu_film_ring_poll(None, 0, None) < 0
+    assert L.emu_film_ring_poll_many(None, None, 0, None, None) < 0
+    assert L.emu_film_ring_ready(None, 0) < 0
