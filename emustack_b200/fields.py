@@ -13,7 +13,7 @@ Device entry points (libemustack_gsm.so):
   backend/fortran/field_value_plane.f:6-132).
 
 Reference-facing functions with the reference's names and arguments:
-``field_values``, ``fields_in_plane``, ``t_r_a_write_files``,
+``field_values``, ``fields_in_plane``, ``fields_vertically``, ``t_r_a_write_files``,
 ``layers_print``, ``zeros_int_str``, ``save_reference_data``.  They write the
 reference's data files (.txt / .npz, same names and formats); figures
 (matplotlib PDFs) and gmsh files are not produced -- ``fields_in_plane``
@@ -306,6 +306,64 @@ def fields_in_plane(stacks_list, lay_interest=1, z_values=[0.1, 3.6], nu_calc_pt
         res = {'x': r, 'y': r, 'z': zs, 'E_x': Ex, 'E_y': Ey, 'E_z': Ez, 'E_abs': Eabs}
         np.savez('%(d)s/stack_%(n)s_E_%(name)s_wl=%(wl)s.npz' % {'d': dir_name, 'n': stack_num, 'name': name_lay,
                                                                  'wl': wl}, **res)
+        out.append(res)
+    return out
+
+
+def fields_vertically(stacks_list, factor_pts_vert=31, nu_pts_hori=41, semi_inf_height=1.0, gradient=None,
+                      no_incoming=False, add_name='', force_eq_ratio=False, colour_res=30, plot_boundaries=True):
+    """Fields on the x-z slice (y = 0) through every ThinFilm layer of each
+    stack, on the grids of backend/plotting.py:2074-2856: nu_pts_hori x
+    points over the cell, round(factor_pts_vert Re(eps) h / wl) z points per
+    layer (at least 11), semi_inf_height (units of the period) into the
+    substrate and superstrate; no_incoming drops the incident field in the
+    superstrate.  Saved to fields_vertically/stack_<n><add_name>.npz (for
+    layer i: E_x_<i>, E_y_<i>, E_z_<i> [x, z], z_<i> on the stack's height
+    axis, x) and returned as one dict per stack.  Nanostructured layers
+    (their fields go to gmsh in the reference) are skipped; the plotting
+    arguments are accepted for compatibility and not used."""
+    dir_name = "fields_vertically"
+    if not os.path.exists(dir_name):
+        os.mkdir(dir_name)
+    if nu_pts_hori % 2 == 0:
+        nu_pts_hori += 1
+    out = []
+    for stack_num, pstack in enumerate(stacks_list):
+        num_lays = len(pstack.layers)
+        wl_normed = pstack.layers[0].wl_norm()
+        ind_h_list = list(pstack.heights_norm())
+        h_list = [-semi_inf_height, 0]
+        for h in ind_h_list:
+            h_list.append(h_list[-1] + h)
+        h_list.append(h_list[-1] + semi_inf_height)
+        ind_h_list.append(semi_inf_height)
+        ind_h_list.insert(0, semi_inf_height)
+        x_range = np.linspace(0.0, 1.0, nu_pts_hori)
+        res = {'x': x_range}
+        for lay in range(num_lays):
+            layer = pstack.layers[lay]
+            if not _is_film(layer):
+                continue
+            eps = np.asarray(layer.n()) ** 2
+            nz = int(np.round(factor_pts_vert * (np.real(np.max(eps)) * ind_h_list[lay] / wl_normed)))
+            nz = max(nz, 11)
+            if lay == 0:
+                z_range = np.linspace(h_list[lay], 0.0, nz)
+            else:
+                z_range = np.linspace(0.0, ind_h_list[lay], nz)
+            a = _layer_pw_inputs(pstack, lay)
+            if lay == num_lays - 1 and no_incoming:
+                a['vec_coef_down'] = np.zeros_like(a['vec_coef_down'])
+            if a['height_norm'] is None:
+                a['height_norm'] = 0.0
+            # the routine's z below the stack is negative; the kernel takes the
+            # distance into the substrate
+            zk = -z_range if lay == 0 else z_range
+            E, _ = pw_fields(x=x_range, y=np.zeros(1), z=zk, grid=True, **a)
+            E = E[0].cpu().numpy().reshape(3, nu_pts_hori, 1, nz)[:, :, 0, :]
+            res['E_x_%d' % lay], res['E_y_%d' % lay], res['E_z_%d' % lay] = E[0], E[1], E[2]
+            res['z_%d' % lay] = np.linspace(h_list[lay], 0.0 if lay == 0 else h_list[lay + 1], nz)
+        np.savez('%s/stack_%d%s.npz' % (dir_name, stack_num, add_name), **res)
         out.append(res)
     return out
 

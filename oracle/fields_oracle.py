@@ -8,6 +8,7 @@ Paths are relative to the EMUstack source tree:
 * plane-wave fields in a homogeneous layer   backend/plotting.py:2857-2996 (field_values),
                                              backend/plotting.py:1759-1833 (fields_in_plane,
                                              ThinFilm branch)
+* x-z slices through ThinFilm layers         backend/plotting.py:2380-2505 (fields_vertically)
 * Bloch-mode fields at the P2 nodes of a     backend/fortran/field_value_plane.f:6-132
   2D nanostructured layer
 
@@ -113,3 +114,28 @@ def bloch_field_plane(sol, beta, vec_coef, h, hz):
         mE[:, :, 0:2] += sol[:, m, 0:6, 0:2] * c_t
         mE[:, :, 2] += sol[:, m, 0:6, 2] * c_z
     return mE
+
+
+def vertical_slice(alphas, betas, sort_order, kz, n, vcd, vcu, x_range, z_range, h_norm=None,
+                   world_1d=False):
+    """E_x, E_y, E_z on the x-z slice at y = 0 of one ThinFilm layer as
+    fields_vertically evaluates it (backend/plotting.py:2380-2505): z_range
+    as that routine builds it (negative inside the substrate), the down
+    term exp(-i gamma z) in the substrate and superstrate (h_norm None) and
+    exp(-i gamma (z - h)) in a finite layer; vcu None for the substrate and
+    vcd zero for the superstrate without the incoming field.  Arrays
+    [x, z]."""
+    alpha, beta, gamma, eta = pw_layer_coefs(alphas, betas, sort_order, kz, n, vcd, vcu, world_1d)
+    out = np.zeros((3, len(x_range), len(z_range)), complex)
+    y1 = 0.0
+    for iz, z in enumerate(z_range):
+        for ix, x1 in enumerate(x_range):
+            if h_norm is None:
+                e_dn = np.exp(1j * (alpha * x1 + beta * y1 - gamma * z))
+            else:
+                e_dn = np.exp(1j * (alpha * x1 + beta * y1 - gamma * (z - h_norm)))
+            e_up = np.exp(1j * (alpha * x1 + beta * y1 + gamma * z))
+            for c in range(3):
+                out[c, ix, iz] = (np.sum(eta['down'][0][c] * e_dn + eta['up'][0][c] * e_up)
+                                  + np.sum(eta['down'][1][c] * e_dn + eta['up'][1][c] * e_up))
+    return out[0], out[1], out[2]

@@ -250,3 +250,42 @@ def test_grid_tables_match_the_term_by_term_points(nz, substrate):
         scale = np.abs(P[b]).max()
         np.testing.assert_allclose(G[b], P[b], rtol=0, atol=1e-13 * scale)
     np.testing.assert_allclose(Gabs.cpu().numpy(), Pabs.cpu().numpy(), rtol=1e-12, atol=1e-13 * np.abs(P).max())
+
+
+@pytest.mark.parametrize('name,no_incoming', [('s2d', False), ('s2c', True), ('s1d', False)])
+def test_fields_vertically_matches_the_oracle(name, no_incoming, tmp_path, monkeypatch):
+    """x-z slices through every film layer on fields_vertically's grids (z
+    negative inside the substrate, the superstrate with or without the
+    incident field) against the restatement of its loop."""
+    from emustack_b200.fields import fields_vertically
+    monkeypatch.chdir(tmp_path)
+    (key, st), = _our_stacks(name)[:1]
+    res = fields_vertically([st], factor_pts_vert=11, nu_pts_hori=12, semi_inf_height=0.5,
+                            no_incoming=no_incoming)[0]
+    assert os.path.exists('fields_vertically/stack_0.npz')
+    L = len(st.layers)
+    hs = st.heights_norm()
+    h_list = [-0.5, 0.0] + list(np.cumsum(hs)) + [0.0]
+    h_list[-1] = h_list[-2] + 0.5
+    x = res['x']
+    assert len(x) == 13
+    for lay in range(L):
+        ly = st.layers[lay]
+        S = ly.structure.num_pw_per_pol
+        ind_h = 0.5 if lay in (0, L - 1) else hs[lay - 1]
+        nz = max(11, int(np.round(11 * np.real(np.max(np.asarray(ly.n()) ** 2)) * ind_h / ly.wl_norm())))
+        z_range = np.linspace(-0.5, 0.0, nz) if lay == 0 else np.linspace(0.0, ind_h, nz)
+        row = L - 1 - lay
+        vcd = np.asarray(st.vec_coef_down[row]).ravel()
+        if lay == L - 1 and no_incoming:
+            vcd = np.zeros_like(vcd)
+        vcu = None if lay == 0 else np.asarray(st.vec_coef_up[row]).ravel()
+        betas = np.atleast_1d(np.asarray(ly.betas, float))
+        betas = np.full(S, betas[0]) if betas.size == 1 else betas
+        ref = F.vertical_slice(ly.alphas, betas, ly.sort_order, np.asarray(ly.k_z)[:S], complex(ly.n()), vcd, vcu,
+                               x, z_range, h_norm=None if lay in (0, L - 1) else hs[lay - 1])
+        scale = max(np.abs(r).max() for r in ref)
+        for c, k in enumerate(('E_x_%d', 'E_y_%d', 'E_z_%d')):
+            got = res[k % lay]
+            assert got.shape == (13, nz)
+            np.testing.assert_allclose(got, ref[c], rtol=0, atol=1e-13 * scale, err_msg='%s layer %d' % (k, lay))
