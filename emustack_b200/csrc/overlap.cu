@@ -726,14 +726,18 @@ struct TcPlan {
 };
 
 constexpr size_t kTcGroupBytes = (size_t)4 << 30;  // scratch budget of one group
-// Longest K range one tensor-core accumulation covers.  The tensor cores
-// accumulate in FP32 and the sum drifts toward zero by about 7e-9 x K
-// relative (measured: 1.9e-6 rms at K = 256, 7.3e-6 at 1024, 1.8e-3 at
-// 262144, for random operands); the K splits are summed in FP64.
-constexpr long long kTcMaxKSplit = 256;
+// The tensor cores accumulate in FP32 and the sum drifts toward zero by
+// about 7e-9 x K relative (measured: 1.9e-6 rms at K = 256, 7.3e-6 at 1024,
+// 1.8e-3 at 262144, for random operands).  The GEMM kernel therefore starts
+// a fresh tensor-memory accumulation every 256 K values and sums those
+// chunk results in FP32 (round to nearest) inside the CTA; a CTA's K range
+// holds at most kTcMaxChunksPerCta chunks, and the K splits (CTAs) are
+// summed in FP64.
+constexpr long long kTcChunkK = 256;
+constexpr long long kTcMaxChunksPerCta = 32;
 constexpr int kTcMaxSplits = 256;
-// element chunk whose K range (12 values per element) fits kTcMaxSplits splits
-constexpr long kTcMaxChunk = kTcMaxSplits * kTcMaxKSplit / 12;
+// element chunk (12 K values per element) of one GEMM
+constexpr long kTcMaxChunk = 32768;
 
 static size_t tc_problem_bytes(const EmuOverlap *p, const TcPlan &t) {
   const size_t npw = p->n_pw, M = p->nval;
@@ -762,12 +766,12 @@ static TcPlan tc_plan(const EmuOverlap *p) {
   t.group = (int)g;
   const int tiles = emu::tc_tiles(2 * p->n_pw, t.nb) * t.group;
   int sp = (emu::sm_count() + tiles - 1) / tiles;
-  const int maxsp = (int)(t.K2 / 256 > 0 ? t.K2 / 256 : 1);
+  const int maxsp = (int)(t.K2 / kTcChunkK > 0 ? t.K2 / kTcChunkK : 1);
   if (sp > maxsp) sp = maxsp;
   if (p->tc_splits > 0) sp = p->tc_splits;
-  // accuracy floor, also under an explicit choice: no split longer than
-  // kTcMaxKSplit
-  const int need = (int)((t.K2 + kTcMaxKSplit - 1) / kTcMaxKSplit);
+  // accuracy floor, also under an explicit choice: no CTA sums more than
+  // kTcMaxChunksPerCta chunk results in FP32
+  const int need = (int)((t.K2 + kTcChunkK * kTcMaxChunksPerCta - 1) / (kTcChunkK * kTcMaxChunksPerCta));
   if (sp < need) sp = need;
   if (sp > kTcMaxSplits) sp = kTcMaxSplits;
   if (sp * t.group > 65535) sp = 65535 / t.group;

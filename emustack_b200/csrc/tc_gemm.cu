@@ -20,9 +20,16 @@
 //   warp 1 (one lane) issues 4 k-steps x 3 tcgen05.mma (M=128, N=256, K=8)
 //     per stage and commits them to empty[stage], freeing the buffers.
 // Only x travels from memory (half the bytes of precomputed hi/lo pairs).
-// Warps 2-5 then read the accumulator back with tcgen05.ld (each warp its
-// 32-lane quarter of TMEM) and write FP32 partials of this K split.  Every
-// mbarrier wait is bounded.
+// The tensor cores accumulate in FP32 with a bias that grows with the K
+// range of one accumulation (about -6e-9 x K relative), so each
+// accumulation covers one chunk of 256 K values (8 stages) and starts from
+// zero: after a chunk's MMAs (committed to acc_full), warps 2-5 read the
+// accumulator with tcgen05.ld (each warp its 32-lane quarter of TMEM), add
+// the running sum of the earlier chunks held in the other half of TMEM
+// (FP32, round to nearest) and store it back with tcgen05.st, then free the
+// accumulator (acc_empty) for the next chunk; after the last chunk they write
+// the CTA's sum as the FP32 partial of this K split.  Every mbarrier wait is
+// bounded.
 //
 // Descriptor formats follow the sm100 UMMA definitions (shared-memory matrix
 // descriptor: start >> 4, LBO >> 4, SBO >> 4, version 1, layout type
@@ -40,7 +47,8 @@ namespace {
 constexpr int kTcM = 128, kTcN = 256, kTcK = 32;  // CTA tile and K stage (32 FP32 = 128 B)
 constexpr int kTcThreads = 192;
 constexpr int kSplitThreads = 128;                  // warps 2-5
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // accumulator [0, 256), running sum [256, 512)
+constexpr int kChunkStages = 8;       // K stages per tensor-memory accumulation (256 values)
 constexpr long long kWaitLimit = 1ll << 26;  // bounded mbarrier spins
 
 constexpr int kATileBytes = kTcM * kTcK * 4;  // 16 KB
@@ -122,6 +130,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+      : "memory");
+}
+
 struct TmaMaps {
   CUtensorMap a, b;
 };
@@ -179,7 +206,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t raw = smem_u32(sm_raw);
   unsigned char *buf = sm_raw + (((raw + 1023u) & ~1023u) - raw);
   uint64_t *bars = (uint64_t *)(buf + kStages * kStageBytes);
-  uint32_t *tslot = (uint32_t *)(bars + 3 * kStages + 1);
+  uint32_t *tslot = (uint32_t *)(bars + 3 * kStages + 3);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
   const int split = blockIdx.z % nsplit, prob = blockIdx.z / nsplit;
@@ -187,7 +214,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int kend = min(Kp, kbeg + kper);
   const int nst = kend > kbeg ? (kend - kbeg + kTcK - 1) / kTcK : 0;
   const uint32_t full0 = smem_u32(bars), spl0 = smem_u32(bars + kStages),
-                 empty0 = smem_u32(bars + 2 * kStages), done = smem_u32(bars + 3 * kStages);
+                 empty0 = smem_u32(bars + 2 * kStages), acc_full = smem_u32(bars + 3 * kStages),
+                 acc_empty = smem_u32(bars + 3 * kStages + 1), done = smem_u32(bars + 3 * kStages + 2);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -200,6 +228,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(spl0 + 8 * i, kSplitThreads);
       mbar_init(empty0 + 8 * i, 1);
     }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, kSplitThreads);
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -228,9 +258,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // ---- MMA issuer
-      int issued = 0;
       for (int t = 0; t < nst; ++t) {
-        const int b = t % kStages;
+        const int b = t % kStages, j = t % kChunkStages, c = t / kChunkStages;
+        // a new chunk starts once the epilogue has taken the previous one
+        if (j == 0 && c > 0 && !mbar_wait(acc_empty, (uint32_t)((c - 1) & 1))) {
+          ok = false;
+          break;
+        }
         if (!mbar_wait(spl0 + 8 * b, (uint32_t)((t / kStages) & 1))) {
           ok = false;
           break;
@@ -244,22 +278,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const uint32_t o = (uint32_t)k * 32;
           const uint64_t dAh = smem_desc_sw128(ah + o), dAl = smem_desc_sw128(al + o);
           const uint64_t dBh = smem_desc_sw128(bh + o), dBl = smem_desc_sw128(bl + o);
-          mma_tf32(tmem, dAh, dBh, (t == 0 && k == 0) ? 0u : 1u);
+          mma_tf32(tmem, dAh, dBh, (j == 0 && k == 0) ? 0u : 1u);
           mma_tf32(tmem, dAh, dBl, 1u);
           mma_tf32(tmem, dAl, dBh, 1u);
         }
         mma_commit(empty0 + 8 * b);
-        ++issued;
+        if (j == kChunkStages - 1 || t == nst - 1) mma_commit(acc_full);
       }
-      // tracks every MMA issued above, also when a wait gave up
-      if (issued > 0) mma_commit(done);
+      // tracks every MMA issued above, also when a wait gave up: tensor
+      // memory is freed only after they have completed
+      if (nst > 0) mma_commit(done);
     }
   } else {
-    // ---- splitters (warps 2-5)
+    // ---- splitters and epilogue (warps 2-5)
     const int st = tid - 64;
+    const int q = warp & 3;  // TMEM lane quarter this warp may read
+    const int row = m0 + q * 32 + lane;
+    float *Cs = C + ((size_t)prob * nsplit + split) * Mp * Np;
+    const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16), trun = tacc + 256;
     for (int t = 0; t < nst; ++t) {
-      const int b = t % kStages;
-      if (!mbar_wait(full0 + 8 * b, (uint32_t)((t / kStages) & 1))) {
+      const int b = t % kStages, j = t % kChunkStages, c = t / kChunkStages;
+      // warp-uniform outcomes: the tcgen05.ld / st below need converged warps
+      if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * b, (uint32_t)((t / kStages) & 1)))) {
         ok = false;
         break;
       }
@@ -269,34 +309,50 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  kBTileBytes / 16, st);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(spl0 + 8 * b);
-    }
-  }
-  __syncwarp();
-  // ---- epilogue (warps 2-5): wait for the last MMAs (bounded), TMEM -> global
-  bool fin = true;
-  if (warp >= 2 && nst > 0) fin = mbar_wait(done, 0);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const bool all_ok = __syncthreads_and(ok && fin) != 0;
-  if (!all_ok && tid == 0) atomicExch(err, 1);
-  if (warp >= 2) {
-    const int q = warp & 3;  // TMEM lane quarter this warp may read
-    const int row = m0 + q * 32 + lane;
-    float *Cs = C + ((size_t)prob * nsplit + split) * Mp * Np;
-    if (nst > 0 && all_ok) {
+      if (j != kChunkStages - 1 && t != nst - 1) continue;
+      // end of a chunk: fold its accumulator into the running sum
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)(c & 1)))) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const bool last = t == nst - 1;
       for (int c0 = 0; c0 < kTcN; c0 += 32) {
         float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-        if (row < Mp) {
+        tmem_ld32(tacc + (uint32_t)c0, v);
+        if (c > 0) {
+          float r[32];
+          tmem_ld32(trun + (uint32_t)c0, r);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] += r[i];
+        }
+        if (!last) {
+          tmem_st32(trun + (uint32_t)c0, v);
+        } else if (row < Mp) {
 #pragma unroll
           for (int i = 0; i < 32; ++i)
             if (n0 + c0 + i < Np) Cs[(size_t)row * Np + n0 + c0 + i] = v[i];
         }
       }
-    } else if (row < Mp) {
-      for (int c = 0; c < kTcN; ++c)
-        if (n0 + c < Np) Cs[(size_t)row * Np + n0 + c] = 0.0f;
+      if (!last) {
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(acc_empty);
+      }
     }
   }
+  __syncwarp();
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (!all_ok && tid == 0) atomicExch(err, 1);
+  if (warp >= 2 && (nst == 0 || !all_ok)) {
+    const int q = warp & 3;
+    const int row = m0 + q * 32 + lane;
+    float *Cs = C + ((size_t)prob * nsplit + split) * Mp * Np;
+    if (row < Mp)
+      for (int c = 0; c < kTcN; ++c)
+        if (n0 + c < Np) Cs[(size_t)row * Np + n0 + c] = 0.0f;
+  }
+  if (tid == 0 && nst > 0 && !mbar_wait(done, 0)) atomicExch(err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)

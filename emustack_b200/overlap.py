@@ -106,7 +106,7 @@ def overlap_batch(dmesh, px, py, max_order, bloch, k0, sol1=None, sol2=None, are
     L = lib()
     cands = None
     if d.precision == 1 and tune and not elements_per_chunk and not tc_splits:
-        chunks = sorted({min(c, dmesh.nel) for c in (2048, 4096, 5461)})
+        chunks = sorted({min(c, dmesh.nel) for c in (4096, 8192, 16384)})
         cands = [(c, 0) for c in chunks]
     sizes = []
     for c in (cands or [(d.elements_per_chunk, d.tc_splits)]):

@@ -529,16 +529,19 @@ typedef struct {
   emu_c128 *d_J_dag;       /* [batch][nval][2 Npw] (with d_sol2)            */
   int32_t *d_index_pw_inv; /* [batch][Npw] 0-based sorted positions or NULL */
   int elements_per_chunk;  /* 0 = default (4096); bounds the workspace      */
-  int precision;           /* 0: FP64 SIMT GEMM; 1: tensor cores, split-TF32
-                              (hi + lo) products, FP32 accumulation per K split,
+  int precision;           /* 0: FP64 tensor-core GEMM (mma.sync f64); 1:
+                              tcgen05 tensor cores, split-TF32 (hi + lo)
+                              products, FP32 accumulation per 256 K values,
+                              those chunk sums added in FP32 within a K split,
                               FP64 sum of the splits                          */
   int32_t *d_error;        /* [1] set to 1 if a bounded device wait gave up
                               (tensor-core path), else left untouched; may be NULL */
   int tc_splits;           /* tensor-core path: K splits per GEMM (1-256), 0 = one
-                              wave of CTAs; never fewer than keep each split's K
-                              range within 256 values (the tensor cores'
-                              FP32 accumulation drifts by ~7e-9 x K relative);
-                              results differ by that accumulation error */
+                              wave of CTAs; never fewer than keep each split
+                              within 32 chunks of 256 K values (each chunk is
+                              accumulated apart: the tensor cores' FP32
+                              accumulation drifts by ~7e-9 x K relative);
+                              results differ by rounding between choices */
   int field_c64;           /* tensor-core path only: 1 = d_sol1 / d_sol2 hold
                               complex64 (float re, im) in the same layout (the
                               operands are FP32 anyway; half the bytes read) */
