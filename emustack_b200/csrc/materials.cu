@@ -55,13 +55,15 @@ __device__ __forceinline__ cd table_n(const EmuMaterial &m, double x, bool &bad)
   return cd{__dadd_rn(__dmul_rn(sr, t), yl.re), __dadd_rn(__dmul_rn(si, t), yl.im)};
 }
 
-// sqrt(eps_inf - wp^2 / (w^2 + i wg w)), w = 2 pi c / (wl 1e-9), as the
-// reference writes it (materials.py:140-146)
+// sqrt(eps_inf - wp^2 / (w^2 + i wg w)), w = 2 pi c / (wl 1e-9), with the
+// reference's order of operations (materials.py:140-146): the imaginary
+// part of the denominator is (wg 2 pi c) / (wl 1e-9)
 __device__ __forceinline__ cd drude_n(const EmuMaterial &m, double wl) {
   const double c = 299792458.0;
   const double wp = m.drude[0], wg = m.drude[1], eps_inf = m.drude[2];
-  const double w = __ddiv_rn(__dmul_rn(2.0 * 3.141592653589793, c), __dmul_rn(wl, 1e-9));
-  const cd den{__dmul_rn(w, w), __dmul_rn(wg, w)};
+  const double a = __dmul_rn(2.0 * 3.141592653589793, c), t = __dmul_rn(wl, 1e-9);
+  const double w = __ddiv_rn(a, t);
+  const cd den{__dmul_rn(w, w), __ddiv_rn(__dmul_rn(wg, a), t)};
   const cd q = cdiv(cd{__dmul_rn(wp, wp), 0.0}, den);
   return csqrt_p(cd{__dsub_rn(eps_inf, q.x), -q.y});
 }

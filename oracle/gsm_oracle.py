@@ -527,8 +527,9 @@ def material_n(spec, wl_nm, loss=True):
     elif spec.shape == (3,):
         wp, wg, eps_inf = spec
         c = 299792458
-        w = (2 * np.pi * c) / (wl_nm * 1e-9)
-        n = np.sqrt(eps_inf - wp ** 2 / (w ** 2 + 1j * wg * w))
+        # the reference's expression and evaluation order (materials.py:142)
+        n = np.sqrt(eps_inf - wp ** 2 / (((2 * np.pi * c) / (wl_nm * 1e-9)) ** 2
+                                         + 1j * wg * (2 * np.pi * c) / (wl_nm * 1e-9)))
     else:
         ns = spec[:, 1] if spec.shape[1] == 2 else spec[:, 1] + 1j * spec[:, 2]
         n = interp1d(spec[:, 0], ns)(wl_nm)

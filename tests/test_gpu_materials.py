@@ -66,3 +66,23 @@ def test_sweep_of_tabulated_films_matches_the_oracle():
         np.testing.assert_allclose(out['R_net'][b].cpu().numpy(), np.diag(r.R_net), rtol=1e-9, atol=1e-10)
         np.testing.assert_allclose(out['a_list'][b].cpu().numpy(), np.asarray(r.a_list, float),
                                    rtol=1e-9, atol=1e-10)
+
+
+def test_material_kernel_matches_the_reference_values():
+    """emu_material_n_batch against the reference's own Material.n outputs
+    (tests/golden/materials.npz): tabulated and constant bit for bit, Drude
+    to 2 ulp (complex square roots)."""
+    import os
+    from emustack_b200.materials import Material, n_batch
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'materials.npz'))
+    names = ['const', 'complex_tab', 'real_tab', 'drude']
+    specs = [gold['spec_' + k] for k in names]
+    mats = [Material(s.item() if s.shape == () else s) for s in specs]
+    wl = gold['wl']
+    out = n_batch(mats, torch.tensor(wl, device='cuda'), [True] * 4).cpu().numpy()
+    for l, k in enumerate(names):
+        ref = gold['n_' + k]
+        if k == 'drude':
+            np.testing.assert_allclose(out[:, l], ref, rtol=5e-16, atol=0, err_msg=k)
+        else:
+            np.testing.assert_array_equal(out[:, l], ref, err_msg=k)
