@@ -307,7 +307,7 @@ EXTRA_SIGNATURES.extend([
 ])
 
 
-MAT_CONSTANT, MAT_TABLE, MAT_DRUDE = 0, 1, 2
+MAT_CONSTANT, MAT_TABLE, MAT_DRUDE, MAT_TABLE_REAL = 0, 1, 2, 3
 
 
 class EmuMaterial(C.Structure):

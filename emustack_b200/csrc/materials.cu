@@ -7,11 +7,16 @@
 // materials and the solve.
 //
 // Tabulated data are interpolated linearly as scipy.interpolate.interp1d
-// (kind 'linear', the reference's choice) evaluates it: the interval is
-// found as numpy.searchsorted(x, x_new, side='left') clipped to [1, K-1],
-// lo = hi - 1, and y = (y_hi - y_lo)/(x_hi - x_lo) * (x_new - x_lo) + y_lo,
-// real and imaginary parts alike; wavelengths outside the table are an
-// error (interp1d's bounds_error), reported through d_error and given NaN.
+// (kind 'linear', the reference's choice; scipy 1.18) evaluates it:
+//  * real indices (EMU_MAT_TABLE_REAL) through numpy.interp: j the last node
+//    with x_j <= x, y = y_j at a node (and at the last node), else
+//    y = (y_{j+1} - y_j)/(x_{j+1} - x_j) * (x - x_j) + y_j;
+//  * complex indices (EMU_MAT_TABLE) by interp1d's own form: hi =
+//    numpy.searchsorted(x, x_new, side='left') clipped to [1, K-1],
+//    lo = hi - 1, y = ((x_new - x_lo)/(x_hi - x_lo)) y_hi
+//                     + ((x_hi - x_new)/(x_hi - x_lo)) y_lo, termwise.
+// Wavelengths outside the table are an error (interp1d's bounds_error),
+// reported through d_error and given NaN.
 #include <cuda_runtime.h>
 
 #include "emu_cplx.cuh"
@@ -45,14 +50,22 @@ __device__ __forceinline__ cd table_n(const EmuMaterial &m, double x, bool &bad)
     else
       hi = mid;
   }
+  if (m.kind == EMU_MAT_TABLE_REAL) {
+    // numpy.interp: a node gives its value; else the node below and the slope
+    if (lo < K && xs[lo] == x) return cd{m.d_n[lo].re, 0.0};
+    const int j = lo - 1;  // x_j < x < x_{j+1}
+    const double yj = m.d_n[j].re, yk = m.d_n[j + 1].re;
+    const double slope = __ddiv_rn(__dsub_rn(yk, yj), __dsub_rn(xs[j + 1], xs[j]));
+    return cd{__dadd_rn(__dmul_rn(slope, __dsub_rn(x, xs[j])), yj), 0.0};
+  }
   int ihi = lo < 1 ? 1 : (lo > K - 1 ? K - 1 : lo);
   const int ilo = ihi - 1;
   const double xl = xs[ilo], xh = xs[ihi];
   const emu_c128 yl = m.d_n[ilo], yh = m.d_n[ihi];
-  const double dx = __dsub_rn(xh, xl), t = __dsub_rn(x, xl);
-  const double sr = __ddiv_rn(__dsub_rn(yh.re, yl.re), dx);
-  const double si = __ddiv_rn(__dsub_rn(yh.im, yl.im), dx);
-  return cd{__dadd_rn(__dmul_rn(sr, t), yl.re), __dadd_rn(__dmul_rn(si, t), yl.im)};
+  const double dx = __dsub_rn(xh, xl);
+  const double wh = __ddiv_rn(__dsub_rn(x, xl), dx), wl = __ddiv_rn(__dsub_rn(xh, x), dx);
+  return cd{__dadd_rn(__dmul_rn(wh, yh.re), __dmul_rn(wl, yl.re)),
+            __dadd_rn(__dmul_rn(wh, yh.im), __dmul_rn(wl, yl.im))};
 }
 
 // sqrt(eps_inf - wp^2 / (w^2 + i wg w)), w = 2 pi c / (wl 1e-9), with the
@@ -77,7 +90,7 @@ __global__ void material_kernel(MatArgs a) {
     const double wl = a.wl[b];
     bool bad = false;
     cd n;
-    if (m.kind == EMU_MAT_TABLE)
+    if (m.kind == EMU_MAT_TABLE || m.kind == EMU_MAT_TABLE_REAL)
       n = table_n(m, wl, bad);
     else if (m.kind == EMU_MAT_DRUDE)
       n = drude_n(m, wl);
@@ -102,8 +115,9 @@ extern "C" int emu_material_n_batch(const EmuMaterial *h_materials, int n_layers
   a.n_points = n_points;
   for (int l = 0; l < n_layers; ++l) {
     const EmuMaterial &m = h_materials[l];
-    if (m.kind < EMU_MAT_CONSTANT || m.kind > EMU_MAT_DRUDE) return EMU_E_ARG;
-    if (m.kind == EMU_MAT_TABLE && (m.n_rows < 2 || !m.d_wl || !m.d_n)) return EMU_E_ARG;
+    if (m.kind < EMU_MAT_CONSTANT || m.kind > EMU_MAT_TABLE_REAL) return EMU_E_ARG;
+    if ((m.kind == EMU_MAT_TABLE || m.kind == EMU_MAT_TABLE_REAL) && (m.n_rows < 2 || !m.d_wl || !m.d_n))
+      return EMU_E_ARG;
     a.mat[l] = m;
   }
   a.wl = d_wl_nm;

@@ -35,18 +35,23 @@ class Material(object):
             return self.data_ns
         if isinstance(self.data_wls, str):
             wp, wg, eps_inf, c = self.data_ns
-            w = (2 * np.pi * c) / (wl_nm * 1e-9)
-            val = np.sqrt(eps_inf - wp ** 2 / (w ** 2 + 1j * wg * w))
-            if np.imag(val) < 0:
-                val = -val
-            return val
+            # the reference's expression and order of operations (materials.py:142;
+            # its sign check there tests the lambda, not the value, so never flips)
+            return np.sqrt(eps_inf - wp ** 2 / (((2 * np.pi * c) / (wl_nm * 1e-9)) ** 2
+                                                + 1j * wg * (2 * np.pi * c) / (wl_nm * 1e-9)))
         wl = np.asarray(wl_nm, dtype=float)
         if np.any(wl < self.data_wls[0]) or np.any(wl > self.data_wls[-1]):
             raise ValueError('wavelength outside the tabulated range')
         ns = np.asarray(self.data_ns)
-        if np.iscomplexobj(ns):
-            return np.interp(wl, self.data_wls, ns.real) + 1j * np.interp(wl, self.data_wls, ns.imag)
-        return np.interp(wl, self.data_wls, ns)
+        if not np.iscomplexobj(ns):
+            return np.interp(wl, self.data_wls, ns)
+        # interp1d's evaluation of complex data (scipy 1.18): the interval of
+        # searchsorted(side='left') clipped to [1, K-1], weights of both ends
+        xs = np.asarray(self.data_wls, float)
+        hi = np.clip(np.searchsorted(xs, wl), 1, len(xs) - 1)
+        lo = hi - 1
+        x_lo, x_hi = xs[lo], xs[hi]
+        return ((wl - x_lo) / (x_hi - x_lo)) * ns[hi] + ((x_hi - wl) / (x_hi - x_lo)) * ns[lo]
 
 
 Air = Material(1.00 + 0.0j)
@@ -88,7 +93,9 @@ def n_batch(materials, wl_nm, losses=None):
                 cache = (torch.tensor(np.asarray(m.data_wls, np.float64), device=dev),
                          torch.tensor(np.asarray(m.data_ns, np.complex128), device=dev))
                 m._device_table = cache
-            e.kind = _lib.MAT_TABLE
+            # scipy's interp1d takes real data through numpy.interp and complex
+            # data through its own weighted form; the kernel does the same
+            e.kind = _lib.MAT_TABLE if np.iscomplexobj(m.data_ns) else _lib.MAT_TABLE_REAL
             e.n_rows = int(cache[0].numel())
             e.d_wl, e.d_n = _lib.ptr(cache[0]), _lib.ptr(cache[1])
             keep.append(cache)

@@ -199,20 +199,25 @@ int emu_film_stack_batch(const EmuFilmStackBatch *p, void *d_workspace,
 /* ---------------------------------------- materials: n(lambda) per layer
  * Refractive index of every layer of a stack at a batch of wavelengths,
  * into the [B][L] array the film kernels take: constant, tabulated (linear
- * interpolation with scipy.interpolate.interp1d's arithmetic, the reference's
- * choice) or Drude materials, each with its loss flag applied (imaginary
- * part dropped when loss == 0).  Replaces Material.n
+ * interpolation with the arithmetic of scipy.interpolate.interp1d, the
+ * reference's choice, as scipy 1.18 evaluates it: real indices through
+ * numpy.interp (EMU_MAT_TABLE_REAL), complex ones by the weighted form
+ * ((x - x0) y1 + (x1 - x) y0) / (x1 - x0) termwise (EMU_MAT_TABLE)) or Drude
+ * materials, each with its loss flag applied (imaginary part dropped when
+ * loss == 0).  Replaces Material.n
  * (backend/materials.py:31-186) and Anallo.n (backend/mode_calcs.py:186-192)
  * for a sweep.  Wavelengths outside a table set *d_error = 1 and give NaN
  * (the reference raises ValueError there).  At most 32 layers per call. */
 #define EMU_MAT_CONSTANT 0
 #define EMU_MAT_TABLE 1
 #define EMU_MAT_DRUDE 2
+#define EMU_MAT_TABLE_REAL 3
 typedef struct {
   int kind;              /* EMU_MAT_*                                        */
   int n_rows;            /* table rows (>= 2)                                */
   const double *d_wl;    /* [n_rows] ascending wavelengths (nm), device      */
-  const emu_c128 *d_n;   /* [n_rows] refractive indices, device              */
+  const emu_c128 *d_n;   /* [n_rows] refractive indices, device (real part
+                            only for EMU_MAT_TABLE_REAL)                      */
   emu_c128 n_const;      /* EMU_MAT_CONSTANT                                 */
   double drude[3];       /* omega_plasma, omega_gamma, eps_inf (EMU_MAT_DRUDE) */
   int loss;              /* 0: imaginary part dropped                        */

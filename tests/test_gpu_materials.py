@@ -71,7 +71,7 @@ def test_sweep_of_tabulated_films_matches_the_oracle():
 def test_material_kernel_matches_the_reference_values():
     """emu_material_n_batch against the reference's own Material.n outputs
     (tests/golden/materials.npz): tabulated and constant bit for bit, Drude
-    to 2 ulp (complex square roots)."""
+    to an ulp (the complex square root)."""
     import os
     from emustack_b200.materials import Material, n_batch
     gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'materials.npz'))
