@@ -68,17 +68,89 @@ __device__ __forceinline__ cd table_n(const EmuMaterial &m, double x, bool &bad)
             __dadd_rn(__dmul_rn(wh, yh.im), __dmul_rn(wl, yl.im))};
 }
 
+// |z| as the C library's hypot computes it for operands in the normal range
+// (glibc 2.35+, Borges' corrected form without fma, "An Improved Algorithm
+// for hypot(a,b)", 2019): h = sqrt(ax^2 + ay^2) then one correction step.
+// Outside [1e-150, 1e150] the CUDA hypot stands in (ulp-level agreement).
+__device__ __forceinline__ double hypot_libc(double x, double y) {
+  double ax = fabs(x), ay = fabs(y);
+  if (ax < ay) {
+    const double t = ax;
+    ax = ay;
+    ay = t;
+  }
+  if (!(ax > 1e-150 && ax < 1e150) || !(ay > 1e-150)) return hypot(x, y);
+  double h = __dsqrt_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
+  double t1, t2;
+  if (h <= __dmul_rn(2.0, ay)) {
+    const double delta = __dsub_rn(h, ay);
+    t1 = __dmul_rn(ax, __dsub_rn(__dmul_rn(2.0, delta), ax));
+    t2 = __dmul_rn(__dsub_rn(delta, __dmul_rn(2.0, __dsub_rn(ax, ay))), delta);
+  } else {
+    const double delta = __dsub_rn(h, ax);
+    t1 = __dmul_rn(__dmul_rn(2.0, delta), __dsub_rn(ax, __dmul_rn(2.0, ay)));
+    t2 = __dadd_rn(__dmul_rn(__dsub_rn(__dmul_rn(4.0, delta), ay), ay), __dmul_rn(delta, delta));
+  }
+  return __dsub_rn(h, __ddiv_rn(__dadd_rn(t1, t2), __dmul_rn(2.0, h)));
+}
+
+// Principal square root by the steps of the C library's csqrt (numpy.sqrt
+// of a complex scalar calls it): d = |z|; for x > 0, r = sqrt((d + x)/2)
+// and s = (y/r)/2, else s = sqrt((d - x)/2) and r = |(y/s)/2|; zero real or
+// imaginary parts take the closed forms.
+__device__ __forceinline__ cd csqrt_libc(cd z) {
+  const double x = z.x, y = z.y;
+  if (y == 0.0) {
+    if (x < 0.0) return cd{0.0, copysign(__dsqrt_rn(-x), y)};
+    return cd{fabs(__dsqrt_rn(x)), copysign(0.0, y)};
+  }
+  if (x == 0.0) {
+    const double r = __dsqrt_rn(__dmul_rn(0.5, fabs(y)));
+    return cd{r, copysign(r, y)};
+  }
+  const double d = hypot_libc(x, y);
+  double r, s;
+  if (x > 0.0) {
+    r = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(d, x)));
+    s = __dmul_rn(0.5, __ddiv_rn(y, r));
+  } else {
+    s = __dsqrt_rn(__dmul_rn(0.5, __dsub_rn(d, x)));
+    r = fabs(__dmul_rn(0.5, __ddiv_rn(y, s)));
+  }
+  return cd{r, copysign(s, y)};
+}
+
+// a / b as numpy divides complex numbers (Smith's method with the reciprocal
+// of the scaled denominator taken once).
+__device__ __forceinline__ cd cdiv_numpy(cd a, cd b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    if (b.x == 0.0 && b.y == 0.0) return cdiv(a, b);
+    const double rat = __ddiv_rn(b.y, b.x);
+    const double scl = __ddiv_rn(1.0, __dadd_rn(b.x, __dmul_rn(b.y, rat)));
+    return cd{__dmul_rn(__dadd_rn(a.x, __dmul_rn(a.y, rat)), scl),
+              __dmul_rn(__dsub_rn(a.y, __dmul_rn(a.x, rat)), scl)};
+  }
+  const double rat = __ddiv_rn(b.x, b.y);
+  const double scl = __ddiv_rn(1.0, __dadd_rn(b.y, __dmul_rn(b.x, rat)));
+  return cd{__dmul_rn(__dadd_rn(__dmul_rn(a.x, rat), a.y), scl),
+            __dmul_rn(__dsub_rn(__dmul_rn(a.y, rat), a.x), scl)};
+}
+
 // sqrt(eps_inf - wp^2 / (w^2 + i wg w)), w = 2 pi c / (wl 1e-9), with the
-// reference's order of operations (materials.py:140-146): the imaginary
-// part of the denominator is (wg 2 pi c) / (wl 1e-9)
+// reference's order of operations (materials.py:140-146) and numpy's
+// complex arithmetic: the imaginary part of the denominator is
+// (wg 2 pi c) / (wl 1e-9), the quotient is numpy's complex division and the
+// root the C library's csqrt, so the result is numpy's to the bit except
+// where numpy's w**2 (the C library's pow) rounds w^2 to the other
+// neighbour of the exact square, which w*w here does not.
 __device__ __forceinline__ cd drude_n(const EmuMaterial &m, double wl) {
   const double c = 299792458.0;
   const double wp = m.drude[0], wg = m.drude[1], eps_inf = m.drude[2];
   const double a = __dmul_rn(2.0 * 3.141592653589793, c), t = __dmul_rn(wl, 1e-9);
   const double w = __ddiv_rn(a, t);
   const cd den{__dmul_rn(w, w), __ddiv_rn(__dmul_rn(wg, a), t)};
-  const cd q = cdiv(cd{__dmul_rn(wp, wp), 0.0}, den);
-  return csqrt_p(cd{__dsub_rn(eps_inf, q.x), -q.y});
+  const cd q = cdiv_numpy(cd{__dmul_rn(wp, wp), 0.0}, den);
+  return csqrt_libc(cd{__dsub_rn(eps_inf, q.x), __dsub_rn(0.0, q.y)});
 }
 
 __global__ void material_kernel(MatArgs a) {
