@@ -377,3 +377,42 @@ EXTRA_SIGNATURES.extend([
     ('emu_pw_fields', C.c_int, [C.POINTER(EmuPwFields), vp]),
     ('emu_bloch_fields_plane', C.c_int, [C.POINTER(EmuBlochFieldsPlane), vp]),
 ])
+
+
+class EmuFemTopology(C.Structure):
+    _fields_ = [
+        ('npt', C.c_int), ('nel', C.c_int), ('h_x', vp), ('h_type_nod', vp), ('h_table_nod', vp),
+        ('h_dof', vp), ('h_shift', vp), ('h_ends', vp), ('h_row_ptr', vp), ('h_col', vp),
+        ('h_src_ptr', vp), ('h_src', vp), ('neq', C.c_int), ('nnz', C.c_int),
+    ]
+
+
+class EmuFemElements(C.Structure):
+    _fields_ = [
+        ('nel', C.c_int), ('n_types', C.c_int), ('d_x', vp), ('d_table_nod', vp), ('d_type_el', vp),
+        ('d_shift', vp), ('d_ends', vp), ('n_eff', EmuC128 * 8), ('k0', C.c_double),
+        ('bloch', C.c_double * 2), ('d_Ke', vp), ('d_Me', vp),
+    ]
+
+
+class EmuFemFields(C.Structure):
+    _fields_ = [
+        ('nel', C.c_int), ('neq', C.c_int), ('nval', C.c_int), ('d_x', vp), ('d_table_nod', vp),
+        ('d_shift', vp), ('d_ends', vp), ('d_dof', vp), ('bloch', C.c_double * 2), ('d_vec', vp),
+        ('ldv', C.c_int), ('d_sol', vp),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_fem_topology', C.c_int, [C.POINTER(EmuFemTopology)]),
+    ('emu_fem_element_matrices', C.c_int, [C.POINTER(EmuFemElements), vp]),
+    ('emu_fem_assemble', C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, vp]),
+    ('emu_fem_shifted_dense', C.c_int, [C.c_int, vp, vp, vp, vp, EmuC128, vp, C.c_int, vp]),
+    ('emu_fem_lu', C.c_int, [C.c_int, vp, C.c_int, vp, vp, vp]),
+    ('emu_fem_inverse', C.c_int, [C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]),
+    ('emu_fem_apply_op', C.c_int, [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int,
+                                   vp]),
+    ('emu_fem_mode_order', C.c_int, [C.c_int, vp, vp]),
+    ('emu_fem_fields_workspace_size', C.c_size_t, [C.POINTER(EmuFemFields)]),
+    ('emu_fem_nodal_fields', C.c_int, [C.POINTER(EmuFemFields), vp, C.c_size_t, vp]),
+])

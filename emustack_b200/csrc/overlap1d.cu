@@ -616,3 +616,17 @@ extern "C" int emu_mode_overlap_1d(const EmuNormalise1D *p, int full, void *stre
   emu::note_launch();
   return emu::check_launch();
 }
+
+// Order of Bloch modes after the eigen-solve (py_calc_modes.f:683): z_indexx
+// on the key -Re(beta^2) (z_indexx.f:26-28), 0-based.
+extern "C" int emu_fem_mode_order(int n, const emu_c128 *h_beta, int32_t *h_index) {
+  if (n < 0) return EMU_E_SHAPE;
+  if (n == 0) return EMU_OK;
+  if (!h_beta || !h_index) return EMU_E_ARG;
+  std::vector<double> key(n);
+  for (int i = 0; i < n; ++i) key[i] = -(h_beta[i].re * h_beta[i].re - h_beta[i].im * h_beta[i].im);
+  std::vector<int> idx;
+  if (!nr_indexx(n, key.data(), idx)) return EMU_E_SHAPE;
+  for (int i = 0; i < n; ++i) h_index[i] = idx[i];
+  return EMU_OK;
+}

@@ -1,0 +1,313 @@
+"""FEM Bloch modes of 2D nanostructured layers on the GPU (the reference's
+calc_modes_2d, backend/fortran/py_calc_modes.f:243-700, as
+backend/mode_calcs.py:268-381 calls it: E-field formulation, periodic cell).
+
+Per layer and Bloch vector:
+
+1. element matrices K_e, M_e on the device (``emu_fem_element_matrices``),
+   summed onto the CSR pattern in element order (``emu_fem_assemble``);
+2. the shifted matrix A = K - shift M, dense on the device, factored by a
+   blocked LU with FP64 tensor-core GEMM tiles (``emu_fem_lu``) and inverted
+   (``emu_fem_inverse``), so that every application of the operator is one
+   sparse product and one dense GEMM;
+3. the nval eigenvalues of OP = A^-1 M of largest modulus by a block
+   Krylov-Schur iteration (Stewart, SIAM J. Matrix Anal. Appl. 23, 2001, in
+   block form): OP applied to blocks of ``block`` vectors at once
+   (``emu_fem_apply_op``: sparse M times the block, then A^-1 times that),
+   the basis orthogonalised by two classical Gram-Schmidt passes and
+   Cholesky QR on the device; the small projected matrix (at most
+   ``max_basis`` square) is reduced on the host and the basis restarted with
+   its ordered Schur vectors, as ARPACK's reverse-communication loop does
+   its small dense steps on the host (valpr_umf_64.f:300-470 runs ARPACK's
+   implicitly restarted Arnoldi with one vector per step);
+4. beta^2 = 1/nu + shift with the reference's branch rule, the modes ranked by
+   -Re(beta^2) with the reference's quicksort (``emu_fem_mode_order``), and
+   the nodal fields of array_sol.f with its max-modulus normalisation
+   (``emu_fem_nodal_fields``).
+
+The dense factorisation is exact and simple but grows as neq^2 in memory and
+neq^3 in work (two 16 neq^2-byte matrices: 1.2 GB at the reference's
+518-element test mesh, 29 GB at 30 000 DOFs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_ptr
+
+
+class FemMesh(object):
+    """A P2 mesh of the unit cell with its DOF topology, resident on the GPU.
+
+    ``x`` [npt][2] in units of the period, ``type_nod`` [npt] (non-zero on
+    the cell boundary, the .mail files' node type), ``table_nod`` [nel][6]
+    1-based, ``type_el`` [nel] 1-based material index."""
+
+    def __init__(self, x, type_nod, table_nod, type_el, device=None):
+        self.x = np.ascontiguousarray(x, np.float64)
+        self.type_nod = np.ascontiguousarray(type_nod, np.int32)
+        self.table_nod = np.ascontiguousarray(table_nod, np.int64)
+        self.type_el = np.ascontiguousarray(type_el, np.int64)
+        npt, nel = len(self.x), len(self.table_nod)
+        self.npt, self.nel = npt, nel
+        dof = np.zeros((nel, 22), np.int32)
+        shift = np.zeros((nel, 14, 2), np.float64)
+        ends = np.zeros((nel, 3, 2), np.int8)
+        row_ptr = np.zeros(nel * 22 + 1, np.int32)
+        col = np.zeros(nel * 484, np.int32)
+        src_ptr = np.zeros(nel * 484 + 1, np.int32)
+        src = np.zeros(nel * 484, np.int32)
+        t = _lib.EmuFemTopology()
+        t.npt, t.nel = npt, nel
+        arrays = (self.x, self.type_nod, self.table_nod, dof, shift, ends, row_ptr, col, src_ptr, src)
+        (t.h_x, t.h_type_nod, t.h_table_nod, t.h_dof, t.h_shift, t.h_ends, t.h_row_ptr, t.h_col,
+         t.h_src_ptr, t.h_src) = [a.ctypes.data_as(C.c_void_p) for a in arrays]
+        check(lib().emu_fem_topology(C.byref(t)), 'emu_fem_topology')
+        self.neq, self.nnz = t.neq, t.nnz
+        self.dof, self.shift, self.ends = dof, shift, ends
+        dev = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+        self.device = dev
+        up = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+        self.d_x, self.d_table_nod, self.d_type_el = up(self.x), up(self.table_nod), up(self.type_el)
+        self.d_shift, self.d_ends, self.d_dof = up(shift), up(ends), up(dof)
+        self.d_row_ptr = up(row_ptr[:self.neq + 1])
+        self.d_col = up(col[:self.nnz])
+        self.d_src_ptr = up(src_ptr[:self.nnz + 1])
+        self.d_src = up(src)
+
+    @classmethod
+    def from_mail(cls, path, device=None):
+        """Read a .mail mesh (npt nel; npt rows 'k x y type'; nel rows 'k n1..n6 type')."""
+        with open(path) as f:
+            tok = f.read().split()
+        npt, nel = int(tok[0]), int(tok[1])
+        pts = np.array(tok[2:2 + 4 * npt], dtype=float).reshape(npt, 4)
+        p = 2 + 4 * npt
+        els = np.array(tok[p:p + 8 * nel], dtype=np.int64).reshape(nel, 8)
+        return cls(pts[:, 1:3], pts[:, 3].astype(np.int32), els[:, 1:7], els[:, 7], device)
+
+    @classmethod
+    def from_mesh(cls, mesh, device=None):
+        """From an emustack_b200.mesh.Mesh that carries its boundary node types."""
+        if getattr(mesh, 'type_nod', None) is None:
+            raise ValueError('the FEM solve needs the boundary node types of the mesh (Mesh.from_mail)')
+        return cls(mesh.x, mesh.type_nod, mesh.table_nod, mesh.type_el, device)
+
+
+def _c128(z):
+    z = complex(z)
+    return _lib.EmuC128(z.real, z.imag)
+
+
+def shift_of(n_effs, k0, bloch):
+    """The shift-and-invert centre of backend/mode_calcs.py:300-310 (not
+    hyperbolic): 1.1 max(Re n)^2 k0^2 - |k_parallel|^2."""
+    return 1.1 * np.real(np.asarray(n_effs)).max() ** 2 * k0 ** 2 - bloch[0] ** 2 - bloch[1] ** 2
+
+
+def beta_branch(b2):
+    """sqrt(beta^2) with the branch of py_calc_modes.f:664-674."""
+    b = np.sqrt(np.asarray(b2, complex))
+    flip = np.where(np.abs(b.imag) < 1e-8, b.real < 0, b.imag < 0)
+    return np.where(flip, -b, b)
+
+
+def mode_order(beta):
+    """0-based order of the modes by -Re(beta^2), the reference's quicksort."""
+    beta = np.ascontiguousarray(beta, np.complex128)
+    idx = np.zeros(len(beta), np.int32)
+    check(lib().emu_fem_mode_order(len(beta), beta.ctypes.data_as(C.c_void_p), idx.ctypes.data_as(C.c_void_p)),
+          'emu_fem_mode_order')
+    return idx
+
+
+class FemModeSolver(object):
+    """Shift-and-invert mode solve of one mesh (see the module docstring).
+
+    block: vectors per application of OP; max_basis: Krylov basis size before
+    a restart; tol: residual |OP y - nu y| / |nu| of the wanted Ritz pairs."""
+
+    def __init__(self, mesh, block=16, max_basis=None, keep=None, tol=1e-13, max_restarts=200, seed=20261204):
+        self.mesh = mesh
+        self.block, self.max_basis, self.keep = block, max_basis, keep
+        self.tol, self.max_restarts, self.seed = tol, max_restarts, seed
+        self.stats = {}
+
+    # -- operator -------------------------------------------------------
+    def factor(self, n_effs, k0, bloch, shift, stream=None):
+        """Assemble K, M for this Bloch vector and factor K - shift M."""
+        m = self.mesh
+        dev = m.device
+        s = stream_ptr(stream)
+        n_effs = np.asarray(n_effs, np.complex128).ravel()
+        n_types = int(m.type_el.max())
+        if len(n_effs) < n_types or n_types > 8:
+            raise ValueError('need the index of each of the mesh\'s %d material types' % n_types)
+        Ke = torch.empty((m.nel, 22, 22), dtype=torch.complex128, device=dev)
+        Me = torch.empty_like(Ke)
+        e = _lib.EmuFemElements()
+        e.nel, e.n_types = m.nel, n_types
+        e.d_x, e.d_table_nod, e.d_type_el = ptr(m.d_x), ptr(m.d_table_nod), ptr(m.d_type_el)
+        e.d_shift, e.d_ends = ptr(m.d_shift), ptr(m.d_ends)
+        for i in range(min(8, len(n_effs))):
+            e.n_eff[i] = _c128(n_effs[i])
+        e.k0 = float(k0)
+        e.bloch[0], e.bloch[1] = float(bloch[0]), float(bloch[1])
+        e.d_Ke, e.d_Me = ptr(Ke), ptr(Me)
+        check(lib().emu_fem_element_matrices(C.byref(e), s), 'emu_fem_element_matrices')
+        self.K = torch.empty(m.nnz, dtype=torch.complex128, device=dev)
+        self.M = torch.empty_like(self.K)
+        check(lib().emu_fem_assemble(m.nnz, ptr(m.d_src_ptr), ptr(m.d_src), ptr(Ke), ptr(Me), ptr(self.K),
+                                     ptr(self.M), s), 'emu_fem_assemble')
+        del Ke, Me
+        n = m.neq
+        self.A = torch.empty((n, n), dtype=torch.complex128, device=dev)
+        check(lib().emu_fem_shifted_dense(n, ptr(m.d_row_ptr), ptr(m.d_col), ptr(self.K), ptr(self.M),
+                                          _c128(shift), ptr(self.A), n, s), 'emu_fem_shifted_dense')
+        self.ipiv = torch.empty(n, dtype=torch.int32, device=dev)
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+        check(lib().emu_fem_lu(n, ptr(self.A), n, ptr(self.ipiv), ptr(info), s), 'emu_fem_lu')
+        if int(info.item()) != 0:
+            raise _lib.EmuError(_lib.EMU_E_SINGULAR, 'emu_fem_lu (K - shift M is singular)')
+        self.Ainv = torch.empty((n, n), dtype=torch.complex128, device=dev)
+        check(lib().emu_fem_inverse(n, ptr(self.A), n, ptr(self.ipiv), ptr(self.Ainv), n, s), 'emu_fem_inverse')
+        del self.A
+
+    def apply(self, X, Y, stream=None):
+        """Y = (K - shift M)^-1 M X for a column block X of a row-major
+        [n][ld] tensor (X and Y may be strided views with unit column stride)."""
+        n = self.mesh.neq
+        nrhs = X.shape[1]
+        T = getattr(self, '_T', None)
+        if T is None or T.numel() < n * nrhs:
+            T = self._T = torch.empty(n * nrhs, dtype=torch.complex128, device=X.device)
+        check(lib().emu_fem_apply_op(n, nrhs, ptr(self.Ainv), n, ptr(self.mesh.d_row_ptr), ptr(self.mesh.d_col),
+                                     ptr(self.M), ptr(X), X.stride(0), ptr(T), ptr(Y), Y.stride(0),
+                                     stream_ptr(stream)), 'emu_fem_apply_op')
+
+    # -- block Krylov-Schur ---------------------------------------------
+    @staticmethod
+    def _cholqr(W):
+        """W = Q R with Q orthonormal (two Cholesky QR passes); returns
+        (Q, R) or (None, None) when W is numerically rank deficient."""
+        Rt = None
+        for _ in range(2):
+            G = W.conj().T @ W
+            L, info = torch.linalg.cholesky_ex(G)
+            if int(info.item()) != 0:
+                return None, None
+            R = L.conj().T
+            W = torch.linalg.solve_triangular(R, W, upper=True, left=False)
+            Rt = R if Rt is None else R @ Rt
+        return W, Rt
+
+    def eigs(self, nval, stream=None):
+        """The nval eigenpairs of OP of largest |nu|: (nu [nval] numpy,
+        eigenvectors [n][nval] device tensor)."""
+        import scipy.linalg as sl
+        n = self.mesh.neq
+        dev = self.mesh.device
+        b = min(self.block, n)
+        mmax = self.max_basis or max(2 * nval + nval // 2 + 3, nval + 4 * b)
+        mmax = int(min(-(-mmax // b) * b, n - b))
+        keep = self.keep or min(mmax - b, nval + max(b, nval // 2))
+        if nval + 1 > keep or keep + b > mmax:
+            raise ValueError('basis too small for %d modes (n = %d)' % (nval, n))
+        gen = torch.Generator(device='cpu').manual_seed(self.seed)
+        V = torch.zeros((n, mmax + b), dtype=torch.complex128, device=dev)
+        X0 = torch.complex(torch.randn(n, b, generator=gen, dtype=torch.float64),
+                           torch.randn(n, b, generator=gen, dtype=torch.float64)).to(dev)
+        Q0, _ = self._cholqr(X0)
+        V[:, :b] = Q0
+        H = np.zeros((mmax + b, mmax), complex)
+        W = torch.empty((n, b), dtype=torch.complex128, device=dev)
+        m = 0
+        applies = 0
+        for restart in range(self.max_restarts):
+            while m + b <= mmax:
+                self.apply(V[:, m:m + b], W, stream)
+                applies += 1
+                Vm = V[:, :m + b]
+                Cc = Vm.conj().T @ W
+                W -= Vm @ Cc
+                C2 = Vm.conj().T @ W
+                W -= Vm @ C2
+                Cc += C2
+                Q, R = self._cholqr(W)
+                if Q is None:  # the Krylov space closed: continue with fresh directions
+                    Xr = torch.complex(torch.randn(n, b, generator=gen, dtype=torch.float64),
+                                       torch.randn(n, b, generator=gen, dtype=torch.float64)).to(dev)
+                    Xr -= Vm @ (Vm.conj().T @ Xr)
+                    Xr -= Vm @ (Vm.conj().T @ Xr)
+                    Q, _ = self._cholqr(Xr)
+                    R = torch.zeros((b, b), dtype=torch.complex128, device=dev)
+                H[:m + b, m:m + b] = Cc.cpu().numpy()
+                H[m + b:m + 2 * b, m:m + b] = R.cpu().numpy()
+                V[:, m + b:m + 2 * b] = Q
+                m += b
+            Hm = H[:m, :m]
+            th, Z = np.linalg.eig(Hm)
+            o = np.argsort(-np.abs(th), kind='stable')
+            th, Z = th[o], Z[:, o]
+            res = np.linalg.norm(H[m:m + b, :m] @ Z[:, :nval], axis=0) / np.abs(th[:nval])
+            if res.max() < self.tol:
+                Zd = torch.as_tensor(np.ascontiguousarray(Z[:, :nval])).to(dev)
+                Y = V[:, :m] @ Zd
+                self.stats = {'applies': applies, 'restarts': restart, 'basis': mmax, 'block': b,
+                              'residual': float(res.max())}
+                return th[:nval], Y
+            thr = np.abs(th[keep - 1]) * (1 - 1e-12)
+            T, Qs, k = sl.schur(Hm, output='complex', sort=lambda z: abs(z) >= thr)
+            k = int(min(k, mmax - b))
+            Qk = torch.as_tensor(np.ascontiguousarray(Qs[:, :k])).to(dev)
+            tail = V[:, m:m + b].clone()
+            V[:, :k] = V[:, :m] @ Qk
+            V[:, k:k + b] = tail
+            Hn = np.zeros_like(H)
+            Hn[:k, :k] = T[:k, :k]
+            Hn[k:k + b, :k] = H[m:m + b, :m] @ Qs[:, :k]
+            H = Hn
+            m = k
+        raise RuntimeError('FEM eigen-solve: no convergence in %d restarts (residual %.1e)'
+                           % (self.max_restarts, res.max()))
+
+    # -- the solve of calc_modes_2d -------------------------------------
+    def solve(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None):
+        """beta [nval] (numpy, sorted) and sol [nel][nval][13][3] (device) for
+        the Bloch vector ``bloch`` (k_parallel * period)."""
+        k0 = 2 * np.pi / wl_norm
+        bloch = np.asarray(bloch, np.float64)
+        if shift is None:
+            shift = shift_of(n_effs, k0, bloch)
+        self.factor(n_effs, k0, bloch, shift, stream)
+        nu, Y = self.eigs(nval, stream)
+        del self.Ainv
+        beta = beta_branch(1.0 / nu + shift)
+        order = mode_order(beta)
+        beta = beta[order]
+        Y = Y[:, torch.as_tensor(order.astype(np.int64)).to(Y.device)].contiguous()
+        m = self.mesh
+        sol = torch.empty((m.nel, nval, 13, 3), dtype=torch.complex128, device=m.device)
+        f = _lib.EmuFemFields()
+        f.nel, f.neq, f.nval = m.nel, m.neq, nval
+        f.d_x, f.d_table_nod, f.d_shift, f.d_ends, f.d_dof = (ptr(m.d_x), ptr(m.d_table_nod), ptr(m.d_shift),
+                                                              ptr(m.d_ends), ptr(m.d_dof))
+        f.bloch[0], f.bloch[1] = float(bloch[0]), float(bloch[1])
+        f.d_vec, f.ldv, f.d_sol = ptr(Y), nval, ptr(sol)
+        ws_bytes = lib().emu_fem_fields_workspace_size(C.byref(f))
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=m.device)
+        check(lib().emu_fem_nodal_fields(C.byref(f), ptr(ws), ws_bytes, stream_ptr(stream)), 'emu_fem_nodal_fields')
+        return beta, sol
+
+    def solve_pair(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None):
+        """The prime modes (Bloch vector ``bloch``) and the adjoint modes
+        (-bloch) as calc_modes_2d solves both (py_calc_modes.f:604-616):
+        beta1, sol1, beta2, sol2."""
+        bloch = np.asarray(bloch, np.float64)
+        b1, s1 = self.solve(n_effs, wl_norm, bloch, nval, shift, stream)
+        b2, s2 = self.solve(n_effs, wl_norm, -bloch, nval, shift, stream)
+        return b1, s1, b2, s2

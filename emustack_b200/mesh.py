@@ -14,8 +14,11 @@ import numpy as np
 
 
 class Mesh(object):
-    def __init__(self, x, table_nod, type_el):
+    def __init__(self, x, table_nod, type_el, type_nod=None):
         self.x = np.ascontiguousarray(x, np.float64)
+        # node types of the .mail file: non-zero on the cell boundary (the FEM
+        # solve pairs those nodes periodically)
+        self.type_nod = None if type_nod is None else np.ascontiguousarray(type_nod, np.int32)
         self.table_nod = np.ascontiguousarray(table_nod, np.int64)
         self.type_el = np.ascontiguousarray(type_el, np.int64)
         if self.table_nod.ndim != 2 or self.table_nod.shape[1] != 6:
@@ -41,7 +44,7 @@ class Mesh(object):
         pts = np.array(tok[p:p + 4 * npt], dtype=float).reshape(npt, 4)
         p += 4 * npt
         els = np.array(tok[p:p + 8 * nel], dtype=np.int64).reshape(nel, 8)
-        return cls(pts[:, 1:3], els[:, 1:7], els[:, 7])
+        return cls(pts[:, 1:3], els[:, 1:7], els[:, 7], pts[:, 3].astype(np.int32))
 
     def to_device(self, device='cuda'):
         import torch

@@ -204,8 +204,8 @@ class Anallo(Modes):
 class Simmo(Modes):
     """Bloch modes of a nanostructured layer (backend/mode_calcs.py:255-413).
 
-    The FEM eigen-solve stays outside this package; ``attach_modes`` takes
-    its results.
+    ``calc_modes`` runs the FEM eigen-solve on the GPU (2D_array layers with
+    a .mail mesh); ``attach_modes`` takes modes computed elsewhere.
     """
 
     def __init__(self, structure, light):
@@ -215,10 +215,58 @@ class Simmo(Modes):
         self.prop_consts = None
         self.mode_pol = None
 
+    def calc_modes(self, num_BMs=None, fem_block=16):
+        """Bloch modes of the layer by the FEM solve on the GPU
+        (emustack_b200.fem), then J and J_dag, as Simmo.calc_modes does with
+        its Fortran solver (backend/mode_calcs.py:268-386): indices of the
+        mesh's materials (background, inclusion_a, ...; real when loss is
+        False), num_BMs = 2 Npw + 20 by default, the shift 1.1 max(Re n)^2 k0^2
+        - |k_parallel|^2, prime and adjoint modes.  Needs a 2D_array
+        structure whose ``mesh`` carries its boundary node types
+        (Mesh.from_mail)."""
+        from .fem import FemMesh, FemModeSolver
+        st = self.structure
+        if getattr(st, 'periodicity', '2D_array') != '2D_array':
+            raise ValueError('the GPU FEM solve covers 2D_array layers')
+        mesh = getattr(st, 'mesh', None)
+        if mesh is None:
+            raise ValueError('the FEM solve needs the structure\'s mesh')
+        fm = getattr(st, '_fem_mesh', None)
+        if fm is None or fm.mesh_id != id(mesh):
+            fm = FemMesh.from_mesh(mesh)
+            fm.mesh_id = id(mesh)
+            st._fem_mesh = fm
+        wl = self.light.wl_nm
+        n_types = int(np.max(mesh.type_el))
+        names = ('background', 'inclusion_a', 'inclusion_b', 'inclusion_c', 'inclusion_d', 'inclusion_e')
+        mats = [getattr(st, k, None) for k in names[:n_types]]
+        if any(m is None for m in mats):
+            raise ValueError('the mesh has %d material types; the structure defines fewer' % n_types)
+        n_effs = np.array([np.asarray(m.n(wl)).item() for m in mats], dtype=np.complex128)
+        if st.loss is False:
+            n_effs = n_effs.real.astype(np.complex128)
+        self.n_effs = n_effs
+        pxs, pys = self.calc_2d_grating_orders(self.max_order_PWs)
+        num_pw_per_pol = pxs.size
+        nbm = num_pw_per_pol * 2 + 20 if num_BMs is None else int(num_BMs)
+        if nbm <= num_pw_per_pol * 2:
+            raise ValueError('You must include at least as many BMs as PWs. \nCurrently you have %i BMs < '
+                             '%i PWs.' % (nbm, num_pw_per_pol * 2))
+        k0 = 2 * np.pi * self.air_ref().n() / self.wl_norm()
+        kp = self.k_pll_norm()
+        shift = 1.1 * np.real(n_effs).max() ** 2 * k0 ** 2 - kp[0] ** 2 - kp[1] ** 2
+        solver = FemModeSolver(fm, block=fem_block)
+        b1, s1, b2, s2 = solver.solve_pair(n_effs, self.wl_norm(), kp, nbm, shift=float(np.real(shift)))
+        self.fem_stats = solver.stats
+        self.attach_modes(num_BMs=nbm, k_z=b1,
+                          fields={'sol1': s1, 'sol2': s2, 'beta1': b1, 'mesh': mesh,
+                                  'pp': np.ones(n_types, np.complex128)})
+        return self
+
     def attach_modes(self, num_BMs=None, k_z=None, J=None, J_dag=None, fields=None):
         if k_z is None:
             raise ValueError('Simmo needs the Bloch-mode propagation constants k_z '
-                             '(the FEM mode solve is not part of emustack_b200)')
+                             '(or calc_modes, which solves for them)')
         self.k_z = np.asarray(k_z, dtype=np.complex128)
         self.num_BMs = len(self.k_z) if num_BMs is None else num_BMs
         if J is not None:

@@ -109,8 +109,9 @@ class NanoStruct(object):
             self.world_1d = world_1d
 
     def calc_modes(self, light, num_BMs=None, k_z=None, J=None, J_dag=None, fields=None):
-        """Attach Bloch modes computed elsewhere (the FEM solve is not part
-        of this package) and return a ``Simmo``.
+        """Bloch modes of the layer as a ``Simmo``: with no modes given, the
+        FEM solve on the GPU (2D_array layers whose ``mesh`` came from a .mail
+        file, Simmo.calc_modes); else the modes given are attached.
 
         Either ``k_z`` (M,), ``J`` (P, M) and ``J_dag`` (M, P) -- J already
         divided by the area ratio as in backend/mode_calcs.py:384-386 -- or
@@ -118,5 +119,7 @@ class NanoStruct(object):
         ``self.mesh``; J and J_dag are then computed on the GPU.
         """
         sim = Simmo(self, light)
+        if k_z is None and J is None and fields is None:
+            return sim.calc_modes(num_BMs)
         sim.attach_modes(num_BMs=num_BMs, k_z=k_z, J=J, J_dag=J_dag, fields=fields)
         return sim

@@ -214,6 +214,13 @@ def mode_reorder(dmesh, pp, k0, beta1, sol1, sol2):
     return perm, diag, scale, warn
 
 
+def _on_device(a, dev):
+    """complex128 contiguous tensor on ``dev`` from a numpy array or tensor."""
+    if isinstance(a, torch.Tensor):
+        return a.to(device=dev, dtype=torch.complex128).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a, np.complex128), device=dev)
+
+
 def overlap_from_fields(simmo, fields):
     """J / area_norm and J_dag of a Simmo from its P2 mode fields.
 
@@ -230,8 +237,8 @@ def overlap_from_fields(simmo, fields):
         raise ValueError('overlap integrals need the mesh of the mode fields')
     dev = torch.device('cuda', torch.cuda.current_device())
     dm = fields.get('_device_mesh') or DeviceMesh(mesh, dev)
-    sol1 = torch.as_tensor(np.ascontiguousarray(fields['sol1'], np.complex128), device=dev).unsqueeze(0)
-    sol2 = torch.as_tensor(np.ascontiguousarray(fields['sol2'], np.complex128), device=dev).unsqueeze(0)
+    sol1 = _on_device(fields['sol1'], dev).unsqueeze(0)
+    sol2 = _on_device(fields['sol2'], dev).unsqueeze(0)
     M = sol1.shape[2]
     beta1 = torch.as_tensor(np.asarray(fields.get('beta1', simmo.k_z), np.complex128).reshape(1, M), device=dev)
     n_types = int(mesh.type_el.max())

@@ -807,6 +807,116 @@ int emu_tc_gemm_tf32x3(int m, int n, int k, const double *d_A, const double *d_B
  * counterpart (it has no GPU path). */
 int emu_probe_fp64(int blocks, int threads, int iters, double *d_out, void *stream);
 
+/* ------------------------------------- f1: FEM Bloch modes of a 2D layer
+ * The mode solve of calc_modes_2d (backend/fortran/py_calc_modes.f:243-700)
+ * for the E-field formulation with periodic boundaries, as the reference
+ * runs it (backend/mode_calcs.py:268-381): the mixed element of asmbly.f
+ * (per triangle a face and 3 edges with 3 transverse DOFs each, basis of
+ * basis_ls.f / basis_vec.f, and 10 P3 nodes with one E_z DOF), Bloch phase
+ * factors on periodic images, the generalised problem K x = beta^2 M x
+ * solved by shift and invert, and the nodal fields of array_sol.f.
+ *
+ * emu_fem_topology (host): pairs the periodic boundary nodes as
+ * periodic_node.f does (lowest index of a class is its origin; pairs differ
+ * by a lattice vector ix a1 + iy a2, |ix|, |iy| <= 1, within 1e-6 in the
+ * 1-norm), numbers the DOFs (an entity and its periodic images share
+ * them), and builds the CSR pattern of K and M (row = trial DOF, column =
+ * test DOF, columns ascending) with, for every CSR entry, the element-matrix
+ * entries it sums in element order (src: flat indices e*484 + a*22 + b).
+ * Outputs are caller-allocated to the bounds given; neq and nnz are set.
+ * Returns EMU_E_ARG for a boundary node without a periodic image or an edge
+ * whose ends are images of each other. */
+typedef struct {
+  int npt, nel;
+  const double *h_x;          /* [npt][2], the unit cell in units of the period */
+  const int32_t *h_type_nod;  /* [npt], non-zero on the cell boundary           */
+  const int64_t *h_table_nod; /* [nel][6], 1-based (vertices, then mid-edge
+                                 nodes of edges 1-2, 2-3, 1-3)                  */
+  int32_t *h_dof;             /* out [nel][22]: 12 transverse, 10 E_z           */
+  double *h_shift;            /* out [nel][14][2]: lattice shift of each entity
+                                 instance (face, 3 edges, 10 P3 nodes)          */
+  int8_t *h_ends;             /* out [nel][3][2]: local vertices of each edge,
+                                 the lower mapped node number first             */
+  int32_t *h_row_ptr;         /* out [neq + 1], bound nel*22 + 1                */
+  int32_t *h_col;             /* out [nnz], bound nel*484                       */
+  int32_t *h_src_ptr;         /* out [nnz + 1], bound nel*484 + 1               */
+  int32_t *h_src;             /* out [nel*484]                                  */
+  int neq, nnz;               /* out */
+} EmuFemTopology;
+
+int emu_fem_topology(EmuFemTopology *t);
+
+/* Element matrices K_e, M_e [nel][22][22] (trial row, test column) of
+ * asmbly.f:130-320 with pp = 1, qq = n^2 k0^2 per material type, each entry
+ * times val_exp(test) conj(val_exp(trial)), val_exp = exp(i bloch . shift),
+ * 16-point rule (quad_triangle.f), affine element maps (curved_elem_tri.f
+ * makes every element straight).  n_types <= 8. */
+typedef struct {
+  int nel, n_types;
+  const double *d_x;            /* [npt][2]                     */
+  const int64_t *d_table_nod;   /* [nel][6], 1-based            */
+  const int64_t *d_type_el;     /* [nel], 1-based               */
+  const double *d_shift;        /* [nel][14][2] (emu_fem_topology) */
+  const int8_t *d_ends;         /* [nel][3][2]                  */
+  emu_c128 n_eff[8];            /* index of each material type  */
+  double k0;                    /* 2 pi / (wl / period)         */
+  double bloch[2];              /* k_parallel * period          */
+  emu_c128 *d_Ke, *d_Me;        /* out [nel][22][22]            */
+} EmuFemElements;
+
+int emu_fem_element_matrices(const EmuFemElements *p, void *stream);
+
+/* Global K, M values on the CSR pattern: each entry the sum of its element
+ * entries in element order (deterministic).  Then, optionally, the dense
+ * shifted matrix A = K - shift M (row-major n x n, lda >= n; every other
+ * entry set to zero), which emu_fem_lu factors in place (partial pivoting;
+ * panels of the dense interface path's LU inside outer blocks of 256
+ * columns; ipiv 0-based, info 0 or the first zero pivot + 1) and
+ * emu_fem_inverse turns into A^-1 (a separate n x n buffer). */
+int emu_fem_assemble(int nnz, const int32_t *d_src_ptr, const int32_t *d_src, const emu_c128 *d_Ke,
+                     const emu_c128 *d_Me, emu_c128 *d_K, emu_c128 *d_M, void *stream);
+int emu_fem_shifted_dense(int neq, const int32_t *d_row_ptr, const int32_t *d_col, const emu_c128 *d_K,
+                          const emu_c128 *d_M, emu_c128 shift, emu_c128 *d_A, int lda, void *stream);
+int emu_fem_lu(int n, emu_c128 *d_A, int lda, int32_t *d_ipiv, int32_t *d_info, void *stream);
+int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv, emu_c128 *d_Ainv, int ldi,
+                    void *stream);
+
+/* Y = (K - shift M)^-1 M X for a block of nrhs vectors (X [n][ldx], Y
+ * [n][ldy], row-major, vector r in column r; T [n][nrhs] scratch): the
+ * operator of the shift-and-invert eigen-solve (valpr_umf_64.f:314-383,
+ * which applies it one vector at a time through UMFPACK's solves), here a
+ * sparse product with M and one dense FP64 tensor-core GEMM with A^-1. */
+int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, const int32_t *d_row_ptr,
+                     const int32_t *d_col, const emu_c128 *d_M, const emu_c128 *d_X, int ldx, emu_c128 *d_T,
+                     emu_c128 *d_Y, int ldy, void *stream);
+
+/* Nodal fields of array_sol.f:88-300: sol [nel][nval][13][3] (E_x, E_y,
+ * E_z at the six P2 nodes, E_z interpolated from the P3 values; E_z at P3
+ * nodes 4-10 in entries 6-12) from eigenvectors vec [neq][ldv] (mode m in
+ * column m, already in output order), each mode divided by its first
+ * largest-modulus P2-node component (elements, then nodes, then
+ * components).  Workspace: emu_fem_fields_workspace_size. */
+typedef struct {
+  int nel, neq, nval;
+  const double *d_x;
+  const int64_t *d_table_nod;
+  const double *d_shift;
+  const int8_t *d_ends;
+  const int32_t *d_dof;
+  double bloch[2];
+  const emu_c128 *d_vec;
+  int ldv;
+  emu_c128 *d_sol;              /* out [nel][nval][13][3] */
+} EmuFemFields;
+
+/* Order of the modes (host): z_indexx.f on the key -Re(beta^2) as
+ * py_calc_modes.f:683 ranks them, ties where that quicksort puts them;
+ * h_index 0-based. */
+int emu_fem_mode_order(int n, const emu_c128 *h_beta, int32_t *h_index);
+
+size_t emu_fem_fields_workspace_size(const EmuFemFields *p);
+int emu_fem_nodal_fields(const EmuFemFields *p, void *d_workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,57 @@
+"""Host side of the FEM mode solve (emu_fem_topology, no GPU needed): the
+periodic pairing, DOF numbering, edge orientation and CSR pattern against
+the oracle's restatement of periodic_node.f / periodic_cond.f / basis_ls.f,
+on the reference's own test meshes; and the CSR gather of element entries
+reproducing the oracle's assembled K and M."""
+import os
+
+import numpy as np
+import pytest
+
+from emustack_b200.fem import FemMesh, mode_order
+from oracle import fem_oracle as F
+from oracle.overlap1d_oracle import z_indexx
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+@pytest.mark.parametrize('name', ['4testing-600_120.mail', '4testing-940_266_sq.mail'])
+def test_topology_matches_the_oracle(name):
+    path = os.path.join(GOLD, name)
+    m = FemMesh.from_mail(path, device='cpu')
+    x, tn, tab, tel = F.read_mail(path)
+    topo = F.Topology(x, tn, tab)
+    assert m.neq == topo.neq
+    np.testing.assert_array_equal(m.dof, topo.dof)
+    np.testing.assert_array_equal(m.ends, topo.ends)
+    np.testing.assert_allclose(m.shift, topo.shift, rtol=0, atol=1e-12)
+    # every boundary node has an image a lattice vector away: shifts are 0 or +-1
+    assert set(np.unique(np.round(m.shift, 9))) <= {-1.0, 0.0, 1.0}
+
+
+def test_csr_gather_reproduces_the_oracle_assembly():
+    path = os.path.join(GOLD, '4testing-600_120.mail')
+    m = FemMesh.from_mail(path, device='cpu')
+    x, tn, tab, tel = F.read_mail(path)
+    topo = F.Topology(x, tn, tab)
+    K, M = F.element_matrices(topo, x, [1.0, 3.5 + 0.01j], tel, 2 * np.pi / 0.9, [0.3, -0.2])
+    Kg, Mg = F.assemble(topo, K, M)
+    sp, src = m.d_src_ptr.numpy(), m.d_src.numpy()
+    rows = np.repeat(np.arange(m.neq, dtype=np.int64), np.diff(m.d_row_ptr.numpy()))
+    cols = np.array(m.d_col.numpy(), dtype=np.int64)
+    Kf, Mf = K.ravel(), M.ravel()
+    Kc = np.add.reduceat(Kf[src], sp[:-1])
+    Mc = np.add.reduceat(Mf[src], sp[:-1])
+    Kd, Md = Kg.tocsr(), Mg.tocsr()
+    np.testing.assert_allclose(Kc, np.asarray(Kd[rows, cols]).ravel(), rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(Mc, np.asarray(Md[rows, cols]).ravel(), rtol=1e-12, atol=1e-12)
+    Kd.eliminate_zeros()
+    assert len(cols) >= Kd.nnz
+
+
+def test_mode_order_is_the_reference_quicksort():
+    rng = np.random.default_rng(3)
+    beta = rng.normal(size=50) + 1j * rng.normal(size=50) * 0.1
+    beta[7] = beta[3]          # a tie
+    beta[20] = -beta[11]       # equal beta^2
+    np.testing.assert_array_equal(mode_order(beta), z_indexx(-np.real(beta * beta)))
