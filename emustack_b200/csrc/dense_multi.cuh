@@ -304,11 +304,11 @@ __global__ void laswp_outside_kernel(cd *A_, long long sA, int lda, int n, int j
 // keep all clusters of the batch resident at once; a batch that already
 // fills the GPU with one wide CTA per matrix keeps panel_kernel.
 inline bool panel_cluster(cd *A, long long sA, int lda, int n, int j0, int jb, int *ipiv, long long sip,
-                          int *info, int code, int batch, cudaStream_t s) {
+                          int *info, int code, int batch, cudaStream_t s, int max_cs = kPanelMaxCS) {
   const size_t row_bytes = (size_t)kNB * sizeof(cd);
   const long long nr = n - j0;
   int cs = 0;
-  for (int c = kPanelMaxCS; c >= 1; --c) {
+  for (int c = max_cs; c >= 1; --c) {
     const size_t smem = (size_t)((nr + c - 1) / c) * row_bytes;
     if (smem > kPanelMaxSmem) break;
     const long long per_sm = std::min<long long>(2, (long long)(228 * 1024 / (smem + 2048)));
@@ -318,6 +318,11 @@ inline bool panel_cluster(cd *A, long long sA, int lda, int n, int j0, int jb, i
     }
   }
   if (cs < 2) return false;
+  // clusters above 8 CTAs are a non-portable size (the launch fails, and the
+  // caller falls back to panel_kernel, where the GPU cannot host them)
+  if (cs > 8 &&
+      cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return false;
   const size_t smem = (size_t)((nr + cs - 1) / cs) * row_bytes;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=

@@ -703,7 +703,7 @@ void getrf_blocked(int n, cd *A, int lda, int *ipiv, int *info, cudaStream_t s) 
     const int JB = std::min(kOuterNB, n - J);
     for (int j0 = J; j0 < J + JB; j0 += kNB) {
       const int jb = std::min(kNB, J + JB - j0);
-      if (!panel_cluster(A, 0, lda, n, j0, jb, ipiv, 0, info, 0, 1, s)) {
+      if (!panel_cluster(A, 0, lda, n, j0, jb, ipiv, 0, info, 0, 1, s, 16)) {
         cudaGetLastError();
         panel_kernel<<<1, kPanelThreads, 0, s>>>(A, 0, lda, n, j0, jb, ipiv, 0, info, 0);
         emu::note_launch();
@@ -729,6 +729,66 @@ void getrf_blocked(int n, cd *A, int lda, int *ipiv, int *info, cudaStream_t s) 
     }
     bgemm(rest, rest, JB, cd{-1.0, 0.0}, A + (size_t)c1 * lda + J, 0, lda, A + (size_t)J * lda + c1, 0, lda,
           cd{1.0, 0.0}, A + (size_t)c1 * lda + c1, 0, lda, 1, s);
+  }
+}
+
+// Y = A^-1 T for a narrow block T [n][nrhs]: A^-1 streamed once per 16
+// vectors, two rows per warp, T staged in shared memory 128 rows at a time
+// (column-major there, so the lanes' reads are consecutive), lanes split
+// the k range and a butterfly sums each output.
+constexpr int kSkRows = 16, kSkK = 128, kSkCols = 16;
+
+__global__ void __launch_bounds__(256) fem_skinny_kernel(int n, int nrhs, const cd *A, int lda, const cd *T, int ldt,
+                                                         cd *Y, int ldy) {
+  __shared__ cd Ts[kSkCols][kSkK];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = blockIdx.x * kSkRows + warp * 2;
+  for (int c0 = 0; c0 < nrhs; c0 += kSkCols) {
+    const int nc = min(kSkCols, nrhs - c0);
+    cd acc0[kSkCols], acc1[kSkCols];
+#pragma unroll
+    for (int c = 0; c < kSkCols; ++c) acc0[c] = acc1[c] = cd{0.0, 0.0};
+    for (int k0 = 0; k0 < n; k0 += kSkK) {
+      // the lane's A entries of this chunk in flight while T is staged
+      cd a0[kSkK / 32], a1[kSkK / 32];
+#pragma unroll
+      for (int j = 0; j < kSkK / 32; ++j) {
+        const int k = k0 + lane + 32 * j;
+        a0[j] = (r0 < n && k < n) ? A[(size_t)r0 * lda + k] : cd{0.0, 0.0};
+        a1[j] = (r0 + 1 < n && k < n) ? A[(size_t)(r0 + 1) * lda + k] : cd{0.0, 0.0};
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < kSkK * kSkCols; e += blockDim.x) {
+        const int c = e / kSkK, kk = e % kSkK;
+        Ts[c][kk] = (k0 + kk < n && c < nc) ? T[(size_t)(k0 + kk) * ldt + c0 + c] : cd{0.0, 0.0};
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < kSkK / 32; ++j) {
+        const int kk = lane + 32 * j;
+#pragma unroll
+        for (int c = 0; c < kSkCols; ++c) {
+          const cd t = Ts[c][kk];
+          acc0[c].x += a0[j].x * t.x - a0[j].y * t.y;
+          acc0[c].y += a0[j].x * t.y + a0[j].y * t.x;
+          acc1[c].x += a1[j].x * t.x - a1[j].y * t.y;
+          acc1[c].y += a1[j].x * t.y + a1[j].y * t.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kSkCols; ++c) {
+      for (int o = 16; o > 0; o >>= 1) {
+        acc0[c].x += __shfl_xor_sync(0xffffffffu, acc0[c].x, o);
+        acc0[c].y += __shfl_xor_sync(0xffffffffu, acc0[c].y, o);
+        acc1[c].x += __shfl_xor_sync(0xffffffffu, acc1[c].x, o);
+        acc1[c].y += __shfl_xor_sync(0xffffffffu, acc1[c].y, o);
+      }
+      if (lane == c && c < nc) {
+        if (r0 < n) Y[(size_t)r0 * ldy + c0 + c] = acc0[c];
+        if (r0 + 1 < n) Y[(size_t)(r0 + 1) * ldy + c0 + c] = acc1[c];
+      }
+    }
   }
 }
 
@@ -774,8 +834,9 @@ extern "C" int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi
   fem_spmm_kernel<<<grid_for((long long)n * 32, 256), 256, 0, s>>>(n, nrhs, d_row_ptr, d_col, (const cd *)d_M,
                                                                    (const cd *)d_X, ldx, (cd *)d_T, nrhs);
   emu::note_launch();
-  bgemm(n, nrhs, n, cd{1.0, 0.0}, (const cd *)d_Ainv, 0, ldi, (const cd *)d_T, 0, nrhs, cd{0.0, 0.0}, (cd *)d_Y, 0,
-        ldy, 1, s);
+  fem_skinny_kernel<<<(n + kSkRows - 1) / kSkRows, 256, 0, s>>>(n, nrhs, (const cd *)d_Ainv, ldi, (const cd *)d_T,
+                                                                 nrhs, (cd *)d_Y, ldy);
+  emu::note_launch();
   return emu::check_launch();
 }
 

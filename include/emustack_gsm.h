@@ -885,7 +885,7 @@ int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv,
  * [n][ldy], row-major, vector r in column r; T [n][nrhs] scratch): the
  * operator of the shift-and-invert eigen-solve (valpr_umf_64.f:314-383,
  * which applies it one vector at a time through UMFPACK's solves), here a
- * sparse product with M and one dense FP64 tensor-core GEMM with A^-1. */
+ * sparse product with M and one pass over A^-1 per 16 vectors. */
 int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, const int32_t *d_row_ptr,
                      const int32_t *d_col, const emu_c128 *d_M, const emu_c128 *d_X, int ldx, emu_c128 *d_T,
                      emu_c128 *d_Y, int ldy, void *stream);
