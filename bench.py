@@ -1062,6 +1062,96 @@ def fields_line(steps, nel=20000):
     return {'workload': 'fields', 'pw_fields': pw, 'bloch_fields_plane': bl}
 
 
+def fem_line(steps):
+    """FEM Bloch-mode solve of one nanostructured layer on the GPU (row f1).
+
+    Workload: the reference's own test mesh 4testing-600_120.mail (518 P2
+    triangles, 6 216 DOFs; a 120 nm Si_c wire in air at period 600 nm), the
+    inputs the reference passes to its solver for test case 1 at 500 nm (40
+    Bloch modes, tests/golden/fem.npz): one layer = the prime and the adjoint
+    solve (element matrices, assembly, LU and inverse of K - shift M, block
+    Krylov-Schur, nodal fields), timed host to host (the projected
+    eigenproblem is reduced on the host).  CPU baseline: the oracle's
+    restatement (scipy ARPACK on a SuperLU factorisation) on one solve."""
+    import torch
+    from emustack_b200.fem import FemMesh, FemModeSolver
+    from emustack_b200.probe import fp64_peak_tflops
+    from oracle import fem_oracle as F
+    gold = os.path.join(ROOT, 'tests', 'golden')
+    mail = os.path.join(gold, '4testing-600_120.mail')
+    fx = np.load(os.path.join(gold, 'fem.npz'))
+    ref_kz = np.load(os.path.join(gold, 'case_1.npz'), allow_pickle=True)['p0_lay1_k_z']
+    key = 'case1_p0_'
+    n_effs, wl_norm = fx[key + 'n_effs'], float(fx[key + 'wl_norm'])
+    bloch, nval = np.asarray(fx[key + 'k_pll_norm'], float), int(fx[key + 'num_BMs'])
+    shift = complex(fx[key + 'shift']).real
+    mesh = FemMesh.from_mail(mail)
+    solver = FemModeSolver(mesh)
+    k0 = 2 * np.pi / wl_norm
+
+    def layer():
+        return solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift)
+
+    for _ in range(2):
+        out = layer()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(max(3, steps)):
+        t0 = time.perf_counter()
+        out = layer()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.median(times))
+    kz_err = float(np.max(np.abs(out[0] - ref_kz) / np.abs(ref_kz)))
+    # parts of one solve (CUDA events around the device steps)
+    n = mesh.neq
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    solver.factor(n_effs, k0, bloch, shift)
+    ev[1].record()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solver.eigs(nval)
+    torch.cuda.synchronize()
+    eig_ms = 1e3 * (time.perf_counter() - t0)
+    st = dict(solver.stats)
+    X = torch.randn(n, 16, dtype=torch.complex128, device='cuda')
+    Y = torch.empty_like(X)
+    apply_ms = _timed(lambda: solver.apply(X, Y), 10, warmup=3)
+    del solver.Ainv
+    nt = len(mesh.trows)
+    lu_flops = 8.0 / 3.0 * n ** 3
+    inv_flops = 8.0 * n ** 2 * nt
+    factor_ms = ev[0].elapsed_time(ev[1])
+    # CPU: the oracle's solve of the prime modes
+    x, tn, tab, tel = F.read_mail(mail)
+    t0 = time.perf_counter()
+    F.solve_modes(x, tn, tab, tel, n_effs, wl_norm, bloch, nval, shift=shift)
+    cpu_s = (time.perf_counter() - t0) / 2.0    # solve_modes does the prime and the adjoint solve
+    peak = fp64_peak_tflops()
+    hbm, hbm_src = hbm_peak()
+    return {
+        'metric': 'FEM layer solves/s (prime + adjoint Bloch modes)', 'value': 1e3 / ms, 'unit': 'layers/s',
+        'ms_per_layer': ms, 'steps': max(3, steps), 'dtype': 'c128',
+        'config': {'workload': 'reference test mesh 4testing-600_120.mail, 518 P2 triangles, %d DOFs, '
+                               '%d Bloch modes, test case 1 at 500 nm' % (n, nval)},
+        'kz_max_rel_err_vs_reference': kz_err,
+        'solve_parts': {'element_matrices_assembly_lu_inverse_ms': factor_ms, 'krylov_schur_ms': eig_ms,
+                        'krylov_stats': st, 'operator_apply_ms_16_vectors': apply_ms},
+        'roofline': {'lu_and_inverse_tflops': (lu_flops + inv_flops) / (factor_ms / 1e3) / 1e12,
+                     'fp64_peak_tflops': peak, 'frac': (lu_flops + inv_flops) / (factor_ms / 1e3) / 1e12 / peak,
+                     'operator_gbs': 16.0 * n * nt / (apply_ms / 1e3) / 1e9, 'hbm_peak_gbs': hbm,
+                     'hbm_source': hbm_src,
+                     'note': 'factor time includes the element matrices and assembly (small); complex LU '
+                             '8/3 n^3, the nt columns of the inverse from the LU 8 n^2 nt real flops (nt '
+                             'transverse DOFs, where M has entries); the operator streams those columns '
+                             '(16 n nt bytes) once per block of 16 vectors'},
+        'cpu_baseline': {'value': 1.0 / (2 * cpu_s), 'unit': 'layers/s', 'cores': 1, 'kind': 'port',
+                         'sample': 'one prime and one adjoint solve of the same layer by the oracle (scipy '
+                                   'ARPACK on SuperLU, numpy assembly)'},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -1074,6 +1164,8 @@ def main():
                     help='time the field reconstruction kernels instead of the GSM')
     ap.add_argument('--fields-elements', type=int, default=20000,
                     help='elements of the nanostructured layer in --fields (a smaller layer for profiling)')
+    ap.add_argument('--fem', action='store_true',
+                    help='time the FEM Bloch-mode solve of a nanostructured layer instead of the GSM')
     ap.add_argument('--cpu-sample', type=int, default=0,
                     help='points in the CPU sample (default: 8 per host core, >= 64)')
     args = ap.parse_args()
@@ -1108,6 +1200,9 @@ def main():
 
     if args.fields:
         print(json.dumps(fields_line(max(args.steps, 5), args.fields_elements)))
+        return
+    if args.fem:
+        print(json.dumps(fem_line(min(args.steps, 10))))
         return
 
     if args.config != 2:

@@ -409,9 +409,9 @@ EXTRA_SIGNATURES.extend([
     ('emu_fem_assemble', C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, vp]),
     ('emu_fem_shifted_dense', C.c_int, [C.c_int, vp, vp, vp, vp, EmuC128, vp, C.c_int, vp]),
     ('emu_fem_lu', C.c_int, [C.c_int, vp, C.c_int, vp, vp, vp]),
-    ('emu_fem_inverse', C.c_int, [C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]),
-    ('emu_fem_apply_op', C.c_int, [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int,
-                                   vp]),
+    ('emu_fem_inverse', C.c_int, [C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]),
+    ('emu_fem_apply_op', C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int, vp, vp,
+                                   C.c_int, vp]),
     ('emu_fem_mode_order', C.c_int, [C.c_int, vp, vp]),
     ('emu_fem_fields_workspace_size', C.c_size_t, [C.POINTER(EmuFemFields)]),
     ('emu_fem_nodal_fields', C.c_int, [C.POINTER(EmuFemFields), vp, C.c_size_t, vp]),

@@ -338,12 +338,14 @@ __global__ void fem_dense_kernel(int n, const int32_t *row_ptr, const int32_t *c
     }
 }
 
-// Y = M X, one warp per row, lanes over the block's vectors
-__global__ void fem_spmm_kernel(int n, int nrhs, const int32_t *row_ptr, const int32_t *col, const cd *M,
-                                const cd *X, int ldx, cd *Y, int ldy) {
+// T = (M X) restricted to rows[0..nr) (all rows when rows is null), one warp
+// per row, lanes over the block's vectors
+__global__ void fem_spmm_kernel(int nr, const int32_t *rows, int nrhs, const int32_t *row_ptr, const int32_t *col,
+                                const cd *M, const cd *X, int ldx, cd *Y, int ldy) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps)
+  for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nr; j += warps) {
+    const int r = rows ? rows[j] : j;
     for (int c = lane; c < nrhs; c += 32) {
       cd y{0.0, 0.0};
       for (int i = row_ptr[r]; i < row_ptr[r + 1]; ++i) {
@@ -352,8 +354,9 @@ __global__ void fem_spmm_kernel(int n, int nrhs, const int32_t *row_ptr, const i
         y.x += mv.x * xv.x - mv.y * xv.y;
         y.y += mv.x * xv.y + mv.y * xv.x;
       }
-      Y[(size_t)r * ldy + c] = y;
+      Y[(size_t)j * ldy + c] = y;
     }
+  }
 }
 
 // ------------------------------------------------------------ nodal fields
@@ -732,72 +735,79 @@ void getrf_blocked(int n, cd *A, int lda, int *ipiv, int *info, cudaStream_t s) 
   }
 }
 
-// Y = A^-1 T for a narrow block T [n][nrhs]: A^-1 streamed once per 16
-// vectors, two rows per warp, T staged in shared memory 128 rows at a time
-// (column-major there, so the lanes' reads are consecutive), lanes split
-// the k range and a butterfly sums each output.
-constexpr int kSkRows = 16, kSkK = 128, kSkCols = 16;
+// Y = A^-1 T for a narrow block T [n][nrhs] (A^-1 rows x n, T n x nrhs;
+// n here is the inner extent, the columns of A^-1 kept): one row of A^-1
+// per warp, streamed once per 16 vectors; T staged in shared memory 128
+// rows at a time (read row by row, stored column-major with one pad entry
+// per column so that both the staging writes and the lanes' reads avoid
+// bank conflicts); the next chunk's A entries are loaded while the current
+// one is summed; lanes split the k range and a butterfly sums each output.
+constexpr int kSkRows = 8, kSkK = 128, kSkCols = 16, kSkPer = kSkK / 32;
 
-__global__ void __launch_bounds__(256) fem_skinny_kernel(int n, int nrhs, const cd *A, int lda, const cd *T, int ldt,
-                                                         cd *Y, int ldy) {
-  __shared__ cd Ts[kSkCols][kSkK];
+__global__ void __launch_bounds__(256, 2) fem_skinny_kernel(int n, int nrhs, const cd *__restrict__ A, int lda,
+                                                            const cd *__restrict__ T, int ldt, cd *Y, int ldy,
+                                                            int rows) {
+  __shared__ cd Ts[kSkCols][kSkK + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r0 = blockIdx.x * kSkRows + warp * 2;
+  const int r = blockIdx.x * kSkRows + warp;
+  const bool live = r < rows;
+  const cd *Ar = A + (size_t)(live ? r : 0) * lda;
   for (int c0 = 0; c0 < nrhs; c0 += kSkCols) {
     const int nc = min(kSkCols, nrhs - c0);
-    cd acc0[kSkCols], acc1[kSkCols];
+    cd acc[kSkCols];
 #pragma unroll
-    for (int c = 0; c < kSkCols; ++c) acc0[c] = acc1[c] = cd{0.0, 0.0};
+    for (int c = 0; c < kSkCols; ++c) acc[c] = cd{0.0, 0.0};
+    cd a[kSkPer];
+#pragma unroll
+    for (int j = 0; j < kSkPer; ++j) {
+      const int k = lane + 32 * j;
+      a[j] = (live && k < n) ? Ar[k] : cd{0.0, 0.0};
+    }
     for (int k0 = 0; k0 < n; k0 += kSkK) {
-      // the lane's A entries of this chunk in flight while T is staged
-      cd a0[kSkK / 32], a1[kSkK / 32];
-#pragma unroll
-      for (int j = 0; j < kSkK / 32; ++j) {
-        const int k = k0 + lane + 32 * j;
-        a0[j] = (r0 < n && k < n) ? A[(size_t)r0 * lda + k] : cd{0.0, 0.0};
-        a1[j] = (r0 + 1 < n && k < n) ? A[(size_t)(r0 + 1) * lda + k] : cd{0.0, 0.0};
-      }
       __syncthreads();
       for (int e = threadIdx.x; e < kSkK * kSkCols; e += blockDim.x) {
-        const int c = e / kSkK, kk = e % kSkK;
+        const int kk = e / kSkCols, c = e % kSkCols;
         Ts[c][kk] = (k0 + kk < n && c < nc) ? T[(size_t)(k0 + kk) * ldt + c0 + c] : cd{0.0, 0.0};
+      }
+      cd an[kSkPer];
+#pragma unroll
+      for (int j = 0; j < kSkPer; ++j) {
+        const int k = k0 + kSkK + lane + 32 * j;
+        an[j] = (live && k < n) ? Ar[k] : cd{0.0, 0.0};
       }
       __syncthreads();
 #pragma unroll
-      for (int j = 0; j < kSkK / 32; ++j) {
+      for (int j = 0; j < kSkPer; ++j) {
         const int kk = lane + 32 * j;
 #pragma unroll
         for (int c = 0; c < kSkCols; ++c) {
           const cd t = Ts[c][kk];
-          acc0[c].x += a0[j].x * t.x - a0[j].y * t.y;
-          acc0[c].y += a0[j].x * t.y + a0[j].y * t.x;
-          acc1[c].x += a1[j].x * t.x - a1[j].y * t.y;
-          acc1[c].y += a1[j].x * t.y + a1[j].y * t.x;
+          acc[c].x += a[j].x * t.x - a[j].y * t.y;
+          acc[c].y += a[j].x * t.y + a[j].y * t.x;
         }
       }
+#pragma unroll
+      for (int j = 0; j < kSkPer; ++j) a[j] = an[j];
     }
 #pragma unroll
     for (int c = 0; c < kSkCols; ++c) {
       for (int o = 16; o > 0; o >>= 1) {
-        acc0[c].x += __shfl_xor_sync(0xffffffffu, acc0[c].x, o);
-        acc0[c].y += __shfl_xor_sync(0xffffffffu, acc0[c].y, o);
-        acc1[c].x += __shfl_xor_sync(0xffffffffu, acc1[c].x, o);
-        acc1[c].y += __shfl_xor_sync(0xffffffffu, acc1[c].y, o);
+        acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
+        acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
       }
-      if (lane == c && c < nc) {
-        if (r0 < n) Y[(size_t)r0 * ldy + c0 + c] = acc0[c];
-        if (r0 + 1 < n) Y[(size_t)(r0 + 1) * ldy + c0 + c] = acc1[c];
-      }
+      if (lane == c && c < nc && live) Y[(size_t)r * ldy + c0 + c] = acc[c];
     }
   }
 }
 
-__global__ void fem_identity_kernel(int n, cd *X, int ldx) {
-  const long long total = (long long)n * n;
+// X [n][nc]: column j = unit vector e_{cols[j]} (cols null: the identity)
+__global__ void fem_identity_kernel(int n, int nc, const int32_t *cols, cd *X, int ldx) {
+  const long long total = (long long)n * nc;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const long long r = i / n, c = i % n;
-    X[r * ldx + c] = cd{r == c ? 1.0 : 0.0, 0.0};
+    const long long r = i / nc, c = i % nc;
+    const long long one = cols ? cols[c] : c;
+    X[r * ldx + c] = cd{r == one ? 1.0 : 0.0, 0.0};
   }
 }
 
@@ -812,30 +822,32 @@ extern "C" int emu_fem_lu(int n, emu_c128 *d_A, int lda, int32_t *d_ipiv, int32_
   return emu::check_launch();
 }
 
-extern "C" int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv, emu_c128 *d_Ainv,
-                               int ldi, void *stream) {
-  if (n < 1 || lda < n || ldi < n) return EMU_E_SHAPE;
+extern "C" int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv, int ncols,
+                               const int32_t *d_cols, emu_c128 *d_Ainv, int ldi, void *stream) {
+  if (n < 1 || lda < n || ncols < 1 || ncols > n || ldi < ncols) return EMU_E_SHAPE;
   if (!d_LU || !d_ipiv || !d_Ainv || (const void *)d_LU == (const void *)d_Ainv) return EMU_E_ARG;
+  if (!d_cols && ncols != n) return EMU_E_ARG;
   const cudaStream_t s = (cudaStream_t)stream;
-  fem_identity_kernel<<<grid_for((long long)n * n, 256), 256, 0, s>>>(n, (cd *)d_Ainv, ldi);
+  fem_identity_kernel<<<grid_for((long long)n * ncols, 256), 256, 0, s>>>(n, ncols, d_cols, (cd *)d_Ainv, ldi);
   emu::note_launch();
-  getrs_multi(n, n, (const cd *)d_LU, 0, lda, (const int *)d_ipiv, 0, (cd *)d_Ainv, 0, ldi, 1, s);
+  getrs_multi(n, ncols, (const cd *)d_LU, 0, lda, (const int *)d_ipiv, 0, (cd *)d_Ainv, 0, ldi, 1, s);
   return emu::check_launch();
 }
 
-extern "C" int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, const int32_t *d_row_ptr,
-                                const int32_t *d_col, const emu_c128 *d_M, const emu_c128 *d_X, int ldx,
-                                emu_c128 *d_T, emu_c128 *d_Y, int ldy, void *stream) {
-  if (n < 1 || nrhs < 0 || ldi < n || ldx < nrhs || ldy < nrhs) return EMU_E_SHAPE;
+extern "C" int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, int ncols, const int32_t *d_cols,
+                                const int32_t *d_row_ptr, const int32_t *d_col, const emu_c128 *d_M,
+                                const emu_c128 *d_X, int ldx, emu_c128 *d_T, emu_c128 *d_Y, int ldy, void *stream) {
+  if (n < 1 || nrhs < 0 || ncols < 1 || ncols > n || ldi < ncols || ldx < nrhs || ldy < nrhs) return EMU_E_SHAPE;
   if (nrhs == 0) return EMU_OK;
   if (!d_Ainv || !d_row_ptr || !d_col || !d_M || !d_X || !d_T || !d_Y) return EMU_E_ARG;
+  if (!d_cols && ncols != n) return EMU_E_ARG;
   if (d_X == d_Y || d_T == d_Y || d_T == d_X) return EMU_E_ARG;
   const cudaStream_t s = (cudaStream_t)stream;
-  fem_spmm_kernel<<<grid_for((long long)n * 32, 256), 256, 0, s>>>(n, nrhs, d_row_ptr, d_col, (const cd *)d_M,
-                                                                   (const cd *)d_X, ldx, (cd *)d_T, nrhs);
+  fem_spmm_kernel<<<grid_for((long long)ncols * 32, 256), 256, 0, s>>>(
+      ncols, d_cols, nrhs, d_row_ptr, d_col, (const cd *)d_M, (const cd *)d_X, ldx, (cd *)d_T, nrhs);
   emu::note_launch();
-  fem_skinny_kernel<<<(n + kSkRows - 1) / kSkRows, 256, 0, s>>>(n, nrhs, (const cd *)d_Ainv, ldi, (const cd *)d_T,
-                                                                 nrhs, (cd *)d_Y, ldy);
+  fem_skinny_kernel<<<(n + kSkRows - 1) / kSkRows, 256, 0, s>>>(ncols, nrhs, (const cd *)d_Ainv, ldi,
+                                                                 (const cd *)d_T, nrhs, (cd *)d_Y, ldy, n);
   emu::note_launch();
   return emu::check_launch();
 }

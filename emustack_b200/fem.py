@@ -13,7 +13,8 @@ Per layer and Bloch vector:
 3. the nval eigenvalues of OP = A^-1 M of largest modulus by a block
    Krylov-Schur iteration (Stewart, SIAM J. Matrix Anal. Appl. 23, 2001, in
    block form): OP applied to blocks of ``block`` vectors at once
-   (``emu_fem_apply_op``: sparse M times the block, then A^-1 times that),
+   (``emu_fem_apply_op``: sparse M times the block, non-zero only on the
+   transverse DOFs, then the matching columns of A^-1 times that),
    the basis orthogonalised by two classical Gram-Schmidt passes and
    Cholesky QR on the device; the small projected matrix (at most
    ``max_basis`` square) is reduced on the host and the basis restarted on
@@ -79,6 +80,9 @@ class FemMesh(object):
         self.d_col = up(col[:self.nnz])
         self.d_src_ptr = up(src_ptr[:self.nnz + 1])
         self.d_src = up(src)
+        # rows where M has entries: the transverse DOFs (faces and edges)
+        self.trows = np.unique(dof[:, :12]).astype(np.int32)
+        self.d_trows = up(self.trows)
 
     @classmethod
     def from_mail(cls, path, device=None):
@@ -115,6 +119,22 @@ def beta_branch(b2):
     b = np.sqrt(np.asarray(b2, complex))
     flip = np.where(np.abs(b.imag) < 1e-8, b.real < 0, b.imag < 0)
     return np.where(flip, -b, b)
+
+
+_LINALG_READY = set()
+
+
+def _linalg_ready(dev):
+    """Run torch's device linear-algebra entry points once in this thread:
+    their first call initialises a library handle, which two threads must not
+    do at once."""
+    if dev in _LINALG_READY:
+        return
+    G = torch.eye(2, dtype=torch.complex128, device=dev)
+    L, _ = torch.linalg.cholesky_ex(G)
+    torch.linalg.solve_triangular(L.conj().T, G, upper=True, left=False)
+    torch.cuda.synchronize(dev)
+    _LINALG_READY.add(dev)
 
 
 def mode_order(beta):
@@ -174,20 +194,23 @@ class FemModeSolver(object):
         check(lib().emu_fem_lu(n, ptr(self.A), n, ptr(self.ipiv), ptr(info), s), 'emu_fem_lu')
         if int(info.item()) != 0:
             raise _lib.EmuError(_lib.EMU_E_SINGULAR, 'emu_fem_lu (K - shift M is singular)')
-        self.Ainv = torch.empty((n, n), dtype=torch.complex128, device=dev)
-        check(lib().emu_fem_inverse(n, ptr(self.A), n, ptr(self.ipiv), ptr(self.Ainv), n, s), 'emu_fem_inverse')
+        nt = len(m.trows)
+        self.Ainv = torch.empty((n, nt), dtype=torch.complex128, device=dev)
+        check(lib().emu_fem_inverse(n, ptr(self.A), n, ptr(self.ipiv), nt, ptr(m.d_trows), ptr(self.Ainv), nt, s),
+              'emu_fem_inverse')
         del self.A
 
     def apply(self, X, Y, stream=None):
         """Y = (K - shift M)^-1 M X for a column block X of a row-major
         [n][ld] tensor (X and Y may be strided views with unit column stride)."""
-        n = self.mesh.neq
+        m = self.mesh
+        n, nt = m.neq, len(m.trows)
         nrhs = X.shape[1]
         T = getattr(self, '_T', None)
-        if T is None or T.numel() < n * nrhs:
-            T = self._T = torch.empty(n * nrhs, dtype=torch.complex128, device=X.device)
-        check(lib().emu_fem_apply_op(n, nrhs, ptr(self.Ainv), n, ptr(self.mesh.d_row_ptr), ptr(self.mesh.d_col),
-                                     ptr(self.M), ptr(X), X.stride(0), ptr(T), ptr(Y), Y.stride(0),
+        if T is None or T.numel() < nt * nrhs:
+            T = self._T = torch.empty(nt * nrhs, dtype=torch.complex128, device=X.device)
+        check(lib().emu_fem_apply_op(n, nrhs, ptr(self.Ainv), nt, nt, ptr(m.d_trows), ptr(m.d_row_ptr),
+                                     ptr(m.d_col), ptr(self.M), ptr(X), X.stride(0), ptr(T), ptr(Y), Y.stride(0),
                                      stream_ptr(stream)), 'emu_fem_apply_op')
 
     # -- block Krylov-Schur ---------------------------------------------
@@ -321,11 +344,41 @@ class FemModeSolver(object):
         check(lib().emu_fem_nodal_fields(C.byref(f), ptr(ws), ws_bytes, stream_ptr(stream)), 'emu_fem_nodal_fields')
         return beta, sol
 
-    def solve_pair(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None):
+    def solve_pair(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None, concurrent=True):
         """The prime modes (Bloch vector ``bloch``) and the adjoint modes
         (-bloch) as calc_modes_2d solves both (py_calc_modes.f:604-616):
-        beta1, sol1, beta2, sol2."""
+        beta1, sol1, beta2, sol2.  ``concurrent``: the two solves run on two
+        streams from two host threads, so that one solve's host steps (the
+        projected eigenproblems) overlap the other's device work."""
         bloch = np.asarray(bloch, np.float64)
-        b1, s1 = self.solve(n_effs, wl_norm, bloch, nval, shift, stream)
-        b2, s2 = self.solve(n_effs, wl_norm, -bloch, nval, shift, stream)
-        return b1, s1, b2, s2
+        if not concurrent:
+            b1, s1 = self.solve(n_effs, wl_norm, bloch, nval, shift, stream)
+            b2, s2 = self.solve(n_effs, wl_norm, -bloch, nval, shift, stream)
+            return b1, s1, b2, s2
+        import threading
+        _linalg_ready(self.mesh.device)
+        other = FemModeSolver(self.mesh, block=self.block, max_basis=self.max_basis, keep=self.keep,
+                              tol=self.tol, max_restarts=self.max_restarts, seed=self.seed)
+        caller = stream if stream is not None else torch.cuda.current_stream()
+        streams = (torch.cuda.Stream(), torch.cuda.Stream())
+        for st in streams:
+            st.wait_stream(caller)
+        out, errs = [None, None], []
+
+        def run(i, solver, b):
+            try:
+                with torch.cuda.stream(streams[i]):
+                    out[i] = solver.solve(n_effs, wl_norm, b, nval, shift, streams[i])
+            except BaseException as e:  # re-raised in the calling thread
+                errs.append(e)
+
+        t = threading.Thread(target=run, args=(1, other, -bloch))
+        t.start()
+        run(0, self, bloch)
+        t.join()
+        for st in streams:
+            caller.wait_stream(st)
+        if errs:
+            raise errs[0]
+        self.stats_adjoint = other.stats
+        return out[0][0], out[0][1], out[1][0], out[1][1]

@@ -872,23 +872,27 @@ int emu_fem_element_matrices(const EmuFemElements *p, void *stream);
  * entry set to zero), which emu_fem_lu factors in place (partial pivoting;
  * panels of the dense interface path's LU inside outer blocks of 256
  * columns; ipiv 0-based, info 0 or the first zero pivot + 1) and
- * emu_fem_inverse turns into A^-1 (a separate n x n buffer). */
+ * emu_fem_inverse turns into the columns d_cols of A^-1 (a separate
+ * [n][ldi] buffer; d_cols NULL with ncols = n for all of A^-1). */
 int emu_fem_assemble(int nnz, const int32_t *d_src_ptr, const int32_t *d_src, const emu_c128 *d_Ke,
                      const emu_c128 *d_Me, emu_c128 *d_K, emu_c128 *d_M, void *stream);
 int emu_fem_shifted_dense(int neq, const int32_t *d_row_ptr, const int32_t *d_col, const emu_c128 *d_K,
                           const emu_c128 *d_M, emu_c128 shift, emu_c128 *d_A, int lda, void *stream);
 int emu_fem_lu(int n, emu_c128 *d_A, int lda, int32_t *d_ipiv, int32_t *d_info, void *stream);
-int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv, emu_c128 *d_Ainv, int ldi,
-                    void *stream);
+int emu_fem_inverse(int n, const emu_c128 *d_LU, int lda, const int32_t *d_ipiv, int ncols,
+                    const int32_t *d_cols, emu_c128 *d_Ainv, int ldi, void *stream);
 
 /* Y = (K - shift M)^-1 M X for a block of nrhs vectors (X [n][ldx], Y
- * [n][ldy], row-major, vector r in column r; T [n][nrhs] scratch): the
+ * [n][ldy], row-major, vector r in column r; T [ncols][nrhs] scratch): the
  * operator of the shift-and-invert eigen-solve (valpr_umf_64.f:314-383,
  * which applies it one vector at a time through UMFPACK's solves), here a
- * sparse product with M and one pass over A^-1 per 16 vectors. */
-int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, const int32_t *d_row_ptr,
-                     const int32_t *d_col, const emu_c128 *d_M, const emu_c128 *d_X, int ldx, emu_c128 *d_T,
-                     emu_c128 *d_Y, int ldy, void *stream);
+ * sparse product with M on the rows d_cols where M has entries (the
+ * transverse DOFs; NULL with ncols = n for all rows) and one pass over
+ * the matching columns of A^-1 ([n][ldi], from emu_fem_inverse with the same
+ * d_cols) per 16 vectors. */
+int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi, int ncols, const int32_t *d_cols,
+                     const int32_t *d_row_ptr, const int32_t *d_col, const emu_c128 *d_M, const emu_c128 *d_X,
+                     int ldx, emu_c128 *d_T, emu_c128 *d_Y, int ldy, void *stream);
 
 /* Nodal fields of array_sol.f:88-300: sol [nel][nval][13][3] (E_x, E_y,
  * E_z at the six P2 nodes, E_z interpolated from the P3 values; E_z at P3

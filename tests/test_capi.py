@@ -69,7 +69,8 @@ def test_grating_orders_1d_and_errors():
 STRUCTS = ('EmuFilmStackBatch', 'EmuAnalloModes', 'EmuLayer', 'EmuStackDense', 'EmuOverlap',
            'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch', 'EmuVarLayer', 'EmuStackPoint',
            'EmuStackVarBatch', 'EmuOverlap1D', 'EmuNormalise1D', 'EmuMaterial', 'EmuFilmRingRequest',
-           'EmuFilmRingResult', 'EmuPwFields', 'EmuBlochFieldsPlane')
+           'EmuFilmRingResult', 'EmuPwFields', 'EmuBlochFieldsPlane', 'EmuFemTopology', 'EmuFemElements',
+           'EmuFemFields')
 
 
 def test_struct_layouts_match_header(tmp_path):

@@ -55,3 +55,46 @@ def test_mode_order_is_the_reference_quicksort():
     beta[7] = beta[3]          # a tie
     beta[20] = -beta[11]       # equal beta^2
     np.testing.assert_array_equal(mode_order(beta), z_indexx(-np.real(beta * beta)))
+
+
+def test_topology_refuses_a_boundary_node_without_image():
+    """A boundary node with no periodic partner is refused (periodic_node.f
+    stops there), as are missing buffers and out-of-range node numbers."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    path = os.path.join(GOLD, '4testing-600_120.mail')
+    x, tn, tab, tel = F.read_mail(path)
+    x = x.copy()
+    b = int(np.nonzero(tn)[0][0])
+    x[b] += 0.01                      # breaks its pairing
+    with pytest.raises(_lib.EmuError):
+        FemMesh(x, tn, tab, tel, device='cpu')
+    bad = tab.copy()
+    bad[0, 0] = len(x) + 1
+    with pytest.raises(_lib.EmuError):
+        FemMesh(F.read_mail(path)[0], tn, bad, tel, device='cpu')
+    t = _lib.EmuFemTopology()
+    t.npt, t.nel = 3, 1
+    assert _lib.lib().emu_fem_topology(C.byref(t)) == _lib.EMU_E_ARG
+
+
+def test_fem_device_entries_check_arguments_on_the_host():
+    """Shape and pointer checks of the device entry points return before any
+    launch (no GPU needed)."""
+    import ctypes as C
+    from emustack_b200 import _lib
+    L = _lib.lib()
+    z = _lib.EmuC128(0.0, 0.0)
+    assert L.emu_fem_lu(0, None, 1, None, None, None) == _lib.EMU_E_SHAPE
+    assert L.emu_fem_lu(4, None, 4, None, None, None) == _lib.EMU_E_ARG
+    assert L.emu_fem_inverse(4, None, 4, None, 5, None, None, 5, None) == _lib.EMU_E_SHAPE
+    assert L.emu_fem_shifted_dense(4, None, None, None, None, z, None, 3, None) == _lib.EMU_E_SHAPE
+    assert L.emu_fem_apply_op(4, 2, None, 4, 4, None, None, None, None, None, 2, None, None, 2, None) == \
+        _lib.EMU_E_ARG
+    assert L.emu_fem_assemble(-1, None, None, None, None, None, None, None) == _lib.EMU_E_SHAPE
+    e = _lib.EmuFemElements()
+    e.nel, e.n_types = 1, 9
+    assert L.emu_fem_element_matrices(C.byref(e), None) == _lib.EMU_E_ARG
+    f = _lib.EmuFemFields()
+    f.nel, f.neq, f.nval, f.ldv = 1, 1, 2, 1
+    assert L.emu_fem_nodal_fields(C.byref(f), None, 0, None) == _lib.EMU_E_ARG
