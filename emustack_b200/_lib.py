@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, 'libemustack_gsm.so')
 EMU_OK = 0
 EMU_E_ARG = 1
 EMU_E_SHAPE = 2
+EMU_E_SINGULAR = 3
 EMU_E_WORKSPACE = 5
 STATUS_NAMES = {
     0: 'EMU_OK', 1: 'EMU_E_ARG', 2: 'EMU_E_SHAPE', 3: 'EMU_E_SINGULAR',
