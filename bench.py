@@ -928,6 +928,15 @@ def north_star_extras(dev, w, solver, value):
         out['serving_device_loop'] = ring_serving_run(20000.0, 1.0)
     except Exception as e:
         out['serving_device_loop'] = {'error': repr(e)}
+    torch.cuda.empty_cache()
+    try:
+        f = fem_line(3)
+        out['fem_modes'] = {k: f[k] for k in ('metric', 'value', 'unit', 'ms_per_layer',
+                                              'kz_max_rel_err_vs_reference', 'cpu_baseline')}
+        out['fem_modes']['workload'] = f['config']['workload']
+        out['fem_modes']['ratio_vs_cpu_baseline'] = f['value'] / f['cpu_baseline']['value']
+    except Exception as e:
+        out['fem_modes'] = {'error': repr(e)}
     out['seconds'] = time.perf_counter() - t0
     return out
 
@@ -1062,7 +1071,7 @@ def fields_line(steps, nel=20000):
     return {'workload': 'fields', 'pw_fields': pw, 'bloch_fields_plane': bl}
 
 
-def fem_line(steps):
+def fem_line(steps, concurrent=True):
     """FEM Bloch-mode solve of one nanostructured layer on the GPU (row f1).
 
     Workload: the reference's own test mesh 4testing-600_120.mail (518 P2
@@ -1090,7 +1099,7 @@ def fem_line(steps):
     k0 = 2 * np.pi / wl_norm
 
     def layer():
-        return solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift)
+        return solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift, concurrent=concurrent)
 
     for _ in range(2):
         out = layer()
@@ -1133,6 +1142,7 @@ def fem_line(steps):
     return {
         'metric': 'FEM layer solves/s (prime + adjoint Bloch modes)', 'value': 1e3 / ms, 'unit': 'layers/s',
         'ms_per_layer': ms, 'steps': max(3, steps), 'dtype': 'c128',
+        'prime_and_adjoint': 'concurrent (two streams, two host threads)' if concurrent else 'one after the other',
         'config': {'workload': 'reference test mesh 4testing-600_120.mail, 518 P2 triangles, %d DOFs, '
                                '%d Bloch modes, test case 1 at 500 nm' % (n, nval)},
         'kz_max_rel_err_vs_reference': kz_err,
@@ -1166,6 +1176,8 @@ def main():
                     help='elements of the nanostructured layer in --fields (a smaller layer for profiling)')
     ap.add_argument('--fem', action='store_true',
                     help='time the FEM Bloch-mode solve of a nanostructured layer instead of the GSM')
+    ap.add_argument('--fem-sequential', action='store_true',
+                    help='with --fem: the prime and adjoint solves one after the other on one stream')
     ap.add_argument('--cpu-sample', type=int, default=0,
                     help='points in the CPU sample (default: 8 per host core, >= 64)')
     args = ap.parse_args()
@@ -1202,7 +1214,7 @@ def main():
         print(json.dumps(fields_line(max(args.steps, 5), args.fields_elements)))
         return
     if args.fem:
-        print(json.dumps(fem_line(min(args.steps, 10))))
+        print(json.dumps(fem_line(min(args.steps, 10), concurrent=not args.fem_sequential)))
         return
 
     if args.config != 2:

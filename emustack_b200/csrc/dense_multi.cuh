@@ -298,6 +298,33 @@ __global__ void laswp_outside_kernel(cd *A_, long long sA, int lda, int n, int j
   }
 }
 
+// The cluster panel's function attributes, set once per device to their
+// largest values (kPanelMaxSmem of dynamic shared memory; non-portable
+// cluster sizes allowed), never lowered afterwards: host threads that launch
+// panels of different sizes at once (two solves on two streams, the server's
+// worker threads) then never see a limit another thread set for a smaller
+// panel.  Bit 0: the shared-memory limit is set; bit 1: clusters above 8
+// CTAs are allowed.  Both threads of a first-call race set the same values.
+inline int panel_cluster_attrs() {
+  static int state[64] = {};  // 0 = not yet set, else attrs | 4
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  int st = __atomic_load_n(&state[dev], __ATOMIC_ACQUIRE);
+  if (st) return st & 3;
+  int attrs = 0;
+  if (cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelMaxSmem) ==
+      cudaSuccess)
+    attrs |= 1;
+  else
+    cudaGetLastError();
+  if (cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess)
+    attrs |= 2;
+  else
+    cudaGetLastError();
+  __atomic_store_n(&state[dev], attrs | 4, __ATOMIC_RELEASE);
+  return attrs;
+}
+
 // Launches the cluster panel; false if it would not beat panel_kernel or
 // cannot run (the caller then uses panel_kernel).  Cluster size: enough
 // CTAs for the panel to fit in shared memory, and as many more (up to 8) as
@@ -318,16 +345,12 @@ inline bool panel_cluster(cd *A, long long sA, int lda, int n, int j0, int jb, i
     }
   }
   if (cs < 2) return false;
+  const int attrs = panel_cluster_attrs();
+  if (!(attrs & 1)) return false;
   // clusters above 8 CTAs are a non-portable size (the launch fails, and the
   // caller falls back to panel_kernel, where the GPU cannot host them)
-  if (cs > 8 &&
-      cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-    return false;
+  if (cs > 8 && !(attrs & 2)) return false;
   const size_t smem = (size_t)((nr + cs - 1) / cs) * row_bytes;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-          cudaSuccess)
-    return false;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(batch * cs));
   cfg.blockDim = dim3(kPanelCTAThreads);
