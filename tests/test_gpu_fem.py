@@ -112,3 +112,36 @@ def test_drop_in_stack_with_gpu_modes_matches_the_reference(case, p, theta, phi)
     np.testing.assert_allclose(np.asarray(st.T_net), gold[g + 'T_net'], rtol=0, atol=1e-6)
     for k in ('a_list', 't_list', 'r_list'):
         np.testing.assert_allclose(np.asarray(getattr(st, k), float), gold[g + k], rtol=1e-6, atol=1e-7)
+
+
+def test_tensor_core_J_meets_the_bar_on_physical_modes():
+    """J / J_dag of the GPU FEM modes of the reference's test layer (case 1,
+    500 nm) by the split-TF32 x3 tensor-core contraction give the same a/t/r
+    lists as the FP64 contraction within 1e-6 through the drop-in Stack (on
+    random synthetic fields the same contraction is not held to that bar)."""
+    from emustack_b200 import materials, objects
+    from emustack_b200.fem import FemMesh, FemModeSolver
+    from emustack_b200.mesh import Mesh
+    from emustack_b200.stack import Stack
+    key, gold, g = _case('case1', 0)
+    fs = FemModeSolver(FemMesh.from_mail(MAIL))
+    b1, s1, b2, s2 = fs.solve_pair(FEM[key + 'n_effs'], float(FEM[key + 'wl_norm']), FEM[key + 'k_pll_norm'],
+                                   int(FEM[key + 'num_BMs']), shift=complex(FEM[key + 'shift']).real)
+    per = float(gold[g + 'period'])
+    light = objects.Light(float(gold[g + 'wl_nm']), max_order_PWs=int(FEM[key + 'max_order']), theta=0.0, phi=0.0)
+    mesh = Mesh.from_mail(MAIL)
+    n_effs = FEM[key + 'n_effs']
+    ns = objects.NanoStruct('2D_array', per, 120, height_nm=float(gold[g + 'heights_nm'][0]),
+                            background=materials.Material(complex(n_effs[0])),
+                            inclusion_a=materials.Material(complex(n_effs[1])), loss=True, mesh=mesh)
+    films = [objects.ThinFilm(period=per, height_nm='semi_inf', material=materials.Material(complex(gold[k])),
+                              loss=False) for k in (g + 'lay0_n', g + 'lay2_n')]
+    lists = {}
+    for prec in ('fp64', 'tf32x3'):
+        sim = ns.calc_modes(light, k_z=b1, fields={'sol1': s1, 'sol2': s2, 'beta1': b1, 'mesh': mesh,
+                                                    'precision': prec})
+        st = Stack((films[0].calc_modes(light), sim, films[1].calc_modes(light)))
+        st.calc_scat(pol='TE')
+        lists[prec] = np.concatenate([np.ravel(np.asarray(v, dtype=complex)).real
+                                      for lst in (st.a_list, st.t_list, st.r_list) for v in lst])
+    np.testing.assert_allclose(lists['tf32x3'], lists['fp64'], rtol=0, atol=1e-6)
