@@ -417,3 +417,35 @@ EXTRA_SIGNATURES.extend([
     ('emu_fem_fields_workspace_size', C.c_size_t, [C.POINTER(EmuFemFields)]),
     ('emu_fem_nodal_fields', C.c_int, [C.POINTER(EmuFemFields), vp, C.c_size_t, vp]),
 ])
+
+
+class EmuFem1dTopology(C.Structure):
+    _fields_ = [
+        ('npt', C.c_int), ('nel', C.c_int), ('h_x', vp), ('h_table_nod', vp), ('h_dof', vp), ('h_shift', vp),
+        ('h_row_ptr', vp), ('h_col', vp), ('h_src_ptr', vp), ('h_src', vp), ('neq', C.c_int), ('nnz', C.c_int),
+        ('period', C.c_double),
+    ]
+
+
+class EmuFem1dElements(C.Structure):
+    _fields_ = [
+        ('nel', C.c_int), ('n_types', C.c_int), ('d_x', vp), ('d_table_nod', vp), ('d_type_el', vp),
+        ('d_shift', vp), ('n_eff', EmuC128 * 8), ('k0', C.c_double), ('bloch', C.c_double * 2),
+        ('d_Ke', vp), ('d_Me', vp),
+    ]
+
+
+class EmuFem1dFields(C.Structure):
+    _fields_ = [
+        ('nel', C.c_int), ('neq', C.c_int), ('nval', C.c_int), ('d_x', vp), ('d_table_nod', vp),
+        ('d_shift', vp), ('d_dof', vp), ('bloch_x', C.c_double), ('adjoint', C.c_int), ('d_vec', vp),
+        ('ldv', C.c_int), ('d_sol', vp),
+    ]
+
+
+EXTRA_SIGNATURES.extend([
+    ('emu_fem1d_topology', C.c_int, [C.POINTER(EmuFem1dTopology)]),
+    ('emu_fem1d_element_matrices', C.c_int, [C.POINTER(EmuFem1dElements), vp]),
+    ('emu_fem1d_fields_workspace_size', C.c_size_t, [C.POINTER(EmuFem1dFields)]),
+    ('emu_fem1d_nodal_fields', C.c_int, [C.POINTER(EmuFem1dFields), vp, C.c_size_t, vp]),
+])

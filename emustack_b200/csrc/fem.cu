@@ -493,6 +493,42 @@ inline int grid_for(long long work, int threads) {
   return (int)std::max(1LL, g);
 }
 
+// CSR pattern of element matrices with nloc local DOFs (row = trial DOF,
+// column = test DOF, columns ascending) and, for every CSR entry, the flat
+// element-matrix entries e*nloc*nloc + a*nloc + b it sums, in element order.
+void csr_pattern(int nel, int nloc, const int32_t *dof, int neq, int32_t *row_ptr, int32_t *col, int32_t *src_ptr,
+                 int32_t *src, int *nnz_out) {
+  const size_t nloc2 = (size_t)nloc * nloc;
+  const size_t total = (size_t)nel * nloc2;
+  std::vector<unsigned long long> rc(total);
+  for (int e = 0; e < nel; ++e) {
+    const int32_t *d = &dof[(size_t)e * nloc];
+    for (int a = 0; a < nloc; ++a)
+      for (int b = 0; b < nloc; ++b)
+        rc[(size_t)e * nloc2 + (size_t)a * nloc + b] = ((unsigned long long)d[a] << 32) | (unsigned)d[b];
+  }
+  std::vector<int32_t> order(total);
+  for (size_t i = 0; i < total; ++i) order[i] = (int32_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t p, int32_t q) { return rc[p] < rc[q]; });
+  int nnz = 0;
+  for (int r = 0; r <= neq; ++r) row_ptr[r] = 0;
+  unsigned long long prev = ~0ULL;
+  for (size_t i = 0; i < total; ++i) {
+    const unsigned long long v = rc[order[i]];
+    if (v != prev) {
+      col[nnz] = (int32_t)(v & 0xffffffffULL);
+      src_ptr[nnz] = (int32_t)i;
+      row_ptr[(v >> 32) + 1] += 1;
+      ++nnz;
+      prev = v;
+    }
+    src[i] = order[i];
+  }
+  src_ptr[nnz] = (int32_t)total;
+  for (int r = 0; r < neq; ++r) row_ptr[r + 1] += row_ptr[r];
+  *nnz_out = nnz;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host topology
@@ -606,36 +642,8 @@ extern "C" int emu_fem_topology(EmuFemTopology *t) {
       for (int q = 0; q < 3; ++q) d[3 * k + q] = (int32_t)(first[en[k]] + q);
     for (int i = 0; i < 10; ++i) d[12 + i] = (int32_t)first[en[4 + i]];
   }
-  // CSR pattern: (row, col, element entry) sorted; row = trial, col = test
-  const size_t total = (size_t)nel * kLoc2;
-  std::vector<unsigned long long> rc(total);
-  for (int e = 0; e < nel; ++e) {
-    const int32_t *d = &t->h_dof[(size_t)e * kLoc];
-    for (int a = 0; a < kLoc; ++a)
-      for (int b = 0; b < kLoc; ++b)
-        rc[(size_t)e * kLoc2 + a * kLoc + b] = ((unsigned long long)d[a] << 32) | (unsigned)d[b];
-  }
-  std::vector<int32_t> order(total);
-  for (size_t i = 0; i < total; ++i) order[i] = (int32_t)i;
-  std::stable_sort(order.begin(), order.end(), [&](int32_t p, int32_t q) { return rc[p] < rc[q]; });
-  int nnz = 0;
-  for (int r = 0; r <= neq; ++r) t->h_row_ptr[r] = 0;
-  unsigned long long prev = ~0ULL;
-  for (size_t i = 0; i < total; ++i) {
-    const unsigned long long v = rc[order[i]];
-    if (v != prev) {
-      t->h_col[nnz] = (int32_t)(v & 0xffffffffULL);
-      t->h_src_ptr[nnz] = (int32_t)i;
-      t->h_row_ptr[(v >> 32) + 1] += 1;
-      ++nnz;
-      prev = v;
-    }
-    t->h_src[i] = order[i];
-  }
-  t->h_src_ptr[nnz] = (int32_t)total;
-  for (int r = 0; r < neq; ++r) t->h_row_ptr[r + 1] += t->h_row_ptr[r];
+  csr_pattern(nel, kLoc, t->h_dof, neq, t->h_row_ptr, t->h_col, t->h_src_ptr, t->h_src, &t->nnz);
   t->neq = neq;
-  t->nnz = nnz;
   return EMU_OK;
 }
 
@@ -884,6 +892,320 @@ extern "C" int emu_fem_nodal_fields(const EmuFemFields *p, void *d_workspace, si
   fem_argmax_kernel<<<p->nval, 256, 0, s>>>(p->nel, p->nval, a.sol, zmax);
   emu::note_launch();
   fem_scale_kernel<<<grid_for((long long)p->nel * p->nval * 39, 256), 256, 0, s>>>(p->nel, p->nval, a.sol, zmax);
+  emu::note_launch();
+  return emu::check_launch();
+}
+
+// =============================================================== 1D gratings
+// The mode solve of calc_modes_1d (backend/fortran/py_calc_modes_1d.f:
+// 330-500) for the E-field formulation: per element E_x at its three P2
+// nodes (discontinuous from element to element), E_y and E_z at its four P3
+// nodes (x_min, x_max, x_min + h/3, x_min + 2h/3; continuous, the last
+// element's x_max values the periodic images of the first element's x_min
+// values), the element matrices of asmbly_1d.f, then the same assembly,
+// factorisation and operator as the 2D solve.
+namespace {
+
+constexpr int kLoc1 = 11;
+constexpr int kLoc1Sq = kLoc1 * kLoc1;
+
+// Lagrange basis polynomials on [0, 1] (monomial coefficients, degree < 4)
+void lagrange_coeffs(const double *nodes, int n, double c[4][4]) {
+  for (int i = 0; i < n; ++i) {
+    double p[4] = {1.0, 0.0, 0.0, 0.0};
+    double den = 1.0;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      double q[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < 3; ++k) {
+        q[k + 1] += p[k];
+        q[k] -= nodes[j] * p[k];
+      }
+      for (int k = 0; k < 4; ++k) p[k] = q[k];
+      den *= nodes[i] - nodes[j];
+    }
+    for (int k = 0; k < 4; ++k) c[i][k] = p[k] / den;
+  }
+}
+
+// int_0^1 f g dt for monomial coefficient vectors
+double poly_int(const double *f, const double *g) {
+  double s = 0.0;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) s += f[a] * g[b] / (a + b + 1);
+  return s;
+}
+
+struct Elem1dIntegrals {
+  double Mxx[3][3], Kxy[3][4], Kyy[4][4], Myy[4][4];
+};
+
+// The reference element's integrals (the closed forms of matrix_mxx_1d.f,
+// matrix_kxy_1d.f, matrix_kyy_1d.f, matrix_myy_1d.f on [0, 1]): P2 mass,
+// P2 times P3 derivative, P3 stiffness, P3 mass.
+Elem1dIntegrals elem1d_integrals() {
+  const double n2[3] = {0.0, 1.0, 0.5}, n3[4] = {0.0, 1.0, 1.0 / 3.0, 2.0 / 3.0};
+  double c2[4][4] = {}, c3[4][4] = {}, d3[4][4] = {};
+  lagrange_coeffs(n2, 3, c2);
+  lagrange_coeffs(n3, 4, c3);
+  for (int i = 0; i < 4; ++i)
+    for (int k = 1; k < 4; ++k) d3[i][k - 1] = k * c3[i][k];
+  Elem1dIntegrals r;
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) r.Mxx[i][j] = poly_int(c2[i], c2[j]);
+    for (int j = 0; j < 4; ++j) r.Kxy[i][j] = poly_int(c2[i], d3[j]);
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      r.Kyy[i][j] = poly_int(d3[i], d3[j]);
+      r.Myy[i][j] = poly_int(c3[i], c3[j]);
+    }
+  return r;
+}
+
+struct Elem1dArgs {
+  int nel;
+  const double *x;
+  const int64_t *tn;
+  const int64_t *type_el;
+  const double *shift;
+  cd qq[8];
+  double by, bx;
+  Elem1dIntegrals I;
+  cd *Ke, *Me;
+};
+
+// one CTA per element, one thread per (trial, test) entry (asmbly_1d.f:
+// 150-250 with pp = 1): groups X = 0..2 (E_x), Y = 3..6 (E_y), Z = 7..10 (E_z)
+__global__ void fem1d_element_kernel(Elem1dArgs a) {
+  const int e = blockIdx.x, idx = threadIdx.x;
+  if (idx >= kLoc1Sq) return;
+  const int ai = idx / kLoc1, bi = idx % kLoc1;   // trial, test
+  const double xmin = a.x[a.tn[(size_t)e * 3] - 1], xmax = a.x[a.tn[(size_t)e * 3 + 1] - 1];
+  const double h = xmax - xmin;
+  const cd q = a.qq[a.type_el[e] - 1];
+  const double by = a.by;
+  const int ga = ai < 3 ? 0 : (ai < 7 ? 1 : 2), gb = bi < 3 ? 0 : (bi < 7 ? 1 : 2);
+  const int la = ga == 0 ? ai : (ga == 1 ? ai - 3 : ai - 7), lb = gb == 0 ? bi : (gb == 1 ? bi - 3 : bi - 7);
+  cd k{0.0, 0.0}, m{0.0, 0.0};
+  const cd xx{by * by - q.x, -q.y};  // pp by^2 - qq
+  if (ga == 0 && gb == 0) {
+    const double v = a.I.Mxx[la][lb] * h;
+    k = cd{xx.x * v, xx.y * v};
+    m = cd{-v, 0.0};
+  } else if (ga == 1 && gb == 0) {
+    k = cd{0.0, -by * a.I.Kxy[lb][la]};   // -i by Kyx, Kyx = Kxy^T
+  } else if (ga == 2 && gb == 0) {
+    k = cd{-a.I.Kxy[lb][la], 0.0};
+  } else if (ga == 0 && gb == 1) {
+    k = cd{0.0, by * a.I.Kxy[la][lb]};
+  } else if (ga == 1 && gb == 1) {
+    const double kyy = a.I.Kyy[la][lb] / h, myy = a.I.Myy[la][lb] * h;
+    k = cd{kyy - q.x * myy, -q.y * myy};
+    m = cd{-myy, 0.0};
+  } else if (ga == 2 && gb == 1) {
+    k = cd{0.0, by * a.I.Myy[la][lb] * h};
+  } else if (ga == 0 && gb == 2) {
+    m = cd{a.I.Kxy[la][lb], 0.0};
+  } else if (ga == 1 && gb == 2) {
+    m = cd{0.0, by * a.I.Myy[la][lb] * h};
+  } else {
+    const double kyy = a.I.Kyy[la][lb] / h, myy = a.I.Myy[la][lb] * h;
+    k = cd{kyy + xx.x * myy, xx.y * myy};
+  }
+  double sa, ca, sb, cb;
+  sincos(a.bx * a.shift[(size_t)e * kLoc1 + ai], &sa, &ca);
+  sincos(a.bx * a.shift[(size_t)e * kLoc1 + bi], &sb, &cb);
+  const cd fac = cmul(cd{ca, -sa}, cd{cb, sb});
+  a.Ke[(size_t)e * kLoc1Sq + idx] = cmul(k, fac);
+  a.Me[(size_t)e * kLoc1Sq + idx] = cmul(m, fac);
+}
+
+struct Field1dArgs {
+  int nel, nval, ldv;
+  const int32_t *dof;
+  const double *shift;
+  double bx;
+  const cd *vec;
+  cd *sol;
+};
+
+__global__ void fem1d_nodal_kernel(Field1dArgs a) {
+  const long long total = (long long)a.nel * a.nval;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i / a.nval), m = (int)(i % a.nval);
+    cd *out = a.sol + ((size_t)e * a.nval + m) * kLoc1;
+    for (int j = 0; j < kLoc1; ++j) {
+      double sn, cs;
+      sincos(a.bx * a.shift[(size_t)e * kLoc1 + j], &sn, &cs);
+      out[j] = cmul(a.vec[(size_t)a.dof[(size_t)e * kLoc1 + j] * a.ldv + m], cd{cs, sn});
+    }
+  }
+}
+
+// x of local DOF j of an element (periodic_cond_1d.f's x_ddl)
+__device__ __forceinline__ double dof1d_x(int j, double xmin, double xmax) {
+  const double h = xmax - xmin;
+  switch (j) {
+    case 0: case 3: case 7: return xmin;
+    case 1: case 4: case 8: return xmax;
+    case 2: return xmin + h / 2.0;
+    case 5: case 9: return xmin + h / 3.0;
+    default: return xmin + 2.0 * h / 3.0;
+  }
+}
+
+// array_sol_1d.f's choice of the value each mode is divided by: the first
+// largest value within dx/4 of the cell's middle when it is at least 0.95 of
+// the first largest value anywhere, else the first largest value right of
+// the middle (prime modes) or left of it (adjoint modes).  One CTA per mode.
+__global__ void fem1d_norm_kernel(int nel, int nval, const double *x, const int64_t *tn, int adjoint,
+                                  const cd *sol, cd *zsel) {
+  const int m = blockIdx.x;
+  const double x0 = x[tn[0] - 1], x1 = x[tn[(size_t)(nel - 1) * 3 + 1] - 1];
+  const double xm = 0.5 * (x0 + x1), dx = (x1 - x0) / nel;
+  double best[4] = {-1.0, -1.0, -1.0, -1.0};  // all, middle, right, left
+  long long bi[4] = {0, 0, 0, 0};
+  const long long total = (long long)nel * kLoc1;
+  for (long long f = threadIdx.x; f < total; f += blockDim.x) {
+    const int e = (int)(f / kLoc1), j = (int)(f % kLoc1);
+    const double xx = dof1d_x(j, x[tn[(size_t)e * 3] - 1], x[tn[(size_t)e * 3 + 1] - 1]);
+    const cd v = sol[((size_t)e * nval + m) * kLoc1 + j];
+    const double mag = hypot(v.x, v.y);
+    const bool in[4] = {true, fabs(xx - xm) < dx / 4.0, xx > xm, xx < xm};
+    for (int c = 0; c < 4; ++c)
+      if (in[c] && mag > best[c]) {
+        best[c] = mag;
+        bi[c] = f;
+      }
+  }
+  __shared__ double s_b[4][256];
+  __shared__ long long s_i[4][256];
+  for (int c = 0; c < 4; ++c) {
+    s_b[c][threadIdx.x] = best[c];
+    s_i[c][threadIdx.x] = bi[c];
+  }
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int c = 0; c < 4; ++c) {
+        const double ob = s_b[c][threadIdx.x + st];
+        const long long oi = s_i[c][threadIdx.x + st];
+        if (ob > s_b[c][threadIdx.x] || (ob == s_b[c][threadIdx.x] && ob >= 0.0 && oi < s_i[c][threadIdx.x])) {
+          s_b[c][threadIdx.x] = ob;
+          s_i[c][threadIdx.x] = oi;
+        }
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    cd z[4];
+    for (int c = 0; c < 4; ++c) {
+      const long long f = s_i[c][0];
+      z[c] = s_b[c][0] >= 0.0 ? sol[((size_t)(f / kLoc1) * nval + m) * kLoc1 + f % kLoc1] : cd{0.0, 0.0};
+    }
+    const double r = (z[0].x == 0.0 && z[0].y == 0.0) ? 0.0 : hypot(z[1].x, z[1].y) / hypot(z[0].x, z[0].y);
+    zsel[m] = r >= 0.95 ? z[1] : (adjoint ? z[3] : z[2]);
+  }
+}
+
+__global__ void fem1d_scale_kernel(int nel, int nval, cd *sol, const cd *z) {
+  const long long total = (long long)nel * nval * kLoc1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    sol[i] = cdiv(sol[i], z[(i / kLoc1) % nval]);
+}
+
+}  // namespace
+
+extern "C" int emu_fem1d_topology(EmuFem1dTopology *t) {
+  if (!t || t->nel < 2 || t->npt < 3 || !t->h_x || !t->h_table_nod || !t->h_dof || !t->h_shift || !t->h_row_ptr ||
+      !t->h_col || !t->h_src_ptr || !t->h_src)
+    return EMU_E_ARG;
+  const int nel = t->nel;
+  const int64_t *tab = t->h_table_nod;
+  for (long long i = 0; i < (long long)nel * 3; ++i)
+    if (tab[i] < 1 || tab[i] > t->npt) return EMU_E_ARG;
+  const double *x = t->h_x;
+  const double x0 = x[tab[0] - 1], x1 = x[tab[(size_t)(nel - 1) * 3 + 1] - 1];
+  const double span = x1 - x0;
+  if (!(span > 0.0)) return EMU_E_ARG;
+  for (int e = 0; e < nel; ++e) {
+    const double a = x[tab[(size_t)e * 3] - 1], b = x[tab[(size_t)e * 3 + 1] - 1];
+    if (!(b > a)) return EMU_E_ARG;  // elements run left to right
+    if (e + 1 < nel && fabs(x[tab[(size_t)(e + 1) * 3] - 1] - b) > 1e-12 * span) return EMU_E_ARG;
+  }
+  // equations element by element: E_x (3), E_y at x_min, h/3, 2h/3, E_z the same
+  for (int e = 0; e < nel; ++e) {
+    int32_t *d = &t->h_dof[(size_t)e * kLoc1];
+    const int b = 9 * e;
+    d[0] = b;
+    d[1] = b + 1;
+    d[2] = b + 2;
+    d[3] = b + 3;
+    d[5] = b + 4;
+    d[6] = b + 5;
+    d[7] = b + 6;
+    d[9] = b + 7;
+    d[10] = b + 8;
+  }
+  for (int e = 0; e < nel; ++e) {
+    const int nx = (e + 1) % nel;
+    t->h_dof[(size_t)e * kLoc1 + 4] = t->h_dof[(size_t)nx * kLoc1 + 3];
+    t->h_dof[(size_t)e * kLoc1 + 8] = t->h_dof[(size_t)nx * kLoc1 + 7];
+    for (int j = 0; j < kLoc1; ++j) t->h_shift[(size_t)e * kLoc1 + j] = 0.0;
+  }
+  t->h_shift[(size_t)(nel - 1) * kLoc1 + 4] = span;
+  t->h_shift[(size_t)(nel - 1) * kLoc1 + 8] = span;
+  t->neq = 9 * nel;
+  t->period = span;
+  csr_pattern(nel, kLoc1, t->h_dof, t->neq, t->h_row_ptr, t->h_col, t->h_src_ptr, t->h_src, &t->nnz);
+  return EMU_OK;
+}
+
+extern "C" int emu_fem1d_element_matrices(const EmuFem1dElements *p, void *stream) {
+  if (!p || p->nel < 2 || p->n_types < 1 || p->n_types > 8) return EMU_E_ARG;
+  if (!p->d_x || !p->d_table_nod || !p->d_type_el || !p->d_shift || !p->d_Ke || !p->d_Me) return EMU_E_ARG;
+  Elem1dArgs a;
+  a.nel = p->nel;
+  a.x = p->d_x;
+  a.tn = p->d_table_nod;
+  a.type_el = p->d_type_el;
+  a.shift = p->d_shift;
+  for (int i = 0; i < 8; ++i) {
+    const cd n{p->n_eff[i].re, p->n_eff[i].im};
+    const cd eps = cmul(n, n);
+    a.qq[i] = cd{eps.x * p->k0 * p->k0, eps.y * p->k0 * p->k0};
+  }
+  a.bx = p->bloch[0];
+  a.by = p->bloch[1];
+  a.I = elem1d_integrals();
+  a.Ke = (cd *)p->d_Ke;
+  a.Me = (cd *)p->d_Me;
+  fem1d_element_kernel<<<p->nel, 128, 0, (cudaStream_t)stream>>>(a);
+  emu::note_launch();
+  return emu::check_launch();
+}
+
+extern "C" size_t emu_fem1d_fields_workspace_size(const EmuFem1dFields *p) {
+  if (!p || p->nval < 1) return 0;
+  return emu::align_up((size_t)p->nval * sizeof(emu_c128), 256);
+}
+
+extern "C" int emu_fem1d_nodal_fields(const EmuFem1dFields *p, void *d_workspace, size_t workspace_bytes,
+                                      void *stream) {
+  if (!p || p->nel < 2 || p->neq < 1 || p->nval < 1 || p->ldv < p->nval) return EMU_E_ARG;
+  if (!p->d_x || !p->d_table_nod || !p->d_shift || !p->d_dof || !p->d_vec || !p->d_sol) return EMU_E_ARG;
+  if (!d_workspace || workspace_bytes < emu_fem1d_fields_workspace_size(p)) return EMU_E_WORKSPACE;
+  const cudaStream_t s = (cudaStream_t)stream;
+  Field1dArgs a{p->nel, p->nval, p->ldv, p->d_dof, p->d_shift, p->bloch_x, (const cd *)p->d_vec, (cd *)p->d_sol};
+  fem1d_nodal_kernel<<<grid_for((long long)p->nel * p->nval, 128), 128, 0, s>>>(a);
+  emu::note_launch();
+  cd *z = (cd *)d_workspace;
+  fem1d_norm_kernel<<<p->nval, 256, 0, s>>>(p->nel, p->nval, p->d_x, p->d_table_nod, p->adjoint, a.sol, z);
+  emu::note_launch();
+  fem1d_scale_kernel<<<grid_for((long long)p->nel * p->nval * kLoc1, 256), 256, 0, s>>>(p->nel, p->nval, a.sol, z);
   emu::note_launch();
   return emu::check_launch();
 }

@@ -102,6 +102,125 @@ class FemMesh(object):
             raise ValueError('the FEM solve needs the boundary node types of the mesh (Mesh.from_mail)')
         return cls(mesh.x, mesh.type_nod, mesh.table_nod, mesh.type_el, device)
 
+    def element_matrices(self, n_effs, k0, bloch, s):
+        """K_e, M_e [nel][22][22] on the device (emu_fem_element_matrices)."""
+        n_effs = np.asarray(n_effs, np.complex128).ravel()
+        n_types = int(self.type_el.max())
+        if len(n_effs) < n_types or n_types > 8:
+            raise ValueError('need the index of each of the mesh\'s %d material types' % n_types)
+        Ke = torch.empty((self.nel, 22, 22), dtype=torch.complex128, device=self.device)
+        Me = torch.empty_like(Ke)
+        e = _lib.EmuFemElements()
+        e.nel, e.n_types = self.nel, n_types
+        e.d_x, e.d_table_nod, e.d_type_el = ptr(self.d_x), ptr(self.d_table_nod), ptr(self.d_type_el)
+        e.d_shift, e.d_ends = ptr(self.d_shift), ptr(self.d_ends)
+        for i in range(min(8, len(n_effs))):
+            e.n_eff[i] = _c128(n_effs[i])
+        e.k0 = float(k0)
+        e.bloch[0], e.bloch[1] = float(bloch[0]), float(bloch[1])
+        e.d_Ke, e.d_Me = ptr(Ke), ptr(Me)
+        check(lib().emu_fem_element_matrices(C.byref(e), s), 'emu_fem_element_matrices')
+        return Ke, Me
+
+    def nodal_fields(self, Y, nval, bloch, adjoint, s):
+        """sol [nel][nval][13][3] from eigenvectors Y [neq][nval] (emu_fem_nodal_fields)."""
+        sol = torch.empty((self.nel, nval, 13, 3), dtype=torch.complex128, device=self.device)
+        f = _lib.EmuFemFields()
+        f.nel, f.neq, f.nval = self.nel, self.neq, nval
+        f.d_x, f.d_table_nod, f.d_shift, f.d_ends, f.d_dof = (ptr(self.d_x), ptr(self.d_table_nod),
+                                                              ptr(self.d_shift), ptr(self.d_ends), ptr(self.d_dof))
+        f.bloch[0], f.bloch[1] = float(bloch[0]), float(bloch[1])
+        f.d_vec, f.ldv, f.d_sol = ptr(Y), nval, ptr(sol)
+        ws_bytes = lib().emu_fem_fields_workspace_size(C.byref(f))
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+        check(lib().emu_fem_nodal_fields(C.byref(f), ptr(ws), ws_bytes, s), 'emu_fem_nodal_fields')
+        return sol
+
+
+class FemMesh1D(object):
+    """A 1D grating's P2 mesh with its DOF topology (emu_fem1d_topology),
+    resident on the GPU.  ``x`` [npt] P2 node coordinates (any unit: the
+    cell is rescaled to length 1, the unit of the normalised wavelength),
+    ``table_nod`` [nel][3] 1-based (x_min node, x_max node, middle node),
+    elements left to right, ``type_el`` [nel] 1-based material index."""
+
+    def __init__(self, x, table_nod, type_el, device=None):
+        x = np.ascontiguousarray(x, np.float64).ravel()
+        self.table_nod = np.ascontiguousarray(table_nod, np.int64)
+        if self.table_nod.ndim != 2 or self.table_nod.shape[1] != 3:
+            raise ValueError('table_nod must be [nel][3]')
+        self.type_el = np.ascontiguousarray(type_el, np.int64)
+        nel = len(self.table_nod)
+        x0 = x[self.table_nod[0, 0] - 1]
+        span = x[self.table_nod[-1, 1] - 1] - x0
+        self.x = (x - x0) / span if span > 0 else x
+        self.npt, self.nel = len(x), nel
+        dof = np.zeros((nel, 11), np.int32)
+        shift = np.zeros((nel, 11), np.float64)
+        row_ptr = np.zeros(9 * nel + 1, np.int32)
+        col = np.zeros(121 * nel, np.int32)
+        src_ptr = np.zeros(121 * nel + 1, np.int32)
+        src = np.zeros(121 * nel, np.int32)
+        t = _lib.EmuFem1dTopology()
+        t.npt, t.nel = self.npt, nel
+        arrays = (self.x, self.table_nod, dof, shift, row_ptr, col, src_ptr, src)
+        (t.h_x, t.h_table_nod, t.h_dof, t.h_shift, t.h_row_ptr, t.h_col, t.h_src_ptr,
+         t.h_src) = [a.ctypes.data_as(C.c_void_p) for a in arrays]
+        check(lib().emu_fem1d_topology(C.byref(t)), 'emu_fem1d_topology')
+        self.neq, self.nnz = t.neq, t.nnz
+        self.dof, self.shift = dof, shift
+        dev = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+        self.device = dev
+        up = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+        self.d_x, self.d_table_nod, self.d_type_el = up(self.x), up(self.table_nod), up(self.type_el)
+        self.d_shift, self.d_dof = up(shift), up(dof)
+        self.d_row_ptr = up(row_ptr[:self.neq + 1])
+        self.d_col = up(col[:self.nnz])
+        self.d_src_ptr = up(src_ptr[:self.nnz + 1])
+        self.d_src = up(src)
+        # rows where M has entries: the E_x and E_y DOFs
+        self.trows = np.unique(dof[:, :7]).astype(np.int32)
+        self.d_trows = up(self.trows)
+
+    @classmethod
+    def from_mesh(cls, mesh, device=None):
+        """From an emustack_b200.mesh.Mesh1D."""
+        return cls(mesh.x, mesh.table_nod, mesh.type_el, device)
+
+    def element_matrices(self, n_effs, k0, bloch, s):
+        """K_e, M_e [nel][11][11] on the device (emu_fem1d_element_matrices)."""
+        n_effs = np.asarray(n_effs, np.complex128).ravel()
+        n_types = int(self.type_el.max())
+        if len(n_effs) < n_types or n_types > 8:
+            raise ValueError('need the index of each of the mesh\'s %d material types' % n_types)
+        Ke = torch.empty((self.nel, 11, 11), dtype=torch.complex128, device=self.device)
+        Me = torch.empty_like(Ke)
+        e = _lib.EmuFem1dElements()
+        e.nel, e.n_types = self.nel, n_types
+        e.d_x, e.d_table_nod, e.d_type_el, e.d_shift = (ptr(self.d_x), ptr(self.d_table_nod),
+                                                        ptr(self.d_type_el), ptr(self.d_shift))
+        for i in range(min(8, len(n_effs))):
+            e.n_eff[i] = _c128(n_effs[i])
+        e.k0 = float(k0)
+        e.bloch[0], e.bloch[1] = float(bloch[0]), float(bloch[1])
+        e.d_Ke, e.d_Me = ptr(Ke), ptr(Me)
+        check(lib().emu_fem1d_element_matrices(C.byref(e), s), 'emu_fem1d_element_matrices')
+        return Ke, Me
+
+    def nodal_fields(self, Y, nval, bloch, adjoint, s):
+        """sol [nel][nval][11] from eigenvectors Y [neq][nval] (emu_fem1d_nodal_fields)."""
+        sol = torch.empty((self.nel, nval, 11), dtype=torch.complex128, device=self.device)
+        f = _lib.EmuFem1dFields()
+        f.nel, f.neq, f.nval = self.nel, self.neq, nval
+        f.d_x, f.d_table_nod, f.d_shift, f.d_dof = (ptr(self.d_x), ptr(self.d_table_nod), ptr(self.d_shift),
+                                                    ptr(self.d_dof))
+        f.bloch_x, f.adjoint = float(bloch[0]), int(bool(adjoint))
+        f.d_vec, f.ldv, f.d_sol = ptr(Y), nval, ptr(sol)
+        ws_bytes = lib().emu_fem1d_fields_workspace_size(C.byref(f))
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+        check(lib().emu_fem1d_nodal_fields(C.byref(f), ptr(ws), ws_bytes, s), 'emu_fem1d_nodal_fields')
+        return sol
+
 
 def _c128(z):
     z = complex(z)
@@ -164,22 +283,7 @@ class FemModeSolver(object):
         m = self.mesh
         dev = m.device
         s = stream_ptr(stream)
-        n_effs = np.asarray(n_effs, np.complex128).ravel()
-        n_types = int(m.type_el.max())
-        if len(n_effs) < n_types or n_types > 8:
-            raise ValueError('need the index of each of the mesh\'s %d material types' % n_types)
-        Ke = torch.empty((m.nel, 22, 22), dtype=torch.complex128, device=dev)
-        Me = torch.empty_like(Ke)
-        e = _lib.EmuFemElements()
-        e.nel, e.n_types = m.nel, n_types
-        e.d_x, e.d_table_nod, e.d_type_el = ptr(m.d_x), ptr(m.d_table_nod), ptr(m.d_type_el)
-        e.d_shift, e.d_ends = ptr(m.d_shift), ptr(m.d_ends)
-        for i in range(min(8, len(n_effs))):
-            e.n_eff[i] = _c128(n_effs[i])
-        e.k0 = float(k0)
-        e.bloch[0], e.bloch[1] = float(bloch[0]), float(bloch[1])
-        e.d_Ke, e.d_Me = ptr(Ke), ptr(Me)
-        check(lib().emu_fem_element_matrices(C.byref(e), s), 'emu_fem_element_matrices')
+        Ke, Me = m.element_matrices(n_effs, k0, bloch, s)
         self.K = torch.empty(m.nnz, dtype=torch.complex128, device=dev)
         self.M = torch.empty_like(self.K)
         check(lib().emu_fem_assemble(m.nnz, ptr(m.d_src_ptr), ptr(m.d_src), ptr(Ke), ptr(Me), ptr(self.K),
@@ -317,9 +421,11 @@ class FemModeSolver(object):
                            % (self.max_restarts, res.max()))
 
     # -- the solve of calc_modes_2d -------------------------------------
-    def solve(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None):
-        """beta [nval] (numpy, sorted) and sol [nel][nval][13][3] (device) for
-        the Bloch vector ``bloch`` (k_parallel * period)."""
+    def solve(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None, adjoint=False):
+        """beta [nval] (numpy, sorted) and the nodal fields (device; 2D:
+        [nel][nval][13][3], 1D: [nel][nval][11]) for the Bloch vector
+        ``bloch`` (k_parallel * period); ``adjoint`` marks the solve of the
+        adjoint modes (the 1D normalisation differs for them)."""
         k0 = 2 * np.pi / wl_norm
         bloch = np.asarray(bloch, np.float64)
         if shift is None:
@@ -331,17 +437,7 @@ class FemModeSolver(object):
         order = mode_order(beta)
         beta = beta[order]
         Y = Y[:, torch.as_tensor(order.astype(np.int64)).to(Y.device)].contiguous()
-        m = self.mesh
-        sol = torch.empty((m.nel, nval, 13, 3), dtype=torch.complex128, device=m.device)
-        f = _lib.EmuFemFields()
-        f.nel, f.neq, f.nval = m.nel, m.neq, nval
-        f.d_x, f.d_table_nod, f.d_shift, f.d_ends, f.d_dof = (ptr(m.d_x), ptr(m.d_table_nod), ptr(m.d_shift),
-                                                              ptr(m.d_ends), ptr(m.d_dof))
-        f.bloch[0], f.bloch[1] = float(bloch[0]), float(bloch[1])
-        f.d_vec, f.ldv, f.d_sol = ptr(Y), nval, ptr(sol)
-        ws_bytes = lib().emu_fem_fields_workspace_size(C.byref(f))
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=m.device)
-        check(lib().emu_fem_nodal_fields(C.byref(f), ptr(ws), ws_bytes, stream_ptr(stream)), 'emu_fem_nodal_fields')
+        sol = self.mesh.nodal_fields(Y, nval, bloch, adjoint, stream_ptr(stream))
         return beta, sol
 
     def solve_pair(self, n_effs, wl_norm, bloch, nval, shift=None, stream=None, concurrent=True):
@@ -353,7 +449,7 @@ class FemModeSolver(object):
         bloch = np.asarray(bloch, np.float64)
         if not concurrent:
             b1, s1 = self.solve(n_effs, wl_norm, bloch, nval, shift, stream)
-            b2, s2 = self.solve(n_effs, wl_norm, -bloch, nval, shift, stream)
+            b2, s2 = self.solve(n_effs, wl_norm, -bloch, nval, shift, stream, adjoint=True)
             return b1, s1, b2, s2
         import threading
         _linalg_ready(self.mesh.device)
@@ -368,7 +464,7 @@ class FemModeSolver(object):
         def run(i, solver, b):
             try:
                 with torch.cuda.stream(streams[i]):
-                    out[i] = solver.solve(n_effs, wl_norm, b, nval, shift, streams[i])
+                    out[i] = solver.solve(n_effs, wl_norm, b, nval, shift, streams[i], adjoint=i == 1)
             except BaseException as e:  # re-raised in the calling thread
                 errs.append(e)
 

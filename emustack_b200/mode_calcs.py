@@ -221,19 +221,19 @@ class Simmo(Modes):
         its Fortran solver (backend/mode_calcs.py:268-386): indices of the
         mesh's materials (background, inclusion_a, ...; real when loss is
         False), num_BMs = 2 Npw + 20 by default, the shift 1.1 max(Re n)^2 k0^2
-        - |k_parallel|^2, prime and adjoint modes.  Needs a 2D_array
-        structure whose ``mesh`` carries its boundary node types
-        (Mesh.from_mail)."""
-        from .fem import FemMesh, FemModeSolver
+        - |k_parallel|^2, prime and adjoint modes.  Needs the structure's
+        ``mesh``: for 2D_array layers one that carries its boundary node types
+        (Mesh.from_mail), for 1D_array layers a Mesh1D (calc_modes_1d,
+        backend/mode_calcs.py:323-355)."""
+        from .fem import FemMesh, FemMesh1D, FemModeSolver
         st = self.structure
-        if getattr(st, 'periodicity', '2D_array') != '2D_array':
-            raise ValueError('the GPU FEM solve covers 2D_array layers')
+        one_d = getattr(st, 'periodicity', '2D_array') == '1D_array'
         mesh = getattr(st, 'mesh', None)
         if mesh is None:
             raise ValueError('the FEM solve needs the structure\'s mesh')
         fm = getattr(st, '_fem_mesh', None)
         if fm is None or fm.mesh_id != id(mesh):
-            fm = FemMesh.from_mesh(mesh)
+            fm = FemMesh1D.from_mesh(mesh) if one_d else FemMesh.from_mesh(mesh)
             fm.mesh_id = id(mesh)
             st._fem_mesh = fm
         wl = self.light.wl_nm
@@ -246,8 +246,11 @@ class Simmo(Modes):
         if st.loss is False:
             n_effs = n_effs.real.astype(np.complex128)
         self.n_effs = n_effs
-        pxs, pys = self.calc_2d_grating_orders(self.max_order_PWs)
-        num_pw_per_pol = pxs.size
+        if one_d:
+            num_pw_per_pol = self.calc_1d_grating_orders(self.max_order_PWs).size
+        else:
+            pxs, pys = self.calc_2d_grating_orders(self.max_order_PWs)
+            num_pw_per_pol = pxs.size
         nbm = num_pw_per_pol * 2 + 20 if num_BMs is None else int(num_BMs)
         if nbm <= num_pw_per_pol * 2:
             raise ValueError('You must include at least as many BMs as PWs. \nCurrently you have %i BMs < '

@@ -447,8 +447,8 @@ def overlap_from_fields_1d(simmo, fields):
         raise ValueError('overlap integrals need the mesh of the mode fields')
     dev = torch.device('cuda', torch.cuda.current_device())
     dm = DeviceMesh1D(mesh, dev)
-    sol1 = torch.as_tensor(np.ascontiguousarray(fields['sol1'], np.complex128), device=dev).unsqueeze(0)
-    sol2 = torch.as_tensor(np.ascontiguousarray(fields['sol2'], np.complex128), device=dev).unsqueeze(0)
+    sol1 = _on_device(fields['sol1'], dev).unsqueeze(0)
+    sol2 = _on_device(fields['sol2'], dev).unsqueeze(0)
     M = sol1.shape[2]
     beta1 = torch.as_tensor(np.asarray(fields.get('beta1', simmo.k_z), np.complex128).reshape(1, M),
                             device=dev)

@@ -921,6 +921,78 @@ int emu_fem_mode_order(int n, const emu_c128 *h_beta, int32_t *h_index);
 size_t emu_fem_fields_workspace_size(const EmuFemFields *p);
 int emu_fem_nodal_fields(const EmuFemFields *p, void *d_workspace, size_t workspace_bytes, void *stream);
 
+/* ------------------------------- f1: FEM Bloch modes of a 1D grating
+ * The mode solve of calc_modes_1d (backend/fortran/py_calc_modes_1d.f:
+ * 330-500, as backend/mode_calcs.py:323-341 calls it): E_x on discontinuous
+ * P2 elements, E_y and E_z on continuous P3 elements, periodic
+ * (periodic_cond_1d.f); element matrices of asmbly_1d.f; then the same
+ * emu_fem_assemble / _shifted_dense / _lu / _inverse / _apply_op as the 2D
+ * solve (11 local DOFs instead of 22) and emu_fem_mode_order.
+ *
+ * emu_fem1d_topology (host): elements must run left to right without gaps
+ * (table_nod: x_min node, x_max node, middle node); equations numbered
+ * element by element (E_x 3, then E_y and E_z at x_min, h/3, 2h/3), the last
+ * element's x_max values sharing the first element's x_min equations with
+ * the Bloch phase of one period.  Outputs caller-allocated to the bounds
+ * given; neq (= 9 nel), nnz and the period are set.  EMU_E_ARG for
+ * out-of-range nodes or unordered elements. */
+typedef struct {
+  int npt, nel;
+  const double *h_x;           /* [npt] P2 node coordinates                      */
+  const int64_t *h_table_nod;  /* [nel][3], 1-based                              */
+  int32_t *h_dof;              /* out [nel][11]: E_x (3), E_y (4), E_z (4)       */
+  double *h_shift;             /* out [nel][11]: the period for the last
+                                  element's x_max values, else 0                 */
+  int32_t *h_row_ptr;          /* out [neq + 1], bound 9 nel + 1                 */
+  int32_t *h_col;              /* out [nnz], bound 121 nel                       */
+  int32_t *h_src_ptr;          /* out [nnz + 1], bound 121 nel + 1               */
+  int32_t *h_src;              /* out [121 nel]                                  */
+  int neq, nnz;                /* out */
+  double period;               /* out: span of the cell                          */
+} EmuFem1dTopology;
+
+int emu_fem1d_topology(EmuFem1dTopology *t);
+
+/* Element matrices K_e, M_e [nel][11][11] (trial row, test column) of
+ * asmbly_1d.f:150-250 with pp = 1, qq = n^2 k0^2, the reference element's
+ * integrals of matrix_*_1d.f, each entry times val_exp(test)
+ * conj(val_exp(trial)), val_exp = exp(i bloch_x shift). */
+typedef struct {
+  int nel, n_types;
+  const double *d_x;            /* [npt]                 */
+  const int64_t *d_table_nod;   /* [nel][3], 1-based     */
+  const int64_t *d_type_el;     /* [nel], 1-based        */
+  const double *d_shift;        /* [nel][11]             */
+  emu_c128 n_eff[8];
+  double k0;                    /* 2 pi / (wl / period)  */
+  double bloch[2];              /* k_parallel * period   */
+  emu_c128 *d_Ke, *d_Me;        /* out [nel][11][11]     */
+} EmuFem1dElements;
+
+int emu_fem1d_element_matrices(const EmuFem1dElements *p, void *stream);
+
+/* Nodal values of array_sol_1d.f:60-220: sol [nel][nval][11] from
+ * eigenvectors vec [neq][ldv] (mode m in column m, in output order), each
+ * mode divided by its first largest value within a quarter element of the
+ * cell's middle when that is at least 0.95 of its first largest value,
+ * else by its first largest value right of the middle (adjoint = 0, prime
+ * modes) or left of it (adjoint = 1). */
+typedef struct {
+  int nel, neq, nval;
+  const double *d_x;
+  const int64_t *d_table_nod;
+  const double *d_shift;
+  const int32_t *d_dof;
+  double bloch_x;
+  int adjoint;
+  const emu_c128 *d_vec;
+  int ldv;
+  emu_c128 *d_sol;              /* out [nel][nval][11] */
+} EmuFem1dFields;
+
+size_t emu_fem1d_fields_workspace_size(const EmuFem1dFields *p);
+int emu_fem1d_nodal_fields(const EmuFem1dFields *p, void *d_workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,7 +70,7 @@ STRUCTS = ('EmuFilmStackBatch', 'EmuAnalloModes', 'EmuLayer', 'EmuStackDense', '
            'EmuNormalise', 'EmuFilmPoint', 'EmuFilmVarBatch', 'EmuVarLayer', 'EmuStackPoint',
            'EmuStackVarBatch', 'EmuOverlap1D', 'EmuNormalise1D', 'EmuMaterial', 'EmuFilmRingRequest',
            'EmuFilmRingResult', 'EmuPwFields', 'EmuBlochFieldsPlane', 'EmuFemTopology', 'EmuFemElements',
-           'EmuFemFields')
+           'EmuFemFields', 'EmuFem1dTopology', 'EmuFem1dElements', 'EmuFem1dFields')
 
 
 def test_struct_layouts_match_header(tmp_path):

@@ -98,3 +98,32 @@ def test_fem_device_entries_check_arguments_on_the_host():
     f = _lib.EmuFemFields()
     f.nel, f.neq, f.nval, f.ldv = 1, 1, 2, 1
     assert L.emu_fem_nodal_fields(C.byref(f), None, 0, None) == _lib.EMU_E_ARG
+
+
+def test_1d_topology_matches_the_oracle():
+    """emu_fem1d_topology: the DOF numbering and periodic shifts of
+    periodic_cond_1d.f as the oracle restates them, on the reference's own
+    case-4 grating mesh; the CSR gather reproduces the oracle's assembly;
+    unordered elements are refused."""
+    from emustack_b200 import _lib
+    from emustack_b200.fem import FemMesh1D
+    from oracle import fem1d_oracle as F1
+    d = np.load(os.path.join(GOLD, 'fem1d.npz'))
+    tab = d['g1_table_nod'].astype(np.int64).T
+    x, tel = d['g1_x_arr'], d['g1_type_el'].astype(np.int64)
+    m = FemMesh1D(x, tab, tel, device='cpu')
+    topo = F1.Topology1D(x, tab)
+    assert m.neq == topo.neq == 9 * len(tab)
+    np.testing.assert_array_equal(m.dof, topo.dof)
+    np.testing.assert_allclose(m.shift, topo.shift, rtol=0, atol=1e-15)
+    K, M = F1.element_matrices(topo, d['g1_n_effs'], tel, 2 * np.pi / 1.05, 0.3, -0.2)
+    Kg, Mg = F1.assemble(topo, K, M)
+    sp, src = m.d_src_ptr.numpy(), m.d_src.numpy()
+    rows = np.repeat(np.arange(m.neq, dtype=np.int64), np.diff(m.d_row_ptr.numpy()))
+    cols = np.array(m.d_col.numpy(), dtype=np.int64)
+    Kc = np.add.reduceat(K.ravel()[src], sp[:-1])
+    Mc = np.add.reduceat(M.ravel()[src], sp[:-1])
+    np.testing.assert_allclose(Kc, np.asarray(Kg.tocsr()[rows, cols]).ravel(), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(Mc, np.asarray(Mg.tocsr()[rows, cols]).ravel(), rtol=1e-13, atol=1e-13)
+    with pytest.raises(_lib.EmuError):
+        FemMesh1D(x, tab[::-1].copy(), tel, device='cpu')
