@@ -17,8 +17,8 @@ Per layer and Bloch vector:
    transverse DOFs, then the matching columns of A^-1 times that),
    the basis orthogonalised by two classical Gram-Schmidt passes and
    Cholesky QR on the device; the small projected matrix (at most
-   ``max_basis`` square) is reduced on the host and the basis restarted on
-   the span of its wanted Ritz vectors, as ARPACK's reverse-communication loop does
+   ``max_basis`` square) is reduced to an ordered Schur form on the host and
+   the basis restarted on its leading Schur vectors, as ARPACK's reverse-communication loop does
    its small dense steps on the host (valpr_umf_64.f:300-470 runs ARPACK's
    implicitly restarted Arnoldi with one vector per step);
 4. beta^2 = 1/nu + shift with the reference's branch rule, the modes ranked by
@@ -240,6 +240,26 @@ def beta_branch(b2):
     return np.where(flip, -b, b)
 
 
+class _NoLimit(object):
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def _one_blas_thread():
+    """An entered context that limits the host BLAS / LAPACK to one thread
+    (threadpoolctl; a no-op where it is absent); leave it with __exit__."""
+    try:
+        from threadpoolctl import threadpool_limits
+        ctx = threadpool_limits(limits=1)
+    except Exception:
+        ctx = _NoLimit()
+    ctx.__enter__()
+    return ctx
+
+
 _LINALG_READY = set()
 
 
@@ -336,6 +356,8 @@ class FemModeSolver(object):
     def eigs(self, nval, stream=None):
         """The nval eigenpairs of OP of largest |nu|: (nu [nval] numpy,
         eigenvectors [n][nval] device tensor)."""
+        import scipy.linalg as sl
+        from scipy.linalg import lapack
         n = self.mesh.neq
         dev = self.mesh.device
         b = min(self.block, n)
@@ -391,29 +413,44 @@ class FemModeSolver(object):
                 m += b
             t_host = time.perf_counter()
             Hm = H[:m, :m]
-            th, Z = np.linalg.eig(Hm)
+            # the projected matrix is small: one host thread reduces it as fast as
+            # many, and two solves running side by side then do not oversubscribe
+            blas1 = _one_blas_thread()
+            # Krylov-Schur restart (Stewart 2001): a unitary Schur form of the
+            # projected matrix, reordered so that the wanted Ritz values lead;
+            # the kept basis V Q_k and block T_k keep the Krylov relation exact
+            T, Q = sl.schur(Hm, output='complex')
+            ev = np.diag(T)
+            order = np.argsort(-np.abs(ev), kind='stable')
+            sel = np.zeros(m, np.int32)
+            sel[order[:nval]] = 1
+            Tw, Qw = lapack.ztrsen(sel, T, Q, job='N')[:2]
+            th, Wv = np.linalg.eig(Tw[:nval, :nval])
             o = np.argsort(-np.abs(th), kind='stable')
-            th, Z = th[o], Z[:, o]
-            res = np.linalg.norm(H[m:m + b, :m] @ Z[:, :nval], axis=0) / np.abs(th[:nval])
+            th, Wv = th[o], Wv[:, o]
+            Z = Qw[:, :nval] @ Wv
+            Z /= np.linalg.norm(Z, axis=0)
+            res = np.linalg.norm(H[m:m + b, :m] @ Z, axis=0) / np.abs(th)
+            blas1.__exit__(None, None, None)
             if res.max() < self.tol:
-                Zd = torch.as_tensor(np.ascontiguousarray(Z[:, :nval])).to(dev)
+                Zd = torch.as_tensor(np.ascontiguousarray(Z)).to(dev)
                 Y = V[:, :m] @ Zd
                 host_s += time.perf_counter() - t_host
                 self.stats = {'applies': applies, 'restarts': restart, 'basis': mmax, 'block': b,
                               'residual': float(res.max()), 'host_projection_s': host_s}
-                return th[:nval], Y
-            # thick restart on the wanted Ritz vectors: their span is invariant
-            # under Hm, so V Qz (Qz an orthonormal basis of it) keeps an exact
-            # Krylov decomposition with projection Qz^H Hm Qz
+                return th, Y
             k = int(min(keep, mmax - b))
-            Qz, _ = np.linalg.qr(Z[:, :k])
-            Qk = torch.as_tensor(np.ascontiguousarray(Qz)).to(dev)
+            sel = np.zeros(m, np.int32)
+            sel[order[:k]] = 1
+            with _one_blas_thread():
+                Tk, Qk_h = lapack.ztrsen(sel, T, Q, job='N')[:2]
+            Qk = torch.as_tensor(np.ascontiguousarray(Qk_h[:, :k])).to(dev)
             tail = V[:, m:m + b].clone()
             V[:, :k] = V[:, :m] @ Qk
             V[:, k:k + b] = tail
             Hn = np.zeros_like(H)
-            Hn[:k, :k] = Qz.conj().T @ Hm @ Qz
-            Hn[k:k + b, :k] = H[m:m + b, :m] @ Qz
+            Hn[:k, :k] = np.triu(Tk[:k, :k])
+            Hn[k:k + b, :k] = H[m:m + b, :m] @ Qk_h[:, :k]
             H = Hn
             m = k
             host_s += time.perf_counter() - t_host

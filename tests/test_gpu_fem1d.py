@@ -6,10 +6,9 @@ reference's stored run, as tests/test_oracle_fem1d.py explains):
 
 * element matrices and assembly against the oracle (oracle/fem1d_oracle.py),
   1e-12;
-* the Bloch-mode propagation constants of both gratings within 1e-7 of the
-  reference's stored values (measured 1.2e-8: the 1D pencil is far from
-  normal, so the Krylov residual of 1e-13 leaves eigenvalue errors of that
-  size, where the oracle's ARPACK runs to machine precision), and the nodal
+* the Bloch-mode propagation constants of both gratings within 2e-9 of the
+  reference's stored values (the 1D pencil is far from normal: eigenvalue
+  errors run a few hundred times the Krylov residual of 1e-13), and the nodal
   values of the well-separated leading modes against the oracle's solve
   within 5e-5 of their largest value (up to a factor of modulus one per
   mode; the eigenvectors of clustered evanescent modes are less settled);
@@ -69,9 +68,9 @@ def test_1d_fem_solve_matches_the_reference_and_the_oracle(i):
     shift = complex(FX[p + 'shift']).real
     s = FemModeSolver(FemMesh1D(x, tab, tel))
     b1, s1, b2, s2 = s.solve_pair(FX[p + 'n_effs'], wln, bloch, nval, shift=shift)
-    np.testing.assert_allclose(b1, CASE4['p0_lay%d_k_z' % i], rtol=1e-7, atol=0)
+    np.testing.assert_allclose(b1, CASE4['p0_lay%d_k_z' % i], rtol=2e-9, atol=0)
     ob1, os1, ob2, os2 = F1.solve_modes(x, tab, tel, FX[p + 'n_effs'], wln, bloch[0], bloch[1], nval, shift)
-    np.testing.assert_allclose(b2, ob2, rtol=1e-7, atol=0)
+    np.testing.assert_allclose(b2, ob2, rtol=2e-9, atol=0)
     gap = np.minimum(np.r_[np.abs(np.diff(b1)), np.inf], np.r_[np.inf, np.abs(np.diff(b1))])
     sep = np.nonzero(gap[:16] > 1e-2 * np.abs(b1[:16]))[0]
     assert len(sep) >= 4
@@ -106,7 +105,7 @@ def test_drop_in_stack_of_gpu_gratings_matches_the_reference():
         ns = objects.NanoStruct('1D_array', period, 190, height_nm=h, world_1d=True, loss=True,
                                 mesh=Mesh1D(x, tab, tel), **mats)
         sim = ns.calc_modes(light)
-        np.testing.assert_allclose(sim.k_z, CASE4['p0_lay%d_k_z' % i], rtol=1e-7)
+        np.testing.assert_allclose(sim.k_z, CASE4['p0_lay%d_k_z' % i], rtol=2e-9)
         lays.append(sim)
     lays.append(sup.calc_modes(light))
     st = Stack(tuple(lays))
