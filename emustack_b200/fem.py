@@ -249,15 +249,13 @@ class _NoLimit(object):
 
 
 def _one_blas_thread():
-    """An entered context that limits the host BLAS / LAPACK to one thread
-    (threadpoolctl; a no-op where it is absent); leave it with __exit__."""
+    """A context that limits the host BLAS / LAPACK to one thread
+    (threadpoolctl; a no-op where it is absent)."""
     try:
         from threadpoolctl import threadpool_limits
-        ctx = threadpool_limits(limits=1)
+        return threadpool_limits(limits=1)
     except Exception:
-        ctx = _NoLimit()
-    ctx.__enter__()
-    return ctx
+        return _NoLimit()
 
 
 _LINALG_READY = set()
@@ -415,23 +413,22 @@ class FemModeSolver(object):
             Hm = H[:m, :m]
             # the projected matrix is small: one host thread reduces it as fast as
             # many, and two solves running side by side then do not oversubscribe
-            blas1 = _one_blas_thread()
-            # Krylov-Schur restart (Stewart 2001): a unitary Schur form of the
-            # projected matrix, reordered so that the wanted Ritz values lead;
-            # the kept basis V Q_k and block T_k keep the Krylov relation exact
-            T, Q = sl.schur(Hm, output='complex')
-            ev = np.diag(T)
-            order = np.argsort(-np.abs(ev), kind='stable')
-            sel = np.zeros(m, np.int32)
-            sel[order[:nval]] = 1
-            Tw, Qw = lapack.ztrsen(sel, T, Q, job='N')[:2]
-            th, Wv = np.linalg.eig(Tw[:nval, :nval])
-            o = np.argsort(-np.abs(th), kind='stable')
-            th, Wv = th[o], Wv[:, o]
-            Z = Qw[:, :nval] @ Wv
-            Z /= np.linalg.norm(Z, axis=0)
-            res = np.linalg.norm(H[m:m + b, :m] @ Z, axis=0) / np.abs(th)
-            blas1.__exit__(None, None, None)
+            with _one_blas_thread():
+                # Krylov-Schur restart (Stewart 2001): a unitary Schur form of the
+                # projected matrix, reordered so that the wanted Ritz values lead;
+                # the kept basis V Q_k and block T_k keep the Krylov relation exact
+                T, Q = sl.schur(Hm, output='complex')
+                ev = np.diag(T)
+                order = np.argsort(-np.abs(ev), kind='stable')
+                sel = np.zeros(m, np.int32)
+                sel[order[:nval]] = 1
+                Tw, Qw = lapack.ztrsen(sel, T, Q, job='N')[:2]
+                th, Wv = np.linalg.eig(Tw[:nval, :nval])
+                o = np.argsort(-np.abs(th), kind='stable')
+                th, Wv = th[o], Wv[:, o]
+                Z = Qw[:, :nval] @ Wv
+                Z /= np.linalg.norm(Z, axis=0)
+                res = np.linalg.norm(H[m:m + b, :m] @ Z, axis=0) / np.abs(th)
             if res.max() < self.tol:
                 Zd = torch.as_tensor(np.ascontiguousarray(Z)).to(dev)
                 Y = V[:, :m] @ Zd
