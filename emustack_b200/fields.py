@@ -310,6 +310,46 @@ def fields_in_plane(stacks_list, lay_interest=1, z_values=[0.1, 3.6], nu_calc_pt
     return out
 
 
+# E_y / E_z at an element's middle from its four P3 values (array_sol_P2_1d.f:20-40)
+_P3_MID = (-1.0 / 16.0, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0)
+
+
+def grating_slice_1d(sol1, k_z, vec_coef, h_norm, z_range):
+    """E_x, E_y, E_z [2 nel + 1][nz] on the x-z slice through a 1D grating
+    layer from its Bloch-mode nodal values ``sol1`` ([nel][M][11], device or
+    host) and amplitudes ``vec_coef`` (2M, down then up), as fields_vertically
+    builds it (backend/plotting.py:2244-2282 with array_sol_P2_1d.f): per
+    element the P2 values (x_min, x_max, middle) placed at slice entries 0
+    (first element's x_min), 2e + 1 (x_max) and 2e + 2 (middle), and each
+    mode weighted by vec_coef_down e^{i beta (h - z)} + vec_coef_up e^{i beta z}
+    (E_z: their difference over beta).  One GEMM per component on the GPU."""
+    dev = torch.device('cuda', torch.cuda.current_device())
+    s = sol1 if isinstance(sol1, torch.Tensor) else torch.as_tensor(np.asarray(sol1, np.complex128))
+    s = s.to(device=dev, dtype=torch.complex128)
+    nel, M = s.shape[0], s.shape[1]
+    beta = np.asarray(k_z, np.complex128).ravel()
+    vc = np.asarray(vec_coef, np.complex128).ravel()
+    z = np.asarray(z_range, np.float64).ravel()
+    cd = vc[:M, None] * np.exp(1j * beta[:, None] * (h_norm - z[None, :]))
+    cu = vc[M:, None] * np.exp(1j * beta[:, None] * z[None, :])
+    coef_t = torch.as_tensor(cu + cd, device=dev)
+    coef_z = torch.as_tensor((cu - cd) / beta[:, None], device=dev)
+    w = torch.tensor(_P3_MID, dtype=torch.complex128, device=dev)
+    out = []
+    for comp in range(3):
+        if comp == 0:
+            p2 = s[:, :, 0:3]
+        else:
+            lo = 3 if comp == 1 else 7
+            p2 = torch.stack([s[:, :, lo], s[:, :, lo + 1], s[:, :, lo:lo + 4] @ w], dim=2)
+        nodes = torch.empty((2 * nel + 1, M), dtype=torch.complex128, device=dev)
+        nodes[0] = p2[0, :, 0]
+        nodes[1::2] = p2[:, :, 1]
+        nodes[2::2] = p2[:, :, 2]
+        out.append((nodes @ (coef_z if comp == 2 else coef_t)).cpu().numpy())
+    return tuple(out)
+
+
 def fields_vertically(stacks_list, factor_pts_vert=31, nu_pts_hori=41, semi_inf_height=1.0, gradient=None,
                       no_incoming=False, add_name='', force_eq_ratio=False, colour_res=30, plot_boundaries=True):
     """Fields on the x-z slice (y = 0) through every ThinFilm layer of each
@@ -319,9 +359,12 @@ def fields_vertically(stacks_list, factor_pts_vert=31, nu_pts_hori=41, semi_inf_
     substrate and superstrate; no_incoming drops the incident field in the
     superstrate.  Saved to fields_vertically/stack_<n><add_name>.npz (for
     layer i: E_x_<i>, E_y_<i>, E_z_<i> [x, z], z_<i> on the stack's height
-    axis, x) and returned as one dict per stack.  Nanostructured layers
-    (their fields go to gmsh in the reference) are skipped; the plotting
-    arguments are accepted for compatibility and not used."""
+    axis, x) and returned as one dict per stack.  1D gratings whose Bloch-mode
+    fields are known (``sol1``, from calc_modes) give their slice on the
+    mesh's nodes as the routine assembles it (grating_slice_1d; x_<i> the
+    node coordinates); 2D nanostructured layers (gmsh files in the
+    reference) are skipped; the plotting arguments are accepted for
+    compatibility and not used."""
     dir_name = "fields_vertically"
     if not os.path.exists(dir_name):
         os.mkdir(dir_name)
@@ -343,6 +386,22 @@ def fields_vertically(stacks_list, factor_pts_vert=31, nu_pts_hori=41, semi_inf_
         for lay in range(num_lays):
             layer = pstack.layers[lay]
             if not _is_film(layer):
+                st = getattr(layer, 'structure', None)
+                sol1 = getattr(layer, 'sol1', None)
+                if (getattr(st, 'periodicity', None) == '1D_array' and sol1 is not None
+                        and getattr(st, 'mesh', None) is not None):
+                    eps = np.asarray(getattr(layer, 'n_effs', [1.0])) ** 2
+                    nz = max(int(np.round(factor_pts_vert * (np.real(np.max(eps)) * ind_h_list[lay] / wl_normed))),
+                             11)
+                    z_range = np.linspace(0.0, ind_h_list[lay], nz)
+                    vi = num_lays - lay - 1
+                    vc = np.concatenate([np.asarray(pstack.vec_coef_down[vi]).ravel(),
+                                         np.asarray(pstack.vec_coef_up[vi]).ravel()])
+                    ex, ey, ez = grating_slice_1d(sol1, layer.k_z, vc, ind_h_list[lay], z_range)
+                    res['E_x_%d' % lay], res['E_y_%d' % lay], res['E_z_%d' % lay] = ex, ey, ez
+                    xm = np.sort(np.asarray(st.mesh.x, float))
+                    res['x_%d' % lay] = (xm - xm[0]) / (xm[-1] - xm[0])
+                    res['z_%d' % lay] = np.linspace(h_list[lay], h_list[lay + 1], nz)
                 continue
             eps = np.asarray(layer.n()) ** 2
             nz = int(np.round(factor_pts_vert * (np.real(np.max(eps)) * ind_h_list[lay] / wl_normed)))

@@ -139,3 +139,41 @@ def vertical_slice(alphas, betas, sort_order, kz, n, vcd, vcu, x_range, z_range,
                 out[c, ix, iz] = (np.sum(eta['down'][0][c] * e_dn + eta['up'][0][c] * e_up)
                                   + np.sum(eta['down'][1][c] * e_dn + eta['up'][1][c] * e_up))
     return out[0], out[1], out[2]
+
+
+# the E_y / E_z value at an element's middle from its four P3 values
+# (x_min, x_max, h/3, 2h/3): array_sol_P2_1d.f:20-40
+P3_MID = np.array([-1.0 / 16.0, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0])
+
+
+def vertical_slice_1d(sol1, k_z, vec_coef, h_norm, z_range):
+    """E_x, E_y, E_z [2 nel + 1][len(z_range)] of a 1D grating layer as
+    fields_vertically assembles them (backend/plotting.py:2244-2282): the
+    P2 values of array_sol_P2_1d.f per element (x_min, x_max, middle), placed
+    in the slice as the routine's loop places them (entry 0 the first
+    element's x_min value, then per element its x_max value and its middle
+    value), each Bloch mode weighted by vec_coef_down e^{i beta (h - z)} +
+    vec_coef_up e^{i beta z} (E_z: the difference over beta).  ``sol1`` is
+    [nel][M][11]; ``vec_coef`` the 2M down-then-up amplitudes."""
+    sol1 = np.asarray(sol1)
+    nel, M = sol1.shape[0], sol1.shape[1]
+    vc = np.asarray(vec_coef, complex).ravel()
+    out = []
+    for comp in range(3):
+        if comp == 0:
+            p2 = sol1[:, :, 0:3]
+        else:
+            lo = 3 if comp == 1 else 7
+            p2 = np.stack([sol1[:, :, lo], sol1[:, :, lo + 1], sol1[:, :, lo:lo + 4] @ P3_MID], axis=2)
+        E = np.zeros((2 * nel + 1, len(z_range)), complex)
+        for bm in range(M):
+            beta = k_z[bm]
+            for h, hz in enumerate(z_range):
+                cd = vc[bm] * np.exp(1j * beta * (h_norm - hz))
+                cu = vc[bm + M] * np.exp(1j * beta * hz)
+                c = (cu - cd) / beta if comp == 2 else cu + cd
+                E[0, h] += p2[0, bm, 0] * c
+                E[1::2, h] += p2[:, bm, 1] * c      # element x: entry 2x + 1
+                E[2::2, h] += p2[:, bm, 2] * c      # element x: entry 2x + 2
+        out.append(E)
+    return tuple(out)

@@ -116,3 +116,27 @@ def test_drop_in_stack_of_gpu_gratings_matches_the_reference():
                                atol=1e-8)
     np.testing.assert_allclose(float(np.real(st.t_list[-1])), CASE4['txt_Transmittance_stack0001'][0][1], rtol=0,
                                atol=1e-8)
+    # x-z slices through the two gratings (fields_vertically's 1D branch)
+    # against the restatement of its loop, from the same modes and amplitudes
+    from emustack_b200.fields import fields_vertically
+    from oracle import fields_oracle as FO
+    import tempfile
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            res = fields_vertically([st])[0]
+        finally:
+            os.chdir(cwd)
+    nl = len(st.layers)
+    hn = st.heights_norm()
+    for lay in (1, 2):
+        layer = st.layers[lay]
+        vi = nl - lay - 1
+        vc = np.concatenate([np.asarray(st.vec_coef_down[vi]).ravel(), np.asarray(st.vec_coef_up[vi]).ravel()])
+        z = np.linspace(0.0, hn[lay - 1], len(res['z_%d' % lay]))
+        ref = FO.vertical_slice_1d(layer.sol1.cpu().numpy(), layer.k_z, vc, hn[lay - 1], z)
+        for c, name in enumerate('xyz'):
+            got = res['E_%s_%d' % (name, lay)]
+            assert got.shape == (2 * len(_mesh(lay)[1]) + 1, len(z))
+            np.testing.assert_allclose(got, ref[c], rtol=0, atol=1e-12 * max(np.abs(ref[c]).max(), 1e-300))
