@@ -673,6 +673,70 @@ def config1_chain(dev, batch=50, steps=10):
                         'eager' % batch}
 
 
+def config1_physical(dev, batch=50, steps=10):
+    """The config-1 chain on physical Bloch modes: the GPU FEM solve
+    (emustack_b200.fem) of a 2D array layer on the reference's own test mesh
+    (4testing-600_120.mail: period 600 nm, a wire of 120 nm diameter, 518
+    triangles) with the config-1 materials (n = 3.5 + 0.01i in 1.46, h = 100
+    nm, substrate 1.46, air above), max order 3 (P = 58), 60 Bloch modes, at
+    `batch` wavelengths 400-900 nm.  The modes are solved first (not timed);
+    then the chain (J / J_dag, normalisation, interfaces, cascade, fluxes) is
+    timed as in config1_chain: plain = one wavelength per call, FP64; batched
+    = one CUDA graph, with the FP64 and the split-TF32 x3 J."""
+    import torch
+    from emustack_b200.fem import FemMesh, FemModeSolver
+    from emustack_b200.mesh import Mesh
+    from emustack_b200.pipeline import NanoStackPipeline
+    period, M, mo = 600.0, 60, 3
+    mail = os.path.join(ROOT, 'tests', 'golden', '4testing-600_120.mail')
+    mesh = Mesh.from_mail(mail)
+    fem = FemModeSolver(FemMesh.from_mesh(mesh))
+    wl = np.linspace(400.0, 900.0, batch)
+    th = np.radians(1e-5)
+    k = 2 * np.pi / wl
+    kp = np.stack([k * np.sin(th) * np.cos(th), k * np.sin(th) * np.sin(th)], axis=1)
+    n_effs = np.array([1.46, 3.5 + 0.01j])
+    t0 = time.perf_counter()
+    s1 = torch.empty((batch, mesh.nel, M, 13, 3), dtype=torch.complex128, device=dev)
+    s2 = torch.empty_like(s1)
+    beta = torch.empty((batch, M), dtype=torch.complex128, device=dev)
+    for i in range(batch):
+        b1, f1, b2, f2 = fem.solve_pair(n_effs, wl[i] / period, kp[i] * period, M)
+        s1[i], s2[i] = f1, f2
+        beta[i] = torch.as_tensor(b1)
+    torch.cuda.synchronize()
+    fem_s = time.perf_counter() - t0
+    res, lists = {}, {}
+    for prec in ('fp64', 'tf32x3'):
+        pl = NanoStackPipeline(mesh, period, mo, M, batch, 100.0, precision=prec)
+        pl.load(wl, kp, s1, s2, beta)
+        out = pl.capture()
+        ms = _timed(pl.replay, steps, warmup=2)
+        res[prec] = batch / (ms / 1e3)
+        lists[prec] = np.concatenate([out[k].cpu().numpy().reshape(batch, -1)
+                                      for k in ('a_list', 't_list', 'r_list')], axis=1)
+        del pl
+    pl1 = NanoStackPipeline(mesh, period, mo, M, 1, 100.0, precision='fp64')
+    n_plain = 10
+    loads = [(wl[i:i + 1], kp[i:i + 1], s1[i:i + 1].clone(), s2[i:i + 1].clone(), beta[i:i + 1].clone())
+             for i in range(n_plain)]
+
+    def plain():
+        for a in loads:
+            pl1.load(*a)
+            pl1.forward()
+
+    ms1 = _timed(plain, 3, warmup=1)
+    plain_wl = n_plain / (ms1 / 1e3)
+    return {'batched_fp64_wl_per_s': res['fp64'], 'plain_wl_per_s': plain_wl, 'ratio': res['fp64'] / plain_wl,
+            'batched_tf32x3_wl_per_s': res['tf32x3'], 'ratio_tf32x3': res['tf32x3'] / plain_wl,
+            'tf32x3_max_abs_delta_RTA_vs_fp64': float(np.abs(lists['tf32x3'] - lists['fp64']).max()),
+            'fem_modes_s': fem_s,
+            'workload': 'config 1 chain on physical modes: GPU FEM modes of the reference test mesh '
+                        '(518 triangles, 60 modes, P = 58), n = 3.5 + 0.01i in 1.46, h = 100 nm, %d '
+                        'wavelengths 400-900 nm' % batch}
+
+
 def array_pool(n_points, seed=0, period=500.0):
     """Spectral points with two synthetic nanostructured-array layers each
     (ArrayLayer: Bloch k_z and J / J_dag made on the device): P = 2 Npw
@@ -1215,6 +1279,8 @@ def main():
                     help='time the field reconstruction kernels instead of the GSM')
     ap.add_argument('--fields-elements', type=int, default=20000,
                     help='elements of the nanostructured layer in --fields (a smaller layer for profiling)')
+    ap.add_argument('--physical', action='store_true',
+                    help='with --config 1: the chain on the GPU FEM modes of a real layer')
     ap.add_argument('--fem', action='store_true',
                     help='time the FEM Bloch-mode solve of a nanostructured layer instead of the GSM')
     ap.add_argument('--fem-sequential', action='store_true',
@@ -1261,7 +1327,9 @@ def main():
     if args.config != 2:
         import torch
         dev = torch.device('cuda')
-        if args.config == 1:
+        if args.config == 1 and args.physical:
+            print(json.dumps(dict(config1_physical(dev, steps=args.steps), config=1)))
+        elif args.config == 1:
             print(json.dumps(dict(config1_chain(dev, steps=args.steps), config=1)))
         elif args.config == 3:
             print(json.dumps(config3_line(args.steps)))
