@@ -682,7 +682,8 @@ def config1_physical(dev, batch=50, steps=10):
     `batch` wavelengths 400-900 nm.  The modes are solved first (not timed);
     then the chain (J / J_dag, normalisation, interfaces, cascade, fluxes) is
     timed as in config1_chain: plain = one wavelength per call, FP64; batched
-    = one CUDA graph, with the FP64 and the split-TF32 x3 J."""
+    = one CUDA graph, with the FP64 and the split-TF32 x3 J.  The modes of the
+    wavelengths are solved by 4 host threads at once (fem.solve_pairs)."""
     import torch
     from emustack_b200.fem import FemMesh, FemModeSolver
     from emustack_b200.mesh import Mesh
@@ -700,8 +701,9 @@ def config1_physical(dev, batch=50, steps=10):
     s1 = torch.empty((batch, mesh.nel, M, 13, 3), dtype=torch.complex128, device=dev)
     s2 = torch.empty_like(s1)
     beta = torch.empty((batch, M), dtype=torch.complex128, device=dev)
-    for i in range(batch):
-        b1, f1, b2, f2 = fem.solve_pair(n_effs, wl[i] / period, kp[i] * period, M)
+    from emustack_b200.fem import solve_pairs
+    jobs = [(n_effs, wl[i] / period, kp[i] * period, None) for i in range(batch)]
+    for i, (b1, f1, b2, f2) in enumerate(solve_pairs(fem.mesh, jobs, M, workers=4)):
         s1[i], s2[i] = f1, f2
         beta[i] = torch.as_tensor(b1)
     torch.cuda.synchronize()

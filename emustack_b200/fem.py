@@ -512,3 +512,35 @@ class FemModeSolver(object):
             raise errs[0]
         self.stats_adjoint = other.stats
         return out[0][0], out[0][1], out[1][0], out[1][1]
+
+
+def solve_pairs(mesh, jobs, nval, workers=4, **solver_args):
+    """Prime and adjoint modes of one mesh for many (n_effs, wl_norm, bloch,
+    shift) jobs (a wavelength sweep, as the reference maps calc_modes over
+    wavelengths with a process pool): ``workers`` host threads, each with its
+    own solver and stream, so that one job's host steps overlap the others'
+    device work.  Returns [(beta1, sol1, beta2, sol2)] in the order of
+    ``jobs``; the results equal those of solving the jobs one by one."""
+    import concurrent.futures as cf
+    import threading
+    jobs = list(jobs)
+    _linalg_ready(mesh.device)
+    caller = torch.cuda.current_stream(mesh.device)
+    local = threading.local()
+
+    def run(job):
+        if not hasattr(local, 'solver'):
+            local.solver = FemModeSolver(mesh, **solver_args)
+            local.stream = torch.cuda.Stream(mesh.device)
+            local.stream.wait_stream(caller)
+        n_effs, wl_norm, bloch, shift = job
+        with torch.cuda.stream(local.stream):
+            out = local.solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift, stream=local.stream,
+                                          concurrent=False)
+            local.stream.synchronize()
+        return out
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, int(workers))) as ex:
+        results = list(ex.map(run, jobs))
+    torch.cuda.synchronize(mesh.device)
+    return results

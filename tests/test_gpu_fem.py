@@ -145,3 +145,20 @@ def test_tensor_core_J_meets_the_bar_on_physical_modes():
         lists[prec] = np.concatenate([np.ravel(np.asarray(v, dtype=complex)).real
                                       for lst in (st.a_list, st.t_list, st.r_list) for v in lst])
     np.testing.assert_allclose(lists['tf32x3'], lists['fp64'], rtol=0, atol=1e-6)
+
+
+def test_sweep_of_solves_equals_one_by_one():
+    """fem.solve_pairs (several host threads and streams) returns what the
+    solves give one after the other."""
+    from emustack_b200.fem import FemMesh, FemModeSolver, solve_pairs
+    m = FemMesh.from_mail(MAIL)
+    key = 'case1_p0_'
+    n_effs = FEM[key + 'n_effs']
+    jobs = [(n_effs, w, np.asarray(FEM[key + 'k_pll_norm'], float) * (1.0 + 0.1 * i), None)
+            for i, w in enumerate((0.8, 0.9, 1.1))]
+    got = solve_pairs(m, jobs, 24, workers=3)
+    s = FemModeSolver(m)
+    for job, g in zip(jobs, got):
+        ref = s.solve_pair(job[0], job[1], job[2], 24, concurrent=False)
+        np.testing.assert_allclose(g[0], ref[0], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(g[2], ref[2], rtol=1e-12, atol=0)
