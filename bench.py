@@ -1004,7 +1004,7 @@ def north_star_extras(dev, w, solver, value):
         f = fem_line(3)
         out['fem_modes'] = {k: f[k] for k in ('metric', 'value', 'unit', 'ms_per_layer',
                                               'kz_max_rel_err_vs_reference', 'tensor_core_J_on_these_modes',
-                                              'cpu_baseline')}
+                                              'cpu_baseline', 'gratings_1d')}
         out['fem_modes']['workload'] = f['config']['workload']
         out['fem_modes']['ratio_vs_cpu_baseline'] = f['value'] / f['cpu_baseline']['value']
     except Exception as e:
@@ -1230,7 +1230,8 @@ def fem_line(steps, concurrent=True):
     torch.cuda.synchronize()
     eig_ms = 1e3 * (time.perf_counter() - t0)
     st = dict(solver.stats)
-    X = torch.randn(n, 16, dtype=torch.complex128, device='cuda')
+    blk = solver.block
+    X = torch.randn(n, blk, dtype=torch.complex128, device='cuda')
     Y = torch.empty_like(X)
     apply_ms = _timed(lambda: solver.apply(X, Y), 10, warmup=3)
     del solver.Ainv
@@ -1245,6 +1246,7 @@ def fem_line(steps, concurrent=True):
     cpu_s = (time.perf_counter() - t0) / 2.0    # solve_modes does the prime and the adjoint solve
     peak = fp64_peak_tflops()
     hbm, hbm_src = hbm_peak()
+    g1d = fem1d_part(steps, concurrent)
     return {
         'metric': 'FEM layer solves/s (prime + adjoint Bloch modes)', 'value': 1e3 / ms, 'unit': 'layers/s',
         'ms_per_layer': ms, 'steps': max(3, steps), 'dtype': 'c128',
@@ -1254,7 +1256,7 @@ def fem_line(steps, concurrent=True):
         'kz_max_rel_err_vs_reference': kz_err,
         'tensor_core_J_on_these_modes': tc,
         'solve_parts': {'element_matrices_assembly_lu_inverse_ms': factor_ms, 'krylov_schur_ms': eig_ms,
-                        'krylov_stats': st, 'operator_apply_ms_16_vectors': apply_ms},
+                        'krylov_stats': st, 'operator_apply_ms': apply_ms, 'vectors_per_apply': blk},
         'roofline': {'lu_and_inverse_tflops': (lu_flops + inv_flops) / (factor_ms / 1e3) / 1e12,
                      'fp64_peak_tflops': peak, 'frac': (lu_flops + inv_flops) / (factor_ms / 1e3) / 1e12 / peak,
                      'operator_gbs': 16.0 * n * nt / (apply_ms / 1e3) / 1e9, 'hbm_peak_gbs': hbm,
@@ -1262,11 +1264,65 @@ def fem_line(steps, concurrent=True):
                      'note': 'factor time includes the element matrices and assembly (small); complex LU '
                              '8/3 n^3, the nt columns of the inverse from the LU 8 n^2 nt real flops (nt '
                              'transverse DOFs, where M has entries); the operator streams those columns '
-                             '(16 n nt bytes) once per block of 16 vectors'},
+                             '(16 n nt bytes) once per block of vectors'},
         'cpu_baseline': {'value': 1.0 / (2 * cpu_s), 'unit': 'layers/s', 'cores': 1, 'kind': 'port',
                          'sample': 'one prime and one adjoint solve of the same layer by the oracle (scipy '
                                    'ARPACK on SuperLU, numpy assembly)'},
+        'gratings_1d': g1d,
     }
+
+
+def fem1d_part(steps, concurrent=True):
+    """The 1D FEM solve of the two gratings of the reference's test case 4
+    (period 760 nm, 800 nm, tests/golden/fem1d.npz: the meshes and solver
+    inputs the reference passes, the centre inclusion given the width of
+    its stored run): one layer = prime + adjoint solve, timed host to host,
+    k_z against the reference's stored values, and the oracle's solve
+    (scipy ARPACK on SuperLU) of the same layer on one host core."""
+    import torch
+    from emustack_b200.fem import FemMesh1D, FemModeSolver
+    from oracle import fem1d_oracle as F1
+    gold = os.path.join(ROOT, 'tests', 'golden')
+    fx = np.load(os.path.join(gold, 'fem1d.npz'))
+    case4 = np.load(os.path.join(gold, 'case_4.npz'), allow_pickle=True)
+    out = {}
+    for i in (1, 2):
+        p = 'g%d_' % i
+        tab = fx[p + 'table_nod'].astype(np.int64).T
+        x = fx[p + 'x_arr']
+        tel = fx[p + 'type_el'].astype(np.int64).copy()
+        tel[(tel == 2) & (np.abs(x[tab[:, 0] - 1] - 0.37) < 1e-9)] = 1
+        bloch = [float(fx[p + 'kx']), float(fx[p + 'ky'])]
+        wln, nval = float(fx[p + 'wl_norm']), int(fx[p + 'num_BMs'])
+        shift = complex(fx[p + 'shift']).real
+        n_effs = fx[p + 'n_effs']
+        mesh = FemMesh1D(x, tab, tel)
+        solver = FemModeSolver(mesh)
+
+        def layer():
+            return solver.solve_pair(n_effs, wln, bloch, nval, shift=shift, concurrent=concurrent)
+
+        for _ in range(2):
+            res = layer()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(max(3, steps)):
+            t0 = time.perf_counter()
+            res = layer()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        ms = 1e3 * float(np.median(times))
+        ref = case4['p0_lay%d_k_z' % i]
+        t0 = time.perf_counter()
+        F1.solve_modes(x, tab, tel, n_effs, wln, bloch[0], bloch[1], nval, shift)
+        cpu_s = time.perf_counter() - t0
+        out['grating_%d' % i] = {
+            'elements': int(len(tab)), 'dofs': int(mesh.neq), 'modes': nval, 'ms_per_layer': ms,
+            'layers_per_s': 1e3 / ms, 'kz_max_rel_err_vs_reference': float(np.max(np.abs(res[0] - ref) / np.abs(ref))),
+            'krylov_stats': dict(solver.stats),
+            'cpu_baseline': {'value': 1.0 / cpu_s, 'unit': 'layers/s', 'cores': 1, 'kind': 'port',
+                             'sample': 'the oracle\'s prime and adjoint solve of the same grating'}}
+    return out
 
 
 def main():

@@ -215,7 +215,7 @@ class Simmo(Modes):
         self.prop_consts = None
         self.mode_pol = None
 
-    def calc_modes(self, num_BMs=None, fem_block=16):
+    def calc_modes(self, num_BMs=None, fem_block=4):
         """Bloch modes of the layer by the FEM solve on the GPU
         (emustack_b200.fem), then J and J_dag, as Simmo.calc_modes does with
         its Fortran solver (backend/mode_calcs.py:268-386): indices of the
