@@ -1272,6 +1272,70 @@ def fem_line(steps, concurrent=True):
     }
 
 
+def fem_holes_line(steps):
+    """FEM Bloch-mode solve of a larger layer: the gold film with 266 nm
+    square holes at period 940 nm of the reference's test case 5 on its mesh
+    4testing-940_266_sq.mail (2 528 P2 triangles, 30 336 DOFs), 100 Bloch
+    modes at 1043.4 nm and 5 degrees (the inputs the reference passes,
+    tests/golden/fem.npz).  One layer = prime + adjoint solve, timed host to
+    host after one untimed layer; CPU baseline: the oracle's prime solve
+    (scipy ARPACK on SuperLU) on one host core, doubled for a layer."""
+    import torch
+    from emustack_b200.fem import FemMesh, FemModeSolver
+    from emustack_b200.probe import fp64_peak_tflops
+    from oracle import fem_oracle as F
+    gold = os.path.join(ROOT, 'tests', 'golden')
+    mail = os.path.join(gold, '4testing-940_266_sq.mail')
+    fx = np.load(os.path.join(gold, 'fem.npz'))
+    ref = np.load(os.path.join(gold, 'case_5.npz'), allow_pickle=True)['p0_lay1_k_z']
+    key = 'case5_p0_'
+    n_effs, wl_norm = fx[key + 'n_effs'], float(fx[key + 'wl_norm'])
+    bloch, nval = np.asarray(fx[key + 'k_pll_norm'], float), int(fx[key + 'num_BMs'])
+    shift = complex(fx[key + 'shift']).real
+    mesh = FemMesh.from_mail(mail)
+    solver = FemModeSolver(mesh)
+    solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        out = solver.solve_pair(n_effs, wl_norm, bloch, nval, shift=shift)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    s_layer = float(np.median(times))
+    kz_err = float(np.max(np.abs(out[0] - ref) / np.abs(ref)))
+    n, nt = mesh.neq, len(mesh.trows)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    solver.factor(n_effs, 2 * np.pi / wl_norm, bloch, shift)
+    ev[1].record()
+    torch.cuda.synchronize()
+    factor_ms = ev[0].elapsed_time(ev[1])
+    del solver.Ainv
+    torch.cuda.empty_cache()
+    flops = 8.0 / 3.0 * n ** 3 + 8.0 * n ** 2 * nt
+    peak = fp64_peak_tflops()
+    x, tn, tab, tel = F.read_mail(mail)
+    t0 = time.perf_counter()
+    topo = F.Topology(x, tn, tab)
+    K, M = F.element_matrices(topo, x, n_effs, tel, 2 * np.pi / wl_norm, bloch)
+    Kg, Mg = F.assemble(topo, K, M)
+    F.eigen_solve(Kg, Mg, nval, shift)
+    cpu_s = time.perf_counter() - t0
+    return {
+        'metric': 'FEM layer solves/s (prime + adjoint Bloch modes)', 'value': 1.0 / s_layer, 'unit': 'layers/s',
+        's_per_layer': s_layer, 'steps': max(1, steps), 'dtype': 'c128',
+        'config': {'workload': 'reference test mesh 4testing-940_266_sq.mail, 2528 P2 triangles, %d DOFs, '
+                               '%d Bloch modes, test case 5 (gold film with square holes) at 1043.4 nm' % (n, nval)},
+        'kz_max_rel_err_vs_reference': kz_err, 'krylov_stats': dict(solver.stats),
+        'factor_ms': factor_ms, 'lu_and_inverse_tflops': flops / (factor_ms / 1e3) / 1e12,
+        'fp64_peak_tflops': peak, 'frac': flops / (factor_ms / 1e3) / 1e12 / peak,
+        'max_memory_gb': torch.cuda.max_memory_allocated() / 1e9,
+        'cpu_baseline': {'value': 1.0 / (2 * cpu_s), 'unit': 'layers/s', 'cores': 1, 'kind': 'port',
+                         'sample': 'the oracle\'s prime solve of the same layer (scipy ARPACK on SuperLU), '
+                                   'doubled for prime + adjoint'},
+    }
+
 def fem1d_part(steps, concurrent=True):
     """The 1D FEM solve of the two gratings of the reference's test case 4
     (period 760 nm, 800 nm, tests/golden/fem1d.npz: the meshes and solver
@@ -1341,6 +1405,8 @@ def main():
                     help='with --config 1: the chain on the GPU FEM modes of a real layer')
     ap.add_argument('--fem', action='store_true',
                     help='time the FEM Bloch-mode solve of a nanostructured layer instead of the GSM')
+    ap.add_argument('--fem-holes', action='store_true',
+                    help='time the FEM solve of the 30 336-DOF gold-hole layer of the reference\'s case 5')
     ap.add_argument('--fem-sequential', action='store_true',
                     help='with --fem: the prime and adjoint solves one after the other on one stream')
     ap.add_argument('--cpu-sample', type=int, default=0,
@@ -1380,6 +1446,9 @@ def main():
         return
     if args.fem:
         print(json.dumps(fem_line(min(args.steps, 10), concurrent=not args.fem_sequential)))
+        return
+    if args.fem_holes:
+        print(json.dumps(fem_holes_line(min(args.steps, 3))))
         return
 
     if args.config != 2:

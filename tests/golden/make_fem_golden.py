@@ -2,12 +2,15 @@
 its FEM mode solver (calc_modes_2d, backend/mode_calcs.py:371-381) for the
 nanostructured layer of its test cases 1 and 2 (tests/test_case_1_simple_struct.py,
 tests/test_case_2_simple_non_norm_inc.py: the mesh 4testing-600_120.mail, a
-120 nm Si_c wire in air at period 600 nm).  The reference's Simmo.calc_modes
+120 nm Si_c wire in air at period 600 nm) and of its test case 5
+(tests/test_case_5_EOT_5_degrees.py.bak: the mesh 4testing-940_266_sq.mail,
+266 nm square holes in gold at period 940 nm, 100 Bloch modes, 5 degrees).  The reference's Simmo.calc_modes
 runs up to the Fortran call, which is intercepted here and its inputs
 recorded: normalised wavelength, number of Bloch modes, plane-wave order,
 the materials' indices (loss applied), the normalised Bloch vector and the
 shift of the shift-and-invert solve.  The reference's results for these
-layers (k_z, interface and net matrices) are in case_1.npz / case_2.npz.
+layers (k_z, interface and net matrices) are in case_1.npz, case_2.npz and
+case_5.npz.
 
     EMUSTACK_REF=<path to the EMUstack tree> python tests/golden/make_fem_golden.py
 """
@@ -39,14 +42,19 @@ def main():
         raise _Captured()
 
     fortran.calc_modes_2d = capture
-    cases = {'case1': ([500.0, 1000.0], 2, 0.0, 0.0, 40), 'case2': ([500.0], 1, 20.0, 40.0, 20)}
+    wire = dict(period=600, diameter=120, height_nm=2330, inclusion_a=materials.Si_c, background=materials.Air,
+                mesh_file='4testing-600_120.mail')
+    holes = dict(period=940, diameter=266, height_nm=200, inclusion_a=materials.Air, background=materials.Au,
+                 inc_shape='square', mesh_file='4testing-940_266_sq.mail')
+    cases = {'case1': ([500.0, 1000.0], 2, 0.0, 0.0, 40, wire), 'case2': ([500.0], 1, 20.0, 40.0, 20, wire),
+             'case5': ([1.11 * 940], 4, 5.0, 0.0, 100, holes)}
     d = {}
-    for name, (wls, max_order, theta, phi, num_BMs) in cases.items():
+    for name, (wls, max_order, theta, phi, num_BMs, geo) in cases.items():
         for i, wl in enumerate(wls):
             light = objects.Light(wl, max_order_PWs=max_order, theta=theta, phi=phi)
-            ns = objects.NanoStruct('2D_array', 600, 120, height_nm=2330, inclusion_a=materials.Si_c,
-                                    background=materials.Air, loss=True, make_mesh_now=False,
-                                    mesh_file='4testing-600_120.mail')
+            g = dict(geo)
+            ns = objects.NanoStruct('2D_array', g.pop('period'), g.pop('diameter'), loss=True, make_mesh_now=False,
+                                    **g)
             seen.clear()
             try:
                 ns.calc_modes(light, num_BMs=num_BMs)

@@ -11,6 +11,9 @@
 * End to end through the drop-in objects (NanoStruct.calc_modes on the GPU,
   Stack.calc_scat): the reference's stored R12 of the layer, R_net, T_net
   and a/t/r lists within 1e-6 (the reference's own test tolerance).
+* A second, larger mesh: the gold film with square holes of the reference's
+  test case 5 (4testing-940_266_sq.mail, 2 528 elements, 30 336 DOFs, 100
+  Bloch modes at 5 degrees), its stored propagation constants within 1e-9.
 """
 import os
 
@@ -162,3 +165,18 @@ def test_sweep_of_solves_equals_one_by_one():
         ref = s.solve_pair(job[0], job[1], job[2], 24, concurrent=False)
         np.testing.assert_allclose(g[0], ref[0], rtol=1e-12, atol=0)
         np.testing.assert_allclose(g[2], ref[2], rtol=1e-12, atol=0)
+
+
+def test_fem_solve_on_the_gold_hole_mesh_matches_the_reference_case_5():
+    from emustack_b200.fem import FemMesh, FemModeSolver
+    key = 'case5_p0_'
+    ref = np.load(os.path.join(GOLD, 'case_5.npz'), allow_pickle=True)['p0_lay1_k_z']
+    mesh = FemMesh.from_mail(os.path.join(GOLD, '4testing-940_266_sq.mail'))
+    assert mesh.neq == 30336
+    s = FemModeSolver(mesh)
+    beta, sol = s.solve(FEM[key + 'n_effs'], float(FEM[key + 'wl_norm']), np.asarray(FEM[key + 'k_pll_norm'], float),
+                        int(FEM[key + 'num_BMs']), shift=complex(FEM[key + 'shift']).real)
+    np.testing.assert_allclose(beta, ref, rtol=1e-9, atol=0)
+    assert np.all(np.isfinite(sol.cpu().numpy()))
+    del s, sol
+    torch.cuda.empty_cache()

@@ -77,3 +77,23 @@ def test_fem_oracle_matches_the_reference(case, p):
         assert np.abs(r - r[0]).max() < 1e-5 * abs(r[0]), i
         checked += 1
     assert checked >= 4
+
+
+def test_fem_oracle_on_the_gold_hole_mesh_matches_the_reference_case_5():
+    """The oracle's prime solve on the reference's second test mesh
+    (4testing-940_266_sq.mail: 266 nm square holes in gold at period 940 nm,
+    30 336 DOFs) with the inputs the reference passes for its test case 5
+    (100 Bloch modes, 1043.4 nm, 5 degrees) against its stored k_z."""
+    fem = np.load(os.path.join(GOLD, 'fem.npz'))
+    key = 'case5_p0_'
+    ref = np.load(os.path.join(GOLD, 'case_5.npz'), allow_pickle=True)['p0_lay1_k_z']
+    x, tn, tab, tel = F.read_mail(os.path.join(GOLD, '4testing-940_266_sq.mail'))
+    topo = F.Topology(x, tn, tab)
+    k0 = 2 * np.pi / float(fem[key + 'wl_norm'])
+    bloch = np.asarray(fem[key + 'k_pll_norm'], float)
+    K, M = F.element_matrices(topo, x, fem[key + 'n_effs'], tel, k0, bloch)
+    Kg, Mg = F.assemble(topo, K, M)
+    b2, _ = F.eigen_solve(Kg, Mg, int(fem[key + 'num_BMs']), complex(fem[key + 'shift']).real)
+    beta = F.beta_from(b2)
+    beta = beta[F.z_indexx(-np.real(beta ** 2))]
+    np.testing.assert_allclose(beta, ref, rtol=1e-9, atol=0)
