@@ -152,7 +152,9 @@ def test_tensor_core_J_meets_the_bar_on_physical_modes():
 
 def test_sweep_of_solves_equals_one_by_one():
     """fem.solve_pairs (several host threads and streams) returns what the
-    solves give one after the other."""
+    solves give one after the other, within the solves' own accuracy (1e-10,
+    the tolerance of the parity tests above; cuBLAS's reductions in the
+    Krylov basis may round differently when several streams run at once)."""
     from emustack_b200.fem import FemMesh, FemModeSolver, solve_pairs
     m = FemMesh.from_mail(MAIL)
     key = 'case1_p0_'
@@ -163,8 +165,8 @@ def test_sweep_of_solves_equals_one_by_one():
     s = FemModeSolver(m)
     for job, g in zip(jobs, got):
         ref = s.solve_pair(job[0], job[1], job[2], 24, concurrent=False)
-        np.testing.assert_allclose(g[0], ref[0], rtol=1e-12, atol=0)
-        np.testing.assert_allclose(g[2], ref[2], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(g[0], ref[0], rtol=1e-10, atol=0)
+        np.testing.assert_allclose(g[2], ref[2], rtol=1e-10, atol=0)
 
 
 def test_fem_solve_on_the_gold_hole_mesh_matches_the_reference_case_5():
