@@ -529,7 +529,9 @@ def solve_pairs(mesh, jobs, nval, workers=4, **solver_args):
     wavelengths with a process pool): ``workers`` host threads, each with its
     own solver and stream, so that one job's host steps overlap the others'
     device work.  Returns [(beta1, sol1, beta2, sol2)] in the order of
-    ``jobs``; the results equal those of solving the jobs one by one."""
+    ``jobs``; the results agree with those of solving the jobs one by one to
+    the solver's accuracy (cuBLAS's reductions in the Krylov basis may round
+    differently while several streams run)."""
     import concurrent.futures as cf
     import threading
     jobs = list(jobs)
