@@ -745,26 +745,30 @@ void getrf_blocked(int n, cd *A, int lda, int *ipiv, int *info, cudaStream_t s) 
 
 // Y = A^-1 T for a narrow block T [n][nrhs] (A^-1 rows x n, T n x nrhs;
 // n here is the inner extent, the columns of A^-1 kept): one row of A^-1
-// per warp, streamed once per 16 vectors; T staged in shared memory 128
+// per warp, streamed once per COLS vectors; T staged in shared memory 128
 // rows at a time (read row by row, stored column-major with one pad entry
 // per column so that both the staging writes and the lanes' reads avoid
 // bank conflicts); the next chunk's A entries are loaded while the current
 // one is summed; lanes split the k range and a butterfly sums each output.
-constexpr int kSkRows = 8, kSkK = 128, kSkCols = 16, kSkPer = kSkK / 32;
+// COLS = 16 for wide blocks (2 CTAs per SM), 4 for the Krylov iteration's
+// blocks of up to 4 vectors (no multiply-adds and shared-memory reads for
+// empty columns; 78 registers, so 3 CTAs per SM keep more loads in flight).
+constexpr int kSkRows = 8, kSkK = 128, kSkPer = kSkK / 32;
 
-__global__ void __launch_bounds__(256, 2) fem_skinny_kernel(int n, int nrhs, const cd *__restrict__ A, int lda,
+template <int COLS>
+__global__ void __launch_bounds__(256, COLS <= 4 ? 3 : 2) fem_skinny_kernel(int n, int nrhs, const cd *__restrict__ A, int lda,
                                                             const cd *__restrict__ T, int ldt, cd *Y, int ldy,
                                                             int rows) {
-  __shared__ cd Ts[kSkCols][kSkK + 1];
+  __shared__ cd Ts[COLS][kSkK + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = blockIdx.x * kSkRows + warp;
   const bool live = r < rows;
   const cd *Ar = A + (size_t)(live ? r : 0) * lda;
-  for (int c0 = 0; c0 < nrhs; c0 += kSkCols) {
-    const int nc = min(kSkCols, nrhs - c0);
-    cd acc[kSkCols];
+  for (int c0 = 0; c0 < nrhs; c0 += COLS) {
+    const int nc = min(COLS, nrhs - c0);
+    cd acc[COLS];
 #pragma unroll
-    for (int c = 0; c < kSkCols; ++c) acc[c] = cd{0.0, 0.0};
+    for (int c = 0; c < COLS; ++c) acc[c] = cd{0.0, 0.0};
     cd a[kSkPer];
 #pragma unroll
     for (int j = 0; j < kSkPer; ++j) {
@@ -773,8 +777,8 @@ __global__ void __launch_bounds__(256, 2) fem_skinny_kernel(int n, int nrhs, con
     }
     for (int k0 = 0; k0 < n; k0 += kSkK) {
       __syncthreads();
-      for (int e = threadIdx.x; e < kSkK * kSkCols; e += blockDim.x) {
-        const int kk = e / kSkCols, c = e % kSkCols;
+      for (int e = threadIdx.x; e < kSkK * COLS; e += blockDim.x) {
+        const int kk = e / COLS, c = e % COLS;
         Ts[c][kk] = (k0 + kk < n && c < nc) ? T[(size_t)(k0 + kk) * ldt + c0 + c] : cd{0.0, 0.0};
       }
       cd an[kSkPer];
@@ -788,7 +792,7 @@ __global__ void __launch_bounds__(256, 2) fem_skinny_kernel(int n, int nrhs, con
       for (int j = 0; j < kSkPer; ++j) {
         const int kk = lane + 32 * j;
 #pragma unroll
-        for (int c = 0; c < kSkCols; ++c) {
+        for (int c = 0; c < COLS; ++c) {
           const cd t = Ts[c][kk];
           acc[c].x += a[j].x * t.x - a[j].y * t.y;
           acc[c].y += a[j].x * t.y + a[j].y * t.x;
@@ -798,7 +802,7 @@ __global__ void __launch_bounds__(256, 2) fem_skinny_kernel(int n, int nrhs, con
       for (int j = 0; j < kSkPer; ++j) a[j] = an[j];
     }
 #pragma unroll
-    for (int c = 0; c < kSkCols; ++c) {
+    for (int c = 0; c < COLS; ++c) {
       for (int o = 16; o > 0; o >>= 1) {
         acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
         acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
@@ -854,8 +858,13 @@ extern "C" int emu_fem_apply_op(int n, int nrhs, const emu_c128 *d_Ainv, int ldi
   fem_spmm_kernel<<<grid_for((long long)ncols * 32, 256), 256, 0, s>>>(
       ncols, d_cols, nrhs, d_row_ptr, d_col, (const cd *)d_M, (const cd *)d_X, ldx, (cd *)d_T, nrhs);
   emu::note_launch();
-  fem_skinny_kernel<<<(n + kSkRows - 1) / kSkRows, 256, 0, s>>>(ncols, nrhs, (const cd *)d_Ainv, ldi,
-                                                                 (const cd *)d_T, nrhs, (cd *)d_Y, ldy, n);
+  const int grid = (n + kSkRows - 1) / kSkRows;
+  if (nrhs <= 4)
+    fem_skinny_kernel<4><<<grid, 256, 0, s>>>(ncols, nrhs, (const cd *)d_Ainv, ldi, (const cd *)d_T, nrhs,
+                                              (cd *)d_Y, ldy, n);
+  else
+    fem_skinny_kernel<16><<<grid, 256, 0, s>>>(ncols, nrhs, (const cd *)d_Ainv, ldi, (const cd *)d_T, nrhs,
+                                               (cd *)d_Y, ldy, n);
   emu::note_launch();
   return emu::check_launch();
 }

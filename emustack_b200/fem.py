@@ -294,7 +294,7 @@ class FemModeSolver(object):
     20 blocks), nval + nval / 2 kept) trade more applications of the operator
     for fewer and smaller Schur forms on the host, which cost more than the
     operator's pass over A^-1: on the reference's 2D test mesh (6 216 DOFs,
-    40 modes) one layer takes 0.64 s against 0.96-0.99 s with blocks of 16
+    40 modes) one layer takes 0.58 s against 0.96-0.99 s with blocks of 16
     and a basis of 176, on its 1D gratings (1 800 DOFs, 46 modes) 0.11-0.12 s
     against 0.25-0.40 s."""
 
